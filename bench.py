@@ -1,0 +1,345 @@
+"""Benchmark of the iterNLM hot path on B200 (one JSON line on stdout).
+
+Workload (the 512^3 plain-filter configuration): a float32 512x512x512
+grain-pack volume (uint16-quantised to [0,1], correlated noise sigma 0.04
+blurred 1.2, concentric z-axis rings amplitude 0.02 period 6), patch radius 2,
+search radius 5 (514 offsets, 33 taps), 4 iterations, alpha 0.5, z-adaptive
+noise with a 100-slice window, 1e5 noise samples. Synthetic, seeded.
+
+A step is one whole job: sigma0 on the raw volume, iteration 1, sigma1 on its
+result, the alpha blend, iterations 2-4, all on the device (inlm_denoise).
+``value`` = voxel-iterations/s with the input resident in HBM; ``e2e`` = the
+same through the host-pointer API with the H2D of the raw volume and the D2H
+of the result inside the timed region (pinned host memory). Inputs (537 MB)
+exceed L2 (126 MB) between steps.
+
+    python bench.py [--gpus N --steps K --warmup W]
+    python bench.py --impl reference     # the reference CPU filter on host cores
+
+Multi-GPU (torchrun): each rank denoises its own volume (independent jobs,
+weak scaling, no data-path collective); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "voxel-iter/s 512^3 p2 s5 (plain FP32, whole job incl. noise estimates)"
+SHAPE = (512, 512, 512)
+PR, SR, ITERS = (2, 2, 2), (5, 5, 5), 4
+S_OFFSETS, P_TAPS = 514, 33
+FLOP_PER_VOXEL_ITER = S_OFFSETS * (2 * P_TAPS + 20)   # algorithmic, see DESIGN.md
+BYTES_PER_VOXEL_ITER_F32 = 12                          # read raw + prev, write result
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def workload_config():
+    return {"workload": "grain-pack 512x512x512 f32, patch r2 (33 taps), search r5 (514 offsets), "
+                        "4 iterations, alpha 0.5, z-adaptive noise (window 100, 1e5 samples)",
+            "shape_xyz": [SHAPE[2], SHAPE[1], SHAPE[0]], "patch_radius": 2, "search_radius": 5,
+            "iterations": ITERS, "offsets": S_OFFSETS, "taps": P_TAPS,
+            "l2": "inputs (537 MB) larger than L2 (126 MB)"}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def profile_traffic():
+    """DRAM bytes per filter launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "nlm_tile_f32_p2s5_512.md")
+    try:
+        for ln in open(path):
+            if ln.startswith("traffic_bytes_per_launch:"):
+                return float(ln.split(":", 1)[1].strip())
+    except Exception:
+        pass
+    return None
+
+
+def make_volume(seed=0):
+    from microtomodenoise_b200 import synth
+    t = time.time()
+    v = synth.grain_pack_volume(SHAPE, seed=seed)
+    log(f"generated 512^3 volume in {time.time() - t:.1f}s")
+    return v
+
+
+def cpu_reference_rate(vol, target_s=15.0, threads=None):
+    """Rate of the reference CPU filter (oracle/_ref, else the port) on a
+    bounded slab sample; returns (rate, info)."""
+    from oracle.oracle import FilterParams, Port, Reference, reference_available
+    threads = threads or os.cpu_count()
+    p = FilterParams(search_radius=SR, patch_radius=PR)
+    kind = "reference" if reference_available() else "port"
+    if kind == "reference":
+        impl = Reference()
+
+        def run(slab, sig):
+            out, secs = impl.denoise(slab, p, sig, n_threads=threads)
+            return secs
+    else:
+        impl = Port()
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+
+        def run(slab, sig):
+            t = time.time()
+            impl.denoise_f32(slab, p, sig)
+            return time.time() - t
+    ny, nx = vol.shape[1], vol.shape[2]
+    calib = 2
+    slab = np.ascontiguousarray(vol[:calib])
+    secs = run(slab, np.full((1, calib), 0.045, np.float32))
+    rate = calib * ny * nx / max(secs, 1e-6)
+    depth = int(np.clip(target_s * rate / (ny * nx), 2, vol.shape[0]))
+    slab = np.ascontiguousarray(vol[:depth])
+    secs = run(slab, np.full((1, depth), 0.045, np.float32))
+    rate = depth * ny * nx / secs
+    info = {"value": rate, "unit": "voxel-iter/s", "cores": threads, "kind": kind,
+            "sample": f"{nx}x{ny}x{depth} slab of the 512^3 volume, 1 iteration of "
+                      f"IterativeNLM_CPU::Run_GaussianNoise (p2 s5, sigma fixed), {secs:.1f}s, "
+                      f"OpenMP {threads} threads"}
+    return rate, info
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    vol = make_volume()
+    threads = os.cpu_count()
+    rates = []
+    for i in range(args.warmup + args.steps):
+        rate, info = cpu_reference_rate(vol, target_s=8.0, threads=threads)
+        if i >= args.warmup:
+            rates.append(rate)
+    value = float(np.mean(rates))
+    info["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "voxel-iter/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded grain pack)",
+            "config": workload_config(), "cpu_baseline": info,
+            "e2e": {"value": value, "unit": "voxel-iter/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, _lib
+    import ctypes as C
+
+    L = _lib.load()
+    peak = C.c_double(0)
+    _lib.check(L.inlm_probe_fp32_peak(local, C.byref(peak)), "probe")
+    fp32_peak = peak.value
+
+    vol = make_volume(seed=0)
+    dp = DenoiseParameters(radius_patchspace=PR, radius_searchspace=SR, maxiterations=ITERS,
+                           alpha=0.5, noise_mode="z-adaptive", zwindow=100, n_samples=100000,
+                           noise_seed=0, deviceID=local)
+    g = IterativeNLM_GPU()
+    assert g.configure_device(vol.shape, dp) > 0
+    stream = torch.cuda.Stream()
+    g.set_stream(stream.cuda_stream)
+    raw_dev = torch.from_numpy(vol).cuda()
+    out_dev = torch.empty_like(raw_dev)
+    torch.cuda.synchronize()
+
+    def step():
+        g.denoise(raw_dev.data_ptr(), on_device=True, out=out_dev.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    g.filter_kernel_ms()  # drop warm-up launches
+    cnt = C.c_uint64(0)
+    L.inlm_kernel_launches(g._h, C.byref(cnt))
+    launches0 = cnt.value
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    L.inlm_kernel_launches(g._h, C.byref(cnt))
+    gpu_launches = int(cnt.value - launches0)
+    filt_ms, filt_n = g.filter_kernel_ms()
+
+    # end-to-end through the host-pointer API (pinned host buffers)
+    host_raw = torch.from_numpy(vol).pin_memory()
+    host_out = torch.empty(vol.shape, dtype=torch.float32).pin_memory()
+    nz = vol.shape[0]
+    s0 = np.zeros(nz, np.float32)
+    s1 = np.zeros(nz, np.float32)
+
+    def step_e2e():
+        rc = L.inlm_denoise(g._h, host_raw.data_ptr(), host_out.data_ptr(), 0, s0.ctypes.data,
+                            s1.ctypes.data)
+        _lib.check(rc, "denoise")
+
+    step_e2e()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.e2e_steps):
+        step_e2e()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = f0.elapsed_time(f1)
+
+    # max over ranks
+    t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, ms_e2e = float(t[0]), float(t[1])
+
+    vox = float(np.prod(SHAPE))
+    value = world * vox * ITERS * args.steps / (ms / 1e3)
+    value_e2e = world * vox * ITERS * args.e2e_steps / (ms_e2e / 1e3)
+    achieved = FLOP_PER_VOXEL_ITER * vox / (filt_ms * 1e-3) / 1e12
+    traffic = profile_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "voxel-iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded grain pack, 512^3)", "config": workload_config(),
+        "e2e": {"value": value_e2e, "unit": "voxel-iter/s",
+                "h2d_bytes_per_step": int(vol.nbytes), "d2h_bytes_per_step": int(vol.nbytes),
+                "ms_per_step": ms_e2e / args.e2e_steps},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak if fp32_peak else None,
+                     "traffic": traffic,
+                     "kernel": g.describe(), "kernel_avg_ms": filt_ms, "kernel_launches": filt_n,
+                     "flop_per_voxel_iter": FLOP_PER_VOXEL_ITER,
+                     "peak_source": "measured in this run: all-SM FFMA loop (2 flop/FFMA)",
+                     "hbm": {"achieved_gbs": BYTES_PER_VOXEL_ITER_F32 * vox / (filt_ms * 1e-3) / 1e9,
+                             "peak_gbs": measured_peaks().get("hbm_gbs"),
+                             "bytes_per_voxel_iter": BYTES_PER_VOXEL_ITER_F32}},
+        "gpu_launches": gpu_launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            _, info = cpu_reference_rate(vol)
+            line["cpu_baseline"] = info
+        except Exception as e:  # the GPU number stands without it
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    g.free_device()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,190 @@
+/*
+ * inlm.h — C ABI of the B200 iterNLM hot path (iterative 3D nonlocal means
+ * filter and two-cluster noise estimators).
+ *
+ * Plain C types only: pointers, sizes, ints, floats. Every call returns an
+ * int status (INLM_OK = 0, negative = error); inlm_last_error() gives the
+ * text of the calling thread's last error. Handles are not thread-safe: one
+ * host thread drives one handle, on that handle's own CUDA stream.
+ *
+ * Reference call surface each entry point replaces (file:line in
+ * iterNLM_v0.3):
+ *   inlm_denoiser_create   <- denoise::IterativeNLM_GPU::configure_device
+ *                             (Denoiser/iternlm_gpu.h:27, iternlm_gpu.cu:1440)
+ *   inlm_denoiser_destroy  <- IterativeNLM_GPU::free_device (iternlm_gpu.h:28,
+ *                             iternlm_gpu.cu:1619)
+ *   inlm_set_sigma         <- IterativeNLM_GPU::set_sigma (iternlm_gpu.h:34,
+ *                             iternlm_gpu.cu:2341)
+ *   inlm_run_iteration     <- IterativeNLM_GPU::Run_GaussianNoise (iternlm_gpu.h:30,
+ *                             iternlm_gpu.cu:1651)
+ *   inlm_get_result        <- IterativeNLM_GPU::get_result (iternlm_gpu.h:35,
+ *                             iternlm_gpu.cu:2356)
+ *   inlm_noise_create      <- noise::NoiseLevel::NoiseLevel (Noise/noiselevel.h:21)
+ *   inlm_noise_estimate    <- noise::NoiseLevel::get_noiselevel (noiselevel.h:31,
+ *                             noiselevel.cpp:9)
+ *   inlm_denoise           <- the σ0/σ1 schedule and iteration loop of the
+ *                             iterNLM driver (main.cpp:327-545)
+ *
+ * Shapes are {nx, ny, nz}, x fastest, as the reference stores stacks.
+ */
+#ifndef INLM_H
+#define INLM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define INLM_OK 0
+#define INLM_ERR_ARG -1        /* bad argument (shape, radius, null pointer) */
+#define INLM_ERR_CUDA -2       /* CUDA runtime error (reference: configure_device -2) */
+#define INLM_ERR_NODEVICE -3   /* no CUDA device (reference: configure_device -1) */
+#define INLM_ERR_NOMEM -4      /* device allocation failed */
+#define INLM_ERR_STATE -5      /* call out of order (e.g. iteration 2 before 1) */
+#define INLM_ERR_TIMEOUT -6    /* a bounded device wait ran out */
+#define INLM_ERR_UNSUPPORTED -7
+
+/* noise estimation modes (denoise_parameters.h:22) */
+#define INLM_NOISE_ZADAPTIVE 0
+#define INLM_NOISE_GLOBAL 1
+#define INLM_NOISE_MANUAL 2
+#define INLM_NOISE_SEMIMANUAL 3
+
+/* storage / arithmetic form of the filter */
+#define INLM_PRECISION_F32 0   /* FP32, bit-identical to the reference CPU filter */
+#define INLM_PRECISION_F16 1   /* FP16 storage, FP32 accumulation */
+
+/* patch-weight table */
+#define INLM_WEIGHTS_CPU 0        /* the table the reference CPU filter applies (default) */
+#define INLM_WEIGHTS_DISTWEIGHT 1 /* setup_distweight values for every shape */
+
+typedef struct {
+    /* filter (protocol::DenoiseParameters, denoise_parameters.h:11-20) */
+    float alpha;             /* 0.5 */
+    int maxiterations;       /* 4 */
+    int nslices;             /* 11 */
+    int search_radius[3];    /* {10,10,10} */
+    int patch_radius[3];     /* {1,1,1} */
+    float beta;              /* 1 */
+    float z_anisotropy;      /* 1 */
+    /* noise (denoise_parameters.h:20-34) */
+    int noise_mode;          /* INLM_NOISE_ZADAPTIVE */
+    int zwindow;             /* 100 */
+    float sigma[2];          /* manual / semimanual values */
+    uint64_t n_samples;      /* 100000 */
+    int noise_patchsize;     /* 15 */
+    float stds_from_mean;    /* 1 */
+    int continuous_estimate; /* 0 */
+    int circular_mask_diameter; /* 0 */
+    unsigned int noise_seed; /* seed of the glibc-rand() sample draw (reference: time(NULL)) */
+    /* device */
+    int device_id;           /* 0 */
+    int precision;           /* INLM_PRECISION_F32 */
+    int weight_table;        /* INLM_WEIGHTS_CPU */
+} inlm_params;
+
+typedef struct inlm_denoiser inlm_denoiser;
+typedef struct inlm_noise inlm_noise;
+
+/* Fills the reference defaults (denoise_parameters.h). */
+void inlm_default_params(inlm_params* p);
+
+const char* inlm_last_error(void);
+
+/* ---------------- denoiser (IterativeNLM_GPU) ---------------- */
+
+/* Allocates the padded raw / previous-iterate volumes and the result on
+ * device p->device_id and builds the search and patch tables.
+ * Returns INLM_ERR_NODEVICE when no CUDA device exists (the reference's -1,
+ * where its driver falls back to the CPU). */
+int inlm_denoiser_create(const int shape[3], const inlm_params* p, inlm_denoiser** out);
+int inlm_denoiser_destroy(inlm_denoiser* d);
+
+/* Uploads nz sigma values (host) and derives the per-slice multiplier
+ * -1/(sigma^2 beta) (iternlm_cpu.cpp:94-95). */
+int inlm_set_sigma(inlm_denoiser* d, const float* sigma_host);
+
+/* One iteration. iter == 1 needs raw_host (copied and padded on the device,
+ * prepare_iteration1, iternlm_gpu.cu:2117); iter > 1 pads the previous result
+ * (prepare_nextiteration, :2230) and raw_host may be NULL. */
+int inlm_run_iteration(inlm_denoiser* d, int iter, const float* raw_host);
+
+/* Copies the last iteration's nx*ny*nz result to host memory. */
+int inlm_get_result(inlm_denoiser* d, float* out_host);
+
+/* Device-resident forms (no host copies): raw_dev / out_dev are device
+ * pointers on the denoiser's device. */
+int inlm_run_iteration_device(inlm_denoiser* d, int iter, const float* raw_dev);
+int inlm_get_result_device(inlm_denoiser* d, float* out_dev);
+
+/* Whole job on the device, the driver's schedule (main.cpp:327-545):
+ * sigma0 = noise(raw); iteration 1; sigma1 = noise(result);
+ * sigma1 = alpha*sigma0 + (1-alpha)*sigma1; iterations 2..maxiterations
+ * (re-estimating before each under continuous_estimate). raw and out are
+ * host pointers when on_device == 0, device pointers otherwise.
+ * sigma0_out / sigma1_out (nullable, host) receive the two estimates. */
+int inlm_denoise(inlm_denoiser* d, const float* raw, float* out, int on_device,
+                 float* sigma0_out, float* sigma1_out);
+
+/* Stream the denoiser launches on (cudaStream_t as void*); NULL = its own. */
+int inlm_set_stream(inlm_denoiser* d, void* stream);
+
+/* Average duration in ms of the filter-kernel launches since the last call
+ * (CUDA events on the launching stream); *n_launches gets their count. */
+int inlm_filter_kernel_ms(inlm_denoiser* d, double* avg_ms, int* n_launches);
+
+/* Description of the chosen filter kernel (name, tile, taps, offsets). */
+int inlm_describe(inlm_denoiser* d, char* buf, size_t len);
+
+/* Number of kernels this handle has launched since creation. */
+int inlm_kernel_launches(inlm_denoiser* d, uint64_t* count);
+
+/* Measures the FP32 FMA throughput of the device in TFLOP/s (2 flops per
+ * FFMA) with an all-SM loop of independent FMA chains timed by CUDA events;
+ * the roofline denominator of the FP32-bound filter. */
+int inlm_probe_fp32_peak(int device_id, double* tflops);
+
+/* ---------------- noise level (NoiseLevel) ---------------- */
+
+/* shape as above; n_samples random 2D patches of patchsize^2 voxels. The
+ * sample positions are drawn on the first estimate and kept (the reference
+ * caches them in NoiseLevel::samples). */
+int inlm_noise_create(const int shape[3], uint64_t n_samples, int patchsize, unsigned int seed,
+                      int device_id, inlm_noise** out);
+int inlm_noise_destroy(inlm_noise* n);
+
+/* NoiseLevel::get_noiselevel: sigma_out receives nz values (host).
+ * stack is a host pointer when on_device == 0, else a device pointer.
+ * Uses p->noise_mode, zwindow, sigma[], stds_from_mean,
+ * circular_mask_diameter. In semimanual mode the second and later calls write
+ * the chosen value to p->sigma[1], as the reference does (noiselevel.cpp:74). */
+int inlm_noise_estimate(inlm_noise* n, inlm_params* p, const float* stack, int on_device,
+                        float* sigma_out);
+
+/* Sorted sample positions (linear voxel indices) drawn so far; returns the
+ * count through *n_out. */
+int inlm_noise_samples(inlm_noise* n, int64_t* out, uint64_t max_n, uint64_t* n_out);
+
+/* Per-sample patch std of the last estimate (host copy). */
+int inlm_noise_patchstd(inlm_noise* n, float* out, uint64_t max_n);
+
+/* ---------------- host-only helpers (no device needed) ---------------- */
+
+/* Geometry of a parameter set (setup_searchspace / setup_patchspace /
+ * setup_distweight, Denoiser/iternlm_prepare.cpp:102-262): offsets as
+ * (x,y,z) triples in reference order and the patch weights the filter applies.
+ * Pass NULL arrays to query the counts. pad3 gets the padding per axis. */
+int inlm_geometry(const inlm_params* p, int nz, int* search_xyz, int* n_search, int* patch_xyz,
+                  float* weights, int* n_patch, int pad3[3]);
+
+/* NoiseLevel::drawsamples (Noise/noiselevel.cpp:192) with the glibc rand()
+ * sequence of srand(seed), sorted ascending. */
+int inlm_noise_draw_samples(const int shape[3], uint64_t n_samples, int patchsize,
+                            int circular_mask_diameter, unsigned int seed, int64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INLM_H */

@@ -1,0 +1,275 @@
+"""iterNLM on B200: the iterative 3D nonlocal-means filter and the two-cluster
+noise estimators of iternlm/microtomodenoise (iterNLM_v0.3), as hand-written
+sm_100a CUDA kernels behind a C ABI (include/inlm.h).
+
+The Python classes mirror the reference's C++ call surface:
+
+* ``DenoiseParameters``  <- protocol::DenoiseParameters (denoise_parameters.h:9-74)
+* ``IterativeNLM_GPU``   <- denoise::IterativeNLM_GPU (Denoiser/iternlm_gpu.h:20-56)
+* ``NoiseLevel``         <- noise::NoiseLevel (Noise/noiselevel.h:14-46)
+* ``denoise()``          <- the iterNLM driver's sigma0/sigma1 schedule and loop
+                            (main.cpp:327-545), run on the device
+
+Volumes are numpy float32 arrays of shape (nz, ny, nx) (x fastest), or device
+pointers (ints) for the ``*_device`` forms. Everything runs in libinlm.so; if
+it is missing, importing this package's GPU classes raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import InlmError, InlmParams, NOISE_MODES, PRECISIONS
+
+__all__ = ["DenoiseParameters", "IterativeNLM_GPU", "NoiseLevel", "denoise", "InlmError"]
+
+
+@dataclass
+class DenoiseParameters:
+    """Knobs and defaults of protocol::DenoiseParameters (denoise_parameters.h:11-73)
+    that the GPU path uses, plus the device-side additions."""
+
+    alpha: float = 0.5
+    maxiterations: int = 4
+    nslices: int = 11
+    radius_searchspace: Tuple[int, int, int] = (10, 10, 10)
+    radius_patchspace: Tuple[int, int, int] = (1, 1, 1)
+    beta: float = 1.0
+    z_anisotropy: float = 1.0
+    # NoiseLevel
+    noise_mode: str = "z-adaptive"
+    zwindow: int = 100
+    sigma: Tuple[float, float] = (0.0, 0.0)
+    n_samples: int = 100000
+    patchsize: int = 15
+    stds_from_mean: float = 1.0
+    continuous_estimate: bool = False
+    circular_mask_diameter: int = 0
+    noise_seed: int = 0
+    # GPU
+    deviceID: int = 0
+    precision: str = "f32"
+    weight_table: str = "cpu"   # "cpu" = the reference CPU filter's table, "distweight"
+
+    def to_c(self) -> InlmParams:
+        p = InlmParams()
+        _lib.load().inlm_default_params(C.byref(p))
+        p.alpha = self.alpha
+        p.maxiterations = self.maxiterations
+        p.nslices = self.nslices
+        for i in range(3):
+            p.search_radius[i] = int(self.radius_searchspace[i])
+            p.patch_radius[i] = int(self.radius_patchspace[i])
+        p.beta = self.beta
+        p.z_anisotropy = self.z_anisotropy
+        if self.noise_mode not in NOISE_MODES:
+            raise ValueError(f"unknown noise mode {self.noise_mode!r}")
+        p.noise_mode = NOISE_MODES[self.noise_mode]
+        p.zwindow = self.zwindow
+        p.sigma[0], p.sigma[1] = float(self.sigma[0]), float(self.sigma[1])
+        p.n_samples = int(self.n_samples)
+        p.noise_patchsize = int(self.patchsize)
+        p.stds_from_mean = self.stds_from_mean
+        p.continuous_estimate = int(bool(self.continuous_estimate))
+        p.circular_mask_diameter = int(self.circular_mask_diameter)
+        p.noise_seed = int(self.noise_seed) & 0xFFFFFFFF
+        p.device_id = int(self.deviceID)
+        p.precision = PRECISIONS[self.precision]
+        p.weight_table = 0 if self.weight_table == "cpu" else 1
+        return p
+
+
+def _shape_c(shape_zyx) -> "C.Array":
+    nz, ny, nx = shape_zyx
+    return (C.c_int * 3)(int(nx), int(ny), int(nz))
+
+
+def _f32c(a: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class IterativeNLM_GPU:
+    """denoise::IterativeNLM_GPU on one B200.
+
+    configure_device(shape, params) allocates and builds the tables;
+    set_sigma(sigma); Run_GaussianNoise(iter, instack); get_result();
+    free_device(). Shapes are (nz, ny, nx).
+    """
+
+    def __init__(self):
+        self._h = C.c_void_p(None)
+        self.shape = None
+        self.n_parallelslices = 0
+        self.resumed = False
+
+    def configure_device(self, shape_zyx, params: DenoiseParameters) -> int:
+        L = _lib.load()
+        cp = params.to_c()
+        rc = L.inlm_denoiser_create(_shape_c(shape_zyx), C.byref(cp), C.byref(self._h))
+        if rc == -3:
+            return -1  # no GPU, as the reference reports it (iternlm_gpu.cu:1444)
+        _lib.check(rc, "configure_device")
+        self.shape = tuple(int(s) for s in shape_zyx)
+        self.n_parallelslices = self.shape[0]
+        return self.n_parallelslices
+
+    def _need(self):
+        if not self._h:
+            raise InlmError(-5, "IterativeNLM_GPU", "configure_device first")
+
+    def set_sigma(self, sigma: np.ndarray) -> None:
+        self._need()
+        s = _f32c(sigma)
+        assert s.shape == (self.shape[0],)
+        _lib.check(_lib.load().inlm_set_sigma(self._h, s.ctypes.data), "set_sigma")
+
+    def Run_GaussianNoise(self, iteration: int, instack: Optional[np.ndarray] = None) -> None:
+        self._need()
+        ptr = None
+        if iteration == 1:
+            if instack is None:
+                raise ValueError("iteration 1 needs the raw stack")
+            instack = _f32c(instack)
+            assert instack.shape == self.shape
+            ptr = instack.ctypes.data
+        _lib.check(_lib.load().inlm_run_iteration(self._h, int(iteration), ptr),
+                   "Run_GaussianNoise")
+
+    def Run_GaussianNoise_device(self, iteration: int, raw_dev_ptr: Optional[int] = None) -> None:
+        self._need()
+        _lib.check(_lib.load().inlm_run_iteration_device(self._h, int(iteration), raw_dev_ptr),
+                   "Run_GaussianNoise_device")
+
+    def get_result(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        self._need()
+        if out is None:
+            out = np.empty(self.shape, np.float32)
+        _lib.check(_lib.load().inlm_get_result(self._h, out.ctypes.data), "get_result")
+        return out
+
+    def get_result_device(self, out_dev_ptr: int) -> None:
+        self._need()
+        _lib.check(_lib.load().inlm_get_result_device(self._h, out_dev_ptr), "get_result_device")
+
+    def denoise(self, raw, on_device: bool = False, out=None):
+        """Whole job (noise estimates + all iterations) on the device.
+        Returns (result, sigma0, sigma1)."""
+        self._need()
+        nz = self.shape[0]
+        s0 = np.zeros(nz, np.float32)
+        s1 = np.zeros(nz, np.float32)
+        if on_device:
+            rc = _lib.load().inlm_denoise(self._h, raw, out, 1, s0.ctypes.data, s1.ctypes.data)
+            _lib.check(rc, "denoise")
+            return out, s0, s1
+        raw = _f32c(raw)
+        if out is None:
+            out = np.empty(self.shape, np.float32)
+        rc = _lib.load().inlm_denoise(self._h, raw.ctypes.data, out.ctypes.data, 0,
+                                      s0.ctypes.data, s1.ctypes.data)
+        _lib.check(rc, "denoise")
+        return out, s0, s1
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self._need()
+        _lib.check(_lib.load().inlm_set_stream(self._h, stream_ptr), "set_stream")
+
+    def filter_kernel_ms(self):
+        """(average ms, launches) of the filter kernel since the last call."""
+        self._need()
+        ms = C.c_double(0)
+        n = C.c_int(0)
+        _lib.check(_lib.load().inlm_filter_kernel_ms(self._h, C.byref(ms), C.byref(n)),
+                   "filter_kernel_ms")
+        return ms.value, n.value
+
+    def describe(self) -> str:
+        self._need()
+        buf = C.create_string_buffer(512)
+        _lib.check(_lib.load().inlm_describe(self._h, buf, 512), "describe")
+        return buf.value.decode()
+
+    def free_device(self) -> None:
+        if self._h:
+            _lib.load().inlm_denoiser_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.free_device()
+        except Exception:
+            pass
+
+
+class NoiseLevel:
+    """noise::NoiseLevel(n_samples, patchsize, shape) on the device.
+
+    get_noiselevel(stack, params) returns the per-slice sigma (nz floats).
+    Sample positions are drawn on the first call from params.noise_seed (the
+    reference seeds with time(NULL)) and reused afterwards.
+    """
+
+    def __init__(self, n_samples: int, patchsize: int, shape_zyx, seed: int = 0,
+                 device: int = 0):
+        self.shape = tuple(int(s) for s in shape_zyx)
+        self._h = C.c_void_p(None)
+        _lib.check(_lib.load().inlm_noise_create(_shape_c(shape_zyx), int(n_samples), int(patchsize),
+                                                 int(seed) & 0xFFFFFFFF, int(device),
+                                                 C.byref(self._h)), "NoiseLevel")
+        self.n_samples = int(n_samples)
+
+    def get_noiselevel(self, stack, params: DenoiseParameters, on_device: bool = False) -> np.ndarray:
+        cp = params.to_c()
+        out = np.zeros(self.shape[0], np.float32)
+        if on_device:
+            ptr = stack
+        else:
+            stack = _f32c(stack)
+            assert stack.shape == self.shape
+            ptr = stack.ctypes.data
+        _lib.check(_lib.load().inlm_noise_estimate(self._h, C.byref(cp), ptr, int(on_device),
+                                                   out.ctypes.data), "get_noiselevel")
+        if params.noise_mode == "semimanual":
+            params.sigma = (params.sigma[0], float(cp.sigma[1]))
+        return out
+
+    def samples(self) -> np.ndarray:
+        out = np.zeros(self.n_samples, np.int64)
+        n = C.c_uint64(0)
+        _lib.check(_lib.load().inlm_noise_samples(self._h, out.ctypes.data, self.n_samples,
+                                                  C.byref(n)), "samples")
+        return out[: n.value]
+
+    def patchstd(self) -> np.ndarray:
+        out = np.zeros(self.n_samples, np.float32)
+        _lib.check(_lib.load().inlm_noise_patchstd(self._h, out.ctypes.data, self.n_samples),
+                   "patchstd")
+        return out
+
+    def close(self):
+        if self._h:
+            _lib.load().inlm_noise_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def denoise(raw: np.ndarray, params: Optional[DenoiseParameters] = None):
+    """Runs the iterNLM schedule on one GPU; returns (result, sigma0, sigma1)."""
+    params = params or DenoiseParameters()
+    g = IterativeNLM_GPU()
+    rc = g.configure_device(raw.shape, params)
+    if rc < 0:
+        raise InlmError(-3, "denoise", "no CUDA device")
+    try:
+        return g.denoise(raw)
+    finally:
+        g.free_device()

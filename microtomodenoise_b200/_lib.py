@@ -1,0 +1,116 @@
+"""ctypes binding of the C ABI in include/inlm.h (libinlm.so, built in-tree).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libinlm.so")
+
+INLM_OK = 0
+ERRORS = {
+    -1: "INLM_ERR_ARG",
+    -2: "INLM_ERR_CUDA",
+    -3: "INLM_ERR_NODEVICE",
+    -4: "INLM_ERR_NOMEM",
+    -5: "INLM_ERR_STATE",
+    -6: "INLM_ERR_TIMEOUT",
+    -7: "INLM_ERR_UNSUPPORTED",
+}
+NOISE_MODES = {"z-adaptive": 0, "auto": 0, "global": 1, "manual": 2, "semimanual": 3}
+PRECISIONS = {"f32": 0, "f16": 1}
+
+# Every entry point include/inlm.h declares.
+EXPORTS = (
+    "inlm_default_params", "inlm_last_error", "inlm_denoiser_create", "inlm_denoiser_destroy",
+    "inlm_set_sigma", "inlm_run_iteration", "inlm_get_result", "inlm_run_iteration_device",
+    "inlm_get_result_device", "inlm_denoise", "inlm_set_stream", "inlm_filter_kernel_ms",
+    "inlm_describe", "inlm_noise_create", "inlm_noise_destroy", "inlm_noise_estimate",
+    "inlm_noise_samples", "inlm_noise_patchstd", "inlm_geometry", "inlm_noise_draw_samples",
+    "inlm_kernel_launches", "inlm_probe_fp32_peak",
+)
+
+
+class InlmParams(C.Structure):
+    _fields_ = [
+        ("alpha", C.c_float),
+        ("maxiterations", C.c_int),
+        ("nslices", C.c_int),
+        ("search_radius", C.c_int * 3),
+        ("patch_radius", C.c_int * 3),
+        ("beta", C.c_float),
+        ("z_anisotropy", C.c_float),
+        ("noise_mode", C.c_int),
+        ("zwindow", C.c_int),
+        ("sigma", C.c_float * 2),
+        ("n_samples", C.c_uint64),
+        ("noise_patchsize", C.c_int),
+        ("stds_from_mean", C.c_float),
+        ("continuous_estimate", C.c_int),
+        ("circular_mask_diameter", C.c_int),
+        ("noise_seed", C.c_uint),
+        ("device_id", C.c_int),
+        ("precision", C.c_int),
+        ("weight_table", C.c_int),
+    ]
+
+
+class InlmError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        self.code = code
+        super().__init__(f"{where}: {ERRORS.get(code, code)}: {msg}")
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Loads libinlm.so once; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build it with `python -m microtomodenoise_b200.build` "
+            "(the package has no CPU fallback)")
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    L.inlm_last_error.restype = C.c_char_p
+    L.inlm_default_params.argtypes = [C.POINTER(InlmParams)]
+    L.inlm_default_params.restype = None
+    L.inlm_denoiser_create.argtypes = [C.c_int * 3, C.POINTER(InlmParams), C.POINTER(vp)]
+    L.inlm_denoiser_destroy.argtypes = [vp]
+    L.inlm_set_sigma.argtypes = [vp, vp]
+    L.inlm_run_iteration.argtypes = [vp, C.c_int, vp]
+    L.inlm_get_result.argtypes = [vp, vp]
+    L.inlm_run_iteration_device.argtypes = [vp, C.c_int, vp]
+    L.inlm_get_result_device.argtypes = [vp, vp]
+    L.inlm_denoise.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+    L.inlm_set_stream.argtypes = [vp, vp]
+    L.inlm_filter_kernel_ms.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    L.inlm_describe.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.inlm_noise_create.argtypes = [C.c_int * 3, C.c_uint64, C.c_int, C.c_uint, C.c_int,
+                                    C.POINTER(vp)]
+    L.inlm_noise_destroy.argtypes = [vp]
+    L.inlm_noise_estimate.argtypes = [vp, C.POINTER(InlmParams), vp, C.c_int, vp]
+    L.inlm_noise_samples.argtypes = [vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]
+    L.inlm_noise_patchstd.argtypes = [vp, vp, C.c_uint64]
+    L.inlm_geometry.argtypes = [C.POINTER(InlmParams), C.c_int, vp, C.POINTER(C.c_int), vp, vp,
+                                C.POINTER(C.c_int), vp]
+    L.inlm_noise_draw_samples.argtypes = [C.c_int * 3, C.c_uint64, C.c_int, C.c_int, C.c_uint, vp]
+    L.inlm_kernel_launches.argtypes = [vp, C.POINTER(C.c_uint64)]
+    L.inlm_probe_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    for name in EXPORTS:
+        if name not in ("inlm_last_error", "inlm_default_params"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(rc: int, where: str) -> None:
+    if rc != INLM_OK:
+        msg = _lib.inlm_last_error().decode(errors="replace") if _lib else ""
+        raise InlmError(rc, where, msg)

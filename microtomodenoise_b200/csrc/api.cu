@@ -1,0 +1,951 @@
+// C ABI (include/inlm.h): denoiser and noise-level handles over the sm_100a
+// kernels. Host orchestration follows IterativeNLM_GPU (Denoiser/iternlm_gpu.cu:
+// configure_device :1440, Run_GaussianNoise :1651, prepare_iteration1 :2117,
+// prepare_nextiteration :2230, set_sigma :2341, get_result :2356) and
+// NoiseLevel::get_noiselevel (Noise/noiselevel.cpp:9), on one device and one
+// stream per handle, without the reference's per-step device synchronisation.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/inlm.h"
+#include "filter_kernels.cuh"
+#include "geometry.hpp"
+#include "noise_kernels.cuh"
+#include "sampling.hpp"
+#include "probe.cuh"
+
+using namespace inlm;
+
+// ---------------- error plumbing ----------------
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                       \
+    do {                                                                                     \
+        cudaError_t _e = (expr);                                                             \
+        if (_e != cudaSuccess) {                                                             \
+            int _code = (_e == cudaErrorMemoryAllocation) ? INLM_ERR_NOMEM : INLM_ERR_CUDA;  \
+            return fail(_code, "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, \
+                        __LINE__);                                                           \
+        }                                                                                    \
+    } while (0)
+
+extern "C" const char* inlm_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" void inlm_default_params(inlm_params* p) {
+    // protocol::DenoiseParameters defaults, denoise_parameters.h:11-73
+    std::memset(p, 0, sizeof *p);
+    p->alpha = 0.5f;
+    p->maxiterations = 4;
+    p->nslices = 11;
+    for (int i = 0; i < 3; i++) {
+        p->search_radius[i] = 10;
+        p->patch_radius[i] = 1;
+    }
+    p->beta = 1.f;
+    p->z_anisotropy = 1.f;
+    p->noise_mode = INLM_NOISE_ZADAPTIVE;
+    p->zwindow = 100;
+    p->sigma[0] = p->sigma[1] = 0.0f;
+    p->n_samples = 100000;
+    p->noise_patchsize = 15;
+    p->stds_from_mean = 1.f;
+    p->continuous_estimate = 0;
+    p->circular_mask_diameter = 0;
+    p->noise_seed = 0;
+    p->device_id = 0;
+    p->precision = INLM_PRECISION_F32;
+    p->weight_table = INLM_WEIGHTS_CPU;
+}
+
+template <typename T>
+static cudaError_t dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    return cudaMalloc((void**)p, n * sizeof(T));
+}
+
+// ---------------- TMA descriptor encoding ----------------
+
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                    const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                    const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled get_encode_fn() {
+    static PFN_encodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_encodeTiled)p;
+    }
+    return fn;
+}
+
+// 3D float32 map over a padded volume (pitch in elements), box (bx,by,bz).
+static int encode_map_3d(CUtensorMap* tm, const float* base, int ex, int ey, int ez,
+                         long long pitch_y, long long pitch_z, int bx, int by, int bz) {
+    PFN_encodeTiled enc = get_encode_fn();
+    if (!enc) return fail(INLM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[3] = {(cuuint64_t)ex, (cuuint64_t)ey, (cuuint64_t)ez};
+    cuuint64_t strides[2] = {(cuuint64_t)pitch_y * 4, (cuuint64_t)pitch_z * 4};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(INLM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return INLM_OK;
+}
+
+// ---------------- noise handle ----------------
+
+struct inlm_noise {
+    int shape[3] = {0, 0, 0};
+    uint64_t n_samples = 0;
+    int patchsize = 15;
+    unsigned int seed = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int mask_drawn = -1;
+    std::vector<long long> samples;
+    long long* d_samples = nullptr;
+    float* d_patchstd = nullptr;
+    float* d_stack = nullptr;  // staging for host stacks
+    int zwindow_cached = -1;
+    int2* d_windows = nullptr;
+    long long* d_scratch_off = nullptr;
+    signed char* d_assign = nullptr;
+    size_t assign_cap = 0;
+    float* d_mean = nullptr;
+    float* d_sd = nullptr;
+    float* d_sigma = nullptr;
+    int ncalls = 0;
+    long long ref_sample_semimanual = 0;
+};
+
+static void noise_free(inlm_noise* n) {
+    if (!n) return;
+    cudaSetDevice(n->device);
+    cudaFree(n->d_samples);
+    cudaFree(n->d_patchstd);
+    cudaFree(n->d_stack);
+    cudaFree(n->d_windows);
+    cudaFree(n->d_scratch_off);
+    cudaFree(n->d_assign);
+    cudaFree(n->d_mean);
+    cudaFree(n->d_sd);
+    cudaFree(n->d_sigma);
+    if (n->own_stream && n->stream) cudaStreamDestroy(n->stream);
+}
+
+extern "C" int inlm_noise_create(const int shape[3], uint64_t n_samples, int patchsize,
+                                 unsigned int seed, int device_id, inlm_noise** out) {
+    if (!shape || !out) return fail(INLM_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (shape[0] <= patchsize || shape[1] <= patchsize || shape[2] < 1)
+        return fail(INLM_ERR_ARG, "shape %dx%dx%d too small for noise patch %d", shape[0], shape[1],
+                    shape[2], patchsize);
+    if (n_samples == 0 || n_samples > (1ull << 31))
+        return fail(INLM_ERR_ARG, "n_samples out of range");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return fail(INLM_ERR_NODEVICE, "no CUDA device");
+    if (device_id < 0 || device_id >= ndev) return fail(INLM_ERR_ARG, "bad device id");
+    inlm_noise* n = new inlm_noise();
+    for (int i = 0; i < 3; i++) n->shape[i] = shape[i];
+    n->n_samples = n_samples;
+    n->patchsize = patchsize;
+    n->seed = seed;
+    n->device = device_id;
+    cudaSetDevice(device_id);
+    cudaError_t e = cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete n;
+        return fail(INLM_ERR_CUDA, "stream create: %s", cudaGetErrorString(e));
+    }
+    n->own_stream = true;
+    int nz = shape[2];
+    if (dalloc(&n->d_samples, n_samples) != cudaSuccess || dalloc(&n->d_patchstd, n_samples) != cudaSuccess ||
+        dalloc(&n->d_windows, nz) != cudaSuccess || dalloc(&n->d_scratch_off, nz) != cudaSuccess ||
+        dalloc(&n->d_mean, nz) != cudaSuccess || dalloc(&n->d_sd, nz) != cudaSuccess ||
+        dalloc(&n->d_sigma, nz) != cudaSuccess) {
+        noise_free(n);
+        delete n;
+        return fail(INLM_ERR_NOMEM, "noise buffers");
+    }
+    *out = n;
+    return INLM_OK;
+}
+
+extern "C" int inlm_noise_destroy(inlm_noise* n) {
+    noise_free(n);
+    delete n;
+    return INLM_OK;
+}
+
+// Runs the estimate for a device stack (pitches in elements); the result stays
+// in n->d_sigma. Host-side decisions (manual, semimanual) fill host_sigma.
+static int noise_estimate_device(inlm_noise* n, inlm_params* p, const float* d_stack,
+                                 long long pitch_y, long long pitch_z, std::vector<float>* host_sigma,
+                                 bool* sigma_on_host) {
+    const int nz = n->shape[2];
+    *sigma_on_host = false;
+    const int mode = p->noise_mode;
+    if (mode == INLM_NOISE_MANUAL) {
+        // noiselevel.cpp:84-91
+        float v = p->sigma[n->ncalls > 0 ? 1 : 0];
+        host_sigma->assign(nz, v);
+        *sigma_on_host = true;
+        n->ncalls++;
+        return INLM_OK;
+    }
+    if (mode != INLM_NOISE_ZADAPTIVE && mode != INLM_NOISE_GLOBAL && mode != INLM_NOISE_SEMIMANUAL)
+        return fail(INLM_ERR_ARG, "unknown noise mode %d", mode);
+    bool first = n->samples.empty();
+    if (first) {
+        n->samples = draw_noise_samples(n->shape, n->n_samples, n->patchsize,
+                                        p->circular_mask_diameter, n->seed);
+        CUDA_TRY(cudaMemcpyAsync(n->d_samples, n->samples.data(), n->samples.size() * 8,
+                                 cudaMemcpyHostToDevice, n->stream));
+    }
+    const long long ns = (long long)n->samples.size();
+    CUDA_TRY(launch_noise_patchstd(d_stack, pitch_y, pitch_z, n->shape[0],
+                                   (long long)n->shape[0] * n->shape[1], n->d_samples, ns,
+                                   n->patchsize, n->d_patchstd, n->stream));
+    if (mode == INLM_NOISE_SEMIMANUAL) {
+        // noiselevel.cpp:62-79
+        std::vector<float> ps(ns);
+        CUDA_TRY(cudaMemcpyAsync(ps.data(), n->d_patchstd, ns * 4, cudaMemcpyDeviceToHost, n->stream));
+        CUDA_TRY(cudaStreamSynchronize(n->stream));
+        float v;
+        if (first) {
+            float best = 1e9f;
+            v = p->sigma[0];
+            for (long long i = 0; i < ns; i++) {
+                float d = std::fabs(ps[i] - v);
+                if (d < best) {
+                    best = d;
+                    n->ref_sample_semimanual = i;
+                }
+            }
+        } else {
+            v = ps[n->ref_sample_semimanual];
+            p->sigma[1] = v;
+        }
+        host_sigma->assign(nz, v);
+        *sigma_on_host = true;
+        n->ncalls++;
+        return INLM_OK;
+    }
+    int nwin;
+    if (mode == INLM_NOISE_ZADAPTIVE) {
+        if (n->zwindow_cached != p->zwindow || first) {
+            std::vector<int> st, en;
+            noise_zwindows(n->samples, n->shape, p->zwindow, st, en);
+            std::vector<int2> w(nz);
+            std::vector<long long> off(nz);
+            long long total = 0;
+            for (int z = 0; z < nz; z++) {
+                w[z] = make_int2(st[z], en[z]);
+                off[z] = total;
+                total += std::max(0, en[z] - st[z] + 1);
+            }
+            if ((size_t)total > n->assign_cap) {
+                cudaFree(n->d_assign);
+                n->d_assign = nullptr;
+                n->assign_cap = 0;
+                CUDA_TRY(dalloc(&n->d_assign, (size_t)total));
+                n->assign_cap = (size_t)total;
+            }
+            CUDA_TRY(cudaMemcpyAsync(n->d_windows, w.data(), nz * sizeof(int2),
+                                     cudaMemcpyHostToDevice, n->stream));
+            CUDA_TRY(cudaMemcpyAsync(n->d_scratch_off, off.data(), nz * 8, cudaMemcpyHostToDevice,
+                                     n->stream));
+            CUDA_TRY(cudaStreamSynchronize(n->stream));  // host vectors go out of scope
+            n->zwindow_cached = p->zwindow;
+        }
+        nwin = nz;
+    } else {
+        if (n->zwindow_cached != -2) {
+            int2 w = make_int2(0, (int)ns - 1);
+            long long off = 0;
+            if ((size_t)ns > n->assign_cap) {
+                cudaFree(n->d_assign);
+                n->d_assign = nullptr;
+                n->assign_cap = 0;
+                CUDA_TRY(dalloc(&n->d_assign, (size_t)ns));
+                n->assign_cap = (size_t)ns;
+            }
+            CUDA_TRY(cudaMemcpyAsync(n->d_windows, &w, sizeof w, cudaMemcpyHostToDevice, n->stream));
+            CUDA_TRY(cudaMemcpyAsync(n->d_scratch_off, &off, 8, cudaMemcpyHostToDevice, n->stream));
+            CUDA_TRY(cudaStreamSynchronize(n->stream));
+            n->zwindow_cached = -2;
+        }
+        nwin = 1;
+    }
+    CUDA_TRY(launch_noise_em(n->d_patchstd, n->d_windows, nwin, n->d_scratch_off, n->d_assign,
+                             n->d_mean, n->d_sd, n->stream));
+    CUDA_TRY(launch_noise_finalize(n->d_mean, n->d_sd, nz, mode == INLM_NOISE_ZADAPTIVE ? 1 : 0,
+                                   p->stds_from_mean, n->d_sigma, n->stream));
+    n->ncalls++;
+    return INLM_OK;
+}
+
+extern "C" int inlm_noise_estimate(inlm_noise* n, inlm_params* p, const float* stack,
+                                   int on_device, float* sigma_out) {
+    if (!n || !p || !stack || !sigma_out) return fail(INLM_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(n->device));
+    const long long nvox = (long long)n->shape[0] * n->shape[1] * n->shape[2];
+    const float* d_stack = stack;
+    if (!on_device) {
+        if (!n->d_stack) CUDA_TRY(dalloc(&n->d_stack, nvox));
+        CUDA_TRY(cudaMemcpyAsync(n->d_stack, stack, nvox * 4, cudaMemcpyHostToDevice, n->stream));
+        d_stack = n->d_stack;
+    }
+    std::vector<float> hs;
+    bool on_host = false;
+    int rc = noise_estimate_device(n, p, d_stack, n->shape[0], (long long)n->shape[0] * n->shape[1],
+                                   &hs, &on_host);
+    if (rc != INLM_OK) return rc;
+    if (on_host) {
+        std::memcpy(sigma_out, hs.data(), n->shape[2] * 4);
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(sigma_out, n->d_sigma, n->shape[2] * 4, cudaMemcpyDeviceToHost,
+                                 n->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(n->stream));
+    return INLM_OK;
+}
+
+extern "C" int inlm_noise_samples(inlm_noise* n, int64_t* out, uint64_t max_n, uint64_t* n_out) {
+    if (!n) return fail(INLM_ERR_ARG, "null handle");
+    if (n_out) *n_out = n->samples.size();
+    if (out)
+        for (uint64_t i = 0; i < max_n && i < n->samples.size(); i++) out[i] = n->samples[i];
+    return INLM_OK;
+}
+
+extern "C" int inlm_noise_patchstd(inlm_noise* n, float* out, uint64_t max_n) {
+    if (!n || !out) return fail(INLM_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(n->device));
+    uint64_t cnt = std::min<uint64_t>(max_n, n->samples.size());
+    CUDA_TRY(cudaMemcpyAsync(out, n->d_patchstd, cnt * 4, cudaMemcpyDeviceToHost, n->stream));
+    CUDA_TRY(cudaStreamSynchronize(n->stream));
+    return INLM_OK;
+}
+
+// ---------------- denoiser handle ----------------
+
+struct TimedLaunch {
+    cudaEvent_t a, b;
+};
+
+struct inlm_denoiser {
+    int shape[3] = {0, 0, 0};
+    inlm_params p;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Geometry geo;
+    int nxp = 0, nyp = 0, nzp = 0;
+    long long pitch_y = 0, pitch_z = 0;
+    float* d_raw_pad = nullptr;
+    float* d_prev_pad = nullptr;
+    float* d_next = nullptr;
+    float* d_sigma = nullptr;
+    float* d_sigma0 = nullptr;
+    float* d_mult = nullptr;
+    int* d_err = nullptr;
+    int2* d_search_delta = nullptr;
+    long long* d_search_off = nullptr;
+    long long* d_patch_off = nullptr;
+    float* d_weights = nullptr;
+    bool use_tile = false;
+    TileConfig tcfg{};
+    TileArgs targs{};
+    GenericArgs gargs{};
+    CUtensorMap tm_prev{}, tm_raw{};
+    int last_iter = 0;
+    bool sigma_set = false;
+    uint64_t launches = 0;
+    std::vector<TimedLaunch> pending;
+    std::vector<TimedLaunch> event_pool;
+    double timed_ms = 0.0;
+    int timed_n = 0;
+    inlm_noise* noise = nullptr;
+};
+
+static void denoiser_free(inlm_denoiser* d) {
+    if (!d) return;
+    cudaSetDevice(d->device);
+    if (d->stream) cudaStreamSynchronize(d->stream);
+    for (auto& t : d->pending) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (auto& t : d->event_pool) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    cudaFree(d->d_raw_pad);
+    cudaFree(d->d_prev_pad);
+    cudaFree(d->d_next);
+    cudaFree(d->d_sigma);
+    cudaFree(d->d_sigma0);
+    cudaFree(d->d_mult);
+    cudaFree(d->d_err);
+    cudaFree(d->d_search_delta);
+    cudaFree(d->d_search_off);
+    cudaFree(d->d_patch_off);
+    cudaFree(d->d_weights);
+    if (d->noise) {
+        noise_free(d->noise);
+        delete d->noise;
+    }
+    if (d->own_stream && d->stream) cudaStreamDestroy(d->stream);
+}
+
+static int choose_tile_config(inlm_denoiser* d) {
+    const Geometry& g = d->geo;
+    const int* pr = g.patch_radius;
+    d->use_tile = false;
+    if (!tile_kernel_available(pr[0], pr[1], pr[2])) return INLM_OK;
+    if (d->p.nslices / 2 < pr[2]) return INLM_OK;           // z-clipped patch
+    if ((int)g.taps.size() > kMaxTaps) return INLM_OK;
+    // the kernel's compile-time tap order must equal the host table
+    std::vector<int> order(3 * kMaxTaps);
+    int nt = tile_kernel_tap_order(pr[0], pr[1], pr[2], order.data(), kMaxTaps);
+    if (nt != (int)g.taps.size()) return INLM_OK;
+    for (int t = 0; t < nt; t++)
+        if (order[3 * t] != g.taps[t].x || order[3 * t + 1] != g.taps[t].y ||
+            order[3 * t + 2] != g.taps[t].z)
+            return INLM_OK;
+
+    TileArgs& a = d->targs;
+    a.nx = d->shape[0];
+    a.ny = d->shape[1];
+    a.nz = d->shape[2];
+    a.px = g.pad[0];
+    a.py = g.pad[1];
+    a.pz = g.pad[2];
+    a.sxr = g.search_radius[0];
+    a.syr = g.search_radius[1];
+    a.szc = std::min(d->p.nslices / 2, g.search_radius[2]);
+    a.S = (int)g.search.size();
+    a.gpitch_y = d->pitch_y;
+    a.gpitch_z = d->pitch_z;
+    a.pbx = (kTX + 2 * a.px + 3) / 4 * 4;
+    a.pby = kTY + 2 * a.py;
+    a.rbx = (pr[0] + kTX + 2 * a.sxr + 3) / 4 * 4;
+    a.rby = kTY + 2 * a.syr;
+    for (int t = 0; t < nt; t++) a.w[t] = g.weights[t];
+    int smem_max = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
+    const struct {
+        int tz;
+        bool raw;
+    } cands[] = {{8, true}, {8, false}, {4, false}};
+    for (auto c : cands) {
+        a.pbz = c.tz + 2 * a.pz;
+        a.rbz = c.tz + 2 * a.szc;
+        if (a.pbx > 256 || a.pby > 256 || a.pbz > 256) continue;
+        if (c.raw && (a.rbx > 256 || a.rby > 256 || a.rbz > 256)) continue;
+        if ((long long)a.pbx * a.pby * a.pbz >= 65536) continue;  // 16-bit index table
+        TileConfig tc{pr[0], pr[1], pr[2], c.tz, c.raw, 0};
+        size_t sm = tile_smem_bytes(tc, a);
+        if (sm == 0 || sm > (size_t)smem_max) continue;
+        tc.smem_bytes = sm;
+        d->tcfg = tc;
+        d->use_tile = true;
+        break;
+    }
+    if (!d->use_tile) return INLM_OK;
+    a.tiles_x = (d->shape[0] + kTX - 1) / kTX;
+    a.tiles_y = (d->shape[1] + kTY - 1) / kTY;
+    // search deltas inside the shared-memory boxes (raw: box or global)
+    std::vector<int2> dl(a.S);
+    const int pplane = a.pbx * a.pby, rplane = a.rbx * a.rby;
+    for (int s = 0; s < a.S; s++) {
+        const Offset3& o = g.search[s];
+        dl[s].x = o.z * pplane + o.y * a.pbx + o.x;
+        dl[s].y = d->tcfg.raw_smem ? o.z * rplane + o.y * a.rbx + o.x
+                                   : (int)(o.z * d->pitch_z + o.y * d->pitch_y + o.x);
+    }
+    CUDA_TRY(dalloc(&d->d_search_delta, a.S));
+    CUDA_TRY(cudaMemcpy(d->d_search_delta, dl.data(), a.S * sizeof(int2), cudaMemcpyHostToDevice));
+    a.search_delta = d->d_search_delta;
+    a.raw_pad = d->d_raw_pad;
+    a.out = d->d_next;
+    a.mult = d->d_mult;
+    a.err = d->d_err;
+    int rc = encode_map_3d(&d->tm_prev, d->d_prev_pad, d->nxp, d->nyp, d->nzp, d->pitch_y, d->pitch_z,
+                           a.pbx, a.pby, a.pbz);
+    if (rc) return rc;
+    if (d->tcfg.raw_smem) {
+        rc = encode_map_3d(&d->tm_raw, d->d_raw_pad, d->nxp, d->nyp, d->nzp, d->pitch_y, d->pitch_z,
+                           a.rbx, a.rby, a.rbz);
+        if (rc) return rc;
+    } else {
+        d->tm_raw = d->tm_prev;  // unused by the raw-global form
+    }
+    return INLM_OK;
+}
+
+extern "C" int inlm_denoiser_create(const int shape[3], const inlm_params* p, inlm_denoiser** out) {
+    if (!shape || !p || !out) return fail(INLM_ERR_ARG, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return fail(INLM_ERR_NODEVICE, "no CUDA device");
+    if (p->device_id < 0 || p->device_id >= ndev) return fail(INLM_ERR_ARG, "bad device id");
+    for (int i = 0; i < 3; i++) {
+        if (shape[i] < 1) return fail(INLM_ERR_ARG, "shape must be positive");
+        if (p->search_radius[i] < 0 || p->patch_radius[i] < 0)
+            return fail(INLM_ERR_ARG, "radii must be >= 0");
+    }
+    if (p->nslices < 1) return fail(INLM_ERR_ARG, "nslices must be >= 1");
+    if (p->precision != INLM_PRECISION_F32)
+        return fail(INLM_ERR_UNSUPPORTED, "precision %d not available in this build", p->precision);
+
+    inlm_denoiser* d = new inlm_denoiser();
+    d->p = *p;
+    d->device = p->device_id;
+    for (int i = 0; i < 3; i++) d->shape[i] = shape[i];
+    cudaSetDevice(d->device);
+    int pad0[3] = {p->search_radius[0] + p->patch_radius[0], p->search_radius[1] + p->patch_radius[1],
+                   std::min(p->nslices / 2, p->search_radius[2]) + p->patch_radius[2]};
+    for (int i = 0; i < 3; i++)
+        if (shape[i] == 1 && pad0[i] > 0) {
+            delete d;
+            return fail(INLM_ERR_ARG,
+                        "axis %d has length 1 but needs padding %d: set its search and patch "
+                        "radius to 0 (the reference does so for single slices, main.cpp:268-272)",
+                        i, pad0[i]);
+        }
+    d->geo = make_geometry(p->search_radius, p->patch_radius, p->nslices, p->z_anisotropy,
+                           p->weight_table, shape[2] + 2 * pad0[2]);
+    const Geometry& g = d->geo;
+    d->nxp = shape[0] + 2 * g.pad[0];
+    d->nyp = shape[1] + 2 * g.pad[1];
+    d->nzp = shape[2] + 2 * g.pad[2];
+    d->pitch_y = (d->nxp + 31) / 32 * 32;
+    d->pitch_z = d->pitch_y * d->nyp;
+    // Tiles that stick out of the volume (z up to TZ-1 planes, y up to TY-1
+    // rows, x up to 31 columns past the end) read raw from global memory at
+    // positions they never store; kSlackPlanes zeroed planes after the padded
+    // volume keep every such read inside the allocation.
+    const long long kSlackPlanes = 9;
+    const long long npad = d->pitch_z * (d->nzp + kSlackPlanes);
+    const long long nvox = (long long)shape[0] * shape[1] * shape[2];
+    int rc = INLM_OK;
+    auto bail = [&](int code) {
+        denoiser_free(d);
+        delete d;
+        return code;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(fail(INLM_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
+    d->own_stream = true;
+    if (dalloc(&d->d_raw_pad, npad) != cudaSuccess || dalloc(&d->d_prev_pad, npad) != cudaSuccess ||
+        dalloc(&d->d_next, nvox) != cudaSuccess || dalloc(&d->d_sigma, shape[2]) != cudaSuccess ||
+        dalloc(&d->d_sigma0, shape[2]) != cudaSuccess || dalloc(&d->d_mult, shape[2]) != cudaSuccess ||
+        dalloc(&d->d_err, 1) != cudaSuccess)
+        return bail(fail(INLM_ERR_NOMEM, "device allocation of %.2f GB failed",
+                         (2.0 * npad + nvox) * 4 / 1e9));
+    // pitch padding columns stay zero
+    if (cudaMemset(d->d_raw_pad, 0, npad * 4) != cudaSuccess ||
+        cudaMemset(d->d_prev_pad, 0, npad * 4) != cudaSuccess ||
+        cudaMemset(d->d_err, 0, 4) != cudaSuccess)
+        return bail(fail(INLM_ERR_CUDA, "memset failed"));
+    // generic-kernel tables (padded-linear offsets)
+    {
+        std::vector<long long> so(g.search.size()), po(g.taps.size());
+        for (size_t s = 0; s < g.search.size(); s++)
+            so[s] = g.search[s].z * d->pitch_z + g.search[s].y * d->pitch_y + g.search[s].x;
+        for (size_t q = 0; q < g.taps.size(); q++)
+            po[q] = g.taps[q].z * d->pitch_z + g.taps[q].y * d->pitch_y + g.taps[q].x;
+        if (dalloc(&d->d_search_off, so.size()) != cudaSuccess ||
+            dalloc(&d->d_patch_off, po.size()) != cudaSuccess ||
+            dalloc(&d->d_weights, g.weights.size()) != cudaSuccess)
+            return bail(fail(INLM_ERR_NOMEM, "table allocation"));
+        cudaMemcpy(d->d_search_off, so.data(), so.size() * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(d->d_patch_off, po.data(), po.size() * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(d->d_weights, g.weights.data(), g.weights.size() * 4, cudaMemcpyHostToDevice);
+        GenericArgs& ga = d->gargs;
+        ga.nx = shape[0];
+        ga.ny = shape[1];
+        ga.nz = shape[2];
+        ga.px = g.pad[0];
+        ga.py = g.pad[1];
+        ga.pz = g.pad[2];
+        ga.gpitch_y = d->pitch_y;
+        ga.gpitch_z = d->pitch_z;
+        ga.S = (int)g.search.size();
+        ga.P = (int)g.taps.size();
+        ga.search_off = d->d_search_off;
+        ga.patch_off = d->d_patch_off;
+        ga.weights = d->d_weights;
+        ga.raw_pad = d->d_raw_pad;
+        ga.prev_pad = d->d_prev_pad;
+        ga.out = d->d_next;
+        ga.mult = d->d_mult;
+    }
+    rc = choose_tile_config(d);
+    if (rc != INLM_OK) return bail(rc);
+    if (shape[0] > p->noise_patchsize && shape[1] > p->noise_patchsize && p->n_samples > 0) {
+        rc = inlm_noise_create(shape, p->n_samples, p->noise_patchsize, p->noise_seed, d->device,
+                               &d->noise);
+        if (rc != INLM_OK) return bail(rc);
+        cudaStreamDestroy(d->noise->stream);
+        d->noise->stream = d->stream;  // one stream per job
+        d->noise->own_stream = false;
+    }
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return bail(fail(INLM_ERR_CUDA, "configure: %s", cudaGetErrorString(e)));
+    *out = d;
+    return INLM_OK;
+}
+
+extern "C" int inlm_denoiser_destroy(inlm_denoiser* d) {
+    denoiser_free(d);
+    delete d;
+    return INLM_OK;
+}
+
+extern "C" int inlm_set_stream(inlm_denoiser* d, void* stream) {
+    if (!d) return fail(INLM_ERR_ARG, "null handle");
+    CUDA_TRY(cudaSetDevice(d->device));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    if (stream) {
+        if (d->own_stream) cudaStreamDestroy(d->stream);
+        d->stream = (cudaStream_t)stream;
+        d->own_stream = false;
+    } else if (!d->own_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+        d->own_stream = true;
+    }
+    if (d->noise) d->noise->stream = d->stream;
+    return INLM_OK;
+}
+
+static int upload_sigma_device(inlm_denoiser* d) {
+    CUDA_TRY(launch_sigma_to_mult(d->d_sigma, d->p.beta, d->d_mult, d->shape[2], d->stream));
+    d->launches++;
+    d->sigma_set = true;
+    return INLM_OK;
+}
+
+extern "C" int inlm_set_sigma(inlm_denoiser* d, const float* sigma_host) {
+    if (!d || !sigma_host) return fail(INLM_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(d->device));
+    CUDA_TRY(cudaMemcpyAsync(d->d_sigma, sigma_host, d->shape[2] * 4, cudaMemcpyHostToDevice,
+                             d->stream));
+    int rc = upload_sigma_device(d);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    return INLM_OK;
+}
+
+static int launch_filter(inlm_denoiser* d) {
+    TimedLaunch t;
+    if (!d->event_pool.empty()) {
+        t = d->event_pool.back();
+        d->event_pool.pop_back();
+    } else {
+        CUDA_TRY(cudaEventCreate(&t.a));
+        CUDA_TRY(cudaEventCreate(&t.b));
+    }
+    CUDA_TRY(cudaEventRecord(t.a, d->stream));
+    if (d->use_tile) {
+        int tiles_z = (d->shape[2] + d->tcfg.tz - 1) / d->tcfg.tz;
+        CUDA_TRY(launch_tile_kernel(d->tcfg, &d->tm_prev, &d->tm_raw, d->targs, tiles_z, d->stream));
+    } else {
+        CUDA_TRY(launch_generic_kernel(d->gargs, d->stream));
+    }
+    CUDA_TRY(cudaEventRecord(t.b, d->stream));
+    d->pending.push_back(t);
+    d->launches++;
+    return INLM_OK;
+}
+
+// Pads the unpadded volume `src` (device) into the padded buffer `dst`.
+static int pad_into(inlm_denoiser* d, const float* src, float* dst) {
+    const Geometry& g = d->geo;
+    CUDA_TRY(launch_pad_reflective(src, d->shape[0], d->shape[1], d->shape[2], dst, g.pad[0],
+                                   g.pad[1], g.pad[2], d->pitch_y, d->pitch_z, d->stream));
+    d->launches++;
+    return INLM_OK;
+}
+
+static int check_device_error(inlm_denoiser* d) {
+    int h = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h, d->d_err, 4, cudaMemcpyDeviceToHost, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    if (h != 0) {
+        cudaMemsetAsync(d->d_err, 0, 4, d->stream);
+        return fail(INLM_ERR_TIMEOUT, "device wait gave up (code %d)", h);
+    }
+    return INLM_OK;
+}
+
+// Enqueues one iteration; raw_dev is the unpadded raw volume on the device
+// (iteration 1 only). No host synchronisation.
+static int enqueue_iteration(inlm_denoiser* d, int iter, const float* raw_dev) {
+    if (iter < 1) return fail(INLM_ERR_ARG, "iteration must be >= 1");
+    if (!d->sigma_set) return fail(INLM_ERR_STATE, "set_sigma before running an iteration");
+    int rc;
+    if (iter == 1) {
+        if (!raw_dev) return fail(INLM_ERR_ARG, "iteration 1 needs the raw volume");
+        rc = pad_into(d, raw_dev, d->d_raw_pad);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(d->d_prev_pad, d->d_raw_pad, d->pitch_z * d->nzp * 4,
+                                 cudaMemcpyDeviceToDevice, d->stream));
+    } else {
+        if (d->last_iter < 1) return fail(INLM_ERR_STATE, "iteration %d before iteration 1", iter);
+        rc = pad_into(d, d->d_next, d->d_prev_pad);
+        if (rc) return rc;
+    }
+    rc = launch_filter(d);
+    if (rc) return rc;
+    d->last_iter = iter;
+    return INLM_OK;
+}
+
+extern "C" int inlm_run_iteration(inlm_denoiser* d, int iter, const float* raw_host) {
+    if (!d) return fail(INLM_ERR_ARG, "null handle");
+    CUDA_TRY(cudaSetDevice(d->device));
+    const long long nvox = (long long)d->shape[0] * d->shape[1] * d->shape[2];
+    if (iter == 1) {
+        if (!raw_host) return fail(INLM_ERR_ARG, "iteration 1 needs the raw volume");
+        // stage through the result buffer, as prepare_iteration1 does
+        CUDA_TRY(cudaMemcpyAsync(d->d_next, raw_host, nvox * 4, cudaMemcpyHostToDevice, d->stream));
+        int rc = enqueue_iteration(d, 1, d->d_next);
+        if (rc) return rc;
+    } else {
+        int rc = enqueue_iteration(d, iter, nullptr);
+        if (rc) return rc;
+    }
+    return check_device_error(d);
+}
+
+extern "C" int inlm_run_iteration_device(inlm_denoiser* d, int iter, const float* raw_dev) {
+    if (!d) return fail(INLM_ERR_ARG, "null handle");
+    CUDA_TRY(cudaSetDevice(d->device));
+    int rc = enqueue_iteration(d, iter, raw_dev);
+    if (rc) return rc;
+    return check_device_error(d);
+}
+
+extern "C" int inlm_get_result(inlm_denoiser* d, float* out_host) {
+    if (!d || !out_host) return fail(INLM_ERR_ARG, "null argument");
+    if (d->last_iter < 1) return fail(INLM_ERR_STATE, "no iteration has run");
+    CUDA_TRY(cudaSetDevice(d->device));
+    const long long nvox = (long long)d->shape[0] * d->shape[1] * d->shape[2];
+    CUDA_TRY(cudaMemcpyAsync(out_host, d->d_next, nvox * 4, cudaMemcpyDeviceToHost, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    return check_device_error(d);
+}
+
+extern "C" int inlm_get_result_device(inlm_denoiser* d, float* out_dev) {
+    if (!d || !out_dev) return fail(INLM_ERR_ARG, "null argument");
+    if (d->last_iter < 1) return fail(INLM_ERR_STATE, "no iteration has run");
+    CUDA_TRY(cudaSetDevice(d->device));
+    const long long nvox = (long long)d->shape[0] * d->shape[1] * d->shape[2];
+    CUDA_TRY(cudaMemcpyAsync(out_dev, d->d_next, nvox * 4, cudaMemcpyDeviceToDevice, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    return check_device_error(d);
+}
+
+// Noise estimate of a device volume into d->d_sigma (or sigma0 buffer).
+static int estimate_into(inlm_denoiser* d, const float* vol_dev, float* d_dst, std::vector<float>* host_copy) {
+    if (!d->noise) return fail(INLM_ERR_ARG, "volume too small for the noise patch");
+    std::vector<float> hs;
+    bool on_host = false;
+    int rc = noise_estimate_device(d->noise, &d->p, vol_dev, d->shape[0],
+                                   (long long)d->shape[0] * d->shape[1], &hs, &on_host);
+    if (rc) return rc;
+    if (!on_host) d->launches += 3;  // patch std, EM, finalize
+    const int nz = d->shape[2];
+    if (on_host) {
+        CUDA_TRY(cudaMemcpyAsync(d_dst, hs.data(), nz * 4, cudaMemcpyHostToDevice, d->stream));
+        CUDA_TRY(cudaStreamSynchronize(d->stream));
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(d_dst, d->noise->d_sigma, nz * 4, cudaMemcpyDeviceToDevice, d->stream));
+    }
+    if (host_copy) {
+        host_copy->resize(nz);
+        CUDA_TRY(cudaMemcpyAsync(host_copy->data(), d_dst, nz * 4, cudaMemcpyDeviceToHost, d->stream));
+    }
+    return INLM_OK;
+}
+
+extern "C" int inlm_denoise(inlm_denoiser* d, const float* raw, float* out, int on_device,
+                            float* sigma0_out, float* sigma1_out) {
+    if (!d || !raw || !out) return fail(INLM_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(d->device));
+    const long long nvox = (long long)d->shape[0] * d->shape[1] * d->shape[2];
+    const int nz = d->shape[2];
+    const float* raw_dev = raw;
+    if (!on_device) {
+        CUDA_TRY(cudaMemcpyAsync(d->d_next, raw, nvox * 4, cudaMemcpyHostToDevice, d->stream));
+        raw_dev = d->d_next;
+    }
+    // sigma0 on the raw data (main.cpp:327-351)
+    std::vector<float> s0h, s1h;
+    int rc = estimate_into(d, raw_dev, d->d_sigma0, sigma0_out ? &s0h : nullptr);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(d->d_sigma, d->d_sigma0, nz * 4, cudaMemcpyDeviceToDevice, d->stream));
+    rc = upload_sigma_device(d);
+    if (rc) return rc;
+    rc = enqueue_iteration(d, 1, raw_dev);
+    if (rc) return rc;
+    const int maxit = d->p.maxiterations;
+    if (maxit > 1) {
+        // sigma1 on the first result, blended with sigma0 (main.cpp:422-448)
+        rc = estimate_into(d, d->d_next, d->d_sigma, sigma1_out ? &s1h : nullptr);
+        if (rc) return rc;
+        CUDA_TRY(launch_sigma_blend(d->d_sigma0, d->d_sigma, d->p.alpha, nz, d->stream));
+        d->launches++;
+        rc = upload_sigma_device(d);
+        if (rc) return rc;
+    }
+    for (int it = 2; it <= maxit; it++) {
+        rc = enqueue_iteration(d, it, nullptr);
+        if (rc) return rc;
+        // --continuous (main.cpp:517-544)
+        if (d->p.continuous_estimate && maxit > it + 1) {
+            rc = estimate_into(d, d->d_next, d->d_sigma, nullptr);
+            if (rc) return rc;
+            CUDA_TRY(launch_sigma_blend(d->d_sigma0, d->d_sigma, d->p.alpha, nz, d->stream));
+            d->launches++;
+            rc = upload_sigma_device(d);
+            if (rc) return rc;
+        }
+    }
+    if (on_device) {
+        CUDA_TRY(cudaMemcpyAsync(out, d->d_next, nvox * 4, cudaMemcpyDeviceToDevice, d->stream));
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(out, d->d_next, nvox * 4, cudaMemcpyDeviceToHost, d->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    if (sigma0_out) std::memcpy(sigma0_out, s0h.data(), nz * 4);
+    if (sigma1_out && maxit > 1) {
+        // the pre-blend estimate is what the reference reports (main.cpp:438)
+        std::memcpy(sigma1_out, s1h.data(), nz * 4);
+    }
+    return check_device_error(d);
+}
+
+extern "C" int inlm_filter_kernel_ms(inlm_denoiser* d, double* avg_ms, int* n_launches) {
+    if (!d) return fail(INLM_ERR_ARG, "null handle");
+    CUDA_TRY(cudaSetDevice(d->device));
+    double tot = 0.0;
+    int n = 0;
+    for (auto& t : d->pending) {
+        CUDA_TRY(cudaEventSynchronize(t.b));
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, t.a, t.b));
+        tot += ms;
+        n++;
+        d->event_pool.push_back(t);
+    }
+    d->pending.clear();
+    if (avg_ms) *avg_ms = n ? tot / n : 0.0;
+    if (n_launches) *n_launches = n;
+    return INLM_OK;
+}
+
+extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
+    if (!d || !buf) return fail(INLM_ERR_ARG, "null argument");
+    const Geometry& g = d->geo;
+    if (d->use_tile)
+        snprintf(buf, len,
+                 "nlm_tile_f32<%d,%d,%d> tz=%d raw_%s smem=%zu S=%zu P=%zu weights=%s pad=%d,%d,%d",
+                 d->tcfg.rx, d->tcfg.ry, d->tcfg.rz, d->tcfg.tz, d->tcfg.raw_smem ? "smem" : "global",
+                 d->tcfg.smem_bytes, g.search.size(), g.taps.size(),
+                 g.specialised && d->p.weight_table == INLM_WEIGHTS_CPU ? "cpu-table" : "distweight",
+                 g.pad[0], g.pad[1], g.pad[2]);
+    else
+        snprintf(buf, len, "nlm_generic_f32 S=%zu P=%zu pad=%d,%d,%d", g.search.size(), g.taps.size(),
+                 g.pad[0], g.pad[1], g.pad[2]);
+    return INLM_OK;
+}
+
+// ---------------- host-only helpers ----------------
+
+extern "C" int inlm_geometry(const inlm_params* p, int nz, int* search_xyz, int* n_search,
+                             int* patch_xyz, float* weights, int* n_patch, int pad3[3]) {
+    if (!p) return fail(INLM_ERR_ARG, "null params");
+    int pad2 = std::min(p->nslices / 2, p->search_radius[2]) + p->patch_radius[2];
+    Geometry g = make_geometry(p->search_radius, p->patch_radius, p->nslices, p->z_anisotropy,
+                               p->weight_table, nz + 2 * pad2);
+    if (n_search) *n_search = (int)g.search.size();
+    if (n_patch) *n_patch = (int)g.taps.size();
+    if (pad3)
+        for (int i = 0; i < 3; i++) pad3[i] = g.pad[i];
+    if (search_xyz)
+        for (size_t s = 0; s < g.search.size(); s++) {
+            search_xyz[3 * s] = g.search[s].x;
+            search_xyz[3 * s + 1] = g.search[s].y;
+            search_xyz[3 * s + 2] = g.search[s].z;
+        }
+    if (patch_xyz)
+        for (size_t q = 0; q < g.taps.size(); q++) {
+            patch_xyz[3 * q] = g.taps[q].x;
+            patch_xyz[3 * q + 1] = g.taps[q].y;
+            patch_xyz[3 * q + 2] = g.taps[q].z;
+        }
+    if (weights)
+        for (size_t q = 0; q < g.weights.size(); q++) weights[q] = g.weights[q];
+    return INLM_OK;
+}
+
+extern "C" int inlm_noise_draw_samples(const int shape[3], uint64_t n_samples, int patchsize,
+                                       int circular_mask_diameter, unsigned int seed, int64_t* out) {
+    if (!shape || !out) return fail(INLM_ERR_ARG, "null argument");
+    if (shape[0] <= patchsize || shape[1] <= patchsize || shape[2] < 1)
+        return fail(INLM_ERR_ARG, "shape too small for the noise patch");
+    std::vector<long long> s =
+        draw_noise_samples(shape, n_samples, patchsize, circular_mask_diameter, seed);
+    for (size_t i = 0; i < s.size(); i++) out[i] = s[i];
+    return INLM_OK;
+}
+
+extern "C" int inlm_kernel_launches(inlm_denoiser* d, uint64_t* count) {
+    if (!d || !count) return fail(INLM_ERR_ARG, "null argument");
+    *count = d->launches;
+    return INLM_OK;
+}
+
+extern "C" int inlm_probe_fp32_peak(int device_id, double* tflops) {
+    if (!tflops) return fail(INLM_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(device_id));
+    double best = 0.0;
+    int rc = probe_fp32_fma(device_id, &best);
+    if (rc) return fail(INLM_ERR_CUDA, "fp32 probe failed");
+    *tflops = best;
+    return INLM_OK;
+}

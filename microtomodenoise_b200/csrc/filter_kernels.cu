@@ -1,0 +1,441 @@
+// Plain FP32 iterNLM filter for sm_100a, bit-identical to the reference CPU
+// filter (Denoiser/iternlm_cpu_kernels.cpp:7-1108, iternlm_cpu.cpp:758-843).
+//
+// Per voxel x and search offset s (reference order, iternlm_prepare.cpp:102):
+//   dist  = sum_p w_p * (prev[x+s+p] - prev[x+p])^2      (taps in reference order)
+//   w     = dist*m > -3.56648 ? Pade33(dist*m) : 0          (m = -1/(sigma_z^2 beta))
+//   acc  += w*raw[x+s];  wsum += w;  wmax = max(wmax, w)
+// out = wmax > 0 ? (acc + wmax*raw[x]) / (wsum + wmax) : raw[x].
+// Every product and sum is rounded separately (__fmul_rn/__fadd_rn) in the
+// reference's order, so the result equals the reference's g++ -O3 (SSE, no
+// FMA) build bit for bit.
+//
+// Tiled kernel: a CTA stages the padded previous iterate over its tile plus
+// search+patch halo (and, when it fits, raw over the tile plus search halo)
+// into shared memory with one 3D TMA load each. For every search offset it
+// writes the squared-difference volume D_s = (prev(.+s) - prev(.))^2 over the
+// tile plus patch halo to shared memory, then each thread applies the patch
+// stencil to D_s for 8 consecutive x voxels from a 16-float register window
+// per patch row (float4 loads, conflict-free row pitch), so each D value is
+// computed once and read by every voxel whose patch covers it.
+#include <cstdio>
+
+#include "common.cuh"
+#include "filter_kernels.cuh"
+#include "geometry.hpp"
+
+namespace inlm {
+
+// D-plane row pitch: a multiple of 4 floats with an odd number of 16-byte
+// chunks, so the 8 y-lanes x 4 x-lanes of a warp hit distinct bank quads.
+constexpr int dpitch(int w) {
+    int p = (w + 3) / 4 * 4;
+    return ((p / 4) % 2 == 0) ? p + 4 : p;
+}
+constexpr int round_up32(int v) { return (v + 31) / 32 * 32; }
+
+template <int RX, int RY, int RZ, int TZ>
+struct TileGeom {
+    static constexpr PatchRows rows = make_patch_rows(RX, RY, RZ);
+    static constexpr int DW = kTX + 2 * RX;
+    static constexpr int DH = kTY + 2 * RY;
+    static constexpr int DD = TZ + 2 * RZ;
+    static constexpr int DP = dpitch(DW);
+    static constexpr int DPLANE = DP * DH;
+    static constexpr int ND = DW * DH * DD;
+    static constexpr int NT = 32 * TZ;
+};
+
+// Tap counts of the reference geometry (float32 ellipsoid test).
+static_assert(make_patch_rows(1, 1, 1).ntaps == 7, "p111");
+static_assert(make_patch_rows(1, 1, 2).ntaps == 9, "p112");
+static_assert(make_patch_rows(1, 1, 3).ntaps == 11, "p113");
+static_assert(make_patch_rows(2, 2, 1).ntaps == 15, "p221");
+static_assert(make_patch_rows(2, 2, 2).ntaps == 33, "p222");
+static_assert(make_patch_rows(3, 3, 1).ntaps == 31, "p331");
+static_assert(make_patch_rows(3, 3, 2).ntaps == 73, "p332");
+static_assert(make_patch_rows(3, 3, 3).ntaps == 115, "p333");
+
+// Index of the first tap (xp = -e) of row RI in the reference tap list.
+template <int RX, int RY, int RZ, int RI>
+struct RowFirst {
+    static constexpr PatchRows rows = make_patch_rows(RX, RY, RZ);
+    static constexpr int value =
+        RowFirst<RX, RY, RZ, RI - 1>::value + 2 * rows.e[RI - 1] + 1 -
+        ((rows.zp[RI - 1] == 0 && rows.yp[RI - 1] == 0) ? 1 : 0);
+};
+template <int RX, int RY, int RZ>
+struct RowFirst<RX, RY, RZ, 0> {
+    static constexpr int value = 1;
+};
+
+// Loads the 16-float window covering columns [x0, x0+16) of one D row.
+template <int LO, int HI>
+__device__ __forceinline__ void load_window(const float* __restrict__ rowp, float (&win)[16]) {
+#pragma unroll
+    for (int c = LO; c <= HI; c++) {
+        float4 v = reinterpret_cast<const float4*>(rowp)[c];
+        win[4 * c + 0] = v.x;
+        win[4 * c + 1] = v.y;
+        win[4 * c + 2] = v.z;
+        win[4 * c + 3] = v.w;
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ, int RI>
+__device__ __forceinline__ void accumulate_rows(const float* __restrict__ D, int k, int j, int x0,
+                                                float (&dist)[kVoxPerThread],
+                                                const TileArgs& a) {
+    using G = TileGeom<RX, RY, RZ, TZ>;
+    if constexpr (RI < G::rows.n) {
+        constexpr int zp = G::rows.zp[RI];
+        constexpr int yp = G::rows.yp[RI];
+        constexpr int e = G::rows.e[RI];
+        constexpr int first = RowFirst<RX, RY, RZ, RI>::value;
+        constexpr int lo = (RX - e) / 4;
+        constexpr int hi = (RX + kVoxPerThread - 1 + e) / 4;
+        const float* rowp = D + (k + zp + RZ) * G::DPLANE + (j + yp + RY) * G::DP + x0;
+        float win[16];
+        load_window<lo, hi>(rowp, win);
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) {
+#pragma unroll
+            for (int xp = -e; xp <= e; xp++) {
+                if (zp == 0 && yp == 0 && xp == 0) continue;
+                const int t = first + (xp + e) - ((zp == 0 && yp == 0 && xp > 0) ? 1 : 0);
+                dist[r] = __fadd_rn(dist[r], __fmul_rn(win[RX + r + xp], a.w[t]));
+            }
+        }
+        accumulate_rows<RX, RY, RZ, TZ, RI + 1>(D, k, j, x0, dist, a);
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
+__global__ void __launch_bounds__(32 * TZ, 1)
+    nlm_tile_f32_kernel(const __grid_constant__ CUtensorMap tm_prev,
+                        const __grid_constant__ CUtensorMap tm_raw,
+                        const __grid_constant__ TileArgs a) {
+    using G = TileGeom<RX, RY, RZ, TZ>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+    float* prevb = reinterpret_cast<float*>(smem + 128);
+    const int pplane = a.pbx * a.pby;
+    const int PB = pplane * a.pbz;
+    float* rawb = prevb + round_up32(PB);
+    const int RB = RAW_SMEM ? a.rbx * a.rby * a.rbz : 0;
+    float* D = rawb + round_up32(RB);
+    int* tab = reinterpret_cast<int*>(D + round_up32(G::DPLANE * G::DD));
+
+    const int tid = threadIdx.x;
+    const int X0 = blockIdx.x * kTX;
+    const int Y0 = blockIdx.y * kTY;
+    const int Z0 = blockIdx.z * TZ;
+
+    if (tid == 0) {
+        prefetch_tmap(&tm_prev);
+        if (RAW_SMEM) prefetch_tmap(&tm_raw);
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(PB + RB) * 4u);
+        // prev box starts at the tile origin in padded coordinates (x aligned to 32)
+        tma_load_3d(prevb, &tm_prev, X0, Y0, Z0, bar);
+        if (RAW_SMEM) tma_load_3d(rawb, &tm_raw, X0, Y0 + RY, Z0 + RZ, bar);
+    }
+
+    // Shared-memory index table of the D volume: prev-box index of the
+    // origin (low 16 bits) and D index (high 16 bits).
+    for (int f = tid; f < G::ND; f += G::NT) {
+        int c = f % G::DW;
+        int rest = f / G::DW;
+        int r = rest % G::DH;
+        int p = rest / G::DH;
+        int pi = (p - RZ + a.pz) * pplane + (r - RY + a.py) * a.pbx + (c - RX + a.px);
+        int di = p * G::DPLANE + r * G::DP + c;
+        tab[f] = pi | (di << 16);
+    }
+
+    if (!mbar_wait_bounded(bar, 0)) {
+        set_error(a.err, DEV_TMA_TIMEOUT);
+        return;
+    }
+    __syncthreads();
+
+    const int warp = tid >> 5, lane = tid & 31;
+    const int k = warp;
+    const int j = lane >> 2;
+    const int x0 = (lane & 3) * kVoxPerThread;
+    const int zk = min(Z0 + k, a.nz - 1);
+    const float m = a.mult[zk];
+
+    int rbase;
+    long long gbase;
+    if (RAW_SMEM) {
+        rbase = (a.szc + k) * (a.rbx * a.rby) + (a.syr + j) * a.rbx + (RX + a.sxr + x0);
+        gbase = 0;
+    } else {
+        rbase = 0;
+        gbase = (long long)(Z0 + k + a.pz) * a.gpitch_z + (long long)(Y0 + j + a.py) * a.gpitch_y +
+                (X0 + x0 + a.px);
+    }
+
+    float acc[kVoxPerThread], wsum[kVoxPerThread], wmax[kVoxPerThread];
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) acc[r] = wsum[r] = wmax[r] = 0.0f;
+
+    for (int s = 0; s < a.S; s++) {
+        const int2 dl = __ldg(&a.search_delta[s]);
+        // phase A: D_s over tile + patch halo
+        for (int f = tid; f < G::ND; f += G::NT) {
+            int t = tab[f];
+            int pi = t & 0xffff;
+            float v = __fsub_rn(prevb[pi + dl.x], prevb[pi]);
+            D[t >> 16] = __fmul_rn(v, v);
+        }
+        __syncthreads();
+        // phase B: patch stencil on D_s, weight, accumulate
+        float dist[kVoxPerThread];
+        {
+            float win[16];
+            const float* rowp = D + (k + RZ) * G::DPLANE + (j + RY) * G::DP + x0;
+            load_window<RX / 4, (RX + kVoxPerThread - 1) / 4>(rowp, win);
+#pragma unroll
+            for (int r = 0; r < kVoxPerThread; r++) dist[r] = __fmul_rn(win[RX + r], a.w[0]);
+        }
+        accumulate_rows<RX, RY, RZ, TZ, 0>(D, k, j, x0, dist, a);
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) {
+            float rs = RAW_SMEM ? rawb[rbase + dl.y + r] : __ldg(&a.raw_pad[gbase + dl.y + r]);
+            float wt = pade_weight_exact(__fmul_rn(dist[r], m));
+            acc[r] = __fadd_rn(acc[r], __fmul_rn(wt, rs));
+            wsum[r] = __fadd_rn(wsum[r], wt);
+            wmax[r] = fmaxf(wmax[r], wt);
+        }
+        __syncthreads();
+    }
+
+    const int z = Z0 + k, y = Y0 + j;
+    if (z < a.nz && y < a.ny) {
+        float* orow = a.out + ((long long)z * a.ny + y) * a.nx;
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) {
+            int x = X0 + x0 + r;
+            if (x < a.nx) {
+                float raw0 = RAW_SMEM ? rawb[rbase + r] : __ldg(&a.raw_pad[gbase + r]);
+                float res;
+                if (wmax[r] > 0.0f) {
+                    float ac = __fadd_rn(acc[r], __fmul_rn(wmax[r], raw0));
+                    float ws = __fadd_rn(wsum[r], wmax[r]);
+                    res = __fdiv_rn(ac, ws);
+                } else {
+                    res = raw0;
+                }
+                orow[x] = res;
+            }
+        }
+    }
+}
+
+// ---- generic exact kernel: any patch shape, one thread per voxel ----
+__global__ void __launch_bounds__(256) nlm_generic_f32_kernel(const __grid_constant__ GenericArgs a) {
+    long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long nvox = (long long)a.nx * a.ny * a.nz;
+    if (idx >= nvox) return;
+    int x = (int)(idx % a.nx);
+    long long rest = idx / a.nx;
+    int y = (int)(rest % a.ny);
+    int z = (int)(rest / a.ny);
+    long long i0 = (long long)(z + a.pz) * a.gpitch_z + (long long)(y + a.py) * a.gpitch_y + (x + a.px);
+    const float m = a.mult[z];
+    const float raw0 = a.raw_pad[i0];
+    float acc = 0.0f, wsum = 0.0f, wmax = 0.0f;
+    for (int s = 0; s < a.S; s++) {
+        long long i1 = i0 + a.search_off[s];
+        float dist = 0.0f;
+        for (int q = 0; q < a.P; q++) {
+            long long po = a.patch_off[q];
+            float t = __fsub_rn(a.prev_pad[i1 + po], a.prev_pad[i0 + po]);
+            dist = __fadd_rn(dist, __fmul_rn(__fmul_rn(t, t), a.weights[q]));
+        }
+        float wt = pade_weight_exact(__fmul_rn(dist, m));
+        acc = __fadd_rn(acc, __fmul_rn(wt, a.raw_pad[i1]));
+        wsum = __fadd_rn(wsum, wt);
+        wmax = fmaxf(wmax, wt);
+    }
+    float res = raw0;
+    if (wmax > 0.0f) res = __fdiv_rn(__fadd_rn(acc, __fmul_rn(wmax, raw0)), __fadd_rn(wsum, wmax));
+    a.out[idx] = res;
+}
+
+// ---- reflective padding (iternlm_prepare.cpp:6-48 / iternlm_gpu.cu:27) ----
+__global__ void pad_reflective_kernel(const float* __restrict__ in, int nx, int ny, int nz,
+                                      float* __restrict__ out, int px, int py, int pz,
+                                      long long pitch_y, long long pitch_z) {
+    const int nxp = nx + 2 * px, nyp = ny + 2 * py, nzp = nz + 2 * pz;
+    const long long total = (long long)nxp * nyp * nzp;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        int x1 = (int)(i % nxp);
+        long long r = i / nxp;
+        int y1 = (int)(r % nyp);
+        int z1 = (int)(r / nyp);
+        int x0 = x1 - px, y0 = y1 - py, z0 = z1 - pz;
+        // mirror without edge repeat, repeated while out of range; the host
+        // rejects axes of length 1 that would need padding, so this ends
+        for (int guard = 0; guard < 64 && (z0 < 0 || z0 >= nz || y0 < 0 || y0 >= ny || x0 < 0 ||
+                                           x0 >= nx);
+             guard++) {
+            if (z0 < 0) z0 = -z0;
+            if (y0 < 0) y0 = -y0;
+            if (x0 < 0) x0 = -x0;
+            if (z0 >= nz) z0 = 2 * nz - z0 - 2;
+            if (y0 >= ny) y0 = 2 * ny - y0 - 2;
+            if (x0 >= nx) x0 = 2 * nx - x0 - 2;
+        }
+        x0 = min(max(x0, 0), nx - 1);
+        y0 = min(max(y0, 0), ny - 1);
+        z0 = min(max(z0, 0), nz - 1);
+        out[z1 * pitch_z + y1 * pitch_y + x1] = in[((long long)z0 * ny + y0) * nx + x0];
+    }
+}
+
+__global__ void sigma_to_mult_kernel(const float* __restrict__ sigma, float beta,
+                                     float* __restrict__ mult, int nz) {
+    int z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z < nz) {
+        float s = sigma[z];
+        // -1.f/(sigma*sigma*beta), iternlm_cpu.cpp:95
+        mult[z] = __fdiv_rn(-1.f, __fmul_rn(__fmul_rn(s, s), beta));
+    }
+}
+
+__global__ void sigma_blend_kernel(const float* __restrict__ sigma0, float* __restrict__ sigma1,
+                                   float alpha, int nz) {
+    int z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z < nz) {
+        // alpha*sigma0 + (1-alpha)*sigma1, main.cpp:442-443
+        sigma1[z] = __fadd_rn(__fmul_rn(alpha, sigma0[z]),
+                              __fmul_rn(__fsub_rn(1.f, alpha), sigma1[z]));
+    }
+}
+
+// ---- host-side dispatch ----
+
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
+static size_t smem_bytes_for(const TileArgs& a) {
+    using G = TileGeom<RX, RY, RZ, TZ>;
+    size_t pb = round_up32(a.pbx * a.pby * a.pbz);
+    size_t rb = RAW_SMEM ? round_up32(a.rbx * a.rby * a.rbz) : 0;
+    size_t d = round_up32(G::DPLANE * G::DD);
+    size_t t = G::ND;
+    return 128 + 4 * (pb + rb + d + t);
+}
+
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
+static cudaError_t launch_inst(const CUtensorMap* tmp, const CUtensorMap* tmr, const TileArgs& a,
+                               int tiles_z, size_t smem, cudaStream_t st) {
+    auto kern = nlm_tile_f32_kernel<RX, RY, RZ, TZ, RAW_SMEM>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
+    kern<<<grid, 32 * TZ, smem, st>>>(*tmp, *tmr, a);
+    return cudaGetLastError();
+}
+
+#define INLM_FOR_EACH_SHAPE(X) \
+    X(1, 1, 1) X(1, 1, 2) X(1, 1, 3) X(2, 2, 1) X(2, 2, 2) X(3, 3, 1) X(3, 3, 2) X(3, 3, 3)
+
+bool tile_kernel_available(int rx, int ry, int rz) {
+#define X(a, b, c) \
+    if (rx == a && ry == b && rz == c) return true;
+    INLM_FOR_EACH_SHAPE(X)
+#undef X
+    return false;
+}
+
+size_t tile_smem_bytes(const TileConfig& c, const TileArgs& a) {
+#define X(A, B, C)                                                                    \
+    if (c.rx == A && c.ry == B && c.rz == C) {                                        \
+        if (c.tz == 8 && c.raw_smem) return smem_bytes_for<A, B, C, 8, true>(a);     \
+        if (c.tz == 8 && !c.raw_smem) return smem_bytes_for<A, B, C, 8, false>(a);   \
+        if (c.tz == 4 && !c.raw_smem) return smem_bytes_for<A, B, C, 4, false>(a);   \
+    }
+    INLM_FOR_EACH_SHAPE(X)
+#undef X
+    return 0;
+}
+
+cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,
+                               const CUtensorMap* tm_raw, const TileArgs& a, int tiles_z,
+                               cudaStream_t st) {
+#define X(A, B, C)                                                                             \
+    if (c.rx == A && c.ry == B && c.rz == C) {                                                 \
+        if (c.tz == 8 && c.raw_smem)                                                           \
+            return launch_inst<A, B, C, 8, true>(tm_prev, tm_raw, a, tiles_z, c.smem_bytes, st);  \
+        if (c.tz == 8 && !c.raw_smem)                                                          \
+            return launch_inst<A, B, C, 8, false>(tm_prev, tm_raw, a, tiles_z, c.smem_bytes, st); \
+        if (c.tz == 4 && !c.raw_smem)                                                          \
+            return launch_inst<A, B, C, 4, false>(tm_prev, tm_raw, a, tiles_z, c.smem_bytes, st); \
+    }
+    INLM_FOR_EACH_SHAPE(X)
+#undef X
+    return cudaErrorInvalidConfiguration;
+}
+
+template <int RX, int RY, int RZ>
+static int tap_order_impl(int* xyz, int max_taps) {
+    constexpr PatchRows rows = make_patch_rows(RX, RY, RZ);
+    int n = 0;
+    auto put = [&](int x, int y, int z) {
+        if (n < max_taps) {
+            xyz[3 * n] = x;
+            xyz[3 * n + 1] = y;
+            xyz[3 * n + 2] = z;
+        }
+        n++;
+    };
+    put(0, 0, 0);
+    for (int ri = 0; ri < rows.n; ri++)
+        for (int xp = -rows.e[ri]; xp <= rows.e[ri]; xp++)
+            if (!(rows.zp[ri] == 0 && rows.yp[ri] == 0 && xp == 0)) put(xp, rows.yp[ri], rows.zp[ri]);
+    return n;
+}
+
+int tile_kernel_tap_order(int rx, int ry, int rz, int* xyz, int max_taps) {
+#define X(A, B, C) \
+    if (rx == A && ry == B && rz == C) return tap_order_impl<A, B, C>(xyz, max_taps);
+    INLM_FOR_EACH_SHAPE(X)
+#undef X
+    return -1;
+}
+
+cudaError_t launch_generic_kernel(const GenericArgs& a, cudaStream_t st) {
+    long long nvox = (long long)a.nx * a.ny * a.nz;
+    int blocks = (int)((nvox + 255) / 256);
+    nlm_generic_f32_kernel<<<blocks, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pad_reflective(const float* in, int nx, int ny, int nz, float* out, int px,
+                                  int py, int pz, long long pitch_y, long long pitch_z,
+                                  cudaStream_t st) {
+    pad_reflective_kernel<<<148 * 8, 256, 0, st>>>(in, nx, ny, nz, out, px, py, pz, pitch_y,
+                                                   pitch_z);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sigma_to_mult(const float* sigma, float beta, float* mult, int nz,
+                                 cudaStream_t st) {
+    sigma_to_mult_kernel<<<(nz + 255) / 256, 256, 0, st>>>(sigma, beta, mult, nz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sigma_blend(const float* sigma0, float* sigma1, float alpha, int nz,
+                               cudaStream_t st) {
+    sigma_blend_kernel<<<(nz + 255) / 256, 256, 0, st>>>(sigma0, sigma1, alpha, nz);
+    return cudaGetLastError();
+}
+
+}  // namespace inlm

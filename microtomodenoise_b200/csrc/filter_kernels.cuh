@@ -1,0 +1,76 @@
+// Declarations shared by the filter kernels and the host orchestration.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+namespace inlm {
+
+constexpr int kMaxTaps = 128;
+
+// Tiled FP32 kernel geometry: a CTA owns TX x TY x TZ output voxels; a warp
+// owns one z-plane of 32 x 8 voxels with 4 lanes along x (8 consecutive
+// voxels each) and 8 lanes along y.
+constexpr int kTX = 32;
+constexpr int kTY = 8;
+constexpr int kVoxPerThread = 8;
+
+struct TileArgs {
+    int nx, ny, nz;               // unpadded volume
+    int tiles_x, tiles_y;         // grid decomposition (z from blockIdx)
+    int px, py, pz;               // padding per side
+    int sxr, syr, szc;            // search radius x, y and clipped z
+    int S;                        // number of search offsets
+    const int2* __restrict__ search_delta;  // (prev-box delta, raw delta) per offset
+    int pbx, pby, pbz;            // prev box (shared memory) extents
+    int rbx, rby, rbz;            // raw box extents (raw staged in shared memory)
+    const float* __restrict__ raw_pad;   // padded raw (global) for the raw-global form
+    long long gpitch_y, gpitch_z;        // padded global pitches (elements)
+    float* __restrict__ out;      // unpadded result
+    const float* __restrict__ mult;      // per-slice -1/(sigma^2 beta)
+    int* err;
+    float w[kMaxTaps];            // patch weights in reference tap order
+};
+
+struct GenericArgs {
+    int nx, ny, nz;
+    int px, py, pz;
+    long long gpitch_y, gpitch_z;
+    int S, P;
+    const long long* __restrict__ search_off;  // padded-linear offsets
+    const long long* __restrict__ patch_off;
+    const float* __restrict__ weights;
+    const float* __restrict__ raw_pad;
+    const float* __restrict__ prev_pad;
+    float* __restrict__ out;
+    const float* __restrict__ mult;
+};
+
+// Host-side launch descriptors.
+struct TileConfig {
+    int rx, ry, rz;   // patch radii of the instantiation
+    int tz;           // CTA depth (z-planes = warps)
+    bool raw_smem;    // raw box staged in shared memory
+    size_t smem_bytes;
+};
+
+// Returns false when no tiled instantiation exists for the patch shape.
+bool tile_kernel_available(int rx, int ry, int rz);
+// Shared-memory bytes for a configuration (0 if it cannot fit).
+size_t tile_smem_bytes(const TileConfig& c, const TileArgs& a);
+cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,
+                               const CUtensorMap* tm_raw, const TileArgs& a, int tiles_z,
+                               cudaStream_t st);
+cudaError_t launch_generic_kernel(const GenericArgs& a, cudaStream_t st);
+cudaError_t launch_pad_reflective(const float* in, int nx, int ny, int nz, float* out, int px,
+                                  int py, int pz, long long pitch_y, long long pitch_z,
+                                  cudaStream_t st);
+cudaError_t launch_sigma_to_mult(const float* sigma, float beta, float* mult, int nz,
+                                 cudaStream_t st);
+cudaError_t launch_sigma_blend(const float* sigma0, float* sigma1, float alpha, int nz,
+                               cudaStream_t st);
+// Compile-time tap rows of an instantiation, flattened as (x,y,z) triples in
+// the order the kernel accumulates them; used to check host/device agreement.
+int tile_kernel_tap_order(int rx, int ry, int rz, int* xyz, int max_taps);
+
+}  // namespace inlm

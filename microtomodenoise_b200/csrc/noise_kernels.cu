@@ -1,0 +1,322 @@
+// Noise-level estimators on the device (Noise/noiselevel.cpp).
+//
+//  * patch std: one thread per sample, the 15x15 sums accumulated in the
+//    reference's order in float (noiselevel.cpp:235-283), so every per-sample
+//    std equals the reference's bit for bit.
+//  * two-cluster hard EM (noiselevel.cpp:366-528): one CTA per z window
+//    (z-adaptive) or one CTA over all samples (global). The per-sample
+//    decisions use the reference's formulas; the cluster sums, counts and
+//    variances are block reductions accumulated in FP64 (warp shuffles, then
+//    shared memory). Assignments persist in a global int8 scratch array.
+//  * neighbour fill of empty windows (noiselevel.cpp:571-603) and
+//    sigma = mean + shift*std, sequential in one thread (nz is small).
+#include "common.cuh"
+#include "noise_kernels.cuh"
+
+namespace inlm {
+
+__global__ void __launch_bounds__(256) noise_patchstd_kernel(const float* __restrict__ stack,
+                                                             long long pitch_y, long long pitch_z,
+                                                             int nx, long long nslice,
+                                                             const long long* __restrict__ samples,
+                                                             long long n, int patchsize,
+                                                             float* __restrict__ out) {
+    long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    long long idx = samples[s];
+    int z0 = (int)(idx / nslice);
+    int y0 = (int)((idx - z0 * nslice) / nx);
+    int x0 = (int)(idx - z0 * nslice - (long long)y0 * nx);
+    const int patchlength = patchsize * patchsize;
+    float sum = 0.0f;
+    for (int y = y0; y < y0 + patchsize; y++) {
+        const float* row = stack + z0 * pitch_z + (long long)y * pitch_y + x0;
+        for (int x = 0; x < patchsize; x++) sum = __fadd_rn(sum, row[x]);
+    }
+    float mean = __fdiv_rn(sum, (float)patchlength);
+    float sq = 0.0f;
+    for (int y = y0; y < y0 + patchsize; y++) {
+        const float* row = stack + z0 * pitch_z + (long long)y * pitch_y + x0;
+        for (int x = 0; x < patchsize; x++) {
+            float d = __fsub_rn(row[x], mean);
+            sq = __fadd_rn(sq, __fmul_rn(d, d));
+        }
+    }
+    out[s] = __fsqrt_rn(__fdiv_rn(sq, (float)patchlength));
+}
+
+// Gaussian membership as written at noiselevel.cpp:456-457: 1./sqrtf(...) is a
+// double division and the product is rounded to float.
+__device__ __forceinline__ float cluster_prob(float v, float mean, float var) {
+    const float PI = 3.141592654f;
+    float d = __fsub_rn(v, mean);
+    float q = __fdiv_rn(__fmul_rn(d, d), __fmul_rn(2.f, var));
+    float e = expf(-q);
+    double inv = __ddiv_rn(1.0, (double)__fsqrt_rn(__fmul_rn(__fmul_rn(var, 2.f), PI)));
+    return __double2float_rn(__dmul_rn(inv, (double)e));
+}
+
+constexpr int kEmThreads = 256;
+
+struct EmRed {
+    double s1, s2;
+    long long n1, n2;
+};
+
+// Block-wide sum of (s1, s2, n1, n2) and OR of flag; result broadcast to all.
+__device__ __forceinline__ void block_reduce(EmRed& r, int& flag, EmRed* sh, int* shflag) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        r.s1 += __shfl_down_sync(0xffffffffu, r.s1, o);
+        r.s2 += __shfl_down_sync(0xffffffffu, r.s2, o);
+        r.n1 += __shfl_down_sync(0xffffffffu, r.n1, o);
+        r.n2 += __shfl_down_sync(0xffffffffu, r.n2, o);
+    }
+    int any = __any_sync(0xffffffffu, flag);
+    __syncthreads();
+    if (lane == 0) {
+        sh[warp] = r;
+        shflag[warp] = any;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        constexpr int NW = kEmThreads / 32;
+        EmRed t = (lane < NW) ? sh[lane] : EmRed{0.0, 0.0, 0, 0};
+        int f = (lane < NW) ? shflag[lane] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            t.s1 += __shfl_down_sync(0xffffffffu, t.s1, o);
+            t.s2 += __shfl_down_sync(0xffffffffu, t.s2, o);
+            t.n1 += __shfl_down_sync(0xffffffffu, t.n1, o);
+            t.n2 += __shfl_down_sync(0xffffffffu, t.n2, o);
+        }
+        f = __any_sync(0xffffffffu, f);
+        if (lane == 0) {
+            sh[0] = t;
+            shflag[0] = f;
+        }
+    }
+    __syncthreads();
+    r = sh[0];
+    flag = shflag[0];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kEmThreads) noise_em_kernel(const float* __restrict__ values,
+                                                             const int2* __restrict__ windows,
+                                                             const long long* __restrict__ scratch_off,
+                                                             signed char* __restrict__ assign_scratch,
+                                                             float* __restrict__ out_mean,
+                                                             float* __restrict__ out_sd) {
+    __shared__ EmRed sh[kEmThreads / 32];
+    __shared__ int shflag[kEmThreads / 32];
+    __shared__ float shmin[kEmThreads / 32], shmax[kEmThreads / 32];
+    const int w = blockIdx.x;
+    const int fs = windows[w].x, ls = windows[w].y;
+    signed char* asg = assign_scratch + scratch_off[w] - fs;  // indexed by sample id
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    // min / max (noiselevel.cpp:384-390)
+    float mn = 1e20f, mx = -1e20f;
+    for (int i = fs + tid; i <= ls; i += kEmThreads) {
+        float v = values[i];
+        mn = fminf(mn, v);
+        mx = fmaxf(mx, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_down_sync(0xffffffffu, mn, o));
+        mx = fmaxf(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    }
+    if (lane == 0) {
+        shmin[warp] = mn;
+        shmax[warp] = mx;
+    }
+    __syncthreads();
+    mn = 1e20f;
+    mx = -1e20f;
+    for (int q = 0; q < kEmThreads / 32; q++) {
+        mn = fminf(mn, shmin[q]);
+        mx = fmaxf(mx, shmax[q]);
+    }
+    float range = __fsub_rn(mx, mn);
+    float mean1 = __double2float_rn(__dadd_rn((double)mn, __dmul_rn(0.25, (double)range)));
+    float mean2 = __double2float_rn(__dsub_rn((double)mx, __dmul_rn(0.25, (double)range)));
+
+    // initial assignment, zero values excluded (noiselevel.cpp:398-423)
+    EmRed r{0.0, 0.0, 0, 0};
+    int flag = 0;
+    for (int i = fs + tid; i <= ls; i += kEmThreads) {
+        float v = values[i];
+        signed char a;
+        if (v == 0.0f) {
+            a = -1;
+        } else if (fabsf(__fsub_rn(v, mean1)) < fabsf(__fsub_rn(v, mean2))) {
+            a = 0;
+            r.s1 += (double)v;
+            r.n1++;
+        } else {
+            a = 1;
+            r.s2 += (double)v;
+            r.n2++;
+        }
+        asg[i] = a;
+    }
+    block_reduce(r, flag, sh, shflag);
+    if (r.n1 > 0) mean1 = __double2float_rn(r.s1 / (double)r.n1);
+    if (r.n2 > 0) mean2 = __double2float_rn(r.s2 / (double)r.n2);
+    if (r.n1 == 0 && r.n2 == 0) {
+        if (tid == 0) {
+            out_mean[w] = 0.0f;
+            out_sd[w] = 0.0f;
+        }
+        return;
+    }
+    long long n1 = r.n1, n2 = r.n2;
+
+    // cluster variances (noiselevel.cpp:428-443)
+    auto variances = [&](float m1, float m2, float& v1, float& v2) {
+        EmRed q{0.0, 0.0, 0, 0};
+        int f = 0;
+        for (int i = fs + tid; i <= ls; i += kEmThreads) {
+            float v = values[i];
+            signed char a = asg[i];
+            if (a == 0) {
+                float d = __fsub_rn(v, m1);
+                q.s1 += (double)__fmul_rn(d, d);
+            } else if (a == 1) {
+                float d = __fsub_rn(v, m2);
+                q.s2 += (double)__fmul_rn(d, d);
+            }
+        }
+        block_reduce(q, f, sh, shflag);
+        v1 = __double2float_rn(q.s1 / (double)(n1 > 1 ? n1 : 1));
+        v2 = __double2float_rn(q.s2 / (double)(n2 > 1 ? n2 : 1));
+    };
+    __syncthreads();  // assignments visible to all threads
+    float var1, var2;
+    variances(mean1, mean2, var1, var2);
+
+    // hard EM, at most 1000 passes (noiselevel.cpp:445-521)
+    int change = 1;
+    int iters = 0;
+    while (change && var1 > 0.0f && var2 > 0.0f) {
+        change = 0;
+        iters++;
+        EmRed q{0.0, 0.0, 0, 0};
+        int f = 0;
+        for (int i = fs + tid; i <= ls; i += kEmThreads) {
+            float v = values[i];
+            if (v == 0.0f) continue;
+            float p1 = cluster_prob(v, mean1, var1);
+            float p2 = cluster_prob(v, mean2, var2);
+            signed char a = asg[i];
+            if (p2 > p1) {
+                if (a != 1) {
+                    f = 1;
+                    asg[i] = 1;
+                }
+                q.s2 += (double)v;
+                q.n2++;
+            } else {
+                if (a != 0) {
+                    f = 1;
+                    asg[i] = 0;
+                }
+                q.s1 += (double)v;
+                q.n1++;
+            }
+        }
+        block_reduce(q, f, sh, shflag);
+        change = f;
+        n1 = q.n1;
+        n2 = q.n2;
+        if (n1 > 0) mean1 = __double2float_rn(q.s1 / (double)n1);
+        if (n2 > 0) mean2 = __double2float_rn(q.s2 / (double)n2);
+        variances(mean1, mean2, var1, var2);
+        if (iters == 1000) break;
+    }
+    if (tid == 0) {
+        if (mean1 <= mean2 || var2 <= 0.0f) {
+            out_mean[w] = mean1;
+            out_sd[w] = __fsqrt_rn(var1);
+        } else {
+            out_mean[w] = mean2;
+            out_sd[w] = __fsqrt_rn(var2);
+        }
+    }
+}
+
+// Neighbour fill (z-adaptive) and sigma = mean + shift*sd, single thread.
+__global__ void noise_finalize_kernel(float* __restrict__ mean, float* __restrict__ sd, int nz,
+                                      int zadaptive, float shift, float* __restrict__ sigma) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (!zadaptive) {
+        float s = __fadd_rn(mean[0], __fmul_rn(shift, sd[0]));
+        for (int z = 0; z < nz; z++) sigma[z] = s;
+        return;
+    }
+    float max_std = -1.f;
+    int zero = 0;
+    for (int i = 0; i < nz; i++) {
+        if (mean[i] > max_std) max_std = mean[i];
+        if (mean[i] == 0.0f) zero = 1;
+    }
+    if (zero && max_std > 0.0f) {
+        // every sweep fills at least one more slice next to a filled one
+        for (int sweep = 0; zero && sweep <= nz; sweep++) {
+            zero = 0;
+            for (int i = 0; i < nz; i++) {
+                float this_var = mean[i];
+                if (this_var == 0.0f) {
+                    float nv = 0.0f, nvs = 0.0f;
+                    int count = 0;
+                    if (i > 0 && mean[i - 1] > 0.0f) {
+                        nv = __fadd_rn(nv, mean[i - 1]);
+                        nvs = __fadd_rn(nvs, sd[i - 1]);
+                        count++;
+                    }
+                    if (i < nz - 1 && mean[i + 1] > 0.0f) {
+                        nv = __fadd_rn(nv, mean[i + 1]);
+                        nvs = __fadd_rn(nvs, sd[i + 1]);
+                        count++;
+                    }
+                    if (count > 0) {
+                        this_var = __fdiv_rn(nv, (float)count);
+                        mean[i] = this_var;
+                        sd[i] = __fdiv_rn(nvs, (float)count);
+                    }
+                }
+                if (this_var == 0.0f) zero = 1;
+            }
+        }
+    }
+    for (int z = 0; z < nz; z++) sigma[z] = __fadd_rn(mean[z], __fmul_rn(shift, sd[z]));
+}
+
+cudaError_t launch_noise_patchstd(const float* stack, long long pitch_y, long long pitch_z, int nx,
+                                  long long nslice, const long long* samples, long long n,
+                                  int patchsize, float* out, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    noise_patchstd_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+        stack, pitch_y, pitch_z, nx, nslice, samples, n, patchsize, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_noise_em(const float* values, const int2* windows, int n_windows,
+                            const long long* scratch_off, signed char* scratch, float* out_mean,
+                            float* out_sd, cudaStream_t st) {
+    if (n_windows <= 0) return cudaSuccess;
+    noise_em_kernel<<<n_windows, kEmThreads, 0, st>>>(values, windows, scratch_off, scratch,
+                                                      out_mean, out_sd);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_noise_finalize(float* mean, float* sd, int nz, int zadaptive, float shift,
+                                  float* sigma, cudaStream_t st) {
+    noise_finalize_kernel<<<1, 32, 0, st>>>(mean, sd, nz, zadaptive, shift, sigma);
+    return cudaGetLastError();
+}
+
+}  // namespace inlm

@@ -1,0 +1,18 @@
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace inlm {
+
+cudaError_t launch_noise_patchstd(const float* stack, long long pitch_y, long long pitch_z, int nx,
+                                  long long nslice, const long long* samples, long long n,
+                                  int patchsize, float* out, cudaStream_t st);
+// windows[w] = inclusive sample range; scratch_off[w] = byte offset of the
+// window's assignment array inside scratch.
+cudaError_t launch_noise_em(const float* values, const int2* windows, int n_windows,
+                            const long long* scratch_off, signed char* scratch, float* out_mean,
+                            float* out_sd, cudaStream_t st);
+cudaError_t launch_noise_finalize(float* mean, float* sd, int nz, int zadaptive, float shift,
+                                  float* sigma, cudaStream_t st);
+
+}  // namespace inlm
