@@ -47,7 +47,7 @@ def log(*a):
 
 
 def workload_config():
-    return {"workload": "grain-pack 512x512x512 f32, patch r2 (33 taps), search r5 (514 offsets), "
+    return {"workload": f"grain-pack {SHAPE[2]}x{SHAPE[1]}x{SHAPE[0]} f32, patch r2 (33 taps), search r5 (514 offsets), "
                         "4 iterations, alpha 0.5, z-adaptive noise (window 100, 1e5 samples)",
             "shape_xyz": [SHAPE[2], SHAPE[1], SHAPE[0]], "patch_radius": 2, "search_radius": 5,
             "iterations": ITERS, "offsets": S_OFFSETS, "taps": P_TAPS,
@@ -134,7 +134,7 @@ def make_volume(seed=0):
     from microtomodenoise_b200 import synth
     t = time.time()
     v = synth.grain_pack_volume(SHAPE, seed=seed)
-    log(f"generated 512^3 volume in {time.time() - t:.1f}s")
+    log(f"generated {SHAPE} volume in {time.time() - t:.1f}s")
     return v
 
 
@@ -159,17 +159,22 @@ def cpu_reference_rate(vol, target_s=15.0, threads=None):
             t = time.time()
             impl.denoise_f32(slab, p, sig)
             return time.time() - t
-    ny, nx = vol.shape[1], vol.shape[2]
-    calib = 2
-    slab = np.ascontiguousarray(vol[:calib])
+    ny, nx, nzv = vol.shape[1], vol.shape[2], vol.shape[0]
+    # The reference parallelises over z-slices (iternlm_cpu.cpp:91): slab
+    # depths are whole multiples of the thread count so no thread idles.
+    calib = min(threads, nzv)
+    z0 = max(0, nzv // 2 - calib // 2)
+    slab = np.ascontiguousarray(vol[z0:z0 + calib])
     secs = run(slab, np.full((1, calib), 0.045, np.float32))
     rate = calib * ny * nx / max(secs, 1e-6)
-    depth = int(np.clip(target_s * rate / (ny * nx), 2, vol.shape[0]))
-    slab = np.ascontiguousarray(vol[:depth])
+    depth = int(target_s * rate / (ny * nx)) // threads * threads
+    depth = int(np.clip(depth, calib, nzv))
+    z0 = max(0, nzv // 2 - depth // 2)
+    slab = np.ascontiguousarray(vol[z0:z0 + depth])
     secs = run(slab, np.full((1, depth), 0.045, np.float32))
     rate = depth * ny * nx / secs
     info = {"value": rate, "unit": "voxel-iter/s", "cores": threads, "kind": kind,
-            "sample": f"{nx}x{ny}x{depth} slab of the 512^3 volume, 1 iteration of "
+            "sample": f"{nx}x{ny}x{depth} slab (z {z0}..{z0 + depth - 1}) of the volume, 1 iteration of "
                       f"IterativeNLM_CPU::Run_GaussianNoise (p2 s5, sigma fixed), {secs:.1f}s, "
                       f"OpenMP {threads} threads"}
     return rate, info
@@ -205,6 +210,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default="512,512,512",
+                    help="nz,ny,nx of the volume (smaller shapes only for profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -212,6 +219,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    global SHAPE
+    SHAPE = tuple(int(v) for v in args.shape.split(","))
     if args.impl == "reference":
         run_reference_arm(args, rank)
         return

@@ -15,9 +15,11 @@
 // into shared memory with one 3D TMA load each. For every search offset it
 // writes the squared-difference volume D_s = (prev(.+s) - prev(.))^2 over the
 // tile plus patch halo to shared memory, then each thread applies the patch
-// stencil to D_s for 8 consecutive x voxels from a 16-float register window
-// per patch row (float4 loads, conflict-free row pitch), so each D value is
-// computed once and read by every voxel whose patch covers it.
+// stencil to D_s for 8 consecutive x voxels held as 4 register pairs: a tap
+// is two scalar FMULs (weight as a constant operand) and one paired FADD2
+// (sm_100 f32x2), from a 16-float register window per patch row loaded as
+// float4s from a conflict-free row pitch. Each D value is computed once per
+// offset and read by every voxel whose patch covers it.
 #include <cstdio>
 
 #include "common.cuh"
@@ -69,7 +71,51 @@ struct RowFirst<RX, RY, RZ, 0> {
     static constexpr int value = 1;
 };
 
-// Loads the 16-float window covering columns [x0, x0+16) of one D row.
+// Packed-pair arithmetic (sm_100 f32x2: one FADD2/FMUL2 instruction does two
+// IEEE round-to-nearest operations). ptxas fuses an FMUL2 whose result feeds
+// an FADD2 into one FFMA2 even with explicit .rn modifiers, which would round
+// once instead of twice; scalar products feeding paired sums (or paired
+// products feeding only products) keep every rounding of the reference, so
+// the kernels below never let an FMUL2 result reach an addition.
+// A pair is a 64-bit register holding (element 0, element 1).
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+// Paired product; its result must only feed multiplications (see above).
+__device__ __forceinline__ f32x2 mul2_to_mul(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
+    f32x2 d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ float2 unpack2(f32x2 a) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(a));
+    return r;
+}
+__device__ __forceinline__ f32x2 splat2(float v) { return pack2(v, v); }
+// Two scalar products as a pair (safe to feed add2).
+__device__ __forceinline__ f32x2 mul_pair(float a0, float a1, float b) {
+    return pack2(__fmul_rn(a0, b), __fmul_rn(a1, b));
+}
+__device__ __forceinline__ f32x2 mul_pair(float2 a, float2 b) {
+    return pack2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+}
+
+// Loads columns [x0 + 4*LO, x0 + 4*HI + 4) of one D row into win (float4s).
 template <int LO, int HI>
 __device__ __forceinline__ void load_window(const float* __restrict__ rowp, float (&win)[16]) {
 #pragma unroll
@@ -83,8 +129,8 @@ __device__ __forceinline__ void load_window(const float* __restrict__ rowp, floa
 }
 
 template <int RX, int RY, int RZ, int TZ, int RI>
-__device__ __forceinline__ void accumulate_rows(const float* __restrict__ D, int k, int j, int x0,
-                                                float (&dist)[kVoxPerThread],
+__device__ __forceinline__ void accumulate_rows(const float* __restrict__ D, int rowoff,
+                                                f32x2 (&dist)[kVoxPerThread / 2],
                                                 const TileArgs& a) {
     using G = TileGeom<RX, RY, RZ, TZ>;
     if constexpr (RI < G::rows.n) {
@@ -94,19 +140,20 @@ __device__ __forceinline__ void accumulate_rows(const float* __restrict__ D, int
         constexpr int first = RowFirst<RX, RY, RZ, RI>::value;
         constexpr int lo = (RX - e) / 4;
         constexpr int hi = (RX + kVoxPerThread - 1 + e) / 4;
-        const float* rowp = D + (k + zp + RZ) * G::DPLANE + (j + yp + RY) * G::DP + x0;
         float win[16];
-        load_window<lo, hi>(rowp, win);
+        load_window<lo, hi>(D + rowoff + (zp + RZ) * G::DPLANE + (yp + RY) * G::DP, win);
 #pragma unroll
-        for (int r = 0; r < kVoxPerThread; r++) {
+        for (int xp = -e; xp <= e; xp++) {
+            if (zp == 0 && yp == 0 && xp == 0) continue;
+            const int t = first + (xp + e) - ((zp == 0 && yp == 0 && xp > 0) ? 1 : 0);
+            const float w = a.w[t];
 #pragma unroll
-            for (int xp = -e; xp <= e; xp++) {
-                if (zp == 0 && yp == 0 && xp == 0) continue;
-                const int t = first + (xp + e) - ((zp == 0 && yp == 0 && xp > 0) ? 1 : 0);
-                dist[r] = __fadd_rn(dist[r], __fmul_rn(win[RX + r + xp], a.w[t]));
+            for (int p = 0; p < kVoxPerThread / 2; p++) {
+                const int i = RX + 2 * p + xp;
+                dist[p] = add2(dist[p], mul_pair(win[i], win[i + 1], w));
             }
         }
-        accumulate_rows<RX, RY, RZ, TZ, RI + 1>(D, k, j, x0, dist, a);
+        accumulate_rows<RX, RY, RZ, TZ, RI + 1>(D, rowoff, dist, a);
     }
 }
 
@@ -124,7 +171,10 @@ __global__ void __launch_bounds__(32 * TZ, 1)
     float* rawb = prevb + round_up32(PB);
     const int RB = RAW_SMEM ? a.rbx * a.rby * a.rbz : 0;
     float* D = rawb + round_up32(RB);
-    int* tab = reinterpret_cast<int*>(D + round_up32(G::DPLANE * G::DD));
+    constexpr int DSZ = round_up32(G::DPLANE * G::DD);
+    // D is double-buffered: phase A of offset s+1 writes one buffer while
+    // phase B of offset s reads the other, one barrier per offset.
+    float* const D0 = D;
 
     const int tid = threadIdx.x;
     const int X0 = blockIdx.x * kTX;
@@ -145,23 +195,31 @@ __global__ void __launch_bounds__(32 * TZ, 1)
         if (RAW_SMEM) tma_load_3d(rawb, &tm_raw, X0, Y0 + RY, Z0 + RZ, bar);
     }
 
-    // Shared-memory index table of the D volume: prev-box index of the
-    // origin (low 16 bits) and D index (high 16 bits).
-    for (int f = tid; f < G::ND; f += G::NT) {
+    // Each thread owns NQ fixed column pairs of the D volume (rows have an
+    // even width); their prev-box and D indices, and the origin values, are
+    // the same for every search offset and stay in registers.
+    constexpr int NPAIR = G::ND / 2;
+    constexpr int NQ = (NPAIR + G::NT - 1) / G::NT;
+    int qpi[NQ], qdi[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; k++) {
+        int q = min(tid + k * G::NT, NPAIR - 1);  // the tail repeats the last pair
+        int f = 2 * q;
         int c = f % G::DW;
         int rest = f / G::DW;
         int r = rest % G::DH;
         int p = rest / G::DH;
-        int pi = (p - RZ + a.pz) * pplane + (r - RY + a.py) * a.pbx + (c - RX + a.px);
-        int di = p * G::DPLANE + r * G::DP + c;
-        tab[f] = pi | (di << 16);
+        qpi[k] = (p - RZ + a.pz) * pplane + (r - RY + a.py) * a.pbx + (c - RX + a.px);
+        qdi[k] = p * G::DPLANE + r * G::DP + c;
     }
 
     if (!mbar_wait_bounded(bar, 0)) {
         set_error(a.err, DEV_TMA_TIMEOUT);
         return;
     }
-    __syncthreads();
+    f32x2 qog[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; k++) qog[k] = pack2(prevb[qpi[k]], prevb[qpi[k] + 1]);
 
     const int warp = tid >> 5, lane = tid & 31;
     const int k = warp;
@@ -169,6 +227,8 @@ __global__ void __launch_bounds__(32 * TZ, 1)
     const int x0 = (lane & 3) * kVoxPerThread;
     const int zk = min(Z0 + k, a.nz - 1);
     const float m = a.mult[zk];
+    const f32x2 m2 = splat2(m);
+    const int rowoff = k * G::DPLANE + j * G::DP + x0;
 
     int rbase;
     long long gbase;
@@ -181,37 +241,73 @@ __global__ void __launch_bounds__(32 * TZ, 1)
                 (X0 + x0 + a.px);
     }
 
-    float acc[kVoxPerThread], wsum[kVoxPerThread], wmax[kVoxPerThread];
+    constexpr int NP = kVoxPerThread / 2;
+    f32x2 acc[NP], wsum[NP];
+    float wmax[kVoxPerThread];
 #pragma unroll
-    for (int r = 0; r < kVoxPerThread; r++) acc[r] = wsum[r] = wmax[r] = 0.0f;
+    for (int p = 0; p < NP; p++) acc[p] = wsum[p] = 0ull;  // (+0, +0)
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) wmax[r] = 0.0f;
 
-    for (int s = 0; s < a.S; s++) {
-        const int2 dl = __ldg(&a.search_delta[s]);
-        // phase A: D_s over tile + patch halo
-        for (int f = tid; f < G::ND; f += G::NT) {
-            int t = tab[f];
-            int pi = t & 0xffff;
-            float v = __fsub_rn(prevb[pi + dl.x], prevb[pi]);
-            D[t >> 16] = __fmul_rn(v, v);
+    const f32x2 c12 = splat2(12.f), c120 = splat2(120.f);
+
+    // phase A for one offset: D = (prev(.+s) - prev(.))^2 over tile + patch halo
+    auto phase_a = [&](float* Dw, int dlx) {
+#pragma unroll
+        for (int k = 0; k < NQ; k++) {
+            f32x2 sh = pack2(prevb[qpi[k] + dlx], prevb[qpi[k] + dlx + 1]);
+            f32x2 v = sub2(sh, qog[k]);
+            *reinterpret_cast<f32x2*>(Dw + qdi[k]) = mul2_to_mul(v, v);  // stored, not added
         }
-        __syncthreads();
-        // phase B: patch stencil on D_s, weight, accumulate
-        float dist[kVoxPerThread];
+    };
+
+    int2 dl = __ldg(&a.search_delta[0]);
+    phase_a(D0, dl.x);
+    __syncthreads();
+    for (int s = 0; s < a.S; s++) {
+        const float* D = D0 + (s & 1) * DSZ;
+        const int dly = dl.y;
+        if (s + 1 < a.S) {
+            dl = __ldg(&a.search_delta[s + 1]);
+            phase_a(D0 + ((s + 1) & 1) * DSZ, dl.x);
+        }
+        // phase B: patch stencil on D_s (centre tap first), weight, accumulate
+        f32x2 dist[NP];
         {
             float win[16];
-            const float* rowp = D + (k + RZ) * G::DPLANE + (j + RY) * G::DP + x0;
-            load_window<RX / 4, (RX + kVoxPerThread - 1) / 4>(rowp, win);
+            load_window<RX / 4, (RX + kVoxPerThread - 1) / 4>(
+                D + rowoff + RZ * G::DPLANE + RY * G::DP, win);
+            const float w0 = a.w[0];
 #pragma unroll
-            for (int r = 0; r < kVoxPerThread; r++) dist[r] = __fmul_rn(win[RX + r], a.w[0]);
+            for (int p = 0; p < NP; p++) dist[p] = mul_pair(win[RX + 2 * p], win[RX + 2 * p + 1], w0);
         }
-        accumulate_rows<RX, RY, RZ, TZ, 0>(D, k, j, x0, dist, a);
+        accumulate_rows<RX, RY, RZ, TZ, 0>(D, rowoff, dist, a);
 #pragma unroll
-        for (int r = 0; r < kVoxPerThread; r++) {
-            float rs = RAW_SMEM ? rawb[rbase + dl.y + r] : __ldg(&a.raw_pad[gbase + dl.y + r]);
-            float wt = pade_weight_exact(__fmul_rn(dist[r], m));
-            acc[r] = __fadd_rn(acc[r], __fmul_rn(wt, rs));
-            wsum[r] = __fadd_rn(wsum[r], wt);
-            wmax[r] = fmaxf(wmax[r], wt);
+        for (int p = 0; p < NP; p++) {
+            float2 rsv;
+            if (RAW_SMEM) {
+                rsv = make_float2(rawb[rbase + dly + 2 * p], rawb[rbase + dly + 2 * p + 1]);
+            } else {
+                rsv = make_float2(__ldg(&a.raw_pad[gbase + dly + 2 * p]),
+                                  __ldg(&a.raw_pad[gbase + dly + 2 * p + 1]));
+            }
+            // Pade[3/3] (120 + 60x + 12x*x + x*x*x) / (120 - 60x + 12x*x - x*x*x):
+            // products that feed the sums are scalar, the sums are paired
+            const f32x2 x = mul2_to_mul(dist[p], m2);
+            const float2 xs = unpack2(x);
+            const float2 x12 = unpack2(mul2_to_mul(c12, x));
+            const float2 xx = unpack2(mul2_to_mul(x, x));
+            const f32x2 ta = mul_pair(xs, make_float2(60.f, 60.f));
+            const f32x2 tb = mul_pair(x12, xs);
+            const f32x2 tc = mul_pair(xx, xs);
+            const float2 num = unpack2(add2(add2(add2(c120, ta), tb), tc));
+            const float2 den = unpack2(sub2(add2(sub2(c120, ta), tb), tc));
+            const float w0 = (xs.x > -3.56648f) ? __fdiv_rn(num.x, den.x) : 0.0f;
+            const float w1 = (xs.y > -3.56648f) ? __fdiv_rn(num.y, den.y) : 0.0f;
+            acc[p] = add2(acc[p], mul_pair(make_float2(w0, w1), rsv));
+            wsum[p] = add2(wsum[p], pack2(w0, w1));
+            wmax[2 * p] = fmaxf(wmax[2 * p], w0);
+            wmax[2 * p + 1] = fmaxf(wmax[2 * p + 1], w1);
         }
         __syncthreads();
     }
@@ -224,10 +320,13 @@ __global__ void __launch_bounds__(32 * TZ, 1)
             int x = X0 + x0 + r;
             if (x < a.nx) {
                 float raw0 = RAW_SMEM ? rawb[rbase + r] : __ldg(&a.raw_pad[gbase + r]);
+                const float2 acp = unpack2(acc[r / 2]), wsp = unpack2(wsum[r / 2]);
+                float ac = (r & 1) ? acp.y : acp.x;
+                float ws = (r & 1) ? wsp.y : wsp.x;
                 float res;
                 if (wmax[r] > 0.0f) {
-                    float ac = __fadd_rn(acc[r], __fmul_rn(wmax[r], raw0));
-                    float ws = __fadd_rn(wsum[r], wmax[r]);
+                    ac = __fadd_rn(ac, __fmul_rn(wmax[r], raw0));
+                    ws = __fadd_rn(ws, wmax[r]);
                     res = __fdiv_rn(ac, ws);
                 } else {
                     res = raw0;
@@ -329,8 +428,7 @@ static size_t smem_bytes_for(const TileArgs& a) {
     size_t pb = round_up32(a.pbx * a.pby * a.pbz);
     size_t rb = RAW_SMEM ? round_up32(a.rbx * a.rby * a.rbz) : 0;
     size_t d = round_up32(G::DPLANE * G::DD);
-    size_t t = G::ND;
-    return 128 + 4 * (pb + rb + d + t);
+    return 128 + 4 * (pb + rb + 2 * d);
 }
 
 template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
