@@ -170,6 +170,30 @@ int inlm_noise_samples(inlm_noise* n, int64_t* out, uint64_t max_n, uint64_t* n_
 /* Per-sample patch std of the last estimate (host copy). */
 int inlm_noise_patchstd(inlm_noise* n, float* out, uint64_t max_n);
 
+/* Two-cluster EM of the noise estimators for callers that cannot allocate
+ * device memory. It has no counterpart in the reference (whose EM runs on
+ * the host). It calls no cudaMalloc, cudaFree or other allocating routine:
+ * its scratch (one byte per sample per window, and the window table) lives
+ * in file-scope device arrays of this library, 16 MiB + 256 KiB, which every
+ * GPU that loads the library holds until the process exits. Callers that
+ * cannot allocate include code running while another thread captures a CUDA
+ * graph in global capture mode (cudaMalloc is a prohibited call then) and
+ * applications whose device memory is owned by their own pool.
+ *
+ * values_dev: n_values per-sample patch stds (device); windows_host: 2 values
+ * per window (first, last sample index, inclusive; last < first = empty),
+ * host memory; mean_dev / sd_dev: n_windows outputs (device), the lower
+ * cluster's mean and std per window, as inlm_noise_estimate computes them.
+ * Runs on the calling thread's current device, on `stream` (NULL = default).
+ * Limits: n_windows <= 16384 and the window lengths summing to at most
+ * 16777216 samples; larger requests return INLM_ERR_ARG.
+ * The first call on a device looks up the arrays' device addresses; make
+ * it before any stream capture. Calls share the arrays and leave the last
+ * call's contents behind: calls that overlap on the GPU race. */
+int inlm_noise_em_noalloc(void* stream, const float* values_dev, int64_t n_values,
+                          const int64_t* windows_host, int n_windows, float* mean_dev,
+                          float* sd_dev);
+
 /* ---------------- host-only helpers (no device needed) ---------------- */
 
 /* Geometry of a parameter set (setup_searchspace / setup_patchspace /

@@ -30,7 +30,7 @@ EXPORTS = (
     "inlm_get_result_device", "inlm_denoise", "inlm_set_stream", "inlm_filter_kernel_ms",
     "inlm_describe", "inlm_noise_create", "inlm_noise_destroy", "inlm_noise_estimate",
     "inlm_noise_samples", "inlm_noise_patchstd", "inlm_geometry", "inlm_noise_draw_samples",
-    "inlm_kernel_launches", "inlm_probe_fp32_peak",
+    "inlm_kernel_launches", "inlm_probe_fp32_peak", "inlm_noise_em_noalloc",
 )
 
 
@@ -103,6 +103,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.inlm_noise_draw_samples.argtypes = [C.c_int * 3, C.c_uint64, C.c_int, C.c_int, C.c_uint, vp]
     L.inlm_kernel_launches.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.inlm_probe_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.inlm_noise_em_noalloc.argtypes = [vp, vp, C.c_int64, vp, C.c_int, vp, vp]
     for name in EXPORTS:
         if name not in ("inlm_last_error", "inlm_default_params"):
             getattr(L, name).restype = C.c_int

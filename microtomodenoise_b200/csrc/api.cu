@@ -949,3 +949,34 @@ extern "C" int inlm_probe_fp32_peak(int device_id, double* tflops) {
     *tflops = best;
     return INLM_OK;
 }
+
+// ---------------- allocation-free EM ----------------
+
+extern "C" int inlm_noise_em_noalloc(void* stream, const float* values_dev, int64_t n_values,
+                                     const int64_t* windows_host, int n_windows, float* mean_dev,
+                                     float* sd_dev) {
+    if (!values_dev || !windows_host || !mean_dev || !sd_dev)
+        return fail(INLM_ERR_ARG, "null argument");
+    if (n_values <= 0 || n_values > INT32_MAX) return fail(INLM_ERR_ARG, "n_values out of range");
+    if (n_windows <= 0 || n_windows > kNoAllocMaxWindows)
+        return fail(INLM_ERR_ARG, "n_windows %d outside 1..%d (static window table size)", n_windows,
+                    kNoAllocMaxWindows);
+    long long total = 0;
+    for (int w = 0; w < n_windows; w++) {
+        int64_t f = windows_host[2 * w], l = windows_host[2 * w + 1];
+        if (l < f) continue;
+        if (f < 0 || l >= n_values)
+            return fail(INLM_ERR_ARG, "window %d [%lld, %lld] outside 0..%lld", w, (long long)f,
+                        (long long)l, (long long)(n_values - 1));
+        total += l - f + 1;
+    }
+    if (total > kNoAllocAssignBytes)
+        return fail(INLM_ERR_ARG,
+                    "windows cover %lld samples in total; the static scratch holds at most %lld",
+                    total, (long long)kNoAllocAssignBytes);
+    int dev = -1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(launch_noise_em_noalloc(dev, values_dev, (const long long*)windows_host, n_windows,
+                                     mean_dev, sd_dev, (cudaStream_t)stream));
+    return INLM_OK;
+}

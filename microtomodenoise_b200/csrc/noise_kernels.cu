@@ -10,6 +10,8 @@
 //    shared memory). Assignments persist in a global int8 scratch array.
 //  * neighbour fill of empty windows (noiselevel.cpp:571-603) and
 //    sigma = mean + shift*std, sequential in one thread (nz is small).
+#include <mutex>
+
 #include "common.cuh"
 #include "noise_kernels.cuh"
 
@@ -103,18 +105,16 @@ __device__ __forceinline__ void block_reduce(EmRed& r, int& flag, EmRed* sh, int
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kEmThreads) noise_em_kernel(const float* __restrict__ values,
-                                                             const int2* __restrict__ windows,
-                                                             const long long* __restrict__ scratch_off,
-                                                             signed char* __restrict__ assign_scratch,
-                                                             float* __restrict__ out_mean,
-                                                             float* __restrict__ out_sd) {
+// Two-cluster EM over values[fs..ls] by one CTA; asg[i] holds sample i's
+// cluster (-1 excluded, 0, 1). Writes out_mean[w], out_sd[w].
+__device__ __forceinline__ void em_window(const float* __restrict__ values, int fs, int ls,
+                                          signed char* __restrict__ asg, int w,
+                                          float* __restrict__ out_mean,
+                                          float* __restrict__ out_sd) {
     __shared__ EmRed sh[kEmThreads / 32];
     __shared__ int shflag[kEmThreads / 32];
     __shared__ float shmin[kEmThreads / 32], shmax[kEmThreads / 32];
-    const int w = blockIdx.x;
-    const int fs = windows[w].x, ls = windows[w].y;
-    signed char* asg = assign_scratch + scratch_off[w] - fs;  // indexed by sample id
+    // assignments indexed by sample id
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     // min / max (noiselevel.cpp:384-390)
@@ -246,6 +246,108 @@ __global__ void __launch_bounds__(kEmThreads) noise_em_kernel(const float* __res
             out_sd[w] = __fsqrt_rn(var2);
         }
     }
+}
+
+__global__ void __launch_bounds__(kEmThreads) noise_em_kernel(const float* __restrict__ values,
+                                                             const int2* __restrict__ windows,
+                                                             const long long* __restrict__ scratch_off,
+                                                             signed char* __restrict__ assign_scratch,
+                                                             float* __restrict__ out_mean,
+                                                             float* __restrict__ out_sd) {
+    const int w = blockIdx.x;
+    const int fs = windows[w].x, ls = windows[w].y;
+    em_window(values, fs, ls, assign_scratch + scratch_off[w] - fs, w, out_mean, out_sd);
+}
+
+// ---- allocation-free EM: scratch in file-scope device arrays ----
+//
+// For callers that cannot allocate device memory. The cluster-assignment
+// scratch (one byte per sample per window) and the window table live in
+// static device arrays that every GPU loading this library holds until the
+// process exits: 16 MiB + 256 KiB. Every call on a device shares them and
+// leaves the last call's contents behind; calls whose work overlaps on the
+// GPU (different streams, or different host threads) race on them.
+// Nothing needs clearing between calls: the EM writes every assignment of a
+// window (its initial pass) before it reads any, and the host rewrites the
+// window table for every call.
+struct NoAllocWindow {
+    int first, last;     // inclusive sample range
+    long long offset;    // byte offset of the window's assignments in the scratch
+};
+
+static __device__ __align__(256) signed char g_noalloc_assign[kNoAllocAssignBytes];
+static __device__ __align__(256) NoAllocWindow g_noalloc_windows[kNoAllocMaxWindows];
+
+__global__ void __launch_bounds__(kEmThreads) noise_em_noalloc_kernel(
+    const float* __restrict__ values, const NoAllocWindow* __restrict__ windows,
+    signed char* __restrict__ assign_scratch, float* __restrict__ out_mean,
+    float* __restrict__ out_sd) {
+    const int w = blockIdx.x;
+    const NoAllocWindow win = windows[w];
+    em_window(values, win.first, win.last, assign_scratch + win.offset - win.first, w, out_mean,
+              out_sd);
+}
+
+// Device addresses of the two arrays, looked up once per device with that
+// device current (host code must not use the symbols themselves: they are
+// host-side stand-ins, not device addresses).
+struct NoAllocPtrs {
+    bool ready = false;
+    signed char* assign = nullptr;
+    NoAllocWindow* windows = nullptr;
+};
+static NoAllocPtrs g_noalloc_ptrs[kNoAllocMaxDevices];
+static std::mutex g_noalloc_mutex;
+
+static cudaError_t noalloc_setup(int device, NoAllocPtrs* out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoAllocPtrs& p = g_noalloc_ptrs[device];
+    if (!p.ready) {
+        int cur = -1;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e != cudaSuccess) return e;
+        if (cur != device) return cudaErrorInvalidDevice;
+        e = cudaGetSymbolAddress((void**)&p.assign, g_noalloc_assign);
+        if (e != cudaSuccess) return e;
+        e = cudaGetSymbolAddress((void**)&p.windows, g_noalloc_windows);
+        if (e != cudaSuccess) return e;
+        p.ready = true;
+    }
+    *out = p;
+    return cudaSuccess;
+}
+
+cudaError_t launch_noise_em_noalloc(int device, const float* values, const long long* windows_host,
+                                    int n_windows, float* out_mean, float* out_sd,
+                                    cudaStream_t st) {
+    if (n_windows <= 0) return cudaSuccess;
+    if (device < 0 || device >= kNoAllocMaxDevices || n_windows > kNoAllocMaxWindows)
+        return cudaErrorInvalidValue;
+    NoAllocPtrs ptrs;
+    cudaError_t e = noalloc_setup(device, &ptrs);
+    if (e != cudaSuccess) return e;
+    NoAllocWindow table[256];
+    long long offset = 0;
+    // the window table goes up in chunks through a small host buffer
+    for (int base = 0; base < n_windows; base += 256) {
+        int cnt = n_windows - base < 256 ? n_windows - base : 256;
+        for (int i = 0; i < cnt; i++) {
+            long long f = windows_host[2 * (base + i)], l = windows_host[2 * (base + i) + 1];
+            table[i].first = (int)f;
+            table[i].last = (int)l;
+            table[i].offset = offset;
+            offset += (l >= f) ? (l - f + 1) : 0;
+        }
+        // synchronous for pageable host memory, so table can be reused
+        e = cudaMemcpyAsync(ptrs.windows + base, table, cnt * sizeof(NoAllocWindow),
+                            cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+        e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+    }
+    noise_em_noalloc_kernel<<<n_windows, kEmThreads, 0, st>>>(values, ptrs.windows, ptrs.assign,
+                                                              out_mean, out_sd);
+    return cudaGetLastError();
 }
 
 // Neighbour fill (z-adaptive) and sigma = mean + shift*sd, single thread.

@@ -12,6 +12,14 @@ cudaError_t launch_noise_patchstd(const float* stack, long long pitch_y, long lo
 cudaError_t launch_noise_em(const float* values, const int2* windows, int n_windows,
                             const long long* scratch_off, signed char* scratch, float* out_mean,
                             float* out_sd, cudaStream_t st);
+// Allocation-free EM (static device scratch): limits of the file-scope arrays.
+constexpr long long kNoAllocAssignBytes = 16ll << 20;  // sum of window lengths, samples
+constexpr int kNoAllocMaxWindows = 16384;
+constexpr int kNoAllocMaxDevices = 64;
+// windows_host: 2 values (first, last inclusive) per window, host memory.
+cudaError_t launch_noise_em_noalloc(int device, const float* values, const long long* windows_host,
+                                    int n_windows, float* out_mean, float* out_sd,
+                                    cudaStream_t st);
 cudaError_t launch_noise_finalize(float* mean, float* sd, int nz, int zadaptive, float shift,
                                   float* sigma, cudaStream_t st);
 
