@@ -472,7 +472,6 @@ static int choose_tile_config(inlm_denoiser* d) {
         a.pbz = c.tz + 2 * a.pz;
         a.rbz = c.tz + 2 * a.szc;
         if (a.pbx > 256 || a.pby > 256 || a.pbz > 256) continue;
-        if (c.raw && (a.rbx > 256 || a.rby > 256 || a.rbz > 256)) continue;
         if ((long long)a.pbx * a.pby * a.pbz >= 65536) continue;  // 16-bit index table
         TileConfig tc{pr[0], pr[1], pr[2], c.tz, c.raw, 0};
         size_t sm = tile_smem_bytes(tc, a);
@@ -487,11 +486,12 @@ static int choose_tile_config(inlm_denoiser* d) {
     a.tiles_y = (d->shape[1] + kTY - 1) / kTY;
     // search deltas inside the shared-memory boxes (raw: box or global)
     std::vector<int2> dl(a.S);
-    const int pplane = a.pbx * a.pby, rplane = a.rbx * a.rby;
+    const int rpx = a.rbx + 1;  // odd shared-memory row pitch of the raw box
+    const int pplane = a.pbx * a.pby, rplane = rpx * a.rby;
     for (int s = 0; s < a.S; s++) {
         const Offset3& o = g.search[s];
         dl[s].x = o.z * pplane + o.y * a.pbx + o.x;
-        dl[s].y = d->tcfg.raw_smem ? o.z * rplane + o.y * a.rbx + o.x
+        dl[s].y = d->tcfg.raw_smem ? o.z * rplane + o.y * rpx + o.x
                                    : (int)(o.z * d->pitch_z + o.y * d->pitch_y + o.x);
     }
     CUDA_TRY(dalloc(&d->d_search_delta, a.S));
@@ -504,13 +504,7 @@ static int choose_tile_config(inlm_denoiser* d) {
     int rc = encode_map_3d(&d->tm_prev, d->d_prev_pad, d->nxp, d->nyp, d->nzp, d->pitch_y, d->pitch_z,
                            a.pbx, a.pby, a.pbz);
     if (rc) return rc;
-    if (d->tcfg.raw_smem) {
-        rc = encode_map_3d(&d->tm_raw, d->d_raw_pad, d->nxp, d->nyp, d->nzp, d->pitch_y, d->pitch_z,
-                           a.rbx, a.rby, a.rbz);
-        if (rc) return rc;
-    } else {
-        d->tm_raw = d->tm_prev;  // unused by the raw-global form
-    }
+    d->tm_raw = d->tm_prev;  // raw is staged with plain loads; the map is unused
     return INLM_OK;
 }
 
@@ -980,3 +974,4 @@ extern "C" int inlm_noise_em_noalloc(void* stream, const float* values_dev, int6
                                      mean_dev, sd_dev, (cudaStream_t)stream));
     return INLM_OK;
 }
+

@@ -11,8 +11,8 @@
 // FMA) build bit for bit.
 //
 // Tiled kernel: a CTA stages the padded previous iterate over its tile plus
-// search+patch halo (and, when it fits, raw over the tile plus search halo)
-// into shared memory with one 3D TMA load each. For every search offset it
+// search+patch halo into shared memory with one 3D TMA load and, when it fits,
+// raw over the tile plus search halo with coalesced loads (odd row pitch). For every search offset it
 // writes the squared-difference volume D_s = (prev(.+s) - prev(.))^2 over the
 // tile plus patch halo to shared memory, then each thread applies the patch
 // stencil to D_s for 8 consecutive x voxels held as 4 register pairs: a tap
@@ -72,11 +72,13 @@ struct RowFirst<RX, RY, RZ, 0> {
 };
 
 // Packed-pair arithmetic (sm_100 f32x2: one FADD2/FMUL2 instruction does two
-// IEEE round-to-nearest operations). ptxas fuses an FMUL2 whose result feeds
-// an FADD2 into one FFMA2 even with explicit .rn modifiers, which would round
-// once instead of twice; scalar products feeding paired sums (or paired
-// products feeding only products) keep every rounding of the reference, so
-// the kernels below never let an FMUL2 result reach an addition.
+// IEEE round-to-nearest operations; measured on B200 it issues in one slot but
+// gives no more FP32 lane throughput than two scalar instructions, so the gain
+// is issue slots left for the loads around it). ptxas fuses an FMUL2 whose
+// result feeds an FADD2 into one FFMA2 even with explicit .rn modifiers, which
+// would round once instead of twice; scalar products feeding paired sums (or
+// paired products feeding only products) keep every rounding of the
+// reference, so the kernels below never let an FMUL2 result reach an addition.
 // A pair is a 64-bit register holding (element 0, element 1).
 typedef unsigned long long f32x2;
 
@@ -169,7 +171,10 @@ __global__ void __launch_bounds__(32 * TZ, 1)
     const int pplane = a.pbx * a.pby;
     const int PB = pplane * a.pbz;
     float* rawb = prevb + round_up32(PB);
-    const int RB = RAW_SMEM ? a.rbx * a.rby * a.rbz : 0;
+    // raw is staged with an odd row pitch (rpx = rbx + 1) so the phase-B reads
+    // of 8 y-lanes x 4 x-lanes fall in 32 distinct banks
+    const int rpx = a.rbx + 1;
+    const int RB = RAW_SMEM ? rpx * a.rby * a.rbz : 0;
     float* D = rawb + round_up32(RB);
     constexpr int DSZ = round_up32(G::DPLANE * G::DD);
     // D is double-buffered: phase A of offset s+1 writes one buffer while
@@ -189,10 +194,25 @@ __global__ void __launch_bounds__(32 * TZ, 1)
     }
     __syncthreads();
     if (tid == 0) {
-        mbar_arrive_expect_tx(bar, (uint32_t)(PB + RB) * 4u);
+        mbar_arrive_expect_tx(bar, (uint32_t)PB * 4u);
         // prev box starts at the tile origin in padded coordinates (x aligned to 32)
         tma_load_3d(prevb, &tm_prev, X0, Y0, Z0, bar);
-        if (RAW_SMEM) tma_load_3d(rawb, &tm_raw, X0, Y0 + RY, Z0 + RZ, bar);
+    }
+    if (RAW_SMEM) {
+        // raw over tile + search halo, coalesced rows re-pitched while the
+        // TMA load is in flight; positions past the volume read the zeroed
+        // slack planes behind it and are never used
+        const int rb_n = a.rbx * a.rby * a.rbz;
+        const float* rsrc = a.raw_pad + (long long)(Z0 + RZ) * a.gpitch_z +
+                            (long long)(Y0 + RY) * a.gpitch_y + X0;
+        for (int i = tid; i < rb_n; i += G::NT) {
+            int xx = i % a.rbx;
+            int rest = i / a.rbx;
+            int yy = rest % a.rby;
+            int zz = rest / a.rby;
+            rawb[(zz * a.rby + yy) * rpx + xx] =
+                __ldg(rsrc + (long long)zz * a.gpitch_z + (long long)yy * a.gpitch_y + xx);
+        }
     }
 
     // Each thread owns NQ fixed column pairs of the D volume (rows have an
@@ -233,7 +253,7 @@ __global__ void __launch_bounds__(32 * TZ, 1)
     int rbase;
     long long gbase;
     if (RAW_SMEM) {
-        rbase = (a.szc + k) * (a.rbx * a.rby) + (a.syr + j) * a.rbx + (RX + a.sxr + x0);
+        rbase = (a.szc + k) * (rpx * a.rby) + (a.syr + j) * rpx + (RX + a.sxr + x0);
         gbase = 0;
     } else {
         rbase = 0;
@@ -426,7 +446,7 @@ template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
 static size_t smem_bytes_for(const TileArgs& a) {
     using G = TileGeom<RX, RY, RZ, TZ>;
     size_t pb = round_up32(a.pbx * a.pby * a.pbz);
-    size_t rb = RAW_SMEM ? round_up32(a.rbx * a.rby * a.rbz) : 0;
+    size_t rb = RAW_SMEM ? round_up32((a.rbx + 1) * a.rby * a.rbz) : 0;
     size_t d = round_up32(G::DPLANE * G::DD);
     return 128 + 4 * (pb + rb + 2 * d);
 }
@@ -537,3 +557,4 @@ cudaError_t launch_sigma_blend(const float* sigma0, float* sigma1, float alpha, 
 }
 
 }  // namespace inlm
+
