@@ -54,7 +54,8 @@ extern "C" {
 
 /* storage / arithmetic form of the filter */
 #define INLM_PRECISION_F32 0   /* FP32, bit-identical to the reference CPU filter */
-#define INLM_PRECISION_F16 1   /* FP16 storage, FP32 accumulation */
+#define INLM_PRECISION_F16 1   /* FP16 volumes and squared-difference planes, FP32 accumulation */
+#define INLM_PRECISION_F16_DF32 2 /* FP16 volumes, FP32 squared-difference planes */
 
 /* patch-weight table */
 #define INLM_WEIGHTS_CPU 0        /* the table the reference CPU filter applies (default) */
@@ -137,6 +138,19 @@ int inlm_filter_kernel_ms(inlm_denoiser* d, double* avg_ms, int* n_launches);
 
 /* Description of the chosen filter kernel (name, tile, taps, offsets). */
 int inlm_describe(inlm_denoiser* d, char* buf, size_t len);
+
+/* Tiling of the filter kernel: tile_shape = voxels per tile {x, y, z},
+ * tiles = tile counts {x, y, z}; tile index = (tz*tiles[1] + ty)*tiles[0] + tx. */
+int inlm_tile_grid(inlm_denoiser* d, int tile_shape[3], int tiles[3]);
+
+/* Per-tile offset plan for the FP16 form (the learned proposal's output):
+ * tile c evaluates the search offsets offsets[start[c] .. start[c]+count[c])
+ * (indices into the reference-order search table, in the order given).
+ * start and count have n_tiles entries, offsets n_offsets; on_device = 1 when
+ * the three arrays are device memory (they are copied). start == NULL
+ * returns to full search. */
+int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const int* count, const int* offsets,
+                         int n_offsets, int on_device);
 
 /* Number of kernels this handle has launched since creation. */
 int inlm_kernel_launches(inlm_denoiser* d, uint64_t* count);

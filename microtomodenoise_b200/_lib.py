@@ -21,7 +21,7 @@ ERRORS = {
     -7: "INLM_ERR_UNSUPPORTED",
 }
 NOISE_MODES = {"z-adaptive": 0, "auto": 0, "global": 1, "manual": 2, "semimanual": 3}
-PRECISIONS = {"f32": 0, "f16": 1}
+PRECISIONS = {"f32": 0, "f16": 1, "f16_df32": 2}
 
 # Every entry point include/inlm.h declares.
 EXPORTS = (
@@ -31,6 +31,7 @@ EXPORTS = (
     "inlm_describe", "inlm_noise_create", "inlm_noise_destroy", "inlm_noise_estimate",
     "inlm_noise_samples", "inlm_noise_patchstd", "inlm_geometry", "inlm_noise_draw_samples",
     "inlm_kernel_launches", "inlm_probe_fp32_peak", "inlm_noise_em_noalloc",
+    "inlm_tile_grid", "inlm_set_offset_plan",
 )
 
 
@@ -103,6 +104,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.inlm_noise_draw_samples.argtypes = [C.c_int * 3, C.c_uint64, C.c_int, C.c_int, C.c_uint, vp]
     L.inlm_kernel_launches.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.inlm_probe_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.inlm_tile_grid.argtypes = [vp, C.c_int * 3, C.c_int * 3]
+    L.inlm_set_offset_plan.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int]
     L.inlm_noise_em_noalloc.argtypes = [vp, vp, C.c_int64, vp, C.c_int, vp, vp]
     for name in EXPORTS:
         if name not in ("inlm_last_error", "inlm_default_params"):

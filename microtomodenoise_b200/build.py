@@ -34,6 +34,7 @@ NVCC_FLAGS = ARCH + [
 
 LIB_SOURCES = [
     "filter_kernels.cu",
+    "filter_fast.cu",
     "probe.cu",
     "noise_kernels.cu",
     "api.cu",

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/inlm.h"
+#include "filter_fast.cuh"
 #include "filter_kernels.cuh"
 #include "geometry.hpp"
 #include "noise_kernels.cuh"
@@ -104,15 +105,17 @@ static PFN_encodeTiled get_encode_fn() {
 }
 
 // 3D float32 map over a padded volume (pitch in elements), box (bx,by,bz).
-static int encode_map_3d(CUtensorMap* tm, const float* base, int ex, int ey, int ez,
-                         long long pitch_y, long long pitch_z, int bx, int by, int bz) {
+static int encode_map_3d(CUtensorMap* tm, const void* base, int ex, int ey, int ez,
+                         long long pitch_y, long long pitch_z, int bx, int by, int bz,
+                         int esize = 4) {
     PFN_encodeTiled enc = get_encode_fn();
     if (!enc) return fail(INLM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     cuuint64_t dims[3] = {(cuuint64_t)ex, (cuuint64_t)ey, (cuuint64_t)ez};
-    cuuint64_t strides[2] = {(cuuint64_t)pitch_y * 4, (cuuint64_t)pitch_z * 4};
+    cuuint64_t strides[2] = {(cuuint64_t)pitch_y * esize, (cuuint64_t)pitch_z * esize};
     cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
     cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, dims, strides, box, estr,
+    CUresult r = enc(tm, esize == 2 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                     3, (void*)base, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(INLM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -384,6 +387,16 @@ struct inlm_denoiser {
     long long* d_patch_off = nullptr;
     float* d_weights = nullptr;
     bool use_tile = false;
+    bool use_fast = false;       // FP16-storage kernel
+    FastConfig fcfg{};
+    FastArgs fargs{};
+    void* d_raw_h = nullptr;     // padded FP16 raw / previous iterate
+    void* d_prev_h = nullptr;
+    CUtensorMap tm_prev_h{};
+    int* d_plan_start = nullptr;  // per-CTA offset lists (learned proposal)
+    int* d_plan_off = nullptr;
+    int plan_cap = 0;
+    int n_cta = 0;
     TileConfig tcfg{};
     TileArgs targs{};
     GenericArgs gargs{};
@@ -421,6 +434,10 @@ static void denoiser_free(inlm_denoiser* d) {
     cudaFree(d->d_search_off);
     cudaFree(d->d_patch_off);
     cudaFree(d->d_weights);
+    cudaFree(d->d_raw_h);
+    cudaFree(d->d_prev_h);
+    cudaFree(d->d_plan_start);
+    cudaFree(d->d_plan_off);
     if (d->noise) {
         noise_free(d->noise);
         delete d->noise;
@@ -508,6 +525,83 @@ static int choose_tile_config(inlm_denoiser* d) {
     return INLM_OK;
 }
 
+// FP16-storage kernel configuration (same tile decomposition as the FP32
+// kernel; prev box in halves, raw staged as FP32 with an odd pitch).
+static int choose_fast_config(inlm_denoiser* d) {
+    const Geometry& g = d->geo;
+    const int* pr = g.patch_radius;
+    d->use_fast = false;
+    if (!tile_kernel_available(pr[0], pr[1], pr[2])) return INLM_OK;
+    if (d->p.nslices / 2 < pr[2]) return INLM_OK;
+    if ((int)g.taps.size() > kMaxTaps) return INLM_OK;
+    std::vector<int> order(3 * kMaxTaps);
+    int nt = tile_kernel_tap_order(pr[0], pr[1], pr[2], order.data(), kMaxTaps);
+    if (nt != (int)g.taps.size()) return INLM_OK;
+    for (int t = 0; t < nt; t++)
+        if (order[3 * t] != g.taps[t].x || order[3 * t + 1] != g.taps[t].y ||
+            order[3 * t + 2] != g.taps[t].z)
+            return INLM_OK;
+    FastArgs& a = d->fargs;
+    a.nx = d->shape[0];
+    a.ny = d->shape[1];
+    a.nz = d->shape[2];
+    a.px = g.pad[0];
+    a.py = g.pad[1];
+    a.pz = g.pad[2];
+    a.sxr = g.search_radius[0];
+    a.syr = g.search_radius[1];
+    a.szc = std::min(d->p.nslices / 2, g.search_radius[2]);
+    a.S = (int)g.search.size();
+    a.gpitch_y = d->pitch_y;
+    a.gpitch_z = d->pitch_z;
+    a.pbx = (kTX + 2 * a.px + 7) / 8 * 8;  // halves, 16-byte TMA rows
+    a.pby = kTY + 2 * a.py;
+    a.rbx = (pr[0] + kTX + 2 * a.sxr + 3) / 4 * 4;
+    a.rby = kTY + 2 * a.syr;
+    for (int t = 0; t < nt; t++) a.w[t] = g.weights[t];
+    int smem_max = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
+    const bool dh = d->p.precision == INLM_PRECISION_F16;
+    const int tzs[] = {8, 4};
+    for (int tz : tzs) {
+        if (tz == 4 && !dh) continue;
+        a.pbz = tz + 2 * a.pz;
+        a.rbz = tz + 2 * a.szc;
+        if (a.pbx > 256 || a.pby > 256 || a.pbz > 256) continue;
+        if ((long long)a.pbx * a.pby * a.pbz >= (1ll << 24)) continue;
+        FastConfig fc{pr[0], pr[1], pr[2], tz, dh, 0};
+        size_t sm = fast_smem_bytes(fc, a);
+        if (sm == 0 || sm > (size_t)smem_max) continue;
+        fc.smem_bytes = sm;
+        d->fcfg = fc;
+        d->use_fast = true;
+        break;
+    }
+    if (!d->use_fast) return INLM_OK;
+    a.tiles_x = (d->shape[0] + kTX - 1) / kTX;
+    a.tiles_y = (d->shape[1] + kTY - 1) / kTY;
+    d->n_cta = a.tiles_x * a.tiles_y * ((d->shape[2] + d->fcfg.tz - 1) / d->fcfg.tz);
+    std::vector<int2> dl(a.S);
+    const int rpx = a.rbx + 1;
+    for (int si = 0; si < a.S; si++) {
+        const Offset3& o = g.search[si];
+        dl[si].x = o.z * a.pbx * a.pby + o.y * a.pbx + o.x;
+        dl[si].y = o.z * rpx * a.rby + o.y * rpx + o.x;
+    }
+    CUDA_TRY(dalloc(&d->d_search_delta, a.S));
+    CUDA_TRY(cudaMemcpy(d->d_search_delta, dl.data(), a.S * sizeof(int2), cudaMemcpyHostToDevice));
+    a.search_delta = d->d_search_delta;
+    a.plan_offsets = nullptr;
+    a.plan_start = nullptr;
+    a.plan_count = nullptr;
+    a.raw_pad = (const __half*)d->d_raw_h;
+    a.out = d->d_next;
+    a.mult = d->d_mult;
+    a.err = d->d_err;
+    return encode_map_3d(&d->tm_prev_h, d->d_prev_h, d->nxp, d->nyp, d->nzp, d->pitch_y, d->pitch_z,
+                         a.pbx, a.pby, a.pbz, 2);
+}
+
 extern "C" int inlm_denoiser_create(const int shape[3], const inlm_params* p, inlm_denoiser** out) {
     if (!shape || !p || !out) return fail(INLM_ERR_ARG, "null argument");
     *out = nullptr;
@@ -521,8 +615,9 @@ extern "C" int inlm_denoiser_create(const int shape[3], const inlm_params* p, in
             return fail(INLM_ERR_ARG, "radii must be >= 0");
     }
     if (p->nslices < 1) return fail(INLM_ERR_ARG, "nslices must be >= 1");
-    if (p->precision != INLM_PRECISION_F32)
-        return fail(INLM_ERR_UNSUPPORTED, "precision %d not available in this build", p->precision);
+    const bool f16 = p->precision == INLM_PRECISION_F16 || p->precision == INLM_PRECISION_F16_DF32;
+    if (p->precision != INLM_PRECISION_F32 && !f16)
+        return fail(INLM_ERR_ARG, "unknown precision %d", p->precision);
 
     inlm_denoiser* d = new inlm_denoiser();
     d->p = *p;
@@ -563,52 +658,69 @@ extern "C" int inlm_denoiser_create(const int shape[3], const inlm_params* p, in
     cudaError_t e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(fail(INLM_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
     d->own_stream = true;
-    if (dalloc(&d->d_raw_pad, npad) != cudaSuccess || dalloc(&d->d_prev_pad, npad) != cudaSuccess ||
-        dalloc(&d->d_next, nvox) != cudaSuccess || dalloc(&d->d_sigma, shape[2]) != cudaSuccess ||
+    if (dalloc(&d->d_next, nvox) != cudaSuccess || dalloc(&d->d_sigma, shape[2]) != cudaSuccess ||
         dalloc(&d->d_sigma0, shape[2]) != cudaSuccess || dalloc(&d->d_mult, shape[2]) != cudaSuccess ||
-        dalloc(&d->d_err, 1) != cudaSuccess)
-        return bail(fail(INLM_ERR_NOMEM, "device allocation of %.2f GB failed",
-                         (2.0 * npad + nvox) * 4 / 1e9));
-    // pitch padding columns stay zero
-    if (cudaMemset(d->d_raw_pad, 0, npad * 4) != cudaSuccess ||
-        cudaMemset(d->d_prev_pad, 0, npad * 4) != cudaSuccess ||
-        cudaMemset(d->d_err, 0, 4) != cudaSuccess)
-        return bail(fail(INLM_ERR_CUDA, "memset failed"));
-    // generic-kernel tables (padded-linear offsets)
-    {
-        std::vector<long long> so(g.search.size()), po(g.taps.size());
-        for (size_t s = 0; s < g.search.size(); s++)
-            so[s] = g.search[s].z * d->pitch_z + g.search[s].y * d->pitch_y + g.search[s].x;
-        for (size_t q = 0; q < g.taps.size(); q++)
-            po[q] = g.taps[q].z * d->pitch_z + g.taps[q].y * d->pitch_y + g.taps[q].x;
-        if (dalloc(&d->d_search_off, so.size()) != cudaSuccess ||
-            dalloc(&d->d_patch_off, po.size()) != cudaSuccess ||
-            dalloc(&d->d_weights, g.weights.size()) != cudaSuccess)
-            return bail(fail(INLM_ERR_NOMEM, "table allocation"));
-        cudaMemcpy(d->d_search_off, so.data(), so.size() * 8, cudaMemcpyHostToDevice);
-        cudaMemcpy(d->d_patch_off, po.data(), po.size() * 8, cudaMemcpyHostToDevice);
-        cudaMemcpy(d->d_weights, g.weights.data(), g.weights.size() * 4, cudaMemcpyHostToDevice);
-        GenericArgs& ga = d->gargs;
-        ga.nx = shape[0];
-        ga.ny = shape[1];
-        ga.nz = shape[2];
-        ga.px = g.pad[0];
-        ga.py = g.pad[1];
-        ga.pz = g.pad[2];
-        ga.gpitch_y = d->pitch_y;
-        ga.gpitch_z = d->pitch_z;
-        ga.S = (int)g.search.size();
-        ga.P = (int)g.taps.size();
-        ga.search_off = d->d_search_off;
-        ga.patch_off = d->d_patch_off;
-        ga.weights = d->d_weights;
-        ga.raw_pad = d->d_raw_pad;
-        ga.prev_pad = d->d_prev_pad;
-        ga.out = d->d_next;
-        ga.mult = d->d_mult;
+        dalloc(&d->d_err, 1) != cudaSuccess || cudaMemset(d->d_err, 0, 4) != cudaSuccess)
+        return bail(fail(INLM_ERR_NOMEM, "device allocation failed"));
+    if (f16) {
+        if (cudaMalloc(&d->d_raw_h, npad * 2) != cudaSuccess ||
+            cudaMalloc(&d->d_prev_h, npad * 2) != cudaSuccess)
+            return bail(fail(INLM_ERR_NOMEM, "device allocation of %.2f GB failed",
+                             (2.0 * npad * 2 + nvox * 4) / 1e9));
+        if (cudaMemset(d->d_raw_h, 0, npad * 2) != cudaSuccess ||
+            cudaMemset(d->d_prev_h, 0, npad * 2) != cudaSuccess)
+            return bail(fail(INLM_ERR_CUDA, "memset failed"));
+        rc = choose_fast_config(d);
+        if (rc != INLM_OK) return bail(rc);
+        if (!d->use_fast)
+            return bail(fail(INLM_ERR_UNSUPPORTED,
+                             "the FP16 form covers patch radii (1,1,1) (1,1,2) (1,1,3) (2,2,1) "
+                             "(2,2,2) (3,3,1) (3,3,2) (3,3,3) with nslices/2 >= z radius"));
+    } else {
+        if (dalloc(&d->d_raw_pad, npad) != cudaSuccess || dalloc(&d->d_prev_pad, npad) != cudaSuccess)
+            return bail(fail(INLM_ERR_NOMEM, "device allocation of %.2f GB failed",
+                             (2.0 * npad + nvox) * 4 / 1e9));
+        // pitch padding columns stay zero
+        if (cudaMemset(d->d_raw_pad, 0, npad * 4) != cudaSuccess ||
+            cudaMemset(d->d_prev_pad, 0, npad * 4) != cudaSuccess)
+            return bail(fail(INLM_ERR_CUDA, "memset failed"));
+        // generic-kernel tables (padded-linear offsets)
+        {
+            std::vector<long long> so(g.search.size()), po(g.taps.size());
+            for (size_t s = 0; s < g.search.size(); s++)
+                so[s] = g.search[s].z * d->pitch_z + g.search[s].y * d->pitch_y + g.search[s].x;
+            for (size_t q = 0; q < g.taps.size(); q++)
+                po[q] = g.taps[q].z * d->pitch_z + g.taps[q].y * d->pitch_y + g.taps[q].x;
+            if (dalloc(&d->d_search_off, so.size()) != cudaSuccess ||
+                dalloc(&d->d_patch_off, po.size()) != cudaSuccess ||
+                dalloc(&d->d_weights, g.weights.size()) != cudaSuccess)
+                return bail(fail(INLM_ERR_NOMEM, "table allocation"));
+            cudaMemcpy(d->d_search_off, so.data(), so.size() * 8, cudaMemcpyHostToDevice);
+            cudaMemcpy(d->d_patch_off, po.data(), po.size() * 8, cudaMemcpyHostToDevice);
+            cudaMemcpy(d->d_weights, g.weights.data(), g.weights.size() * 4, cudaMemcpyHostToDevice);
+            GenericArgs& ga = d->gargs;
+            ga.nx = shape[0];
+            ga.ny = shape[1];
+            ga.nz = shape[2];
+            ga.px = g.pad[0];
+            ga.py = g.pad[1];
+            ga.pz = g.pad[2];
+            ga.gpitch_y = d->pitch_y;
+            ga.gpitch_z = d->pitch_z;
+            ga.S = (int)g.search.size();
+            ga.P = (int)g.taps.size();
+            ga.search_off = d->d_search_off;
+            ga.patch_off = d->d_patch_off;
+            ga.weights = d->d_weights;
+            ga.raw_pad = d->d_raw_pad;
+            ga.prev_pad = d->d_prev_pad;
+            ga.out = d->d_next;
+            ga.mult = d->d_mult;
+        }
+
+        rc = choose_tile_config(d);
+        if (rc != INLM_OK) return bail(rc);
     }
-    rc = choose_tile_config(d);
-    if (rc != INLM_OK) return bail(rc);
     if (shape[0] > p->noise_patchsize && shape[1] > p->noise_patchsize && p->n_samples > 0) {
         rc = inlm_noise_create(shape, p->n_samples, p->noise_patchsize, p->noise_seed, d->device,
                                &d->noise);
@@ -673,7 +785,10 @@ static int launch_filter(inlm_denoiser* d) {
         CUDA_TRY(cudaEventCreate(&t.b));
     }
     CUDA_TRY(cudaEventRecord(t.a, d->stream));
-    if (d->use_tile) {
+    if (d->use_fast) {
+        int tiles_z = (d->shape[2] + d->fcfg.tz - 1) / d->fcfg.tz;
+        CUDA_TRY(launch_fast_kernel(d->fcfg, &d->tm_prev_h, d->fargs, tiles_z, d->stream));
+    } else if (d->use_tile) {
         int tiles_z = (d->shape[2] + d->tcfg.tz - 1) / d->tcfg.tz;
         CUDA_TRY(launch_tile_kernel(d->tcfg, &d->tm_prev, &d->tm_raw, d->targs, tiles_z, d->stream));
     } else {
@@ -681,6 +796,15 @@ static int launch_filter(inlm_denoiser* d) {
     }
     CUDA_TRY(cudaEventRecord(t.b, d->stream));
     d->pending.push_back(t);
+    d->launches++;
+    return INLM_OK;
+}
+
+// Pads the unpadded volume `src` (device) into the FP16 padded buffer `dst`.
+static int pad_into_half(inlm_denoiser* d, const float* src, void* dst) {
+    const Geometry& g = d->geo;
+    CUDA_TRY(launch_pad_reflective_half(src, d->shape[0], d->shape[1], d->shape[2], dst, g.pad[0],
+                                        g.pad[1], g.pad[2], d->pitch_y, d->pitch_z, d->stream));
     d->launches++;
     return INLM_OK;
 }
@@ -711,6 +835,23 @@ static int enqueue_iteration(inlm_denoiser* d, int iter, const float* raw_dev) {
     if (iter < 1) return fail(INLM_ERR_ARG, "iteration must be >= 1");
     if (!d->sigma_set) return fail(INLM_ERR_STATE, "set_sigma before running an iteration");
     int rc;
+    if (d->use_fast) {
+        if (iter == 1) {
+            if (!raw_dev) return fail(INLM_ERR_ARG, "iteration 1 needs the raw volume");
+            rc = pad_into_half(d, raw_dev, d->d_raw_h);
+            if (rc) return rc;
+            CUDA_TRY(cudaMemcpyAsync(d->d_prev_h, d->d_raw_h, d->pitch_z * d->nzp * 2,
+                                     cudaMemcpyDeviceToDevice, d->stream));
+        } else {
+            if (d->last_iter < 1) return fail(INLM_ERR_STATE, "iteration %d before iteration 1", iter);
+            rc = pad_into_half(d, d->d_next, d->d_prev_h);
+            if (rc) return rc;
+        }
+        rc = launch_filter(d);
+        if (rc) return rc;
+        d->last_iter = iter;
+        return INLM_OK;
+    }
     if (iter == 1) {
         if (!raw_dev) return fail(INLM_ERR_ARG, "iteration 1 needs the raw volume");
         rc = pad_into(d, raw_dev, d->d_raw_pad);
@@ -875,7 +1016,13 @@ extern "C" int inlm_filter_kernel_ms(inlm_denoiser* d, double* avg_ms, int* n_la
 extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
     if (!d || !buf) return fail(INLM_ERR_ARG, "null argument");
     const Geometry& g = d->geo;
-    if (d->use_tile)
+    if (d->use_fast)
+        snprintf(buf, len,
+                 "nlm_tile_fast<%d,%d,%d> tz=%d d_planes=%s smem=%zu S=%zu P=%zu plan=%s pad=%d,%d,%d",
+                 d->fcfg.rx, d->fcfg.ry, d->fcfg.rz, d->fcfg.tz, d->fcfg.d_half ? "f16" : "f32",
+                 d->fcfg.smem_bytes, g.search.size(), g.taps.size(),
+                 d->fargs.plan_start ? "per-tile" : "full", g.pad[0], g.pad[1], g.pad[2]);
+    else if (d->use_tile)
         snprintf(buf, len,
                  "nlm_tile_f32<%d,%d,%d> tz=%d raw_%s smem=%zu S=%zu P=%zu weights=%s pad=%d,%d,%d",
                  d->tcfg.rx, d->tcfg.ry, d->tcfg.rz, d->tcfg.tz, d->tcfg.raw_smem ? "smem" : "global",
@@ -975,3 +1122,62 @@ extern "C" int inlm_noise_em_noalloc(void* stream, const float* values_dev, int6
     return INLM_OK;
 }
 
+
+// ---------------- per-tile offset plans ----------------
+
+extern "C" int inlm_tile_grid(inlm_denoiser* d, int tile_shape[3], int tiles[3]) {
+    if (!d) return fail(INLM_ERR_ARG, "null handle");
+    int tz = d->use_fast ? d->fcfg.tz : (d->use_tile ? d->tcfg.tz : 1);
+    if (tile_shape) {
+        tile_shape[0] = kTX;
+        tile_shape[1] = kTY;
+        tile_shape[2] = tz;
+    }
+    if (tiles) {
+        tiles[0] = (d->shape[0] + kTX - 1) / kTX;
+        tiles[1] = (d->shape[1] + kTY - 1) / kTY;
+        tiles[2] = (d->shape[2] + tz - 1) / tz;
+    }
+    return INLM_OK;
+}
+
+extern "C" int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const int* count,
+                                    const int* offsets, int n_offsets, int on_device) {
+    if (!d) return fail(INLM_ERR_ARG, "null handle");
+    if (!d->use_fast) return fail(INLM_ERR_UNSUPPORTED, "offset plans need the FP16 form");
+    CUDA_TRY(cudaSetDevice(d->device));
+    if (!start) {
+        d->fargs.plan_start = nullptr;
+        d->fargs.plan_count = nullptr;
+        d->fargs.plan_offsets = nullptr;
+        return INLM_OK;
+    }
+    if (!count || !offsets || n_offsets < 0) return fail(INLM_ERR_ARG, "null plan array");
+    const int n = d->n_cta;
+    if (!on_device) {
+        for (int c = 0; c < n; c++)
+            if (start[c] < 0 || count[c] < 0 || count[c] > d->fargs.S ||
+                (long long)start[c] + count[c] > n_offsets)
+                return fail(INLM_ERR_ARG, "plan tile %d has a bad offset range", c);
+        for (int i = 0; i < n_offsets; i++)
+            if (offsets[i] < 0 || offsets[i] >= d->fargs.S)
+                return fail(INLM_ERR_ARG, "plan offset %d out of range", offsets[i]);
+    }
+    if (!d->d_plan_start) CUDA_TRY(dalloc(&d->d_plan_start, 2 * (size_t)n));
+    if (d->plan_cap < std::max(n_offsets, 1)) {
+        cudaFree(d->d_plan_off);
+        d->d_plan_off = nullptr;
+        d->plan_cap = 0;
+        CUDA_TRY(dalloc(&d->d_plan_off, (size_t)std::max(n_offsets, 1)));
+        d->plan_cap = std::max(n_offsets, 1);
+    }
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CUDA_TRY(cudaMemcpyAsync(d->d_plan_start, start, (size_t)n * 4, kind, d->stream));
+    CUDA_TRY(cudaMemcpyAsync(d->d_plan_start + n, count, (size_t)n * 4, kind, d->stream));
+    CUDA_TRY(cudaMemcpyAsync(d->d_plan_off, offsets, (size_t)n_offsets * 4, kind, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    d->fargs.plan_start = d->d_plan_start;
+    d->fargs.plan_count = d->d_plan_start + n;
+    d->fargs.plan_offsets = d->d_plan_off;
+    return INLM_OK;
+}

@@ -1,0 +1,359 @@
+// FP16-storage form of the iterNLM filter (sm_100a).
+//
+// Same algorithm as the FP32 kernel (filter_kernels.cu) with the precision
+// split the fast form uses:
+//   * the padded raw and previous-iterate volumes are FP16 in HBM and in
+//     shared memory (the previous-iterate box arrives by one 3D TMA load), so
+//     two CTAs (16 warps) share an SM;
+//   * squared differences D = (prev(.+s) - prev(.))^2 are formed in FP32 and
+//     kept in shared memory as FP16 (D_HALF) or FP32, scaled by the tile's
+//     1/sigma^2 so FP16 holds them in its normal range;
+//   * patch distances, Pade weights, weighted sums and weight sums accumulate
+//     in FP32 with fused multiply-adds;
+//   * the final per-voxel normalisation (acc + wmax*raw)/(wsum + wmax) is FP64.
+// Offsets: every search offset, or a per-CTA list (the learned proposal's
+// top-K for the tile).
+#include <cuda_fp16.h>
+
+#include "common.cuh"
+#include "filter_fast.cuh"
+#include "tile_common.cuh"
+
+namespace inlm {
+
+// D row pitch for FP16 planes: a multiple of 8 halves (16-byte rows) with an
+// odd number of 16-byte chunks, so the warp's row reads spread evenly over
+// the bank groups.
+constexpr int dpitch_h(int w) {
+    int p = (w + 7) / 8 * 8;
+    return ((p / 8) % 2 == 0) ? p + 8 : p;
+}
+
+template <int RX, int RY, int RZ, int TZ, bool D_HALF>
+struct FastGeom {
+    using G = TileGeom<RX, RY, RZ, TZ>;
+    static constexpr int DP = D_HALF ? dpitch_h(G::DW) : G::DP;  // elements
+    static constexpr int DPLANE = DP * G::DH;
+    static constexpr int DSZ = D_HALF ? (DPLANE * G::DD + 63) / 64 * 64
+                                      : round_up32(DPLANE * G::DD);  // elements
+    static constexpr int DBYTES = DSZ * (D_HALF ? 2 : 4);
+};
+
+// 16-value window of one D row (columns [x0, x0+16)) as FP32.
+template <bool D_HALF, int LO, int HI>
+__device__ __forceinline__ void load_row(const void* rowp, float (&win)[16]) {
+    if constexpr (D_HALF) {
+        // halves: columns [8c, 8c+8) per 16-byte chunk; convert the span used
+#pragma unroll
+        for (int c = LO / 8; c <= HI / 8; c++) {
+            uint4 v = reinterpret_cast<const uint4*>(rowp)[c];
+            const __half2* h = reinterpret_cast<const __half2*>(&v);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int i0 = 8 * c + 2 * q;
+                if (i0 + 1 >= LO && i0 <= HI) {
+                    float2 f = __half22float2(h[q]);
+                    win[i0] = f.x;
+                    win[i0 + 1] = f.y;
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int c = LO / 4; c <= HI / 4; c++) {
+            float4 v = reinterpret_cast<const float4*>(rowp)[c];
+            win[4 * c + 0] = v.x;
+            win[4 * c + 1] = v.y;
+            win[4 * c + 2] = v.z;
+            win[4 * c + 3] = v.w;
+        }
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ, bool D_HALF, int RI>
+__device__ __forceinline__ void fast_rows(const unsigned char* __restrict__ Db, int rowoff,
+                                          float (&dist)[kVoxPerThread], const FastArgs& a) {
+    using G = TileGeom<RX, RY, RZ, TZ>;
+    using F = FastGeom<RX, RY, RZ, TZ, D_HALF>;
+    if constexpr (RI < G::rows.n) {
+        constexpr int zp = G::rows.zp[RI];
+        constexpr int yp = G::rows.yp[RI];
+        constexpr int e = G::rows.e[RI];
+        constexpr int first = RowFirst<RX, RY, RZ, RI>::value;
+        constexpr int esz = D_HALF ? 2 : 4;
+        const unsigned char* rowp =
+            Db + (size_t)(rowoff + (zp + RZ) * F::DPLANE + (yp + RY) * F::DP) * esz;
+        float win[16];
+        load_row<D_HALF, RX - e, RX + kVoxPerThread - 1 + e>(rowp, win);
+#pragma unroll
+        for (int xp = -e; xp <= e; xp++) {
+            if (zp == 0 && yp == 0 && xp == 0) continue;
+            const int t = first + (xp + e) - ((zp == 0 && yp == 0 && xp > 0) ? 1 : 0);
+            const float w = a.w[t];
+#pragma unroll
+            for (int r = 0; r < kVoxPerThread; r++) dist[r] = fmaf(win[RX + r + xp], w, dist[r]);
+        }
+        fast_rows<RX, RY, RZ, TZ, D_HALF, RI + 1>(Db, rowoff, dist, a);
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ, bool D_HALF>
+__global__ void __launch_bounds__(32 * TZ, 2)
+    nlm_tile_fast_kernel(const __grid_constant__ CUtensorMap tm_prev,
+                         const __grid_constant__ FastArgs a) {
+    using G = TileGeom<RX, RY, RZ, TZ>;
+    using F = FastGeom<RX, RY, RZ, TZ, D_HALF>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+    __half* prevb = reinterpret_cast<__half*>(smem + 128);
+    const int pplane = a.pbx * a.pby;
+    const int PB = pplane * a.pbz;  // halves
+    __half* rawb = reinterpret_cast<__half*>(smem + 128 + (size_t)(PB + 63) / 64 * 128);
+    const int rpx = a.rbx + 1;
+    const int RB = rpx * a.rby * a.rbz;  // halves
+    unsigned char* D0 = reinterpret_cast<unsigned char*>(rawb) + (size_t)(RB + 63) / 64 * 128;
+
+    const int tid = threadIdx.x;
+    const int X0 = blockIdx.x * kTX;
+    const int Y0 = blockIdx.y * kTY;
+    const int Z0 = blockIdx.z * TZ;
+    const int cta = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+
+    if (tid == 0) {
+        prefetch_tmap(&tm_prev);
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)PB * 2u);
+        tma_load_3d(prevb, &tm_prev, X0, Y0, Z0, bar);
+    }
+    {
+        // raw over tile + search halo (FP16), odd row pitch
+        const int rb_n = a.rbx * a.rby * a.rbz;
+        const __half* rsrc = a.raw_pad + (long long)(Z0 + RZ) * a.gpitch_z +
+                             (long long)(Y0 + RY) * a.gpitch_y + X0;
+        for (int i = tid; i < rb_n; i += G::NT) {
+            int xx = i % a.rbx;
+            int rest = i / a.rbx;
+            int yy = rest % a.rby;
+            int zz = rest / a.rby;
+            rawb[(zz * a.rby + yy) * rpx + xx] =
+                rsrc[(long long)zz * a.gpitch_z + (long long)yy * a.gpitch_y + xx];
+        }
+    }
+
+    // offsets of this CTA: all, or its list
+    int s_begin = 0, s_count = a.S;
+    if (a.plan_start) {
+        s_begin = a.plan_start[cta];
+        s_count = min(a.plan_count[cta], a.S);
+    }
+
+    // scale D by 1/sigma^2 of the tile's middle slice (FP16 normal range)
+    const float scale = -a.mult[min(Z0 + TZ / 2, a.nz - 1)];
+
+    constexpr int NPAIR = G::ND / 2;
+    constexpr int NQ = (NPAIR + G::NT - 1) / G::NT;
+    int qpi[NQ], qdi[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; k++) {
+        int q = min(tid + k * G::NT, NPAIR - 1);
+        int f = 2 * q;
+        int c = f % G::DW;
+        int rest = f / G::DW;
+        int r = rest % G::DH;
+        int p = rest / G::DH;
+        qpi[k] = (p - RZ + a.pz) * pplane + (r - RY + a.py) * a.pbx + (c - RX + a.px);
+        qdi[k] = p * F::DPLANE + r * F::DP + c;
+    }
+    if (!mbar_wait_bounded(bar, 0)) {
+        set_error(a.err, DEV_TMA_TIMEOUT);
+        return;
+    }
+    float og0[NQ], og1[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; k++) {
+        og0[k] = __half2float(prevb[qpi[k]]);
+        og1[k] = __half2float(prevb[qpi[k] + 1]);
+    }
+
+    auto phase_a = [&](unsigned char* Dw, int dlx) {
+#pragma unroll
+        for (int k = 0; k < NQ; k++) {
+            float t0 = __half2float(prevb[qpi[k] + dlx]) - og0[k];
+            float t1 = __half2float(prevb[qpi[k] + dlx + 1]) - og1[k];
+            float d0 = (t0 * scale) * t0, d1 = (t1 * scale) * t1;
+            if constexpr (D_HALF) {
+                reinterpret_cast<__half2*>(Dw)[qdi[k] / 2] = __floats2half2_rn(d0, d1);
+            } else {
+                reinterpret_cast<float2*>(Dw)[qdi[k] / 2] = make_float2(d0, d1);
+            }
+        }
+    };
+
+    const int warp = tid >> 5, lane = tid & 31;
+    const int k = warp;
+    const int j = lane >> 2;
+    const int x0 = (lane & 3) * kVoxPerThread;
+    const int zk = min(Z0 + k, a.nz - 1);
+    const float rel = a.mult[zk] / scale;  // x = dist' * rel
+    const int rowoff = k * F::DPLANE + j * F::DP + x0;
+    const int rbase = (a.szc + k) * (rpx * a.rby) + (a.syr + j) * rpx + (RX + a.sxr + x0);
+
+    float acc[kVoxPerThread], wsum[kVoxPerThread], wmax[kVoxPerThread];
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) acc[r] = wsum[r] = wmax[r] = 0.0f;
+
+    if (s_count > 0) {
+        int sidx = a.plan_offsets ? a.plan_offsets[s_begin] : 0;
+        int2 dl = __ldg(&a.search_delta[sidx]);
+        phase_a(D0, dl.x);
+        __syncthreads();
+        for (int i = 0; i < s_count; i++) {
+            const unsigned char* Dr = D0 + (size_t)(i & 1) * F::DBYTES;
+            const int dly = dl.y;
+            if (i + 1 < s_count) {
+                sidx = a.plan_offsets ? a.plan_offsets[s_begin + i + 1] : i + 1;
+                dl = __ldg(&a.search_delta[sidx]);
+                phase_a(D0 + (size_t)((i + 1) & 1) * F::DBYTES, dl.x);
+            }
+            float dist[kVoxPerThread];
+            {
+                float win[16];
+                constexpr int esz = D_HALF ? 2 : 4;
+                load_row<D_HALF, RX, RX + kVoxPerThread - 1>(
+                    Dr + (size_t)(rowoff + RZ * F::DPLANE + RY * F::DP) * esz, win);
+                const float w0 = a.w[0];
+#pragma unroll
+                for (int r = 0; r < kVoxPerThread; r++) dist[r] = win[RX + r] * w0;
+            }
+            fast_rows<RX, RY, RZ, TZ, D_HALF, 0>(Dr, rowoff, dist, a);
+#pragma unroll
+            for (int r = 0; r < kVoxPerThread; r++) {
+                const float x = dist[r] * rel;
+                // Pade[3/3] of exp in Horner form, FMA
+                const float num = fmaf(fmaf(x + 12.f, x, 60.f), x, 120.f);
+                const float den = fmaf(fmaf(12.f - x, x, -60.f), x, 120.f);
+                const float w = (x > -3.56648f) ? __fdividef(num, den) : 0.0f;
+                const float rs = __half2float(rawb[rbase + dly + r]);
+                acc[r] = fmaf(w, rs, acc[r]);
+                wsum[r] += w;
+                wmax[r] = fmaxf(wmax[r], w);
+            }
+            __syncthreads();
+        }
+    }
+
+    const int z = Z0 + k, y = Y0 + j;
+    if (z < a.nz && y < a.ny) {
+        float* orow = a.out + ((long long)z * a.ny + y) * a.nx;
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) {
+            int x = X0 + x0 + r;
+            if (x < a.nx) {
+                const float raw0 = __half2float(rawb[rbase + r]);
+                float res = raw0;
+                if (wmax[r] > 0.0f) {
+                    // per-voxel weight-sum normalisation in FP64
+                    double num = (double)acc[r] + (double)wmax[r] * (double)raw0;
+                    double den = (double)wsum[r] + (double)wmax[r];
+                    res = (float)(num / den);
+                }
+                orow[x] = res;
+            }
+        }
+    }
+}
+
+// FP32 result -> padded FP16 volume (reflective), for raw and the previous iterate.
+__global__ void pad_reflective_half_kernel(const float* __restrict__ in, int nx, int ny, int nz,
+                                           __half* __restrict__ out, int px, int py, int pz,
+                                           long long pitch_y, long long pitch_z) {
+    const int nxp = nx + 2 * px, nyp = ny + 2 * py, nzp = nz + 2 * pz;
+    const long long total = (long long)nxp * nyp * nzp;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        int x1 = (int)(i % nxp);
+        long long r = i / nxp;
+        int y1 = (int)(r % nyp);
+        int z1 = (int)(r / nyp);
+        int x0 = x1 - px, y0 = y1 - py, z0 = z1 - pz;
+        for (int guard = 0; guard < 64 && (z0 < 0 || z0 >= nz || y0 < 0 || y0 >= ny || x0 < 0 ||
+                                           x0 >= nx);
+             guard++) {
+            if (z0 < 0) z0 = -z0;
+            if (y0 < 0) y0 = -y0;
+            if (x0 < 0) x0 = -x0;
+            if (z0 >= nz) z0 = 2 * nz - z0 - 2;
+            if (y0 >= ny) y0 = 2 * ny - y0 - 2;
+            if (x0 >= nx) x0 = 2 * nx - x0 - 2;
+        }
+        x0 = min(max(x0, 0), nx - 1);
+        y0 = min(max(y0, 0), ny - 1);
+        z0 = min(max(z0, 0), nz - 1);
+        out[z1 * pitch_z + y1 * pitch_y + x1] =
+            __float2half_rn(in[((long long)z0 * ny + y0) * nx + x0]);
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ, bool D_HALF>
+static size_t fast_smem_for(const FastArgs& a) {
+    using F = FastGeom<RX, RY, RZ, TZ, D_HALF>;
+    size_t pb = (size_t)(a.pbx * a.pby * a.pbz + 63) / 64 * 128;  // bytes
+    size_t rb = (size_t)((a.rbx + 1) * a.rby * a.rbz + 63) / 64 * 128;
+    return 128 + pb + rb + 2 * (size_t)F::DBYTES;
+}
+
+template <int RX, int RY, int RZ, int TZ, bool D_HALF>
+static cudaError_t fast_launch_inst(const CUtensorMap* tmp, const FastArgs& a, int tiles_z,
+                                    size_t smem, cudaStream_t st) {
+    auto kern = nlm_tile_fast_kernel<RX, RY, RZ, TZ, D_HALF>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
+    kern<<<grid, 32 * TZ, smem, st>>>(*tmp, a);
+    return cudaGetLastError();
+}
+
+#define INLM_FAST_SHAPES(X) \
+    X(1, 1, 1) X(1, 1, 2) X(1, 1, 3) X(2, 2, 1) X(2, 2, 2) X(3, 3, 1) X(3, 3, 2) X(3, 3, 3)
+
+size_t fast_smem_bytes(const FastConfig& c, const FastArgs& a) {
+#define X(A, B, C)                                                                 \
+    if (c.rx == A && c.ry == B && c.rz == C) {                                     \
+        if (c.tz == 8 && c.d_half) return fast_smem_for<A, B, C, 8, true>(a);      \
+        if (c.tz == 8 && !c.d_half) return fast_smem_for<A, B, C, 8, false>(a);    \
+        if (c.tz == 4 && c.d_half) return fast_smem_for<A, B, C, 4, true>(a);      \
+    }
+    INLM_FAST_SHAPES(X)
+#undef X
+    return 0;
+}
+
+cudaError_t launch_fast_kernel(const FastConfig& c, const CUtensorMap* tm_prev, const FastArgs& a,
+                               int tiles_z, cudaStream_t st) {
+#define X(A, B, C)                                                                              \
+    if (c.rx == A && c.ry == B && c.rz == C) {                                                  \
+        if (c.tz == 8 && c.d_half)                                                              \
+            return fast_launch_inst<A, B, C, 8, true>(tm_prev, a, tiles_z, c.smem_bytes, st);  \
+        if (c.tz == 8 && !c.d_half)                                                             \
+            return fast_launch_inst<A, B, C, 8, false>(tm_prev, a, tiles_z, c.smem_bytes, st); \
+        if (c.tz == 4 && c.d_half)                                                              \
+            return fast_launch_inst<A, B, C, 4, true>(tm_prev, a, tiles_z, c.smem_bytes, st);  \
+    }
+    INLM_FAST_SHAPES(X)
+#undef X
+    return cudaErrorInvalidConfiguration;
+}
+
+cudaError_t launch_pad_reflective_half(const float* in, int nx, int ny, int nz, void* out, int px,
+                                       int py, int pz, long long pitch_y, long long pitch_z,
+                                       cudaStream_t st) {
+    pad_reflective_half_kernel<<<148 * 8, 256, 0, st>>>(in, nx, ny, nz, (__half*)out, px, py, pz,
+                                                        pitch_y, pitch_z);
+    return cudaGetLastError();
+}
+
+}  // namespace inlm

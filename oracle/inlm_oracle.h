@@ -74,6 +74,12 @@ void ora_denoise_f32(const float* raw, const int shape[3], const ora_params* p,
 void ora_denoise_f64(const float* raw, const int shape[3], const ora_params* p,
                      const float* sigmas, int n_iter, double* out_last);
 
+/* ora_denoise_f64 with the search restricted per tile (tile[0] x tile[1] x
+ * tile[2] voxels, x-fastest tile index) to offsets with keep[tile*S + s] set. */
+void ora_denoise_f64_plan(const float* raw, const int shape[3], const ora_params* p,
+                          const float* sigmas, int n_iter, const int tile[3],
+                          const unsigned char* keep, double* out_last);
+
 /* ora_filter_f32 evaluated only at the given unpadded linear voxel indices
  * (sampled parity checks on full-size volumes). */
 void ora_filter_f32_voxels(const float* raw_pad, const float* prev_pad, const int shape[3],

@@ -91,6 +91,10 @@ class Port:
                                       _f64p]
         L.ora_filter_f32_voxels.argtypes = [_f32p, _f32p, C.c_int * 3, C.POINTER(_CParams), _f32p,
                                             C.c_int64, _i64p, _f32p]
+        L.ora_denoise_f64_plan.argtypes = [_f32p, C.c_int * 3, C.POINTER(_CParams), _f32p, C.c_int,
+                                           C.c_int * 3,
+                                           np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"),
+                                           _f64p]
         L.ora_sigma_to_mult.argtypes = [_f32p, C.c_int, C.c_float, _f32p]
         L.ora_srand.argtypes = [C.c_void_p, C.c_uint]
         L.ora_rand.restype = C.c_int
@@ -157,6 +161,17 @@ class Port:
                                  n_iter, out.ravel(),
                                  allbuf.ctypes.data if all_iters else None)
         return allbuf if all_iters else out
+
+    def denoise_f64_plan(self, raw: np.ndarray, p: FilterParams, sigmas: np.ndarray, tile_xyz,
+                         keep: np.ndarray) -> np.ndarray:
+        """FP64 filter with per-tile offset subsets (keep: n_tiles x S, bool)."""
+        raw = np.ascontiguousarray(raw, np.float32)
+        sig = np.ascontiguousarray(np.atleast_2d(sigmas), np.float32)
+        out = np.empty(raw.shape, np.float64)
+        self.lib.ora_denoise_f64_plan(raw.ravel(), _shape3(raw), C.byref(_cparams(p)), sig.ravel(),
+                                      sig.shape[0], (C.c_int * 3)(*tile_xyz),
+                                      np.ascontiguousarray(keep, np.uint8).ravel(), out.ravel())
+        return out
 
     def sigma_to_mult(self, sigma, beta: float = 1.0) -> np.ndarray:
         sigma = np.ascontiguousarray(sigma, np.float32)
