@@ -208,6 +208,64 @@ int inlm_noise_em_noalloc(void* stream, const float* values_dev, int64_t n_value
                           const int64_t* windows_host, int n_windows, float* mean_dev,
                           float* sd_dev);
 
+/* ---------------- learned search-offset proposal ----------------
+ * No counterpart in the reference, whose filter evaluates every search offset
+ * for every voxel (Denoiser/iternlm_cpu.cpp:758-843, iternlm_gpu.cu:80-1437).
+ * A small 3D conv net (4 conv layers of 16 channels with 3^3 kernels, BF16
+ * weights, FP32 accumulation, a linear head and a softmax over the S search
+ * offsets per 8^3 tile) predicts which offsets carry the filter weight; the
+ * FP16 form then evaluates only each tile's top K, or every offset when the
+ * predicted kept mass of the tile is below min_mass.
+ *
+ * Parameters are a flat float vector (inlm_proposal_n_params): conv weights
+ * [27 taps][Cin][16] (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)) and biases [16] for
+ * layers 1..4 (layer 1 has Cin = 1), head weights [S][16], head bias [S].
+ * Network input: a volume (the filter's previous iterate) and a per-slice
+ * scale 1/(sigma sqrt(beta)); layer 1 sees scale * (v(c+tap) - v(c)).
+ * Example volumes are unpadded FP32 device arrays, x fastest, every axis >= 2. */
+typedef struct inlm_proposal inlm_proposal;
+
+int inlm_proposal_create(int n_offsets, int device_id, inlm_proposal** out);
+int inlm_proposal_destroy(inlm_proposal* p);
+int inlm_proposal_n_params(const inlm_proposal* p, int64_t* n);
+/* Sets the FP32 parameters (host), rounds the weights to BF16 and resets the
+ * optimiser state. */
+int inlm_proposal_set_params(inlm_proposal* p, const float* params_host, int64_t n);
+int inlm_proposal_get_params(inlm_proposal* p, float* params_host, int64_t n);
+/* Forward pass of one example: logits_dev gets n_tiles x S values, tiles
+ * ordered (tz*ty_n + ty)*tx_n + tx with tile counts ceil(n/8). */
+int inlm_proposal_logits(inlm_proposal* p, const float* vol_dev, const float* scale_dev,
+                         const int shape[3], float* logits_dev);
+/* One optimiser step (Adam, beta 0.9/0.999) on the summed soft-target cross
+ * entropy of n_examples examples, averaged over all their tiles. targets_dev[e]
+ * holds n_tiles x S per-tile offset distributions (inlm_weight_map). shapes:
+ * 3 ints per example. grad_host != NULL: store the gradient there instead of
+ * updating the parameters. loss_out (nullable) gets the loss. */
+int inlm_proposal_train(inlm_proposal* p, int n_examples, const float* const* vols_dev,
+                        const float* const* scales_dev, const float* const* targets_dev,
+                        const int* shapes, float lr, double* loss_out, float* grad_host);
+/* Top-k selection of one example: bitmap_dev gets n_tiles x ceil(S/32) words
+ * (bit k%32 of word k/32 = offset k evaluated), pred_mass_dev the predicted
+ * kept mass per tile; tiles below min_mass select every offset (counted in
+ * *n_fallback). */
+int inlm_proposal_select(inlm_proposal* p, const float* vol_dev, const float* scale_dev,
+                         const int shape[3], int k, float min_mass, uint32_t* bitmap_dev,
+                         float* pred_mass_dev, int* n_fallback);
+/* Attaches a proposal to an FP16-form denoiser (p == NULL detaches): every
+ * later iteration runs the network on its previous iterate and evaluates the
+ * selected offsets per 8^3 tile. */
+int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass);
+/* Last iteration of an attached proposal: stats = {tiles, fallback tiles,
+ * offsets evaluated summed over filter CTAs, CTAs * S (full search), S}. */
+int inlm_proposal_stats(inlm_denoiser* d, int64_t stats[5]);
+/* Training targets: the last iteration's per-8^3-tile weight mass of every
+ * search offset (full search, FP16 form), each voxel's offset weights divided
+ * by their sum, averaged over the tile's voxels; map_dev: n_tiles x S. */
+int inlm_weight_map(inlm_denoiser* d, float* map_dev);
+/* The last iteration's network input: its previous iterate (unpadded FP32,
+ * the FP16 values the filter read) and the per-slice scale. */
+int inlm_net_input(inlm_denoiser* d, float* vol_dev, float* scale_dev);
+
 /* ---------------- host-only helpers (no device needed) ---------------- */
 
 /* Geometry of a parameter set (setup_searchspace / setup_patchspace /

@@ -193,6 +193,50 @@ class IterativeNLM_GPU:
         _lib.check(_lib.load().inlm_describe(self._h, buf, 512), "describe")
         return buf.value.decode()
 
+    def n_search_offsets(self) -> int:
+        """Number of search offsets S of the configured geometry."""
+        self._need()
+        return int(self.describe().split(" S=")[1].split()[0])
+
+    def tile_grid(self):
+        """(tile shape {x,y,z}, tile counts {x,y,z}) of the filter kernel."""
+        self._need()
+        ts, tc = (C.c_int * 3)(), (C.c_int * 3)()
+        _lib.check(_lib.load().inlm_tile_grid(self._h, ts, tc), "tile_grid")
+        return tuple(ts), tuple(tc)
+
+    def attach_proposal(self, net, k: int = 256, min_mass: float = 0.95) -> None:
+        """Evaluates only each 8^3 tile's top-k offsets predicted by `net` (a
+        proposal.ProposalNet), or every offset where the predicted kept mass
+        is below min_mass. net=None returns to full search. FP16 form only."""
+        self._need()
+        h = net._h if net is not None else None
+        _lib.check(_lib.load().inlm_attach_proposal(self._h, h, int(k), float(min_mass)),
+                   "attach_proposal")
+        self._proposal = net  # keep the network alive while attached
+
+    def proposal_stats(self) -> dict:
+        """Last iteration: tiles, fallback tiles, offsets evaluated, full-search
+        cost (CTAs x S) and S."""
+        self._need()
+        st = (C.c_int64 * 5)()
+        _lib.check(_lib.load().inlm_proposal_stats(self._h, st), "proposal_stats")
+        t, fb, ev, full, S = (int(v) for v in st)
+        return dict(tiles=t, fallback_tiles=fb, offsets_evaluated=ev, full_search=full, S=S,
+                    fraction_evaluated=ev / max(full, 1))
+
+    def weight_map(self, map_dev_ptr: int) -> None:
+        """Per-8^3-tile weight mass of every search offset of the last
+        iteration (device array of tiles x S floats)."""
+        self._need()
+        _lib.check(_lib.load().inlm_weight_map(self._h, map_dev_ptr), "weight_map")
+
+    def net_input(self, vol_dev_ptr: int, scale_dev_ptr: int) -> None:
+        """The last iteration's previous iterate (nz*ny*nx floats) and per-slice
+        scale (nz floats), as the proposal network reads them."""
+        self._need()
+        _lib.check(_lib.load().inlm_net_input(self._h, vol_dev_ptr, scale_dev_ptr), "net_input")
+
     def free_device(self) -> None:
         if self._h:
             _lib.load().inlm_denoiser_destroy(self._h)

@@ -32,6 +32,10 @@ EXPORTS = (
     "inlm_noise_samples", "inlm_noise_patchstd", "inlm_geometry", "inlm_noise_draw_samples",
     "inlm_kernel_launches", "inlm_probe_fp32_peak", "inlm_noise_em_noalloc",
     "inlm_tile_grid", "inlm_set_offset_plan",
+    "inlm_proposal_create", "inlm_proposal_destroy", "inlm_proposal_n_params",
+    "inlm_proposal_set_params", "inlm_proposal_get_params", "inlm_proposal_logits",
+    "inlm_proposal_train", "inlm_proposal_select", "inlm_attach_proposal", "inlm_proposal_stats",
+    "inlm_weight_map", "inlm_net_input",
 )
 
 
@@ -107,6 +111,20 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.inlm_tile_grid.argtypes = [vp, C.c_int * 3, C.c_int * 3]
     L.inlm_set_offset_plan.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int]
     L.inlm_noise_em_noalloc.argtypes = [vp, vp, C.c_int64, vp, C.c_int, vp, vp]
+    L.inlm_proposal_create.argtypes = [C.c_int, C.c_int, C.POINTER(vp)]
+    L.inlm_proposal_destroy.argtypes = [vp]
+    L.inlm_proposal_n_params.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.inlm_proposal_set_params.argtypes = [vp, vp, C.c_int64]
+    L.inlm_proposal_get_params.argtypes = [vp, vp, C.c_int64]
+    L.inlm_proposal_logits.argtypes = [vp, vp, vp, C.c_int * 3, vp]
+    L.inlm_proposal_train.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_float,
+                                      C.POINTER(C.c_double), vp]
+    L.inlm_proposal_select.argtypes = [vp, vp, vp, C.c_int * 3, C.c_int, C.c_float, vp, vp,
+                                       C.POINTER(C.c_int)]
+    L.inlm_attach_proposal.argtypes = [vp, vp, C.c_int, C.c_float]
+    L.inlm_proposal_stats.argtypes = [vp, C.c_int64 * 5]
+    L.inlm_weight_map.argtypes = [vp, vp]
+    L.inlm_net_input.argtypes = [vp, vp, vp]
     for name in EXPORTS:
         if name not in ("inlm_last_error", "inlm_default_params"):
             getattr(L, name).restype = C.c_int

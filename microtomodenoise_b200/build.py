@@ -11,6 +11,7 @@ g++ build does.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import glob
 import os
 import shutil
@@ -38,6 +39,8 @@ LIB_SOURCES = [
     "probe.cu",
     "noise_kernels.cu",
     "api.cu",
+    "proposal.cu",
+    "api_proposal.cu",
     "geometry.cpp",
     "sampling.cpp",
 ]
@@ -70,7 +73,7 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD_DIR, exist_ok=True)
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) + \
         glob.glob(os.path.join(ROOT, "include", "*.h"))
-    objs = []
+    objs, cmds = [], []
     for src in LIB_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD_DIR, src + ".o")
@@ -79,7 +82,10 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
             cmd = [nvcc()] + NVCC_FLAGS + ["-c", s, "-o", o]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
-            r = _run(cmd)
+            cmds.append(cmd)
+    # translation units compile independently
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in ex.map(_run, cmds):
             if verbose:
                 sys.stderr.write(r.stderr)
     if force or _newer(LIB, objs):

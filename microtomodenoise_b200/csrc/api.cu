@@ -15,10 +15,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/inlm.h"
-#include "filter_fast.cuh"
-#include "filter_kernels.cuh"
-#include "geometry.hpp"
+#include "api_internal.hpp"
 #include "noise_kernels.cuh"
 #include "sampling.hpp"
 #include "probe.cuh"
@@ -29,7 +26,7 @@ using namespace inlm;
 
 static thread_local std::string g_last_error;
 
-static int fail(int code, const char* fmt, ...) {
+int inlm::fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -38,16 +35,6 @@ static int fail(int code, const char* fmt, ...) {
     g_last_error = buf;
     return code;
 }
-
-#define CUDA_TRY(expr)                                                                       \
-    do {                                                                                     \
-        cudaError_t _e = (expr);                                                             \
-        if (_e != cudaSuccess) {                                                             \
-            int _code = (_e == cudaErrorMemoryAllocation) ? INLM_ERR_NOMEM : INLM_ERR_CUDA;  \
-            return fail(_code, "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, \
-                        __LINE__);                                                           \
-        }                                                                                    \
-    } while (0)
 
 extern "C" const char* inlm_last_error(void) { return g_last_error.c_str(); }
 
@@ -75,13 +62,6 @@ extern "C" void inlm_default_params(inlm_params* p) {
     p->device_id = 0;
     p->precision = INLM_PRECISION_F32;
     p->weight_table = INLM_WEIGHTS_CPU;
-}
-
-template <typename T>
-static cudaError_t dalloc(T** p, size_t n) {
-    *p = nullptr;
-    if (n == 0) n = 1;
-    return cudaMalloc((void**)p, n * sizeof(T));
 }
 
 // ---------------- TMA descriptor encoding ----------------
@@ -124,32 +104,7 @@ static int encode_map_3d(CUtensorMap* tm, const void* base, int ex, int ey, int 
 
 // ---------------- noise handle ----------------
 
-struct inlm_noise {
-    int shape[3] = {0, 0, 0};
-    uint64_t n_samples = 0;
-    int patchsize = 15;
-    unsigned int seed = 0;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    int mask_drawn = -1;
-    std::vector<long long> samples;
-    long long* d_samples = nullptr;
-    float* d_patchstd = nullptr;
-    float* d_stack = nullptr;  // staging for host stacks
-    int zwindow_cached = -1;
-    int2* d_windows = nullptr;
-    long long* d_scratch_off = nullptr;
-    signed char* d_assign = nullptr;
-    size_t assign_cap = 0;
-    float* d_mean = nullptr;
-    float* d_sd = nullptr;
-    float* d_sigma = nullptr;
-    int ncalls = 0;
-    long long ref_sample_semimanual = 0;
-};
-
-static void noise_free(inlm_noise* n) {
+void inlm::noise_free(inlm_noise* n) {
     if (!n) return;
     cudaSetDevice(n->device);
     cudaFree(n->d_samples);
@@ -362,55 +317,6 @@ extern "C" int inlm_noise_patchstd(inlm_noise* n, float* out, uint64_t max_n) {
 
 // ---------------- denoiser handle ----------------
 
-struct TimedLaunch {
-    cudaEvent_t a, b;
-};
-
-struct inlm_denoiser {
-    int shape[3] = {0, 0, 0};
-    inlm_params p;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    Geometry geo;
-    int nxp = 0, nyp = 0, nzp = 0;
-    long long pitch_y = 0, pitch_z = 0;
-    float* d_raw_pad = nullptr;
-    float* d_prev_pad = nullptr;
-    float* d_next = nullptr;
-    float* d_sigma = nullptr;
-    float* d_sigma0 = nullptr;
-    float* d_mult = nullptr;
-    int* d_err = nullptr;
-    int2* d_search_delta = nullptr;
-    long long* d_search_off = nullptr;
-    long long* d_patch_off = nullptr;
-    float* d_weights = nullptr;
-    bool use_tile = false;
-    bool use_fast = false;       // FP16-storage kernel
-    FastConfig fcfg{};
-    FastArgs fargs{};
-    void* d_raw_h = nullptr;     // padded FP16 raw / previous iterate
-    void* d_prev_h = nullptr;
-    CUtensorMap tm_prev_h{};
-    int* d_plan_start = nullptr;  // per-CTA offset lists (learned proposal)
-    int* d_plan_off = nullptr;
-    int plan_cap = 0;
-    int n_cta = 0;
-    TileConfig tcfg{};
-    TileArgs targs{};
-    GenericArgs gargs{};
-    CUtensorMap tm_prev{}, tm_raw{};
-    int last_iter = 0;
-    bool sigma_set = false;
-    uint64_t launches = 0;
-    std::vector<TimedLaunch> pending;
-    std::vector<TimedLaunch> event_pool;
-    double timed_ms = 0.0;
-    int timed_n = 0;
-    inlm_noise* noise = nullptr;
-};
-
 static void denoiser_free(inlm_denoiser* d) {
     if (!d) return;
     cudaSetDevice(d->device);
@@ -438,6 +344,8 @@ static void denoiser_free(inlm_denoiser* d) {
     cudaFree(d->d_prev_h);
     cudaFree(d->d_plan_start);
     cudaFree(d->d_plan_off);
+    proposal_release(d);
+    d->aux.release();
     if (d->noise) {
         noise_free(d->noise);
         delete d->noise;
@@ -775,7 +683,7 @@ extern "C" int inlm_set_sigma(inlm_denoiser* d, const float* sigma_host) {
     return INLM_OK;
 }
 
-static int launch_filter(inlm_denoiser* d) {
+int inlm::launch_filter(inlm_denoiser* d) {
     TimedLaunch t;
     if (!d->event_pool.empty()) {
         t = d->event_pool.back();
@@ -818,7 +726,7 @@ static int pad_into(inlm_denoiser* d, const float* src, float* dst) {
     return INLM_OK;
 }
 
-static int check_device_error(inlm_denoiser* d) {
+int inlm::check_device_error(inlm_denoiser* d) {
     int h = 0;
     CUDA_TRY(cudaMemcpyAsync(&h, d->d_err, 4, cudaMemcpyDeviceToHost, d->stream));
     CUDA_TRY(cudaStreamSynchronize(d->stream));
@@ -845,6 +753,10 @@ static int enqueue_iteration(inlm_denoiser* d, int iter, const float* raw_dev) {
         } else {
             if (d->last_iter < 1) return fail(INLM_ERR_STATE, "iteration %d before iteration 1", iter);
             rc = pad_into_half(d, d->d_next, d->d_prev_h);
+            if (rc) return rc;
+        }
+        if (d->prop.net) {
+            rc = proposal_enqueue(d);
             if (rc) return rc;
         }
         rc = launch_filter(d);
@@ -1145,6 +1057,7 @@ extern "C" int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const in
                                     const int* offsets, int n_offsets, int on_device) {
     if (!d) return fail(INLM_ERR_ARG, "null handle");
     if (!d->use_fast) return fail(INLM_ERR_UNSUPPORTED, "offset plans need the FP16 form");
+    if (d->prop.net) return fail(INLM_ERR_STATE, "a proposal network is attached; detach it first");
     CUDA_TRY(cudaSetDevice(d->device));
     if (!start) {
         d->fargs.plan_start = nullptr;
@@ -1159,9 +1072,10 @@ extern "C" int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const in
             if (start[c] < 0 || count[c] < 0 || count[c] > d->fargs.S ||
                 (long long)start[c] + count[c] > n_offsets)
                 return fail(INLM_ERR_ARG, "plan tile %d has a bad offset range", c);
+        // entry = offset index | (4-bit x sub-block mask << 16)
         for (int i = 0; i < n_offsets; i++)
-            if (offsets[i] < 0 || offsets[i] >= d->fargs.S)
-                return fail(INLM_ERR_ARG, "plan offset %d out of range", offsets[i]);
+            if (offsets[i] < 0 || (offsets[i] & 0xFFFF) >= d->fargs.S || (offsets[i] >> 20) != 0)
+                return fail(INLM_ERR_ARG, "plan entry %d out of range", offsets[i]);
     }
     if (!d->d_plan_start) CUDA_TRY(dalloc(&d->d_plan_start, 2 * (size_t)n));
     if (d->plan_cap < std::max(n_offsets, 1)) {

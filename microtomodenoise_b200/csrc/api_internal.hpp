@@ -1,0 +1,182 @@
+// Internal state of the C ABI handles, shared by the translation units that
+// implement include/inlm.h (api.cu, api_proposal.cu).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/inlm.h"
+#include "filter_fast.cuh"
+#include "filter_kernels.cuh"
+#include "geometry.hpp"
+#include "proposal.cuh"
+
+namespace inlm {
+
+// Records the calling thread's error text (inlm_last_error) and returns code.
+int fail(int code, const char* fmt, ...);
+
+template <typename T>
+static inline cudaError_t dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    return cudaMalloc((void**)p, n * sizeof(T));
+}
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, n ? n : 1);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    void release() {
+        cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+struct TimedLaunch {
+    cudaEvent_t a, b;
+};
+
+}  // namespace inlm
+
+#define CUDA_TRY(expr)                                                                         \
+    do {                                                                                       \
+        cudaError_t _e = (expr);                                                               \
+        if (_e != cudaSuccess) {                                                               \
+            int _code = (_e == cudaErrorMemoryAllocation) ? INLM_ERR_NOMEM : INLM_ERR_CUDA;    \
+            return inlm::fail(_code, "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, \
+                              __LINE__);                                                       \
+        }                                                                                      \
+    } while (0)
+
+struct inlm_noise {
+    int shape[3] = {0, 0, 0};
+    uint64_t n_samples = 0;
+    int patchsize = 15;
+    unsigned int seed = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int mask_drawn = -1;
+    std::vector<long long> samples;
+    long long* d_samples = nullptr;
+    float* d_patchstd = nullptr;
+    float* d_stack = nullptr;  // staging for host stacks
+    int zwindow_cached = -1;
+    int2* d_windows = nullptr;
+    long long* d_scratch_off = nullptr;
+    signed char* d_assign = nullptr;
+    size_t assign_cap = 0;
+    float* d_mean = nullptr;
+    float* d_sd = nullptr;
+    float* d_sigma = nullptr;
+    int ncalls = 0;
+    long long ref_sample_semimanual = 0;
+};
+
+// Proposal network: FP32 master parameters, BF16 copy, Adam state, training
+// scratch.
+struct inlm_proposal {
+    int device = 0;
+    inlm::NetLayout L;
+    cudaStream_t stream = nullptr;
+    float* d_w = nullptr;
+    float* d_m = nullptr;
+    float* d_v = nullptr;
+    float* d_g = nullptr;
+    __nv_bfloat16* d_wb = nullptr;
+    double* d_loss = nullptr;
+    long long step = 0;
+    inlm::DevBuf pad, a1, a2, a3, a4, glog, d1, d2, d3, d4, counters;
+};
+
+// Per-denoiser inference state of an attached proposal.
+struct ProposalRun {
+    inlm_proposal* net = nullptr;
+    int k = 0;
+    float min_mass = 0.95f;
+    int nwords = 0;
+    long long n_tiles = 0;
+    inlm::Dim3i t8{0, 0, 0};
+    inlm::DevBuf a1, a2, a3, a4, bitmap, pmass, counters, scale, plan_start, plan_off;
+};
+
+struct inlm_denoiser {
+    int shape[3] = {0, 0, 0};
+    inlm_params p;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    inlm::Geometry geo;
+    int nxp = 0, nyp = 0, nzp = 0;
+    long long pitch_y = 0, pitch_z = 0;
+    float* d_raw_pad = nullptr;
+    float* d_prev_pad = nullptr;
+    float* d_next = nullptr;
+    float* d_sigma = nullptr;
+    float* d_sigma0 = nullptr;
+    float* d_mult = nullptr;
+    int* d_err = nullptr;
+    int2* d_search_delta = nullptr;
+    long long* d_search_off = nullptr;
+    long long* d_patch_off = nullptr;
+    float* d_weights = nullptr;
+    bool use_tile = false;
+    bool use_fast = false;       // FP16-storage kernel
+    inlm::FastConfig fcfg{};
+    inlm::FastArgs fargs{};
+    void* d_raw_h = nullptr;     // padded FP16 raw / previous iterate
+    void* d_prev_h = nullptr;
+    CUtensorMap tm_prev_h{};
+    int* d_plan_start = nullptr;  // per-CTA offset lists set by inlm_set_offset_plan
+    int* d_plan_off = nullptr;
+    int plan_cap = 0;
+    int n_cta = 0;
+    ProposalRun prop;             // attached proposal network (prop.net != NULL)
+    inlm::DevBuf aux;             // weight-mass maps: 1 / weight sum per voxel
+    inlm::TileConfig tcfg{};
+    inlm::TileArgs targs{};
+    inlm::GenericArgs gargs{};
+    CUtensorMap tm_prev{}, tm_raw{};
+    int last_iter = 0;
+    bool sigma_set = false;
+    uint64_t launches = 0;
+    std::vector<inlm::TimedLaunch> pending;
+    std::vector<inlm::TimedLaunch> event_pool;
+    double timed_ms = 0.0;
+    int timed_n = 0;
+    inlm_noise* noise = nullptr;
+};
+
+namespace inlm {
+void noise_free(inlm_noise* n);
+int launch_filter(inlm_denoiser* d);
+int check_device_error(inlm_denoiser* d);
+// Runs the attached proposal on the padded previous iterate and points the
+// filter's plan at its per-CTA lists (api_proposal.cu).
+int proposal_enqueue(inlm_denoiser* d);
+void proposal_release(inlm_denoiser* d);
+}  // namespace inlm

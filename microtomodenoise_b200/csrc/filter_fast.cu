@@ -12,7 +12,12 @@
 //     in FP32 with fused multiply-adds;
 //   * the final per-voxel normalisation (acc + wmax*raw)/(wsum + wmax) is FP64.
 // Offsets: every search offset, or a per-CTA list (the learned proposal's
-// top-K for the tile).
+// top-K for the CTA's four 8^3 tiles). A list entry is offset | (mask << 16):
+// bit b of the 4-bit mask says the 8^3 tile of lanes with x sub-block b
+// (voxels 8b..8b+7 of the CTA's 32 columns) uses the offset; mask 0 = all.
+// MASS instantiations evaluate every offset and add each offset's weight,
+// divided by the voxel's weight sum (from a WSUM-only pass), into a per-8^3-
+// tile map: the training targets of the proposal network.
 #include <cuda_fp16.h>
 
 #include "common.cuh"
@@ -97,7 +102,7 @@ __device__ __forceinline__ void fast_rows(const unsigned char* __restrict__ Db, 
     }
 }
 
-template <int RX, int RY, int RZ, int TZ, bool D_HALF>
+template <int RX, int RY, int RZ, int TZ, bool D_HALF, bool MASS>
 __global__ void __launch_bounds__(32 * TZ, 2)
     nlm_tile_fast_kernel(const __grid_constant__ CUtensorMap tm_prev,
                          const __grid_constant__ FastArgs a) {
@@ -205,20 +210,35 @@ __global__ void __launch_bounds__(32 * TZ, 2)
     float acc[kVoxPerThread], wsum[kVoxPerThread], wmax[kVoxPerThread];
 #pragma unroll
     for (int r = 0; r < kVoxPerThread; r++) acc[r] = wsum[r] = wmax[r] = 0.0f;
+    const int xg = lane & 3;
+    float inv[kVoxPerThread];  // MASS: 1 / weight sum of the voxel (0 outside the volume)
+    if constexpr (MASS) {
+        const int z = Z0 + k, y = Y0 + j;
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) {
+            const int x = X0 + x0 + r;
+            inv[r] = (z < a.nz && y < a.ny && x < a.nx)
+                         ? a.aux[((long long)z * a.ny + y) * a.nx + x]
+                         : 0.0f;
+        }
+    }
 
     if (s_count > 0) {
-        int sidx = a.plan_offsets ? a.plan_offsets[s_begin] : 0;
-        int2 dl = __ldg(&a.search_delta[sidx]);
+        int ent = a.plan_offsets ? a.plan_offsets[s_begin] : 0;
+        int2 dl = __ldg(&a.search_delta[min(ent & 0xFFFF, a.S - 1)]);
         phase_a(D0, dl.x);
         __syncthreads();
         for (int i = 0; i < s_count; i++) {
             const unsigned char* Dr = D0 + (size_t)(i & 1) * F::DBYTES;
             const int dly = dl.y;
+            const int emask = ent >> 16;
+            const int scur = min(ent & 0xFFFF, a.S - 1);
             if (i + 1 < s_count) {
-                sidx = a.plan_offsets ? a.plan_offsets[s_begin + i + 1] : i + 1;
-                dl = __ldg(&a.search_delta[sidx]);
+                ent = a.plan_offsets ? a.plan_offsets[s_begin + i + 1] : i + 1;
+                dl = __ldg(&a.search_delta[min(ent & 0xFFFF, a.S - 1)]);
                 phase_a(D0 + (size_t)((i + 1) & 1) * F::DBYTES, dl.x);
             }
+            const bool use = emask == 0 || ((emask >> xg) & 1);
             float dist[kVoxPerThread];
             {
                 float win[16];
@@ -230,25 +250,52 @@ __global__ void __launch_bounds__(32 * TZ, 2)
                 for (int r = 0; r < kVoxPerThread; r++) dist[r] = win[RX + r] * w0;
             }
             fast_rows<RX, RY, RZ, TZ, D_HALF, 0>(Dr, rowoff, dist, a);
+            float part = 0.0f;
 #pragma unroll
             for (int r = 0; r < kVoxPerThread; r++) {
                 const float x = dist[r] * rel;
                 // Pade[3/3] of exp in Horner form, FMA
                 const float num = fmaf(fmaf(x + 12.f, x, 60.f), x, 120.f);
                 const float den = fmaf(fmaf(12.f - x, x, -60.f), x, 120.f);
-                const float w = (x > -3.56648f) ? __fdividef(num, den) : 0.0f;
-                const float rs = __half2float(rawb[rbase + dly + r]);
-                acc[r] = fmaf(w, rs, acc[r]);
-                wsum[r] += w;
-                wmax[r] = fmaxf(wmax[r], w);
+                const float w = (use && x > -3.56648f) ? __fdividef(num, den) : 0.0f;
+                if constexpr (MASS) {
+                    part = fmaf(w, inv[r], part);
+                } else {
+                    const float rs = __half2float(rawb[rbase + dly + r]);
+                    acc[r] = fmaf(w, rs, acc[r]);
+                    wsum[r] += w;
+                    wmax[r] = fmaxf(wmax[r], w);
+                }
+            }
+            if constexpr (MASS) {
+                // the 8 lanes of one x sub-block (same 8^3 tile, rows j = 0..7)
+                part += __shfl_xor_sync(0xffffffffu, part, 4);
+                part += __shfl_xor_sync(0xffffffffu, part, 8);
+                part += __shfl_xor_sync(0xffffffffu, part, 16);
+                if (lane < 4 && part != 0.0f) {
+                    const long long t8 =
+                        ((long long)((Z0 + k) >> 3) * a.t8y + (Y0 >> 3)) * a.t8x + (X0 >> 3) + lane;
+                    atomicAdd(&a.map[t8 * a.S + scur], part);
+                }
             }
             __syncthreads();
         }
     }
+    if constexpr (MASS) return;
 
     const int z = Z0 + k, y = Y0 + j;
     if (z < a.nz && y < a.ny) {
         float* orow = a.out + ((long long)z * a.ny + y) * a.nx;
+        if (a.aux && !MASS) {
+            // weight-sum pass of the mass maps: 1 / (sum of the offsets' weights)
+            float* arow = a.aux + ((long long)z * a.ny + y) * a.nx;
+#pragma unroll
+            for (int r = 0; r < kVoxPerThread; r++) {
+                const int x = X0 + x0 + r;
+                if (x < a.nx) arow[x] = wsum[r] > 0.0f ? 1.0f / wsum[r] : 0.0f;
+            }
+            return;
+        }
 #pragma unroll
         for (int r = 0; r < kVoxPerThread; r++) {
             int x = X0 + x0 + r;
@@ -308,8 +355,9 @@ static size_t fast_smem_for(const FastArgs& a) {
 
 template <int RX, int RY, int RZ, int TZ, bool D_HALF>
 static cudaError_t fast_launch_inst(const CUtensorMap* tmp, const FastArgs& a, int tiles_z,
-                                    size_t smem, cudaStream_t st) {
-    auto kern = nlm_tile_fast_kernel<RX, RY, RZ, TZ, D_HALF>;
+                                    size_t smem, cudaStream_t st, bool mass) {
+    auto kern = mass ? nlm_tile_fast_kernel<RX, RY, RZ, TZ, D_HALF, true>
+                     : nlm_tile_fast_kernel<RX, RY, RZ, TZ, D_HALF, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
@@ -333,15 +381,15 @@ size_t fast_smem_bytes(const FastConfig& c, const FastArgs& a) {
 }
 
 cudaError_t launch_fast_kernel(const FastConfig& c, const CUtensorMap* tm_prev, const FastArgs& a,
-                               int tiles_z, cudaStream_t st) {
+                               int tiles_z, cudaStream_t st, bool mass) {
 #define X(A, B, C)                                                                              \
     if (c.rx == A && c.ry == B && c.rz == C) {                                                  \
         if (c.tz == 8 && c.d_half)                                                              \
-            return fast_launch_inst<A, B, C, 8, true>(tm_prev, a, tiles_z, c.smem_bytes, st);  \
+            return fast_launch_inst<A, B, C, 8, true>(tm_prev, a, tiles_z, c.smem_bytes, st, mass);  \
         if (c.tz == 8 && !c.d_half)                                                             \
-            return fast_launch_inst<A, B, C, 8, false>(tm_prev, a, tiles_z, c.smem_bytes, st); \
+            return fast_launch_inst<A, B, C, 8, false>(tm_prev, a, tiles_z, c.smem_bytes, st, mass); \
         if (c.tz == 4 && c.d_half)                                                              \
-            return fast_launch_inst<A, B, C, 4, true>(tm_prev, a, tiles_z, c.smem_bytes, st);  \
+            return fast_launch_inst<A, B, C, 4, true>(tm_prev, a, tiles_z, c.smem_bytes, st, mass);  \
     }
     INLM_FAST_SHAPES(X)
 #undef X

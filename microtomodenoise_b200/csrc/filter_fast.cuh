@@ -16,7 +16,7 @@ struct FastArgs {
     int sxr, syr, szc;
     int S;                                  // full-search offset count
     const int2* __restrict__ search_delta;  // (prev-box delta, raw shared delta) per offset
-    const int* __restrict__ plan_offsets;   // per-CTA offset lists (NULL: all offsets)
+    const int* __restrict__ plan_offsets;   // per-CTA lists of offset | (x sub-block mask << 16)
     const int* __restrict__ plan_start;     // CTA c uses plan_offsets[start[c] .. start[c]+count[c])
     const int* __restrict__ plan_count;
     int pbx, pby, pbz;                      // FP16 prev box extents (x in halves)
@@ -26,6 +26,10 @@ struct FastArgs {
     float* __restrict__ out;
     const float* __restrict__ mult;
     int* err;
+    float* aux;                             // non-NULL: write 1/weight sum here (no result);
+                                            // MASS launches read it
+    float* map;                             // MASS: per-8^3-tile weight mass [tile][S]
+    int t8x, t8y;                           // 8^3 tile grid (x, y)
     float w[kMaxTaps];
 };
 
@@ -37,8 +41,9 @@ struct FastConfig {
 };
 
 size_t fast_smem_bytes(const FastConfig& c, const FastArgs& a);
+// mass = true: the weight-mass instantiation (training targets).
 cudaError_t launch_fast_kernel(const FastConfig& c, const CUtensorMap* tm_prev, const FastArgs& a,
-                               int tiles_z, cudaStream_t st);
+                               int tiles_z, cudaStream_t st, bool mass = false);
 cudaError_t launch_pad_reflective_half(const float* in, int nx, int ny, int nz, void* out, int px,
                                        int py, int pz, long long pitch_y, long long pitch_z,
                                        cudaStream_t st);

@@ -1,0 +1,92 @@
+// Learned search-offset proposal: network layout, kernels and launchers.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace inlm {
+
+constexpr int kNetC = 16;  // channels of every hidden layer
+
+// Flat parameter vector: conv weights [27 taps][Cin][Cout] (tap = (dz+1)*9 +
+// (dy+1)*3 + (dx+1)), biases [Cout], head weights [S][16], head bias [S].
+struct NetLayout {
+    int S = 0;
+    long long w1 = 0, b1 = 0, w2 = 0, b2 = 0, w3 = 0, b3 = 0, w4 = 0, b4 = 0, wh = 0, bh = 0;
+    long long total = 0;
+};
+NetLayout net_layout(int S);
+
+struct Dim3i {
+    int x, y, z;
+};
+
+// Level sizes: 0 = voxels, 1..3 after each stride-2 layer (level 3 = 8^3 tiles).
+void net_levels(int nx, int ny, int nz, Dim3i lv[4]);
+
+// Network input: a volume with a reflective halo of at least one voxel, and a
+// per-slice scale (1/(sigma sqrt(beta)) of the slice's filter multiplier).
+struct NetIn {
+    const void* base;  // element (0,0,0) inside the padded buffer
+    bool half;         // __half elements (else float)
+    long long py, pz;  // pitches in elements
+    int nx, ny, nz;
+    const float* scale;
+};
+
+struct NetActs {
+    float* a1;  // level 1 x 16
+    float* a2;  // level 2 x 16
+    float* a3;  // level 3 x 16
+    float* a4;  // level 3 x 16 (tile features)
+};
+
+cudaError_t net_forward(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const NetIn& in,
+                        const NetActs& act, cudaStream_t st);
+cudaError_t net_logits(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const float* a4,
+                       int n_tiles, float* logits, cudaStream_t st);
+
+// Backward of the loss sum_tiles inv_n * sum_k t_k (log Z - l_k) (soft-target
+// cross entropy, targets normalised per tile); accumulates into grad.
+// g_logit (n_tiles x S) and d1..d4 (level-sized x 16) are scratch.
+struct NetGradScratch {
+    float* g_logit;
+    float* d1;
+    float* d2;
+    float* d3;
+    float* d4;
+};
+cudaError_t net_backward(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const NetIn& in,
+                         const NetActs& act, const float* target, float inv_n,
+                         const NetGradScratch& s, float* grad, double* loss, cudaStream_t st);
+
+cudaError_t net_adam(float* w, float* m, float* v, const float* g, __nv_bfloat16* wb, long long n,
+                     float lr, float beta1, float beta2, float eps, float bc1, float bc2,
+                     cudaStream_t st);
+cudaError_t net_round_bf16(const float* w, __nv_bfloat16* wb, long long n, cudaStream_t st);
+
+// Per tile: top-K offsets by logit, predicted kept mass, fallback to every
+// offset when it is below min_mass. bitmap: n_tiles x nwords (bit k%32 of
+// word k/32 = offset k kept); counters[0] += fallback tiles.
+cudaError_t net_select(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const float* a4,
+                       int n_tiles, int K, float min_mass, unsigned* bitmap, int nwords,
+                       float* pred_mass, int* counters, cudaStream_t st);
+
+// Per filter CTA (32 x 8 x tz voxels, four 8^3 tiles along x): the union of
+// its tiles' kept offsets in ascending order, each entry offset | (mask << 16)
+// with bit b of mask = the tile at x sub-block b uses it. plan_start[c] = c*S.
+// counters[1] += entries written.
+cudaError_t net_plan_build(const unsigned* bitmap, int nwords, Dim3i tiles8, int cta_x, int cta_y,
+                           int cta_z, int tz, int S, int* plan_off, int* plan_count, int* counters,
+                           cudaStream_t st);
+
+// Per-slice input scale from the filter multiplier m = -1/(sigma^2 beta).
+cudaError_t net_scale_from_mult(const float* mult, int nz, float* scale, cudaStream_t st);
+// Unpadded FP32 copy of the interior of a padded FP16 volume.
+cudaError_t unpad_half_to_float(const void* padded, long long py, long long pz, int px, int pyy,
+                                int pz0, int nx, int ny, int nz, float* out, cudaStream_t st);
+// Per-tile normalisation of weight-mass maps (rows of S sum to 1, or stay 0).
+cudaError_t normalise_rows(float* map, long long rows, int S, cudaStream_t st);
+
+}  // namespace inlm

@@ -743,7 +743,7 @@ void ora_sigma_to_mult(const float* sigma, int nz, float beta, float* mult) {
 
 void ora_denoise_f64_plan(const float* raw, const int shape[3], const ora_params* p,
                           const float* sigmas, int n_iter, const int tile[3],
-                          const unsigned char* keep, double* out_last) {
+                          const unsigned char* keep, long long keep_iter_stride, double* out_last) {
     /* ora_denoise_f64 with the search restricted, per tile of tile[0] x
      * tile[1] x tile[2] voxels (x fastest tile index), to the offsets whose
      * keep[tile * S + s] is set; wmax is taken over the kept offsets. */
@@ -783,7 +783,7 @@ void ora_denoise_f64_plan(const float* raw, const int shape[3], const ora_params
             for (int y = 0; y < ny; y++)
                 for (int x = 0; x < nx; x++) {
                     long long t = ((long long)(z / tile[2]) * nty + y / tile[1]) * ntx + x / tile[0];
-                    const unsigned char* kp = keep + t * ns;
+                    const unsigned char* kp = keep + (it - 1) * keep_iter_stride + t * ns;
                     long long idx0 = (z + pad[2]) * nsl + (y + pad[1]) * nxp + (x + pad[0]);
                     double raw0 = raw_pad[idx0];
                     for (int q = 0; q < np; q++) vorig[q] = prev_pad[idx0 + poff[q]];
@@ -808,4 +808,67 @@ void ora_denoise_f64_plan(const float* raw, const int shape[3], const ora_params
         }
     }
     free(soff); free(rawd); free(raw_pad); free(prev_pad);
+}
+
+void ora_weight_mass_f64(const float* prev, const int shape[3], const ora_params* p,
+                         const float* sigma, const int tile[3], double* out) {
+    /* the weights of ora_filter_f64 (iternlm_cpu.cpp:758-843 in double) */
+    int pad[3];
+    ora_padding(p, pad);
+    int nx = shape[0], ny = shape[1], nz = shape[2];
+    long long nxp = nx + 2 * pad[0], nyp = ny + 2 * pad[1], nzp = nz + 2 * pad[2];
+    long long nsl = nxp * nyp, npad = nsl * nzp, nvox = (long long)nx * ny * nz;
+    static int sdx[ORA_MAXS], sdy[ORA_MAXS], sdz[ORA_MAXS];
+    int pdx[ORA_MAXP], pdy[ORA_MAXP], pdz[ORA_MAXP];
+    float wf[ORA_MAXP];
+    double w[ORA_MAXP];
+    int ns = ora_search_offsets(p, sdx, sdy, sdz, ORA_MAXS);
+    int np = ora_patch_taps(p, pdx, pdy, pdz, ORA_MAXP);
+    ora_filter_weights(p, nz + 2 * pad[2], wf, ORA_MAXP, NULL);
+    for (int q = 0; q < np; q++) w[q] = (double)wf[q];
+    long long* soff = (long long*)malloc(sizeof(long long) * ns);
+    long long poff[ORA_MAXP];
+    for (int s = 0; s < ns; s++) soff[s] = sdz[s] * nsl + sdy[s] * nxp + sdx[s];
+    for (int q = 0; q < np; q++) poff[q] = pdz[q] * nsl + pdy[q] * nxp + pdx[q];
+    int ntx = (nx + tile[0] - 1) / tile[0], nty = (ny + tile[1] - 1) / tile[1];
+    int ntz = (nz + tile[2] - 1) / tile[2];
+    long long ntiles = (long long)ntx * nty * ntz;
+    double* prevd = (double*)malloc(nvox * sizeof(double));
+    double* prev_pad = (double*)malloc(npad * sizeof(double));
+    int sh[3] = {nx, ny, nz};
+    for (long long i = 0; i < nvox; i++) prevd[i] = prev[i];
+    pad_reflective_f64(prevd, sh, pad, prev_pad);
+    memset(out, 0, sizeof(double) * ntiles * ns);
+    const double cut = (double)PADE_CUTOFF;
+    double* wt = (double*)malloc(sizeof(double) * ns);
+    for (int z = 0; z < nz; z++) {
+        double sgm = sigma[z];
+        double m = -1.0 / (sgm * sgm * (double)p->beta);
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++) {
+                long long t = ((long long)(z / tile[2]) * nty + y / tile[1]) * ntx + x / tile[0];
+                long long idx0 = (z + pad[2]) * nsl + (y + pad[1]) * nxp + (x + pad[0]);
+                double sum = 0.0;
+                for (int s = 0; s < ns; s++) {
+                    long long idx1 = idx0 + soff[s];
+                    double dist = 0.0;
+                    for (int q = 0; q < np; q++) {
+                        double tt = prev_pad[idx1 + poff[q]] - prev_pad[idx0 + poff[q]];
+                        dist += tt * tt * w[q];
+                    }
+                    dist *= m;
+                    wt[s] = (dist > cut) ? pade_f64(dist) : 0.0;
+                    sum += wt[s];
+                }
+                if (sum > 0.0)
+                    for (int s = 0; s < ns; s++) out[t * ns + s] += wt[s] / sum;
+            }
+    }
+    for (long long t = 0; t < ntiles; t++) {
+        double sum = 0.0;
+        for (int s = 0; s < ns; s++) sum += out[t * ns + s];
+        if (sum > 0.0)
+            for (int s = 0; s < ns; s++) out[t * ns + s] /= sum;
+    }
+    free(wt); free(soff); free(prevd); free(prev_pad);
 }

@@ -75,10 +75,19 @@ void ora_denoise_f64(const float* raw, const int shape[3], const ora_params* p,
                      const float* sigmas, int n_iter, double* out_last);
 
 /* ora_denoise_f64 with the search restricted per tile (tile[0] x tile[1] x
- * tile[2] voxels, x-fastest tile index) to offsets with keep[tile*S + s] set. */
+ * tile[2] voxels, x-fastest tile index) to offsets with keep[tile*S + s] set.
+ * Iteration k reads keep + (k-1)*keep_iter_stride (0: one table for all). */
 void ora_denoise_f64_plan(const float* raw, const int shape[3], const ora_params* p,
                           const float* sigmas, int n_iter, const int tile[3],
-                          const unsigned char* keep, double* out_last);
+                          const unsigned char* keep, long long keep_iter_stride, double* out_last);
+
+/* Weight mass per tile and search offset of one iteration in FP64: each
+ * voxel's offset weights (Pade + cutoff on m * patch distance over prev,
+ * m = -1/(sigma[z]^2 beta)) divided by their sum, summed over the tile's
+ * voxels, each tile row then normalised to sum 1 (rows of all-zero stay 0).
+ * out: n_tiles x S. The training target of the learned offset proposal. */
+void ora_weight_mass_f64(const float* prev, const int shape[3], const ora_params* p,
+                         const float* sigma, const int tile[3], double* out);
 
 /* ora_filter_f32 evaluated only at the given unpadded linear voxel indices
  * (sampled parity checks on full-size volumes). */

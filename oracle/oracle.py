@@ -94,7 +94,9 @@ class Port:
         L.ora_denoise_f64_plan.argtypes = [_f32p, C.c_int * 3, C.POINTER(_CParams), _f32p, C.c_int,
                                            C.c_int * 3,
                                            np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"),
-                                           _f64p]
+                                           C.c_longlong, _f64p]
+        L.ora_weight_mass_f64.argtypes = [_f32p, C.c_int * 3, C.POINTER(_CParams), _f32p,
+                                          C.c_int * 3, _f64p]
         L.ora_sigma_to_mult.argtypes = [_f32p, C.c_int, C.c_float, _f32p]
         L.ora_srand.argtypes = [C.c_void_p, C.c_uint]
         L.ora_rand.restype = C.c_int
@@ -164,13 +166,31 @@ class Port:
 
     def denoise_f64_plan(self, raw: np.ndarray, p: FilterParams, sigmas: np.ndarray, tile_xyz,
                          keep: np.ndarray) -> np.ndarray:
-        """FP64 filter with per-tile offset subsets (keep: n_tiles x S, bool)."""
+        """FP64 filter with per-tile offset subsets (keep: n_tiles x S bool, or
+        n_iter x n_tiles x S for a subset per iteration)."""
         raw = np.ascontiguousarray(raw, np.float32)
         sig = np.ascontiguousarray(np.atleast_2d(sigmas), np.float32)
         out = np.empty(raw.shape, np.float64)
+        keep = np.ascontiguousarray(keep, np.uint8)
+        stride = keep[0].size if keep.ndim == 3 else 0
+        if keep.ndim == 3:
+            assert keep.shape[0] == sig.shape[0]
         self.lib.ora_denoise_f64_plan(raw.ravel(), _shape3(raw), C.byref(_cparams(p)), sig.ravel(),
-                                      sig.shape[0], (C.c_int * 3)(*tile_xyz),
-                                      np.ascontiguousarray(keep, np.uint8).ravel(), out.ravel())
+                                      sig.shape[0], (C.c_int * 3)(*tile_xyz), keep.ravel(), stride,
+                                      out.ravel())
+        return out
+
+    def weight_mass_f64(self, prev: np.ndarray, p: FilterParams, sigma: np.ndarray,
+                        tile_xyz=(8, 8, 8)) -> np.ndarray:
+        """Per-tile offset weight mass of one iteration (n_tiles x S, rows sum to 1)."""
+        prev = np.ascontiguousarray(prev, np.float32)
+        nz, ny, nx = prev.shape
+        nt = -(-nx // tile_xyz[0]) * -(-ny // tile_xyz[1]) * -(-nz // tile_xyz[2])
+        S = len(self.search_offsets(p))
+        out = np.empty((nt, S), np.float64)
+        self.lib.ora_weight_mass_f64(prev.ravel(), _shape3(prev), C.byref(_cparams(p)),
+                                     np.ascontiguousarray(sigma, np.float32),
+                                     (C.c_int * 3)(*tile_xyz), out.ravel())
         return out
 
     def sigma_to_mult(self, sigma, beta: float = 1.0) -> np.ndarray:
