@@ -18,6 +18,15 @@ exceed L2 (126 MB) between steps.
 
 Multi-GPU (torchrun): each rank denoises its own volume (independent jobs,
 weak scaling, no data-path collective); time = max over ranks.
+
+``forms`` (rank 0, one GPU): the same whole job in the FP16-storage form and
+in the learned-proposal + FP16 form (k = 256 offsets per 8^3 tile, fallback to
+full search below 0.95 predicted kept mass, and without fallback), each with
+its speed-up over the plain FP32 job, the proposal's fallback fraction and
+evaluated-offset fraction, and its accuracy: max-abs error and PSNR against
+the FP64 full-search oracle on two sub-blocks (a corner and a central 40^3
+block, computed on crops with a 28-voxel margin, the reach of 4 iterations),
+plus PSNR against the clean phantom next to the FP64 oracle's own.
 """
 from __future__ import annotations
 
@@ -130,12 +139,119 @@ def profile_traffic():
     return None
 
 
-def make_volume(seed=0):
+def make_volume(seed=0, return_clean=False):
     from microtomodenoise_b200 import synth
     t = time.time()
-    v = synth.grain_pack_volume(SHAPE, seed=seed)
+    v = synth.grain_pack_volume(SHAPE, seed=seed, return_clean=return_clean)
     log(f"generated {SHAPE} volume in {time.time() - t:.1f}s")
     return v
+
+
+def psnr(a, b, peak=1.0):
+    mse = float(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2))
+    return float("inf") if mse == 0 else 10 * np.log10(peak * peak / mse)
+
+
+def sub_blocks(shape, inner=40, margin=28):
+    """(crop slices, interior slices within the crop) of a corner block (the
+    volume's own faces need no margin) and a central block."""
+    out = []
+    c0 = tuple(slice(0, min(n, inner + margin)) for n in shape)
+    i0 = tuple(slice(0, min(n, inner)) for n in shape)
+    out.append((c0, i0))
+    lo = [max(0, n // 2 - inner // 2 - margin) for n in shape]
+    c1 = tuple(slice(l, min(n, n // 2 + inner // 2 + margin)) for l, n in zip(lo, shape))
+    i1 = tuple(slice(n // 2 - inner // 2 - l, n // 2 + inner // 2 - l) for l, n in zip(lo, shape))
+    out.append((c1, i1))
+    return out
+
+
+def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
+    """FP16 and learned + FP16 forms: whole-job throughput and accuracy."""
+    import ctypes as C
+    import torch
+    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, _lib
+    from microtomodenoise_b200.proposal import ProposalNet, default_weights
+    from oracle.oracle import FilterParams, Port
+
+    net = ProposalNet.load(default_weights(PR, SR), device=local)
+    forms = [("f32", "f32", None), ("fp16", "f16", None),
+             ("learned_fp16", "f16", (256, 0.95)), ("learned_fp16_nofallback", "f16", (256, 0.0))]
+    raw_dev = torch.from_numpy(vol).cuda()
+    out_dev = torch.empty_like(raw_dev)
+    vox = float(np.prod(vol.shape))
+    res = {}
+    crops = {}
+    for name, prec, prop in forms:
+        dp = DenoiseParameters(radius_patchspace=PR, radius_searchspace=SR, maxiterations=ITERS,
+                               alpha=0.5, noise_mode="z-adaptive", zwindow=100, n_samples=100000,
+                               noise_seed=0, deviceID=local, precision=prec)
+        g = IterativeNLM_GPU()
+        g.configure_device(vol.shape, dp)
+        g.set_stream(stream.cuda_stream)
+        if prop:
+            g.attach_proposal(net, prop[0], prop[1])
+        r = {"kernel": g.describe()}
+        if name != "f32":
+            for _ in range(1):
+                g.denoise(raw_dev.data_ptr(), on_device=True, out=out_dev.data_ptr())
+            g.filter_kernel_ms()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.form_steps):
+                g.denoise(raw_dev.data_ptr(), on_device=True, out=out_dev.data_ptr())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.form_steps
+            kms, kn = g.filter_kernel_ms()
+            r.update({"value": vox * ITERS / (ms / 1e3), "unit": "voxel-iter/s",
+                      "ms_per_step": ms, "steps": args.form_steps, "warmup": 1,
+                      "speedup_vs_f32": vox * ITERS / (ms / 1e3) / value_f32,
+                      "filter_kernel_avg_ms": kms})
+            if prop:
+                st = g.proposal_stats()
+                r.update({"k": prop[0], "min_mass": prop[1],
+                          "fallback_fraction": st["fallback_tiles"] / max(st["tiles"], 1),
+                          "fraction_evaluated": st["fraction_evaluated"]})
+        # accuracy run: the FP32 job's sigma schedule, fixed, for every form
+        for it in range(ITERS):
+            g.set_sigma(sig_iters[it])
+            g.Run_GaussianNoise_device(it + 1, raw_dev.data_ptr() if it == 0 else None)
+        g.get_result_device(out_dev.data_ptr())
+        torch.cuda.synchronize()
+        out = out_dev.cpu().numpy()
+        crops[name] = [out[c][i] for c, i in sub_blocks(vol.shape)]
+        res[name] = r
+        g.free_device()
+        log(f"form {name}: {r}")
+    net.close()
+    # FP64 full-search oracle on the crops
+    port = Port()
+    fp = FilterParams(search_radius=SR, patch_radius=PR)
+    ref, cl = [], []
+    t = time.time()
+    for c, i in sub_blocks(vol.shape):
+        crop = np.ascontiguousarray(vol[c])
+        sig = np.ascontiguousarray(sig_iters[:, c[0]])
+        ref.append(port.denoise_f64(crop, fp, sig)[i])
+        cl.append(clean[c][i])
+    log(f"FP64 oracle on {len(ref)} sub-blocks: {time.time() - t:.1f}s")
+    cat = lambda xs: np.concatenate([x.ravel() for x in xs])
+    r64, c64 = cat(ref), cat(cl)
+    p64 = psnr(r64, c64)
+    for name in res:
+        got = cat(crops[name])
+        res[name]["accuracy"] = {
+            "max_abs_vs_fp64": float(np.abs(got - r64).max()),
+            "psnr_vs_fp64_db": psnr(got, r64),
+            "psnr_vs_clean_db": psnr(got, c64),
+            "fp64_psnr_vs_clean_db": p64,
+            "delta_vs_fp64_oracle_db": psnr(got, c64) - p64,
+            "sub_blocks": "corner and central 40^3 blocks, FP64 oracle on crops with a 28-voxel "
+                          "margin, sigma schedule of the FP32 job held fixed"}
+    return res
 
 
 def cpu_reference_rate(vol, target_s=15.0, threads=None):
@@ -210,6 +326,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form-steps", type=int, default=2)
+    ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--shape", default="512,512,512",
                     help="nz,ny,nx of the volume (smaller shapes only for profiling runs)")
     args = ap.parse_args()
@@ -241,7 +359,7 @@ def main():
     _lib.check(L.inlm_probe_fp32_peak(local, C.byref(peak)), "probe")
     fp32_peak = peak.value
 
-    vol = make_volume(seed=0)
+    vol, clean = make_volume(seed=0, return_clean=True)
     dp = DenoiseParameters(radius_patchspace=PR, radius_searchspace=SR, maxiterations=ITERS,
                            alpha=0.5, noise_mode="z-adaptive", zwindow=100, n_samples=100000,
                            noise_seed=0, deviceID=local)
@@ -337,13 +455,19 @@ def main():
         "gpu_launches": gpu_launches,
         "clocks": clk.summary(),
     }
+    g.free_device()
+    if rank == 0 and world == 1 and not args.no_forms:
+        sig_iters = np.stack([s0] + [(0.5 * s0 + 0.5 * s1).astype(np.float32)] * (ITERS - 1))
+        try:
+            line["forms"] = run_forms(vol, clean, sig_iters, value, args, local, stream)
+        except Exception as e:
+            line["forms"] = {"error": str(e)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             _, info = cpu_reference_rate(vol)
             line["cpu_baseline"] = info
         except Exception as e:  # the GPU number stands without it
             line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
-    g.free_device()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

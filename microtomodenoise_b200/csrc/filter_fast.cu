@@ -12,9 +12,13 @@
 //     in FP32 with fused multiply-adds;
 //   * the final per-voxel normalisation (acc + wmax*raw)/(wsum + wmax) is FP64.
 // Offsets: every search offset, or a per-CTA list (the learned proposal's
-// top-K for the CTA's four 8^3 tiles). A list entry is offset | (mask << 16):
-// bit b of the 4-bit mask says the 8^3 tile of lanes with x sub-block b
-// (voxels 8b..8b+7 of the CTA's 32 columns) uses the offset; mask 0 = all.
+// top-K for the CTA's four 8^3 tiles, merged). A list entry is
+// offset | (mask << 16): bit b of the 4-bit mask says the 8^3 tile of x
+// sub-block b (voxels 8b..8b+7 of the CTA's 32 columns) uses the offset;
+// mask 0 = all. Squared differences are formed once per listed offset for the
+// whole CTA; the distance and weight work runs only in the warps whose tile
+// uses the offset (each warp covers one tile), so a CTA's cost follows the
+// merged list for the first phase and each tile's own list for the second.
 // MASS instantiations evaluate every offset and add each offset's weight,
 // divided by the voxel's weight sum (from a WSUM-only pass), into a per-8^3-
 // tile map: the training targets of the proposal network.
@@ -198,22 +202,26 @@ __global__ void __launch_bounds__(32 * TZ, 2)
         }
     };
 
+    // Phase B lane map: warp w covers the 8^3 tile of x sub-block g = w % 4
+    // (columns 8g..8g+7 of the CTA), z-planes 4*(w/4) .. +3; lane = (row j,
+    // plane kz), 8 consecutive x voxels each. A warp whose tile does not use
+    // an offset of a plan skips that offset's distances and weights.
     const int warp = tid >> 5, lane = tid & 31;
-    const int k = warp;
-    const int j = lane >> 2;
-    const int x0 = (lane & 3) * kVoxPerThread;
-    const int zk = min(Z0 + k, a.nz - 1);
+    const int g = warp & 3;
+    const int j = lane & 7;
+    const int kp = 4 * (warp >> 2) + (lane >> 3);  // z-plane of the CTA
+    const int x0 = g * kVoxPerThread;
+    const int zk = min(Z0 + kp, a.nz - 1);
     const float rel = a.mult[zk] / scale;  // x = dist' * rel
-    const int rowoff = k * F::DPLANE + j * F::DP + x0;
-    const int rbase = (a.szc + k) * (rpx * a.rby) + (a.syr + j) * rpx + (RX + a.sxr + x0);
+    const int rowoff = kp * F::DPLANE + j * F::DP + x0;
+    const int rbase = (a.szc + kp) * (rpx * a.rby) + (a.syr + j) * rpx + (RX + a.sxr + x0);
 
     float acc[kVoxPerThread], wsum[kVoxPerThread], wmax[kVoxPerThread];
 #pragma unroll
     for (int r = 0; r < kVoxPerThread; r++) acc[r] = wsum[r] = wmax[r] = 0.0f;
-    const int xg = lane & 3;
     float inv[kVoxPerThread];  // MASS: 1 / weight sum of the voxel (0 outside the volume)
     if constexpr (MASS) {
-        const int z = Z0 + k, y = Y0 + j;
+        const int z = Z0 + kp, y = Y0 + j;
 #pragma unroll
         for (int r = 0; r < kVoxPerThread; r++) {
             const int x = X0 + x0 + r;
@@ -238,44 +246,46 @@ __global__ void __launch_bounds__(32 * TZ, 2)
                 dl = __ldg(&a.search_delta[min(ent & 0xFFFF, a.S - 1)]);
                 phase_a(D0 + (size_t)((i + 1) & 1) * F::DBYTES, dl.x);
             }
-            const bool use = emask == 0 || ((emask >> xg) & 1);
-            float dist[kVoxPerThread];
-            {
-                float win[16];
-                constexpr int esz = D_HALF ? 2 : 4;
-                load_row<D_HALF, RX, RX + kVoxPerThread - 1>(
-                    Dr + (size_t)(rowoff + RZ * F::DPLANE + RY * F::DP) * esz, win);
-                const float w0 = a.w[0];
+            // warp-uniform: every lane of the warp is in tile g
+            if (emask == 0 || ((emask >> g) & 1)) {
+                float dist[kVoxPerThread];
+                {
+                    float win[16];
+                    constexpr int esz = D_HALF ? 2 : 4;
+                    load_row<D_HALF, RX, RX + kVoxPerThread - 1>(
+                        Dr + (size_t)(rowoff + RZ * F::DPLANE + RY * F::DP) * esz, win);
+                    const float w0 = a.w[0];
 #pragma unroll
-                for (int r = 0; r < kVoxPerThread; r++) dist[r] = win[RX + r] * w0;
-            }
-            fast_rows<RX, RY, RZ, TZ, D_HALF, 0>(Dr, rowoff, dist, a);
-            float part = 0.0f;
-#pragma unroll
-            for (int r = 0; r < kVoxPerThread; r++) {
-                const float x = dist[r] * rel;
-                // Pade[3/3] of exp in Horner form, FMA
-                const float num = fmaf(fmaf(x + 12.f, x, 60.f), x, 120.f);
-                const float den = fmaf(fmaf(12.f - x, x, -60.f), x, 120.f);
-                const float w = (use && x > -3.56648f) ? __fdividef(num, den) : 0.0f;
-                if constexpr (MASS) {
-                    part = fmaf(w, inv[r], part);
-                } else {
-                    const float rs = __half2float(rawb[rbase + dly + r]);
-                    acc[r] = fmaf(w, rs, acc[r]);
-                    wsum[r] += w;
-                    wmax[r] = fmaxf(wmax[r], w);
+                    for (int r = 0; r < kVoxPerThread; r++) dist[r] = win[RX + r] * w0;
                 }
-            }
-            if constexpr (MASS) {
-                // the 8 lanes of one x sub-block (same 8^3 tile, rows j = 0..7)
-                part += __shfl_xor_sync(0xffffffffu, part, 4);
-                part += __shfl_xor_sync(0xffffffffu, part, 8);
-                part += __shfl_xor_sync(0xffffffffu, part, 16);
-                if (lane < 4 && part != 0.0f) {
-                    const long long t8 =
-                        ((long long)((Z0 + k) >> 3) * a.t8y + (Y0 >> 3)) * a.t8x + (X0 >> 3) + lane;
-                    atomicAdd(&a.map[t8 * a.S + scur], part);
+                fast_rows<RX, RY, RZ, TZ, D_HALF, 0>(Dr, rowoff, dist, a);
+                float part = 0.0f;
+#pragma unroll
+                for (int r = 0; r < kVoxPerThread; r++) {
+                    const float x = dist[r] * rel;
+                    // Pade[3/3] of exp in Horner form, FMA
+                    const float num = fmaf(fmaf(x + 12.f, x, 60.f), x, 120.f);
+                    const float den = fmaf(fmaf(12.f - x, x, -60.f), x, 120.f);
+                    const float w = (x > -3.56648f) ? __fdividef(num, den) : 0.0f;
+                    if constexpr (MASS) {
+                        part = fmaf(w, inv[r], part);
+                    } else {
+                        const float rs = __half2float(rawb[rbase + dly + r]);
+                        acc[r] = fmaf(w, rs, acc[r]);
+                        wsum[r] += w;
+                        wmax[r] = fmaxf(wmax[r], w);
+                    }
+                }
+                if constexpr (MASS) {
+                    // the warp's voxels all lie in one 8^3 tile
+#pragma unroll
+                    for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                    if (lane == 0 && part != 0.0f) {
+                        const long long t8 =
+                            ((long long)((Z0 + 4 * (warp >> 2)) >> 3) * a.t8y + (Y0 >> 3)) * a.t8x +
+                            (X0 >> 3) + g;
+                        atomicAdd(&a.map[t8 * a.S + scur], part);
+                    }
                 }
             }
             __syncthreads();
@@ -283,7 +293,7 @@ __global__ void __launch_bounds__(32 * TZ, 2)
     }
     if constexpr (MASS) return;
 
-    const int z = Z0 + k, y = Y0 + j;
+    const int z = Z0 + kp, y = Y0 + j;
     if (z < a.nz && y < a.ny) {
         float* orow = a.out + ((long long)z * a.ny + y) * a.nx;
         if (a.aux && !MASS) {

@@ -115,12 +115,15 @@ def to_uint16_unit(vol: np.ndarray) -> np.ndarray:
 
 
 def grain_pack_volume(shape=(512, 512, 512), noise_std=0.04, noise_blur=1.2, ring_amp=0.02,
-                      ring_period=6.0, sigma_drift=None, seed=0, quantise=True) -> np.ndarray:
+                      ring_period=6.0, sigma_drift=None, seed=0, quantise=True,
+                      return_clean=False):
     """Grain pack + correlated noise + ring artefacts (the 512^3 workload).
 
-    sigma_drift=(s0, s1) makes the noise std drift linearly along z."""
+    sigma_drift=(s0, s1) makes the noise std drift linearly along z.
+    return_clean=True also returns the noise- and ring-free phantom."""
     rng = np.random.default_rng(seed)
     vol = grain_pack(shape, rng=rng)
+    clean = vol.copy() if return_clean else None
     if sigma_drift is None:
         vol += correlated_noise(shape, noise_std, noise_blur, rng)
     else:
@@ -129,7 +132,10 @@ def grain_pack_volume(shape=(512, 512, 512), noise_std=0.04, noise_blur=1.2, rin
         vol += n * s[:, None, None]
     if ring_amp:
         vol += ring_artefacts(shape, ring_amp, ring_period)
-    return to_uint16_unit(vol) if quantise else vol.astype(np.float32)
+    out = to_uint16_unit(vol) if quantise else vol.astype(np.float32)
+    if return_clean:
+        return out, (to_uint16_unit(clean) if quantise else clean)
+    return out
 
 
 def small_case(shape=(16, 20, 24), seed=0, noise_std=0.05) -> np.ndarray:
