@@ -139,16 +139,18 @@ int inlm_filter_kernel_ms(inlm_denoiser* d, double* avg_ms, int* n_launches);
 /* Description of the chosen filter kernel (name, tile, taps, offsets). */
 int inlm_describe(inlm_denoiser* d, char* buf, size_t len);
 
-/* Tiling of the filter kernel: tile_shape = voxels per tile {x, y, z},
- * tiles = tile counts {x, y, z}; tile index = (tz*tiles[1] + ty)*tiles[0] + tx. */
+/* Tiling of the full-search filter kernel: tile_shape = voxels per CTA
+ * {x, y, z}, tiles = CTA counts {x, y, z}; index = (tz*tiles[1] + ty)*tiles[0] + tx. */
 int inlm_tile_grid(inlm_denoiser* d, int tile_shape[3], int tiles[3]);
 
 /* Per-tile offset plan for the FP16 form (the learned proposal's output):
- * tile c evaluates the search offsets offsets[start[c] .. start[c]+count[c])
- * (indices into the reference-order search table, in the order given).
- * start and count have n_tiles entries, offsets n_offsets; on_device = 1 when
- * the three arrays are device memory (they are copied). start == NULL
- * returns to full search. */
+ * 8^3 tile t (tiles ordered (tz*ceil(ny/8) + ty)*ceil(nx/8) + tx) evaluates
+ * the search offsets offsets[start[t] .. start[t]+count[t]) (indices into
+ * the reference-order search table, in the order given); the filter then
+ * runs one 8^3 tile per CTA. start and count have one entry per tile,
+ * offsets n_offsets; on_device = 1 when the three arrays are device memory
+ * (they are copied; device plans are not range-checked, indices are clamped
+ * to the table). start == NULL returns to full search. */
 int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const int* count, const int* offsets,
                          int n_offsets, int on_device);
 

@@ -344,6 +344,7 @@ static void denoiser_free(inlm_denoiser* d) {
     cudaFree(d->d_prev_h);
     cudaFree(d->d_plan_start);
     cudaFree(d->d_plan_off);
+    cudaFree(d->d_search_delta8);
     proposal_release(d);
     d->aux.release();
     if (d->noise) {
@@ -433,12 +434,14 @@ static int choose_tile_config(inlm_denoiser* d) {
     return INLM_OK;
 }
 
-// FP16-storage kernel configuration (same tile decomposition as the FP32
-// kernel; prev box in halves, raw staged as FP32 with an odd pitch).
-static int choose_fast_config(inlm_denoiser* d) {
+// FP16-storage kernel configurations: CTA width tx = 32 (full search) and
+// tx = 8 (one 8^3 tile per CTA, for per-tile offset plans); prev box in
+// halves arriving by TMA, raw staged in halves with an odd pitch.
+static int build_fast_config(inlm_denoiser* d, int tx, FastConfig* cfg, FastArgs* args,
+                             CUtensorMap* tm, int2** d_delta, bool* ok) {
     const Geometry& g = d->geo;
     const int* pr = g.patch_radius;
-    d->use_fast = false;
+    *ok = false;
     if (!tile_kernel_available(pr[0], pr[1], pr[2])) return INLM_OK;
     if (d->p.nslices / 2 < pr[2]) return INLM_OK;
     if ((int)g.taps.size() > kMaxTaps) return INLM_OK;
@@ -449,7 +452,8 @@ static int choose_fast_config(inlm_denoiser* d) {
         if (order[3 * t] != g.taps[t].x || order[3 * t + 1] != g.taps[t].y ||
             order[3 * t + 2] != g.taps[t].z)
             return INLM_OK;
-    FastArgs& a = d->fargs;
+    FastArgs& a = *args;
+    a = FastArgs{};
     a.nx = d->shape[0];
     a.ny = d->shape[1];
     a.nz = d->shape[2];
@@ -462,9 +466,9 @@ static int choose_fast_config(inlm_denoiser* d) {
     a.S = (int)g.search.size();
     a.gpitch_y = d->pitch_y;
     a.gpitch_z = d->pitch_z;
-    a.pbx = (kTX + 2 * a.px + 7) / 8 * 8;  // halves, 16-byte TMA rows
+    a.pbx = (tx + 2 * a.px + 7) / 8 * 8;  // halves, 16-byte TMA rows
     a.pby = kTY + 2 * a.py;
-    a.rbx = (pr[0] + kTX + 2 * a.sxr + 3) / 4 * 4;
+    a.rbx = (pr[0] + tx + 2 * a.sxr + 3) / 4 * 4;
     a.rby = kTY + 2 * a.syr;
     for (int t = 0; t < nt; t++) a.w[t] = g.weights[t];
     int smem_max = 0;
@@ -472,23 +476,22 @@ static int choose_fast_config(inlm_denoiser* d) {
     const bool dh = d->p.precision == INLM_PRECISION_F16;
     const int tzs[] = {8, 4};
     for (int tz : tzs) {
-        if (tz == 4 && !dh) continue;
+        if (tz == 4 && (!dh || tx != 32)) continue;
         a.pbz = tz + 2 * a.pz;
         a.rbz = tz + 2 * a.szc;
         if (a.pbx > 256 || a.pby > 256 || a.pbz > 256) continue;
         if ((long long)a.pbx * a.pby * a.pbz >= (1ll << 24)) continue;
-        FastConfig fc{pr[0], pr[1], pr[2], tz, dh, 0};
+        FastConfig fc{pr[0], pr[1], pr[2], tz, tx, dh, 0};
         size_t sm = fast_smem_bytes(fc, a);
         if (sm == 0 || sm > (size_t)smem_max) continue;
         fc.smem_bytes = sm;
-        d->fcfg = fc;
-        d->use_fast = true;
+        *cfg = fc;
+        *ok = true;
         break;
     }
-    if (!d->use_fast) return INLM_OK;
-    a.tiles_x = (d->shape[0] + kTX - 1) / kTX;
+    if (!*ok) return INLM_OK;
+    a.tiles_x = (d->shape[0] + tx - 1) / tx;
     a.tiles_y = (d->shape[1] + kTY - 1) / kTY;
-    d->n_cta = a.tiles_x * a.tiles_y * ((d->shape[2] + d->fcfg.tz - 1) / d->fcfg.tz);
     std::vector<int2> dl(a.S);
     const int rpx = a.rbx + 1;
     for (int si = 0; si < a.S; si++) {
@@ -496,9 +499,9 @@ static int choose_fast_config(inlm_denoiser* d) {
         dl[si].x = o.z * a.pbx * a.pby + o.y * a.pbx + o.x;
         dl[si].y = o.z * rpx * a.rby + o.y * rpx + o.x;
     }
-    CUDA_TRY(dalloc(&d->d_search_delta, a.S));
-    CUDA_TRY(cudaMemcpy(d->d_search_delta, dl.data(), a.S * sizeof(int2), cudaMemcpyHostToDevice));
-    a.search_delta = d->d_search_delta;
+    CUDA_TRY(dalloc(d_delta, a.S));
+    CUDA_TRY(cudaMemcpy(*d_delta, dl.data(), a.S * sizeof(int2), cudaMemcpyHostToDevice));
+    a.search_delta = *d_delta;
     a.plan_offsets = nullptr;
     a.plan_start = nullptr;
     a.plan_count = nullptr;
@@ -506,8 +509,21 @@ static int choose_fast_config(inlm_denoiser* d) {
     a.out = d->d_next;
     a.mult = d->d_mult;
     a.err = d->d_err;
-    return encode_map_3d(&d->tm_prev_h, d->d_prev_h, d->nxp, d->nyp, d->nzp, d->pitch_y, d->pitch_z,
-                         a.pbx, a.pby, a.pbz, 2);
+    return encode_map_3d(tm, d->d_prev_h, d->nxp, d->nyp, d->nzp, d->pitch_y, d->pitch_z, a.pbx,
+                         a.pby, a.pbz, 2);
+}
+
+static int choose_fast_config(inlm_denoiser* d) {
+    bool ok32 = false, ok8 = false;
+    int rc = build_fast_config(d, 32, &d->fcfg, &d->fargs, &d->tm_prev_h, &d->d_search_delta, &ok32);
+    if (rc) return rc;
+    d->use_fast = ok32;
+    if (!ok32) return INLM_OK;
+    d->n_cta = d->fargs.tiles_x * d->fargs.tiles_y * ((d->shape[2] + d->fcfg.tz - 1) / d->fcfg.tz);
+    rc = build_fast_config(d, 8, &d->fcfg8, &d->fargs8, &d->tm_prev_h8, &d->d_search_delta8, &ok8);
+    if (rc) return rc;
+    d->use_tile8 = ok8;
+    return INLM_OK;
 }
 
 extern "C" int inlm_denoiser_create(const int shape[3], const inlm_params* p, inlm_denoiser** out) {
@@ -693,7 +709,11 @@ int inlm::launch_filter(inlm_denoiser* d) {
         CUDA_TRY(cudaEventCreate(&t.b));
     }
     CUDA_TRY(cudaEventRecord(t.a, d->stream));
-    if (d->use_fast) {
+    if (d->use_fast && d->plan_active) {
+        // per-tile plans: one 8^3 tile per CTA
+        int tiles_z = (d->shape[2] + d->fcfg8.tz - 1) / d->fcfg8.tz;
+        CUDA_TRY(launch_fast_kernel(d->fcfg8, &d->tm_prev_h8, d->fargs8, tiles_z, d->stream));
+    } else if (d->use_fast) {
         int tiles_z = (d->shape[2] + d->fcfg.tz - 1) / d->fcfg.tz;
         CUDA_TRY(launch_fast_kernel(d->fcfg, &d->tm_prev_h, d->fargs, tiles_z, d->stream));
     } else if (d->use_tile) {
@@ -928,12 +948,15 @@ extern "C" int inlm_filter_kernel_ms(inlm_denoiser* d, double* avg_ms, int* n_la
 extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
     if (!d || !buf) return fail(INLM_ERR_ARG, "null argument");
     const Geometry& g = d->geo;
-    if (d->use_fast)
+    if (d->use_fast) {
+        const FastConfig& c = d->plan_active ? d->fcfg8 : d->fcfg;
         snprintf(buf, len,
-                 "nlm_tile_fast<%d,%d,%d> tz=%d d_planes=%s smem=%zu S=%zu P=%zu plan=%s pad=%d,%d,%d",
-                 d->fcfg.rx, d->fcfg.ry, d->fcfg.rz, d->fcfg.tz, d->fcfg.d_half ? "f16" : "f32",
-                 d->fcfg.smem_bytes, g.search.size(), g.taps.size(),
-                 d->fargs.plan_start ? "per-tile" : "full", g.pad[0], g.pad[1], g.pad[2]);
+                 "nlm_tile_fast<%d,%d,%d> tx=%d tz=%d d_planes=%s smem=%zu S=%zu P=%zu plan=%s "
+                 "pad=%d,%d,%d",
+                 c.rx, c.ry, c.rz, c.tx, c.tz, c.d_half ? "f16" : "f32", c.smem_bytes,
+                 g.search.size(), g.taps.size(), d->plan_active ? "per-tile" : "full", g.pad[0],
+                 g.pad[1], g.pad[2]);
+    }
     else if (d->use_tile)
         snprintf(buf, len,
                  "nlm_tile_f32<%d,%d,%d> tz=%d raw_%s smem=%zu S=%zu P=%zu weights=%s pad=%d,%d,%d",
@@ -1056,25 +1079,28 @@ extern "C" int inlm_tile_grid(inlm_denoiser* d, int tile_shape[3], int tiles[3])
 extern "C" int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const int* count,
                                     const int* offsets, int n_offsets, int on_device) {
     if (!d) return fail(INLM_ERR_ARG, "null handle");
-    if (!d->use_fast) return fail(INLM_ERR_UNSUPPORTED, "offset plans need the FP16 form");
+    if (!d->use_fast || !d->use_tile8)
+        return fail(INLM_ERR_UNSUPPORTED, "offset plans need the FP16 form");
     if (d->prop.net) return fail(INLM_ERR_STATE, "a proposal network is attached; detach it first");
     CUDA_TRY(cudaSetDevice(d->device));
     if (!start) {
-        d->fargs.plan_start = nullptr;
-        d->fargs.plan_count = nullptr;
-        d->fargs.plan_offsets = nullptr;
+        d->plan_active = false;
+        d->fargs8.plan_start = nullptr;
+        d->fargs8.plan_count = nullptr;
+        d->fargs8.plan_offsets = nullptr;
         return INLM_OK;
     }
     if (!count || !offsets || n_offsets < 0) return fail(INLM_ERR_ARG, "null plan array");
-    const int n = d->n_cta;
+    // one list per 8^3 tile (the tx = 8 grid)
+    const long long n = (long long)d->fargs8.tiles_x * d->fargs8.tiles_y *
+                        ((d->shape[2] + d->fcfg8.tz - 1) / d->fcfg8.tz);
     if (!on_device) {
-        for (int c = 0; c < n; c++)
-            if (start[c] < 0 || count[c] < 0 || count[c] > d->fargs.S ||
+        for (long long c = 0; c < n; c++)
+            if (start[c] < 0 || count[c] < 0 || count[c] > d->fargs8.S ||
                 (long long)start[c] + count[c] > n_offsets)
-                return fail(INLM_ERR_ARG, "plan tile %d has a bad offset range", c);
-        // entry = offset index | (4-bit x sub-block mask << 16)
+                return fail(INLM_ERR_ARG, "plan tile %lld has a bad offset range", c);
         for (int i = 0; i < n_offsets; i++)
-            if (offsets[i] < 0 || (offsets[i] & 0xFFFF) >= d->fargs.S || (offsets[i] >> 20) != 0)
+            if (offsets[i] < 0 || offsets[i] >= d->fargs8.S)
                 return fail(INLM_ERR_ARG, "plan entry %d out of range", offsets[i]);
     }
     if (!d->d_plan_start) CUDA_TRY(dalloc(&d->d_plan_start, 2 * (size_t)n));
@@ -1090,8 +1116,9 @@ extern "C" int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const in
     CUDA_TRY(cudaMemcpyAsync(d->d_plan_start + n, count, (size_t)n * 4, kind, d->stream));
     CUDA_TRY(cudaMemcpyAsync(d->d_plan_off, offsets, (size_t)n_offsets * 4, kind, d->stream));
     CUDA_TRY(cudaStreamSynchronize(d->stream));
-    d->fargs.plan_start = d->d_plan_start;
-    d->fargs.plan_count = d->d_plan_start + n;
-    d->fargs.plan_offsets = d->d_plan_off;
+    d->fargs8.plan_start = d->d_plan_start;
+    d->fargs8.plan_count = d->d_plan_start + n;
+    d->fargs8.plan_offsets = d->d_plan_off;
+    d->plan_active = true;
     return INLM_OK;
 }

@@ -151,10 +151,17 @@ struct inlm_denoiser {
     void* d_raw_h = nullptr;     // padded FP16 raw / previous iterate
     void* d_prev_h = nullptr;
     CUtensorMap tm_prev_h{};
-    int* d_plan_start = nullptr;  // per-CTA offset lists set by inlm_set_offset_plan
+    // one 8^3 tile per CTA (tx = 8), the configuration per-tile plans run on
+    bool use_tile8 = false;
+    inlm::FastConfig fcfg8{};
+    inlm::FastArgs fargs8{};
+    CUtensorMap tm_prev_h8{};
+    int2* d_search_delta8 = nullptr;
+    bool plan_active = false;     // fargs8 carries a per-tile plan
+    int* d_plan_start = nullptr;  // per-tile offset lists set by inlm_set_offset_plan
     int* d_plan_off = nullptr;
     int plan_cap = 0;
-    int n_cta = 0;
+    int n_cta = 0;                // CTAs of the full-search (tx = 32) configuration
     ProposalRun prop;             // attached proposal network (prop.net != NULL)
     inlm::DevBuf aux;             // weight-mass maps: 1 / weight sum per voxel
     inlm::TileConfig tcfg{};

@@ -241,13 +241,19 @@ extern "C" int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, f
     CUDA_TRY(cudaSetDevice(d->device));
     CUDA_TRY(cudaStreamSynchronize(d->stream));
     if (!p) {
+        if (d->prop.net) {
+            d->plan_active = false;
+            d->fargs8.plan_start = nullptr;
+            d->fargs8.plan_count = nullptr;
+            d->fargs8.plan_offsets = nullptr;
+        }
         proposal_release(d);
-        d->fargs.plan_start = nullptr;
-        d->fargs.plan_count = nullptr;
-        d->fargs.plan_offsets = nullptr;
         return INLM_OK;
     }
-    if (!d->use_fast) return fail(INLM_ERR_UNSUPPORTED, "the proposal drives the FP16 form only");
+    if (!d->use_fast || !d->use_tile8)
+        return fail(INLM_ERR_UNSUPPORTED, "the proposal drives the FP16 form only");
+    if (d->plan_active && !d->prop.net)
+        return fail(INLM_ERR_STATE, "an offset plan is set; clear it first");
     if (p->device != d->device) return fail(INLM_ERR_ARG, "proposal and denoiser on different devices");
     if (p->L.S != d->fargs.S)
         return fail(INLM_ERR_ARG, "proposal trained for %d offsets, the denoiser searches %d", p->L.S,
@@ -261,7 +267,8 @@ extern "C" int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, f
     net_levels(d->shape[0], d->shape[1], d->shape[2], lv);
     r.t8 = lv[3];
     r.n_tiles = (long long)lv[3].x * lv[3].y * lv[3].z;
-    const int n = d->n_cta;
+    // one plan list per 8^3 tile = per CTA of the tx = 8 configuration
+    const long long n = r.n_tiles;
     CUDA_TRY(prop_levels_alloc(&r.a1, &r.a2, &r.a3, &r.a4, d->shape[0], d->shape[1], d->shape[2]));
     CUDA_TRY(r.bitmap.ensure((size_t)r.n_tiles * r.nwords * 4));
     CUDA_TRY(r.pmass.ensure((size_t)r.n_tiles * 4));
@@ -269,8 +276,10 @@ extern "C" int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, f
     CUDA_TRY(r.scale.ensure((size_t)d->shape[2] * 4));
     CUDA_TRY(r.plan_start.ensure((size_t)2 * n * 4));
     CUDA_TRY(r.plan_off.ensure((size_t)n * p->L.S * 4));
+    if ((long long)n * p->L.S >= (1ll << 31))
+        return fail(INLM_ERR_ARG, "volume too large for one plan table; stream it in z-slabs");
     std::vector<int> st(n);
-    for (int c = 0; c < n; c++) st[c] = c * p->L.S;
+    for (long long c = 0; c < n; c++) st[c] = (int)(c * p->L.S);
     CUDA_TRY(cudaMemcpyAsync(r.plan_start.p, st.data(), (size_t)n * 4, cudaMemcpyHostToDevice,
                              d->stream));
     CUDA_TRY(cudaMemsetAsync(r.counters.p, 0, 16, d->stream));
@@ -300,16 +309,14 @@ int inlm::proposal_enqueue(inlm_denoiser* d) {
     CUDA_TRY(net_select(p->L, p->d_wb, p->d_w, act.a4, (int)r.n_tiles, r.k, r.min_mass,
                         r.bitmap.as<unsigned>(), r.nwords, r.pmass.as<float>(), r.counters.as<int>(),
                         d->stream));
-    const int tz = d->fcfg.tz;
-    const int cz = (d->shape[2] + tz - 1) / tz;
     int* ps = r.plan_start.as<int>();
-    CUDA_TRY(net_plan_build(r.bitmap.as<unsigned>(), r.nwords, r.t8, d->fargs.tiles_x,
-                            d->fargs.tiles_y, cz, tz, p->L.S, r.plan_off.as<int>(), ps + d->n_cta,
-                            r.counters.as<int>(), d->stream));
-    d->launches += 8;  // scale, 4 layers, select, plan (+ the counter reset)
-    d->fargs.plan_start = ps;
-    d->fargs.plan_count = ps + d->n_cta;
-    d->fargs.plan_offsets = r.plan_off.as<int>();
+    CUDA_TRY(net_plan_tiles(r.bitmap.as<unsigned>(), r.nwords, r.n_tiles, p->L.S,
+                            r.plan_off.as<int>(), ps + r.n_tiles, r.counters.as<int>(), d->stream));
+    d->launches += 7;  // scale, 4 layers, select, plan
+    d->fargs8.plan_start = ps;
+    d->fargs8.plan_count = ps + r.n_tiles;
+    d->fargs8.plan_offsets = r.plan_off.as<int>();
+    d->plan_active = true;
     return INLM_OK;
 }
 
@@ -323,7 +330,7 @@ extern "C" int inlm_proposal_stats(inlm_denoiser* d, int64_t stats[5]) {
     stats[0] = d->prop.n_tiles;
     stats[1] = cnt[0];
     stats[2] = cnt[1];
-    stats[3] = (int64_t)d->n_cta * d->fargs.S;
+    stats[3] = (int64_t)d->prop.n_tiles * d->fargs.S;
     stats[4] = d->fargs.S;
     return INLM_OK;
 }

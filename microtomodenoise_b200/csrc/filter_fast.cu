@@ -11,14 +11,9 @@
 //   * patch distances, Pade weights, weighted sums and weight sums accumulate
 //     in FP32 with fused multiply-adds;
 //   * the final per-voxel normalisation (acc + wmax*raw)/(wsum + wmax) is FP64.
-// Offsets: every search offset, or a per-CTA list (the learned proposal's
-// top-K for the CTA's four 8^3 tiles, merged). A list entry is
-// offset | (mask << 16): bit b of the 4-bit mask says the 8^3 tile of x
-// sub-block b (voxels 8b..8b+7 of the CTA's 32 columns) uses the offset;
-// mask 0 = all. Squared differences are formed once per listed offset for the
-// whole CTA; the distance and weight work runs only in the warps whose tile
-// uses the offset (each warp covers one tile), so a CTA's cost follows the
-// merged list for the first phase and each tile's own list for the second.
+// Offsets: every search offset, or a per-CTA list of offset indices. With
+// TX = 8 a CTA is one 8^3 tile, so a list is the learned proposal's top-K for
+// that tile and the tile pays for exactly its own offsets.
 // MASS instantiations evaluate every offset and add each offset's weight,
 // divided by the voxel's weight sum (from a WSUM-only pass), into a per-8^3-
 // tile map: the training targets of the proposal network.
@@ -38,9 +33,9 @@ constexpr int dpitch_h(int w) {
     return ((p / 8) % 2 == 0) ? p + 8 : p;
 }
 
-template <int RX, int RY, int RZ, int TZ, bool D_HALF>
+template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF>
 struct FastGeom {
-    using G = TileGeom<RX, RY, RZ, TZ>;
+    using G = TileGeom<RX, RY, RZ, TZ, TX>;
     static constexpr int DP = D_HALF ? dpitch_h(G::DW) : G::DP;  // elements
     static constexpr int DPLANE = DP * G::DH;
     static constexpr int DSZ = D_HALF ? (DPLANE * G::DD + 63) / 64 * 64
@@ -79,11 +74,11 @@ __device__ __forceinline__ void load_row(const void* rowp, float (&win)[16]) {
     }
 }
 
-template <int RX, int RY, int RZ, int TZ, bool D_HALF, int RI>
+template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF, int RI>
 __device__ __forceinline__ void fast_rows(const unsigned char* __restrict__ Db, int rowoff,
                                           float (&dist)[kVoxPerThread], const FastArgs& a) {
-    using G = TileGeom<RX, RY, RZ, TZ>;
-    using F = FastGeom<RX, RY, RZ, TZ, D_HALF>;
+    using G = TileGeom<RX, RY, RZ, TZ, TX>;
+    using F = FastGeom<RX, RY, RZ, TZ, TX, D_HALF>;
     if constexpr (RI < G::rows.n) {
         constexpr int zp = G::rows.zp[RI];
         constexpr int yp = G::rows.yp[RI];
@@ -102,16 +97,18 @@ __device__ __forceinline__ void fast_rows(const unsigned char* __restrict__ Db, 
 #pragma unroll
             for (int r = 0; r < kVoxPerThread; r++) dist[r] = fmaf(win[RX + r + xp], w, dist[r]);
         }
-        fast_rows<RX, RY, RZ, TZ, D_HALF, RI + 1>(Db, rowoff, dist, a);
+        fast_rows<RX, RY, RZ, TZ, TX, D_HALF, RI + 1>(Db, rowoff, dist, a);
     }
 }
 
-template <int RX, int RY, int RZ, int TZ, bool D_HALF, bool MASS>
-__global__ void __launch_bounds__(32 * TZ, 2)
+// TX = 32: CTA of 32 x 8 x TZ voxels (four 8^3 tiles along x when TZ = 8),
+// two CTAs per SM; TX = 8: CTA of one 8 x 8 x TZ tile, four CTAs per SM.
+template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF, bool MASS>
+__global__ void __launch_bounds__(TX * TZ, TX == 32 ? 2 : 4)
     nlm_tile_fast_kernel(const __grid_constant__ CUtensorMap tm_prev,
                          const __grid_constant__ FastArgs a) {
-    using G = TileGeom<RX, RY, RZ, TZ>;
-    using F = FastGeom<RX, RY, RZ, TZ, D_HALF>;
+    using G = TileGeom<RX, RY, RZ, TZ, TX>;
+    using F = FastGeom<RX, RY, RZ, TZ, TX, D_HALF>;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
     __half* prevb = reinterpret_cast<__half*>(smem + 128);
@@ -123,7 +120,7 @@ __global__ void __launch_bounds__(32 * TZ, 2)
     unsigned char* D0 = reinterpret_cast<unsigned char*>(rawb) + (size_t)(RB + 63) / 64 * 128;
 
     const int tid = threadIdx.x;
-    const int X0 = blockIdx.x * kTX;
+    const int X0 = blockIdx.x * TX;
     const int Y0 = blockIdx.y * kTY;
     const int Z0 = blockIdx.z * TZ;
     const int cta = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
@@ -202,14 +199,15 @@ __global__ void __launch_bounds__(32 * TZ, 2)
         }
     };
 
-    // Phase B lane map: warp w covers the 8^3 tile of x sub-block g = w % 4
-    // (columns 8g..8g+7 of the CTA), z-planes 4*(w/4) .. +3; lane = (row j,
-    // plane kz), 8 consecutive x voxels each. A warp whose tile does not use
-    // an offset of a plan skips that offset's distances and weights.
+    // Phase B lane map: a warp covers 8 x 8 x 4 voxels of one 8^3 tile, lane =
+    // (row j, plane), 8 consecutive x voxels each. TX = 32: warp w takes x
+    // sub-block g = w % 4 (columns 8g..8g+7) and planes 4*(w/4)..+3; TX = 8:
+    // planes 4w..4w+3.
     const int warp = tid >> 5, lane = tid & 31;
-    const int g = warp & 3;
+    const int g = (TX == 32) ? (warp & 3) : 0;
     const int j = lane & 7;
-    const int kp = 4 * (warp >> 2) + (lane >> 3);  // z-plane of the CTA
+    const int zw = (TX == 32) ? 4 * (warp >> 2) : 4 * warp;  // first plane of the warp
+    const int kp = zw + (lane >> 3);                          // z-plane of the CTA
     const int x0 = g * kVoxPerThread;
     const int zk = min(Z0 + kp, a.nz - 1);
     const float rel = a.mult[zk] / scale;  // x = dist' * rel
@@ -232,22 +230,20 @@ __global__ void __launch_bounds__(32 * TZ, 2)
     }
 
     if (s_count > 0) {
-        int ent = a.plan_offsets ? a.plan_offsets[s_begin] : 0;
-        int2 dl = __ldg(&a.search_delta[min(ent & 0xFFFF, a.S - 1)]);
+        int ent = a.plan_offsets ? min(max(a.plan_offsets[s_begin], 0), a.S - 1) : 0;
+        int2 dl = __ldg(&a.search_delta[ent]);
         phase_a(D0, dl.x);
         __syncthreads();
         for (int i = 0; i < s_count; i++) {
             const unsigned char* Dr = D0 + (size_t)(i & 1) * F::DBYTES;
             const int dly = dl.y;
-            const int emask = ent >> 16;
-            const int scur = min(ent & 0xFFFF, a.S - 1);
+            const int scur = ent;
             if (i + 1 < s_count) {
-                ent = a.plan_offsets ? a.plan_offsets[s_begin + i + 1] : i + 1;
-                dl = __ldg(&a.search_delta[min(ent & 0xFFFF, a.S - 1)]);
+                ent = a.plan_offsets ? min(max(a.plan_offsets[s_begin + i + 1], 0), a.S - 1) : i + 1;
+                dl = __ldg(&a.search_delta[ent]);
                 phase_a(D0 + (size_t)((i + 1) & 1) * F::DBYTES, dl.x);
             }
-            // warp-uniform: every lane of the warp is in tile g
-            if (emask == 0 || ((emask >> g) & 1)) {
+            {
                 float dist[kVoxPerThread];
                 {
                     float win[16];
@@ -258,7 +254,7 @@ __global__ void __launch_bounds__(32 * TZ, 2)
 #pragma unroll
                     for (int r = 0; r < kVoxPerThread; r++) dist[r] = win[RX + r] * w0;
                 }
-                fast_rows<RX, RY, RZ, TZ, D_HALF, 0>(Dr, rowoff, dist, a);
+                fast_rows<RX, RY, RZ, TZ, TX, D_HALF, 0>(Dr, rowoff, dist, a);
                 float part = 0.0f;
 #pragma unroll
                 for (int r = 0; r < kVoxPerThread; r++) {
@@ -282,8 +278,7 @@ __global__ void __launch_bounds__(32 * TZ, 2)
                     for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
                     if (lane == 0 && part != 0.0f) {
                         const long long t8 =
-                            ((long long)((Z0 + 4 * (warp >> 2)) >> 3) * a.t8y + (Y0 >> 3)) * a.t8x +
-                            (X0 >> 3) + g;
+                            ((long long)((Z0 + zw) >> 3) * a.t8y + (Y0 >> 3)) * a.t8x + (X0 >> 3) + g;
                         atomicAdd(&a.map[t8 * a.S + scur], part);
                     }
                 }
@@ -355,23 +350,29 @@ __global__ void pad_reflective_half_kernel(const float* __restrict__ in, int nx,
     }
 }
 
-template <int RX, int RY, int RZ, int TZ, bool D_HALF>
+template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF>
 static size_t fast_smem_for(const FastArgs& a) {
-    using F = FastGeom<RX, RY, RZ, TZ, D_HALF>;
+    using F = FastGeom<RX, RY, RZ, TZ, TX, D_HALF>;
     size_t pb = (size_t)(a.pbx * a.pby * a.pbz + 63) / 64 * 128;  // bytes
     size_t rb = (size_t)((a.rbx + 1) * a.rby * a.rbz + 63) / 64 * 128;
     return 128 + pb + rb + 2 * (size_t)F::DBYTES;
 }
 
-template <int RX, int RY, int RZ, int TZ, bool D_HALF>
+template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF>
 static cudaError_t fast_launch_inst(const CUtensorMap* tmp, const FastArgs& a, int tiles_z,
                                     size_t smem, cudaStream_t st, bool mass) {
-    auto kern = mass ? nlm_tile_fast_kernel<RX, RY, RZ, TZ, D_HALF, true>
-                     : nlm_tile_fast_kernel<RX, RY, RZ, TZ, D_HALF, false>;
+    auto kern = nlm_tile_fast_kernel<RX, RY, RZ, TZ, TX, D_HALF, false>;
+    if (mass) {
+        // weight-mass maps run on the full-search (TX = 32) configuration
+        if constexpr (TX == 32)
+            kern = nlm_tile_fast_kernel<RX, RY, RZ, TZ, TX, D_HALF, true>;
+        else
+            return cudaErrorInvalidConfiguration;
+    }
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
-    kern<<<grid, 32 * TZ, smem, st>>>(*tmp, a);
+    kern<<<grid, TX * TZ, smem, st>>>(*tmp, a);
     return cudaGetLastError();
 }
 
@@ -379,11 +380,13 @@ static cudaError_t fast_launch_inst(const CUtensorMap* tmp, const FastArgs& a, i
     X(1, 1, 1) X(1, 1, 2) X(1, 1, 3) X(2, 2, 1) X(2, 2, 2) X(3, 3, 1) X(3, 3, 2) X(3, 3, 3)
 
 size_t fast_smem_bytes(const FastConfig& c, const FastArgs& a) {
-#define X(A, B, C)                                                                 \
-    if (c.rx == A && c.ry == B && c.rz == C) {                                     \
-        if (c.tz == 8 && c.d_half) return fast_smem_for<A, B, C, 8, true>(a);      \
-        if (c.tz == 8 && !c.d_half) return fast_smem_for<A, B, C, 8, false>(a);    \
-        if (c.tz == 4 && c.d_half) return fast_smem_for<A, B, C, 4, true>(a);      \
+#define X(A, B, C)                                                                          \
+    if (c.rx == A && c.ry == B && c.rz == C) {                                              \
+        if (c.tx == 32 && c.tz == 8 && c.d_half) return fast_smem_for<A, B, C, 8, 32, true>(a);   \
+        if (c.tx == 32 && c.tz == 8 && !c.d_half) return fast_smem_for<A, B, C, 8, 32, false>(a); \
+        if (c.tx == 32 && c.tz == 4 && c.d_half) return fast_smem_for<A, B, C, 4, 32, true>(a);   \
+        if (c.tx == 8 && c.tz == 8 && c.d_half) return fast_smem_for<A, B, C, 8, 8, true>(a);     \
+        if (c.tx == 8 && c.tz == 8 && !c.d_half) return fast_smem_for<A, B, C, 8, 8, false>(a);   \
     }
     INLM_FAST_SHAPES(X)
 #undef X
@@ -392,14 +395,19 @@ size_t fast_smem_bytes(const FastConfig& c, const FastArgs& a) {
 
 cudaError_t launch_fast_kernel(const FastConfig& c, const CUtensorMap* tm_prev, const FastArgs& a,
                                int tiles_z, cudaStream_t st, bool mass) {
-#define X(A, B, C)                                                                              \
-    if (c.rx == A && c.ry == B && c.rz == C) {                                                  \
-        if (c.tz == 8 && c.d_half)                                                              \
-            return fast_launch_inst<A, B, C, 8, true>(tm_prev, a, tiles_z, c.smem_bytes, st, mass);  \
-        if (c.tz == 8 && !c.d_half)                                                             \
-            return fast_launch_inst<A, B, C, 8, false>(tm_prev, a, tiles_z, c.smem_bytes, st, mass); \
-        if (c.tz == 4 && c.d_half)                                                              \
-            return fast_launch_inst<A, B, C, 4, true>(tm_prev, a, tiles_z, c.smem_bytes, st, mass);  \
+#define X(A, B, C)                                                                           \
+    if (c.rx == A && c.ry == B && c.rz == C) {                                               \
+        const size_t sm = c.smem_bytes;                                                      \
+        if (c.tx == 32 && c.tz == 8 && c.d_half)                                             \
+            return fast_launch_inst<A, B, C, 8, 32, true>(tm_prev, a, tiles_z, sm, st, mass);  \
+        if (c.tx == 32 && c.tz == 8 && !c.d_half)                                            \
+            return fast_launch_inst<A, B, C, 8, 32, false>(tm_prev, a, tiles_z, sm, st, mass); \
+        if (c.tx == 32 && c.tz == 4 && c.d_half)                                             \
+            return fast_launch_inst<A, B, C, 4, 32, true>(tm_prev, a, tiles_z, sm, st, mass);  \
+        if (c.tx == 8 && c.tz == 8 && c.d_half)                                              \
+            return fast_launch_inst<A, B, C, 8, 8, true>(tm_prev, a, tiles_z, sm, st, mass);   \
+        if (c.tx == 8 && c.tz == 8 && !c.d_half)                                             \
+            return fast_launch_inst<A, B, C, 8, 8, false>(tm_prev, a, tiles_z, sm, st, mass);  \
     }
     INLM_FAST_SHAPES(X)
 #undef X

@@ -16,7 +16,7 @@ struct FastArgs {
     int sxr, syr, szc;
     int S;                                  // full-search offset count
     const int2* __restrict__ search_delta;  // (prev-box delta, raw shared delta) per offset
-    const int* __restrict__ plan_offsets;   // per-CTA lists of offset | (x sub-block mask << 16)
+    const int* __restrict__ plan_offsets;   // per-CTA lists of search-offset indices
     const int* __restrict__ plan_start;     // CTA c uses plan_offsets[start[c] .. start[c]+count[c])
     const int* __restrict__ plan_count;
     int pbx, pby, pbz;                      // FP16 prev box extents (x in halves)
@@ -36,6 +36,7 @@ struct FastArgs {
 struct FastConfig {
     int rx, ry, rz;
     int tz;
+    int tx;       // CTA width: 32 (full search) or 8 (one 8^3 tile per CTA, per-tile plans)
     bool d_half;  // squared-difference planes in FP16 (else FP32)
     size_t smem_bytes;
 };

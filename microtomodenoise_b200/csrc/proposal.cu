@@ -589,33 +589,20 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-__global__ void net_plan_build_kernel(const unsigned* __restrict__ bitmap, int nwords, Dim3i t8,
-                                      int cta_x, int cta_y, int n_cta, int tz, int S,
-                                      int* __restrict__ plan_off, int* __restrict__ plan_count,
-                                      int* counters) {
+// Per 8^3 tile (one warp): the kept offsets in ascending order, compacted
+// from the tile's bitmap into plan_off[tile * S ...]; plan_count[tile].
+__global__ void net_plan_tiles_kernel(const unsigned* __restrict__ bitmap, int nwords,
+                                      long long n_tiles, int S, int* __restrict__ plan_off,
+                                      int* __restrict__ plan_count, int* counters) {
     const int lane = threadIdx.x & 31;
-    const long long c = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    if (c >= n_cta) return;
-    const int bx = (int)(c % cta_x);
-    const int by = (int)((c / cta_x) % cta_y);
-    const int bz = (int)(c / ((long long)cta_x * cta_y));
-    const int ty = by, tzz = (bz * tz) / 8;
-    long long trow[4];
-    bool valid[4];
-#pragma unroll
-    for (int b = 0; b < 4; b++) {
-        const int tx = 4 * bx + b;
-        valid[b] = tx < t8.x && ty < t8.y && tzz < t8.z;
-        trow[b] = ((long long)(tzz * t8.y + ty) * t8.x + tx) * nwords;
-    }
-    int* out = plan_off + c * (long long)S;
+    const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    if (t >= n_tiles) return;
+    const unsigned* row = bitmap + t * nwords;
+    int* out = plan_off + t * (long long)S;
     int n = 0;
     for (int w0 = 0; w0 < nwords; w0 += 32) {
         const int wd = w0 + lane;
-        unsigned m[4];
-#pragma unroll
-        for (int b = 0; b < 4; b++) m[b] = (wd < nwords && valid[b]) ? bitmap[trow[b] + wd] : 0u;
-        unsigned u = m[0] | m[1] | m[2] | m[3];
+        unsigned u = wd < nwords ? row[wd] : 0u;
         const int cnt = __popc(u);
         int incl = cnt;
 #pragma unroll
@@ -627,15 +614,14 @@ __global__ void net_plan_build_kernel(const unsigned* __restrict__ bitmap, int n
         while (u) {
             const int bit = __ffs(u) - 1;
             u &= u - 1;
-            const int mask = (int)(((m[0] >> bit) & 1u) | (((m[1] >> bit) & 1u) << 1) |
-                                   (((m[2] >> bit) & 1u) << 2) | (((m[3] >> bit) & 1u) << 3));
-            if (pos < S) out[pos] = (wd * 32 + bit) | (mask << 16);
+            const int k = wd * 32 + bit;
+            if (pos < S && k < S) out[pos] = k;
             pos++;
         }
         n += __shfl_sync(0xffffffffu, incl, 31);
     }
     if (lane == 0) {
-        plan_count[c] = min(n, S);
+        plan_count[t] = min(n, S);
         atomicAdd(&counters[1], min(n, S));
     }
 }
@@ -810,15 +796,12 @@ cudaError_t net_select(const NetLayout& L, const __nv_bfloat16* wb, const float*
     return cudaGetLastError();
 }
 
-cudaError_t net_plan_build(const unsigned* bitmap, int nwords, Dim3i tiles8, int cta_x, int cta_y,
-                           int cta_z, int tz, int S, int* plan_off, int* plan_count, int* counters,
-                           cudaStream_t st) {
-    const long long n_cta = (long long)cta_x * cta_y * cta_z;
-    if (n_cta <= 0) return cudaSuccess;
-    const long long blocks = (n_cta * 32 + 127) / 128;
-    net_plan_build_kernel<<<(unsigned)blocks, 128, 0, st>>>(bitmap, nwords, tiles8, cta_x, cta_y,
-                                                            (int)n_cta, tz, S, plan_off, plan_count,
-                                                            counters);
+cudaError_t net_plan_tiles(const unsigned* bitmap, int nwords, long long n_tiles, int S,
+                           int* plan_off, int* plan_count, int* counters, cudaStream_t st) {
+    if (n_tiles <= 0) return cudaSuccess;
+    const long long blocks = (n_tiles * 32 + 127) / 128;
+    net_plan_tiles_kernel<<<(unsigned)blocks, 128, 0, st>>>(bitmap, nwords, n_tiles, S, plan_off,
+                                                            plan_count, counters);
     return cudaGetLastError();
 }
 

@@ -73,13 +73,10 @@ cudaError_t net_select(const NetLayout& L, const __nv_bfloat16* wb, const float*
                        int n_tiles, int K, float min_mass, unsigned* bitmap, int nwords,
                        float* pred_mass, int* counters, cudaStream_t st);
 
-// Per filter CTA (32 x 8 x tz voxels, four 8^3 tiles along x): the union of
-// its tiles' kept offsets in ascending order, each entry offset | (mask << 16)
-// with bit b of mask = the tile at x sub-block b uses it. plan_start[c] = c*S.
-// counters[1] += entries written.
-cudaError_t net_plan_build(const unsigned* bitmap, int nwords, Dim3i tiles8, int cta_x, int cta_y,
-                           int cta_z, int tz, int S, int* plan_off, int* plan_count, int* counters,
-                           cudaStream_t st);
+// Per 8^3 tile: its kept offsets in ascending order at plan_off[tile * S],
+// their number in plan_count[tile]; counters[1] += entries written.
+cudaError_t net_plan_tiles(const unsigned* bitmap, int nwords, long long n_tiles, int S,
+                           int* plan_off, int* plan_count, int* counters, cudaStream_t st);
 
 // Per-slice input scale from the filter multiplier m = -1/(sigma^2 beta).
 cudaError_t net_scale_from_mult(const float* mult, int nz, float* scale, cudaStream_t st);

@@ -14,16 +14,17 @@ constexpr int dpitch(int w) {
 }
 constexpr int round_up32(int v) { return (v + 31) / 32 * 32; }
 
-template <int RX, int RY, int RZ, int TZ>
+// TX: CTA width in x (32, or 8 for one 8^3 tile per CTA); 8 voxels per thread.
+template <int RX, int RY, int RZ, int TZ, int TX = kTX>
 struct TileGeom {
     static constexpr PatchRows rows = make_patch_rows(RX, RY, RZ);
-    static constexpr int DW = kTX + 2 * RX;
+    static constexpr int DW = TX + 2 * RX;
     static constexpr int DH = kTY + 2 * RY;
     static constexpr int DD = TZ + 2 * RZ;
     static constexpr int DP = dpitch(DW);
     static constexpr int DPLANE = DP * DH;
     static constexpr int ND = DW * DH * DD;
-    static constexpr int NT = 32 * TZ;
+    static constexpr int NT = TX * TZ;
 };
 
 // Tap counts of the reference geometry (float32 ellipsoid test).

@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY: the checker for the device kernels of
 microtomodenoise_b200/csrc/proposal.cu (forward, soft-target cross-entropy
-loss, backward, top-k selection and per-CTA plans). Nothing in the product
+loss, backward, top-k selection and per-tile plans). Nothing in the product
 imports it. The network has no counterpart in the reference; what it prunes
 is the search loop of Denoiser/iternlm_cpu.cpp:758-843.
 
@@ -198,22 +198,6 @@ def select(logits, k, min_mass):
     return keep, pm, fb
 
 
-def plans(keep, tiles8_zyx, cta_grid_zyx, tz):
-    """Per-CTA plan entries (offset | mask << 16) of the FP16 filter's
-    32 x 8 x tz CTAs from per-8^3-tile keep flags."""
-    t8z, t8y, t8x = tiles8_zyx
-    cz, cy, cx = cta_grid_zyx
-    keep = keep.reshape(t8z, t8y, t8x, -1)
-    S = keep.shape[-1]
-    out = []
-    for bz in range(cz):
-        for by in range(cy):
-            for bx in range(cx):
-                masks = np.zeros(S, np.int64)
-                for b in range(4):
-                    tx = 4 * bx + b
-                    if tx < t8x:
-                        masks |= keep[(bz * tz) // 8, by, tx].astype(np.int64) << b
-                ks = np.nonzero(masks)[0]
-                out.append([int(k) | (int(masks[k]) << 16) for k in ks])
-    return out
+def plans(keep):
+    """Per-8^3-tile plan lists (kept offsets in ascending order) from keep flags."""
+    return [np.nonzero(row)[0].tolist() for row in np.asarray(keep, bool)]

@@ -48,9 +48,10 @@ def run(raw, pr, sr, sigmas, precision, plan=None):
     return np.stack(outs), desc
 
 
-def tile_grid(shape_zyx, tz=8):
+def tile_grid(shape_zyx):
+    """8^3 tile counts (x, y, z): plans hold one offset list per 8^3 tile."""
     nz, ny, nx = shape_zyx
-    return (-(-nx // 32), -(-ny // 8), -(-nz // tz))
+    return (-(-nx // 8), -(-ny // 8), -(-nz // 8))
 
 
 @pytest.mark.parametrize("precision", ["f16", "f16_df32"])
@@ -74,7 +75,8 @@ def test_plan_with_every_offset_equals_full_search(gpu):
     n = int(np.prod(tile_grid(vol.shape)))
     plan = (np.arange(n) * S, np.full(n, S), np.tile(np.arange(S), n))
     got, desc = run(vol, (1, 1, 1), (2, 2, 2), sig, "f16", plan)
-    assert "plan=per-tile" in desc
+    assert "plan=per-tile" in desc and "tx=8" in desc
+    # the one-tile-per-CTA kernel rounds every voxel as the full-search kernel does
     assert np.array_equal(got, full)
 
 
@@ -96,7 +98,7 @@ def test_plan_subsets_vs_fp64_oracle(gpu, port):
         offs.extend(sel.tolist())
     sig = np.stack([np.full(vol.shape[0], 0.07, np.float32)] * 2)
     got, _ = run(vol, (1, 1, 1), (3, 3, 3), sig, "f16", (start, count, offs))
-    ref = port.denoise_f64_plan(vol, p, sig, (32, 8, 8), keep)
+    ref = port.denoise_f64_plan(vol, p, sig, (8, 8, 8), keep)
     check_close(got[-1], ref, "plan")
 
 

@@ -205,12 +205,11 @@ def test_proposal_plans_vs_fp64_plan_oracle(gpu, port):
     sig = np.stack([np.full(vol.shape[0], 0.07, np.float32)] * 2)
     got, keeps, stats, (ts, tc) = run_with_net(vol, pr, sr, sig, net, k, 0.0, record=True)
     assert all(kp.sum(axis=1).max() == k for kp in keeps)
-    # entries the filter evaluated = the per-CTA unions of the tiles' top-k
-    t8 = tuple(-(-n // 8) for n in vol.shape)
+    # entries the filter evaluated = each 8^3 tile's own top-k
     for kp, st in zip(keeps, stats):
-        plans = po.plans(kp, t8, (tc[2], tc[1], tc[0]), ts[2])
-        assert st["offsets_evaluated"] == sum(len(x) for x in plans)
+        assert st["offsets_evaluated"] == sum(len(x) for x in po.plans(kp)) == k * kp.shape[0]
         assert st["fallback_tiles"] == 0 and st["tiles"] == kp.shape[0]
+        assert st["fraction_evaluated"] == k / S
     ref = port.denoise_f64_plan(vol, p, sig, (8, 8, 8), np.stack(keeps))
     check_close(got[-1], ref, "plan")
     net.close()

@@ -1,5 +1,5 @@
 """CPU checks of the proposal oracle itself (no GPU): its gradients against
-finite differences, its top-k tie rule and per-CTA plans, and the FP64
+finite differences, its top-k tie rule and per-tile plans, and the FP64
 plan / weight-mass restatements against the plain FP64 filter."""
 import numpy as np
 
@@ -48,15 +48,11 @@ def test_select_ties_and_fallback():
     assert fb.tolist() == [True, False] and keep[0].all()
 
 
-def test_plans_union_and_masks():
-    S = 6
-    keep = np.zeros((1, 1, 5, S), bool)   # t8 grid (1, 1, 5): two CTAs along x
-    keep[0, 0, 0, [0, 2]] = True
-    keep[0, 0, 1, [2, 3]] = True
-    keep[0, 0, 4, [5]] = True
-    plans = po.plans(keep.reshape(5, S), (1, 1, 5), (1, 1, 2), 8)
-    assert plans[0] == [0 | (1 << 16), 2 | (3 << 16), 3 | (2 << 16)]
-    assert plans[1] == [5 | (1 << 16)]
+def test_plans_per_tile():
+    keep = np.zeros((3, 6), bool)
+    keep[0, [0, 2]] = True
+    keep[2, [5, 1]] = True
+    assert po.plans(keep) == [[0, 2], [], [1, 5]]
 
 
 def test_plan_oracle_keep_all_is_full_search(port):
