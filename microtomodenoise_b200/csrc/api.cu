@@ -497,7 +497,9 @@ static int build_fast_config(inlm_denoiser* d, int tx, FastConfig* cfg, FastArgs
     for (int si = 0; si < a.S; si++) {
         const Offset3& o = g.search[si];
         dl[si].x = o.z * a.pbx * a.pby + o.y * a.pbx + o.x;
-        dl[si].y = o.z * rpx * a.rby + o.y * rpx + o.x;
+        // raw: shared-box delta (tx = 32) or padded global delta (tx = 8)
+        dl[si].y = tx == 8 ? (int)(o.z * d->pitch_z + o.y * d->pitch_y + o.x)
+                           : o.z * rpx * a.rby + o.y * rpx + o.x;
     }
     CUDA_TRY(dalloc(d_delta, a.S));
     CUDA_TRY(cudaMemcpy(*d_delta, dl.data(), a.S * sizeof(int2), cudaMemcpyHostToDevice));

@@ -74,9 +74,12 @@ __device__ __forceinline__ void load_row(const void* rowp, float (&win)[16]) {
     }
 }
 
-template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF, int RI>
+// Patch distances of a thread's VPT consecutive voxels: rows of the D planes
+// in the reference tap order. XOFF = the voxels' first column within the
+// 16-byte-aligned row start rowoff points at.
+template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF, int VPT, int XOFF, int RI>
 __device__ __forceinline__ void fast_rows(const unsigned char* __restrict__ Db, int rowoff,
-                                          float (&dist)[kVoxPerThread], const FastArgs& a) {
+                                          float (&dist)[VPT], const FastArgs& a) {
     using G = TileGeom<RX, RY, RZ, TZ, TX>;
     using F = FastGeom<RX, RY, RZ, TZ, TX, D_HALF>;
     if constexpr (RI < G::rows.n) {
@@ -85,38 +88,68 @@ __device__ __forceinline__ void fast_rows(const unsigned char* __restrict__ Db, 
         constexpr int e = G::rows.e[RI];
         constexpr int first = RowFirst<RX, RY, RZ, RI>::value;
         constexpr int esz = D_HALF ? 2 : 4;
+        static_assert(XOFF + RX + VPT - 1 + e < 16, "row window");
         const unsigned char* rowp =
             Db + (size_t)(rowoff + (zp + RZ) * F::DPLANE + (yp + RY) * F::DP) * esz;
         float win[16];
-        load_row<D_HALF, RX - e, RX + kVoxPerThread - 1 + e>(rowp, win);
+        load_row<D_HALF, XOFF + RX - e, XOFF + RX + VPT - 1 + e>(rowp, win);
 #pragma unroll
         for (int xp = -e; xp <= e; xp++) {
             if (zp == 0 && yp == 0 && xp == 0) continue;
             const int t = first + (xp + e) - ((zp == 0 && yp == 0 && xp > 0) ? 1 : 0);
             const float w = a.w[t];
 #pragma unroll
-            for (int r = 0; r < kVoxPerThread; r++) dist[r] = fmaf(win[RX + r + xp], w, dist[r]);
+            for (int r = 0; r < VPT; r++) dist[r] = fmaf(win[XOFF + RX + r + xp], w, dist[r]);
         }
-        fast_rows<RX, RY, RZ, TZ, TX, D_HALF, RI + 1>(Db, rowoff, dist, a);
+        fast_rows<RX, RY, RZ, TZ, TX, D_HALF, VPT, XOFF, RI + 1>(Db, rowoff, dist, a);
     }
 }
 
+template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF, int VPT, int XOFF>
+__device__ __forceinline__ void tile_distances(const unsigned char* __restrict__ Dr, int rowoff,
+                                               float (&dist)[VPT], const FastArgs& a) {
+    using F = FastGeom<RX, RY, RZ, TZ, TX, D_HALF>;
+    float win[16];
+    constexpr int esz = D_HALF ? 2 : 4;
+    load_row<D_HALF, XOFF + RX, XOFF + RX + VPT - 1>(
+        Dr + (size_t)(rowoff + RZ * F::DPLANE + RY * F::DP) * esz, win);
+    const float w0 = a.w[0];
+#pragma unroll
+    for (int r = 0; r < VPT; r++) dist[r] = win[XOFF + RX + r] * w0;
+    fast_rows<RX, RY, RZ, TZ, TX, D_HALF, VPT, XOFF, 0>(Dr, rowoff, dist, a);
+}
+
+// Voxels per thread. 8 for both CTA widths: 4 per thread (a 4-warp one-tile
+// CTA, 20 warps per SM) measured 12% slower than 8 (10 warps per SM), the
+// extra row-window loads and conversions costing more than the occupancy
+// returns.
+template <int TX>
+struct FastThreads {
+    static constexpr int VPT = kVoxPerThread;
+};
+
 // TX = 32: CTA of 32 x 8 x TZ voxels (four 8^3 tiles along x when TZ = 8),
-// two CTAs per SM; TX = 8: CTA of one 8 x 8 x TZ tile, four CTAs per SM.
+// two CTAs per SM; TX = 8: CTA of one 8 x 8 x TZ tile (64 threads), five
+// CTAs per SM.
 template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF, bool MASS>
-__global__ void __launch_bounds__(TX * TZ, TX == 32 ? 2 : 4)
+__global__ void __launch_bounds__(TX * TZ * 8 / FastThreads<TX>::VPT, TX == 32 ? 2 : 5)
     nlm_tile_fast_kernel(const __grid_constant__ CUtensorMap tm_prev,
                          const __grid_constant__ FastArgs a) {
     using G = TileGeom<RX, RY, RZ, TZ, TX>;
     using F = FastGeom<RX, RY, RZ, TZ, TX, D_HALF>;
+    constexpr int VPT = FastThreads<TX>::VPT;
+    constexpr int NT = TX * TZ * 8 / VPT;  // threads
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
     __half* prevb = reinterpret_cast<__half*>(smem + 128);
     const int pplane = a.pbx * a.pby;
     const int PB = pplane * a.pbz;  // halves
+    // TX = 8 reads raw through L1 from global memory (its CTAs are small, so
+    // shared memory bounds how many share an SM); TX = 32 stages the raw box.
+    constexpr bool RAW_G = (TX == 8);
     __half* rawb = reinterpret_cast<__half*>(smem + 128 + (size_t)(PB + 63) / 64 * 128);
     const int rpx = a.rbx + 1;
-    const int RB = rpx * a.rby * a.rbz;  // halves
+    const int RB = RAW_G ? 0 : rpx * a.rby * a.rbz;  // halves
     unsigned char* D0 = reinterpret_cast<unsigned char*>(rawb) + (size_t)(RB + 63) / 64 * 128;
 
     const int tid = threadIdx.x;
@@ -135,12 +168,12 @@ __global__ void __launch_bounds__(TX * TZ, TX == 32 ? 2 : 4)
         mbar_arrive_expect_tx(bar, (uint32_t)PB * 2u);
         tma_load_3d(prevb, &tm_prev, X0, Y0, Z0, bar);
     }
-    {
+    if (!RAW_G) {
         // raw over tile + search halo (FP16), odd row pitch
         const int rb_n = a.rbx * a.rby * a.rbz;
         const __half* rsrc = a.raw_pad + (long long)(Z0 + RZ) * a.gpitch_z +
                              (long long)(Y0 + RY) * a.gpitch_y + X0;
-        for (int i = tid; i < rb_n; i += G::NT) {
+        for (int i = tid; i < rb_n; i += NT) {
             int xx = i % a.rbx;
             int rest = i / a.rbx;
             int yy = rest % a.rby;
@@ -157,15 +190,23 @@ __global__ void __launch_bounds__(TX * TZ, TX == 32 ? 2 : 4)
         s_count = min(a.plan_count[cta], a.S);
     }
 
+    // the (prev box, raw) deltas of this CTA's offsets, staged once
+    int2* sdl = reinterpret_cast<int2*>(D0 + 2 * (size_t)F::DBYTES);
+    for (int i = tid; i < s_count; i += NT) {
+        const int e = a.plan_offsets ? min(max(a.plan_offsets[s_begin + i], 0), a.S - 1) : i;
+        sdl[i] = __ldg(&a.search_delta[e]);
+    }
+    __syncthreads();
+
     // scale D by 1/sigma^2 of the tile's middle slice (FP16 normal range)
     const float scale = -a.mult[min(Z0 + TZ / 2, a.nz - 1)];
 
     constexpr int NPAIR = G::ND / 2;
-    constexpr int NQ = (NPAIR + G::NT - 1) / G::NT;
+    constexpr int NQ = (NPAIR + NT - 1) / NT;
     int qpi[NQ], qdi[NQ];
 #pragma unroll
     for (int k = 0; k < NQ; k++) {
-        int q = min(tid + k * G::NT, NPAIR - 1);
+        int q = min(tid + k * NT, NPAIR - 1);
         int f = 2 * q;
         int c = f % G::DW;
         int rest = f / G::DW;
@@ -199,29 +240,38 @@ __global__ void __launch_bounds__(TX * TZ, TX == 32 ? 2 : 4)
         }
     };
 
-    // Phase B lane map: a warp covers 8 x 8 x 4 voxels of one 8^3 tile, lane =
-    // (row j, plane), 8 consecutive x voxels each. TX = 32: warp w takes x
+    // Phase B lane map: a warp covers VPT x 8 x 4 voxels of one 8^3 tile, lane
+    // = (row j, plane), VPT consecutive x voxels each. TX = 32: warp w takes x
     // sub-block g = w % 4 (columns 8g..8g+7) and planes 4*(w/4)..+3; TX = 8:
-    // planes 4w..4w+3.
+    // x half w / 2 (columns 4*(w/2)..+3) and planes 4*(w%2)..+3.
     const int warp = tid >> 5, lane = tid & 31;
     const int g = (TX == 32) ? (warp & 3) : 0;
+    const int xh = (TX == 32) ? 0 : (warp >> 1);
     const int j = lane & 7;
-    const int zw = (TX == 32) ? 4 * (warp >> 2) : 4 * warp;  // first plane of the warp
-    const int kp = zw + (lane >> 3);                          // z-plane of the CTA
-    const int x0 = g * kVoxPerThread;
+    const int zw = (TX == 32) ? 4 * (warp >> 2) : 4 * (warp & 1);  // first plane of the warp
+    const int kp = zw + (lane >> 3);                                 // z-plane of the CTA
+    const int x0 = (TX == 32) ? g * VPT : xh * VPT;
     const int zk = min(Z0 + kp, a.nz - 1);
     const float rel = a.mult[zk] / scale;  // x = dist' * rel
-    const int rowoff = kp * F::DPLANE + j * F::DP + x0;
-    const int rbase = (a.szc + kp) * (rpx * a.rby) + (a.syr + j) * rpx + (RX + a.sxr + x0);
+    // D row start (16-byte aligned): TX = 32 includes x0, TX = 8 passes the
+    // x half as a compile-time column offset
+    const int rowoff = kp * F::DPLANE + j * F::DP + (TX == 32 ? x0 : 0);
+    // raw of the lane's first voxel: shared box index, or padded global index
+    // (the offset deltas dl.y index the same space)
+    const long long rbase =
+        RAW_G ? (long long)(Z0 + kp + a.pz) * a.gpitch_z + (long long)(Y0 + j + a.py) * a.gpitch_y +
+                    (X0 + x0 + a.px)
+              : (long long)((a.szc + kp) * (rpx * a.rby) + (a.syr + j) * rpx + (RX + a.sxr + x0));
+    const __half* rsrc_v = RAW_G ? a.raw_pad : rawb;
 
-    float acc[kVoxPerThread], wsum[kVoxPerThread], wmax[kVoxPerThread];
+    float acc[VPT], wsum[VPT], wmax[VPT];
 #pragma unroll
-    for (int r = 0; r < kVoxPerThread; r++) acc[r] = wsum[r] = wmax[r] = 0.0f;
-    float inv[kVoxPerThread];  // MASS: 1 / weight sum of the voxel (0 outside the volume)
+    for (int r = 0; r < VPT; r++) acc[r] = wsum[r] = wmax[r] = 0.0f;
+    float inv[VPT];  // MASS: 1 / weight sum of the voxel (0 outside the volume)
     if constexpr (MASS) {
         const int z = Z0 + kp, y = Y0 + j;
 #pragma unroll
-        for (int r = 0; r < kVoxPerThread; r++) {
+        for (int r = 0; r < VPT; r++) {
             const int x = X0 + x0 + r;
             inv[r] = (z < a.nz && y < a.ny && x < a.nx)
                          ? a.aux[((long long)z * a.ny + y) * a.nx + x]
@@ -230,34 +280,49 @@ __global__ void __launch_bounds__(TX * TZ, TX == 32 ? 2 : 4)
     }
 
     if (s_count > 0) {
-        int ent = a.plan_offsets ? min(max(a.plan_offsets[s_begin], 0), a.S - 1) : 0;
-        int2 dl = __ldg(&a.search_delta[ent]);
+        int ent = 0;
+        int2 dl = sdl[0];
+        // global raw (TX = 8): the next offset's VPT values are loaded one
+        // offset ahead so the loads overlap a whole offset's arithmetic
+        float rnext[VPT];
+        if constexpr (RAW_G && !MASS) {
+#pragma unroll
+            for (int r = 0; r < VPT; r++) rnext[r] = __half2float(rsrc_v[rbase + dl.y + r]);
+        }
         phase_a(D0, dl.x);
         __syncthreads();
         for (int i = 0; i < s_count; i++) {
             const unsigned char* Dr = D0 + (size_t)(i & 1) * F::DBYTES;
             const int dly = dl.y;
-            const int scur = ent;
+            const int scur = ent;  // offset index (MASS runs without a plan)
+            float rcur[VPT];
+            if constexpr (RAW_G && !MASS) {
+#pragma unroll
+                for (int r = 0; r < VPT; r++) rcur[r] = rnext[r];
+            }
             if (i + 1 < s_count) {
-                ent = a.plan_offsets ? min(max(a.plan_offsets[s_begin + i + 1], 0), a.S - 1) : i + 1;
-                dl = __ldg(&a.search_delta[ent]);
+                ent = i + 1;
+                dl = sdl[i + 1];
+                if constexpr (RAW_G && !MASS) {
+#pragma unroll
+                    for (int r = 0; r < VPT; r++)
+                        rnext[r] = __half2float(rsrc_v[rbase + dl.y + r]);
+                }
                 phase_a(D0 + (size_t)((i + 1) & 1) * F::DBYTES, dl.x);
             }
             {
-                float dist[kVoxPerThread];
-                {
-                    float win[16];
-                    constexpr int esz = D_HALF ? 2 : 4;
-                    load_row<D_HALF, RX, RX + kVoxPerThread - 1>(
-                        Dr + (size_t)(rowoff + RZ * F::DPLANE + RY * F::DP) * esz, win);
-                    const float w0 = a.w[0];
-#pragma unroll
-                    for (int r = 0; r < kVoxPerThread; r++) dist[r] = win[RX + r] * w0;
+                float dist[VPT];
+                if constexpr (TX == 8 && VPT < kVoxPerThread) {
+                    if (xh)  // warp-uniform
+                        tile_distances<RX, RY, RZ, TZ, TX, D_HALF, VPT, VPT>(Dr, rowoff, dist, a);
+                    else
+                        tile_distances<RX, RY, RZ, TZ, TX, D_HALF, VPT, 0>(Dr, rowoff, dist, a);
+                } else {
+                    tile_distances<RX, RY, RZ, TZ, TX, D_HALF, VPT, 0>(Dr, rowoff, dist, a);
                 }
-                fast_rows<RX, RY, RZ, TZ, TX, D_HALF, 0>(Dr, rowoff, dist, a);
                 float part = 0.0f;
 #pragma unroll
-                for (int r = 0; r < kVoxPerThread; r++) {
+                for (int r = 0; r < VPT; r++) {
                     const float x = dist[r] * rel;
                     // Pade[3/3] of exp in Horner form, FMA
                     const float num = fmaf(fmaf(x + 12.f, x, 60.f), x, 120.f);
@@ -266,7 +331,11 @@ __global__ void __launch_bounds__(TX * TZ, TX == 32 ? 2 : 4)
                     if constexpr (MASS) {
                         part = fmaf(w, inv[r], part);
                     } else {
-                        const float rs = __half2float(rawb[rbase + dly + r]);
+                        float rs;
+                        if constexpr (RAW_G)
+                            rs = rcur[r];
+                        else
+                            rs = __half2float(rsrc_v[rbase + dly + r]);
                         acc[r] = fmaf(w, rs, acc[r]);
                         wsum[r] += w;
                         wmax[r] = fmaxf(wmax[r], w);
@@ -295,17 +364,17 @@ __global__ void __launch_bounds__(TX * TZ, TX == 32 ? 2 : 4)
             // weight-sum pass of the mass maps: 1 / (sum of the offsets' weights)
             float* arow = a.aux + ((long long)z * a.ny + y) * a.nx;
 #pragma unroll
-            for (int r = 0; r < kVoxPerThread; r++) {
+            for (int r = 0; r < VPT; r++) {
                 const int x = X0 + x0 + r;
                 if (x < a.nx) arow[x] = wsum[r] > 0.0f ? 1.0f / wsum[r] : 0.0f;
             }
             return;
         }
 #pragma unroll
-        for (int r = 0; r < kVoxPerThread; r++) {
+        for (int r = 0; r < VPT; r++) {
             int x = X0 + x0 + r;
             if (x < a.nx) {
-                const float raw0 = __half2float(rawb[rbase + r]);
+                const float raw0 = __half2float(rsrc_v[rbase + r]);
                 float res = raw0;
                 if (wmax[r] > 0.0f) {
                     // per-voxel weight-sum normalisation in FP64
@@ -354,8 +423,9 @@ template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF>
 static size_t fast_smem_for(const FastArgs& a) {
     using F = FastGeom<RX, RY, RZ, TZ, TX, D_HALF>;
     size_t pb = (size_t)(a.pbx * a.pby * a.pbz + 63) / 64 * 128;  // bytes
-    size_t rb = (size_t)((a.rbx + 1) * a.rby * a.rbz + 63) / 64 * 128;
-    return 128 + pb + rb + 2 * (size_t)F::DBYTES;
+    size_t rb = TX == 8 ? 0 : (size_t)((a.rbx + 1) * a.rby * a.rbz + 63) / 64 * 128;
+    const size_t dl = ((size_t)a.S * sizeof(int2) + 127) / 128 * 128;  // staged offset deltas
+    return 128 + pb + rb + 2 * (size_t)F::DBYTES + dl;
 }
 
 template <int RX, int RY, int RZ, int TZ, int TX, bool D_HALF>
@@ -372,7 +442,7 @@ static cudaError_t fast_launch_inst(const CUtensorMap* tmp, const FastArgs& a, i
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
-    kern<<<grid, TX * TZ, smem, st>>>(*tmp, a);
+    kern<<<grid, TX * TZ * 8 / FastThreads<TX>::VPT, smem, st>>>(*tmp, a);
     return cudaGetLastError();
 }
 

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(32 * TZ, 1)
     const int PB = pplane * a.pbz;
     float* rawb = prevb + round_up32(PB);
     // raw is staged with an odd row pitch (rpx = rbx + 1) so the phase-B reads
-    // of 8 y-lanes x 4 x-lanes fall in 32 distinct banks
+    // of a warp's 8 rows fall in distinct banks
     const int rpx = a.rbx + 1;
     const int RB = RAW_SMEM ? rpx * a.rby * a.rbz : 0;
     float* D = rawb + round_up32(RB);
@@ -199,10 +199,14 @@ __global__ void __launch_bounds__(32 * TZ, 1)
 #pragma unroll
     for (int k = 0; k < NQ; k++) qog[k] = pack2(prevb[qpi[k]], prevb[qpi[k] + 1]);
 
+    // Phase B lane map: a warp covers 8 x 8 x 4 voxels (x sub-block w % 4 of
+    // the CTA's 32 columns, z-planes 4*(w/4)..+3), lane = (row j, plane), 8
+    // consecutive x voxels each; every voxel's arithmetic is the same under
+    // any map.
     const int warp = tid >> 5, lane = tid & 31;
-    const int k = warp;
-    const int j = lane >> 2;
-    const int x0 = (lane & 3) * kVoxPerThread;
+    const int k = 4 * (warp >> 2) + (lane >> 3);  // z-plane of the CTA
+    const int j = lane & 7;
+    const int x0 = (warp & 3) * kVoxPerThread;
     const int zk = min(Z0 + k, a.nz - 1);
     const float m = a.mult[zk];
     const f32x2 m2 = splat2(m);

@@ -492,98 +492,117 @@ __device__ __forceinline__ unsigned order_key(float f) {
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-__global__ void __launch_bounds__(256)
-    net_select_kernel(const float* __restrict__ a4, int S, const __nv_bfloat16* __restrict__ Wh,
-                      const float* __restrict__ bh, int K, float min_mass, unsigned* __restrict__ bitmap,
-                      int nwords, float* __restrict__ pred_mass, int* counters) {
-    extern __shared__ float sl[];  // S logits, then S selection flags (bytes)
-    unsigned char* sel = reinterpret_cast<unsigned char*>(sl + S);
-    __shared__ float h[kNetC];
-    __shared__ float red[32];
-    __shared__ unsigned hist[256];
-    __shared__ unsigned s_prefix, s_remaining;
-    __shared__ int tie_base[256];
-    const long long tile = blockIdx.x;
-    if (threadIdx.x < kNetC) h[threadIdx.x] = a4[tile * kNetC + threadIdx.x];
-    __syncthreads();
+// One warp per tile: logits in the warp's shared-memory row, softmax
+// normaliser by shuffles, radix select of the K-th largest logit (8 bits per
+// pass, a warp-private 256-bin histogram), ties broken towards lower offsets;
+// offsets k = 32 i + lane are handled in rounds i, so a ballot of the kept
+// flags in round i is bitmap word i.
+constexpr int kSelWarps = 4;
+
+__global__ void __launch_bounds__(32 * kSelWarps)
+    net_select_kernel(const float* __restrict__ a4, long long n_tiles, int S,
+                      const __nv_bfloat16* __restrict__ Wh, const float* __restrict__ bh, int K,
+                      float min_mass, unsigned* __restrict__ bitmap, int nwords,
+                      float* __restrict__ pred_mass, int* counters) {
+    extern __shared__ unsigned sel_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rowlen = (S + 3) / 4 * 4;
+    float* sl = reinterpret_cast<float*>(sel_smem) + warp * rowlen;
+    unsigned* hist = sel_smem + kSelWarps * rowlen + warp * 256;
+    const long long tile = blockIdx.x * (long long)kSelWarps + warp;
+    if (tile >= n_tiles) return;
+    float h[kNetC];
+    load16(a4 + tile * kNetC, h);
     float m = -INFINITY;
-    for (int k = threadIdx.x; k < S; k += blockDim.x) {
+    for (int k = lane; k < S; k += 32) {
         const float l = head_logit(Wh, bh, h, k);
         sl[k] = l;
         m = fmaxf(m, l);
     }
-    const float M = block_reduce<true>(m, red);
+    const float M = warp_max(m);
     float z = 0.f;
-    for (int k = threadIdx.x; k < S; k += blockDim.x) z += expf(sl[k] - M);
-    const float Z = block_reduce<false>(z, red);
+    for (int k = lane; k < S; k += 32) z += expf(sl[k] - M);
+    const float Z = warp_sum(z);
+    __syncwarp();
 
-    // radix select of the K-th largest key, 8 bits at a time from the top
     const int Ke = min(max(K, 1), S);
-    unsigned prefix = 0, pmask = 0, remaining = (unsigned)Ke;
+    unsigned prefix = 0, pmask = 0;
+    int remaining = Ke;
     for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
-        __syncthreads();
-        for (int k = threadIdx.x; k < S; k += blockDim.x) {
+        for (int b = lane; b < 256; b += 32) hist[b] = 0;
+        __syncwarp();
+        for (int k = lane; k < S; k += 32) {
             const unsigned key = order_key(sl[k]);
             if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned cum = 0;
-            int b = 255;
-            for (; b > 0; b--) {
-                if (cum + hist[b] >= remaining) break;
-                cum += hist[b];
-            }
-            s_prefix = prefix | ((unsigned)b << shift);
-            s_remaining = remaining - cum;
+        __syncwarp();
+        // lane L owns bins 255-8L .. 248-8L (from the top); counts above them
+        // by an exclusive scan over the lanes
+        int own[8], tot = 0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            own[q] = (int)hist[255 - 8 * lane - q];
+            tot += own[q];
         }
-        __syncthreads();
-        prefix = s_prefix;
-        remaining = s_remaining;
+        int incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int above = incl - tot;  // keys in higher bins than this lane's
+        int found_bin = -1, found_above = 0;
+        if (above < remaining && incl >= remaining) {
+            int cum = above;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (found_bin < 0 && cum + own[q] >= remaining) {
+                    found_bin = 255 - 8 * lane - q;
+                    found_above = cum;
+                }
+                cum += own[q];
+            }
+        }
+        const unsigned ball = __ballot_sync(0xffffffffu, found_bin >= 0);
+        const int src = __ffs(ball) - 1;  // exactly one lane holds the bin
+        found_bin = __shfl_sync(0xffffffffu, found_bin, src < 0 ? 0 : src);
+        found_above = __shfl_sync(0xffffffffu, found_above, src < 0 ? 0 : src);
+        if (src < 0) found_bin = 0;  // unreachable for consistent counts
+        prefix |= (unsigned)found_bin << shift;
         pmask |= 255u << shift;
-        __syncthreads();
+        remaining -= found_above;
+        __syncwarp();
     }
     // keys above the K-th are kept; of the keys equal to it, the first
     // `remaining` in offset order
-    const int per = (S + blockDim.x - 1) / blockDim.x;
-    const int k0 = threadIdx.x * per, k1 = min(S, k0 + per);
-    int ties = 0;
-    for (int k = k0; k < k1; k++) ties += order_key(sl[k]) == prefix;
-    tie_base[threadIdx.x] = ties;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int i = 0; i < (int)blockDim.x; i++) {
-            const int c = tie_base[i];
-            tie_base[i] = run;
-            run += c;
-        }
-    }
-    __syncthreads();
-    int rank = tie_base[threadIdx.x];
     float kept = 0.f;
-    for (int k = k0; k < k1; k++) {
-        const unsigned key = order_key(sl[k]);
-        bool s = key > prefix;
-        if (key == prefix) {
-            s = rank < (int)remaining;
-            rank++;
-        }
-        sel[k] = s;
+    int ties_before = 0;
+    const int rounds = (S + 31) / 32;
+    for (int i = 0; i < rounds; i++) {
+        const int k = 32 * i + lane;
+        const unsigned key = k < S ? order_key(sl[k]) : 0u;
+        const bool tie = k < S && key == prefix;
+        const unsigned tb = __ballot_sync(0xffffffffu, tie);
+        const int rank = ties_before + __popc(tb & ((1u << lane) - 1u));
+        const bool s = k < S && (key > prefix || (tie && rank < remaining));
+        ties_before += __popc(tb);
         if (s) kept += expf(sl[k] - M);
     }
-    kept = block_reduce<false>(kept, red) / Z;
+    kept = warp_sum(kept) / Z;
     const bool fallback = !(kept >= min_mass);
-    for (int wd = threadIdx.x; wd < nwords; wd += blockDim.x) {
-        unsigned bits = 0;
-        for (int b = 0; b < 32; b++) {
-            const int k = wd * 32 + b;
-            if (k < S && (fallback || sel[k])) bits |= 1u << b;
-        }
-        bitmap[tile * nwords + wd] = bits;
+    ties_before = 0;
+    for (int i = 0; i < rounds; i++) {
+        const int k = 32 * i + lane;
+        const unsigned key = k < S ? order_key(sl[k]) : 0u;
+        const bool tie = k < S && key == prefix;
+        const unsigned tb = __ballot_sync(0xffffffffu, tie);
+        const int rank = ties_before + __popc(tb & ((1u << lane) - 1u));
+        ties_before += __popc(tb);
+        const bool s = k < S && (fallback || key > prefix || (tie && rank < remaining));
+        const unsigned word = __ballot_sync(0xffffffffu, s);
+        if (lane == 0 && i < nwords) bitmap[tile * nwords + i] = word;
     }
-    if (threadIdx.x == 0) {
+    if (lane == 0) {
         pred_mass[tile] = kept;
         if (fallback) atomicAdd(&counters[0], 1);
     }
@@ -785,14 +804,15 @@ cudaError_t net_select(const NetLayout& L, const __nv_bfloat16* wb, const float*
                        int n_tiles, int K, float min_mass, unsigned* bitmap, int nwords,
                        float* pred_mass, int* counters, cudaStream_t st) {
     if (n_tiles <= 0) return cudaSuccess;
-    const size_t sm = (size_t)L.S * 5;
+    const size_t sm = (size_t)kSelWarps * ((L.S + 3) / 4 * 4 + 256) * 4;
     if (sm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(net_select_kernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
     }
-    net_select_kernel<<<n_tiles, 256, sm, st>>>(a4, L.S, wb + L.wh, wf + L.bh, K, min_mass, bitmap,
-                                                nwords, pred_mass, counters);
+    const long long blocks = ((long long)n_tiles + kSelWarps - 1) / kSelWarps;
+    net_select_kernel<<<(unsigned)blocks, 32 * kSelWarps, sm, st>>>(
+        a4, n_tiles, L.S, wb + L.wh, wf + L.bh, K, min_mass, bitmap, nwords, pred_mass, counters);
     return cudaGetLastError();
 }
 
