@@ -28,6 +28,13 @@ evaluated-offset fraction, and its accuracy: max-abs error and PSNR against
 the FP64 full-search oracle on two sub-blocks (a corner and a central 40^3
 block, computed on crops with a 28-voxel margin, the reach of 4 iterations),
 plus PSNR against the clean phantom next to the FP64 oracle's own.
+
+``batch`` (rank 0, one GPU): 24 seeded volumes, sizes uniform from 64^3 to
+384x384x256, spheres on a background with blurred noise of sigma uniform in
+0.02-0.08, patch radius from {1,2,3} and search radius from {3,5,7} per volume,
+4 iterations, global noise: the whole schedule as one CUDA graph with one
+persistent kernel per iteration (inlm_batch_run), against the same volumes
+run one after another (inlm_denoise each), in voxel-iterations/s.
 """
 from __future__ import annotations
 
@@ -165,6 +172,86 @@ def sub_blocks(shape, inner=40, margin=28):
     i1 = tuple(slice(n // 2 - inner // 2 - l, n // 2 + inner // 2 - l) for l, n in zip(lo, shape))
     out.append((c1, i1))
     return out
+
+
+def batch_workload(seed=0, n=24, lo=(64, 64, 64), hi=(384, 384, 256)):
+    from microtomodenoise_b200 import DenoiseParameters, synth
+    rng = np.random.default_rng(seed)
+    vols, params = [], []
+    for i in range(n):
+        nx = int(rng.integers(lo[0], hi[0] + 1))
+        ny = int(rng.integers(lo[1], hi[1] + 1))
+        nz = int(rng.integers(lo[2], hi[2] + 1))
+        sigma = float(rng.uniform(0.02, 0.08))
+        pr = int(rng.choice([1, 2, 3]))
+        sr = int(rng.choice([3, 5, 7]))
+        vols.append(synth.spheres_volume((nz, ny, nx), n_spheres=40, rmin=4.0, rmax=20.0,
+                                         noise_std=sigma, noise_blur=1.0, seed=1000 + i))
+        params.append(DenoiseParameters(radius_patchspace=(pr,) * 3, radius_searchspace=(sr,) * 3,
+                                        maxiterations=ITERS, alpha=0.5, noise_mode="global",
+                                        n_samples=100000, noise_seed=i))
+    return vols, params
+
+
+def run_batch(args, local, small=False):
+    """Batched graph vs one-after-another single-volume jobs."""
+    import torch
+    from microtomodenoise_b200 import Batch, IterativeNLM_GPU
+    t = time.time()
+    vols, params = (batch_workload(seed=1, lo=(32, 32, 32), hi=(96, 96, 96)) if small
+                    else batch_workload())
+    log(f"batch workload generated in {time.time() - t:.1f}s")
+    vox_iters = float(sum(v.size for v in vols)) * ITERS
+    dev = [torch.from_numpy(v).cuda() for v in vols]
+    outs = [torch.empty_like(v) for v in dev]
+    torch.cuda.synchronize()
+    t = time.time()
+    b = Batch([v.shape for v in vols], params)
+    setup_s = time.time() - t
+    desc = b.describe()
+    ptrs = [v.data_ptr() for v in dev]
+    optrs = [o.data_ptr() for o in outs]
+    b.run(ptrs, optrs, on_device=True)  # warm-up
+    ms_graph = []
+    for _ in range(args.form_steps):
+        b.run(ptrs, optrs, on_device=True)
+        ms_graph.append(b.last_ms)
+    ms_b = float(np.mean(ms_graph))
+    host_outs = [np.empty_like(v) for v in vols]
+    t0 = time.time()
+    b.run(vols, host_outs)
+    e2e_s = time.time() - t0
+    b.close()
+    # the same jobs one after another
+    stream = torch.cuda.Stream()
+    total_ms = 0.0
+    for v, p, o in zip(dev, params, outs):
+        g = IterativeNLM_GPU()
+        g.configure_device(tuple(v.shape), p)
+        g.set_stream(stream.cuda_stream)
+        g.denoise(v.data_ptr(), on_device=True, out=o.data_ptr())  # warm-up
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.denoise(v.data_ptr(), on_device=True, out=o.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        g.free_device()
+    size = "32^3..96^3" if small else "64^3..384x384x256"
+    return {"workload": f"24 volumes {size}, spheres + blurred noise sigma 0.02-0.08, "
+                        "patch r in {1,2,3}, search r in {3,5,7}, 4 iterations, global noise",
+            "voxel_iterations": vox_iters,
+            "value": vox_iters / (ms_b / 1e3), "unit": "voxel-iter/s", "ms_per_job": ms_b,
+            "steps": args.form_steps, "warmup": 1,
+            "sequential_value": vox_iters / (total_ms / 1e3), "sequential_ms": total_ms,
+            "speedup_vs_sequential": total_ms / ms_b,
+            "e2e": {"value": vox_iters / e2e_s, "unit": "voxel-iter/s",
+                    "h2d_bytes_per_step": int(sum(v.nbytes for v in vols)),
+                    "d2h_bytes_per_step": int(sum(v.nbytes for v in vols))},
+            "setup_s": setup_s, "describe": desc,
+            "small_volumes": run_batch(args, local, small=True) if not small else None}
 
 
 def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
@@ -329,6 +416,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form-steps", type=int, default=2)
     ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--shape", default="512,512,512",
                     help="nz,ny,nx of the volume (smaller shapes only for profiling runs)")
     args = ap.parse_args()
@@ -463,6 +551,11 @@ def main():
             line["forms"] = run_forms(vol, clean, sig_iters, value, args, local, stream)
         except Exception as e:
             line["forms"] = {"error": str(e)[:300]}
+    if rank == 0 and world == 1 and not args.no_batch:
+        try:
+            line["batch"] = run_batch(args, local)
+        except Exception as e:
+            line["batch"] = {"error": str(e)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             _, info = cpu_reference_rate(vol)

@@ -268,6 +268,37 @@ int inlm_weight_map(inlm_denoiser* d, float* map_dev);
  * the FP16 values the filter read) and the per-slice scale. */
 int inlm_net_input(inlm_denoiser* d, float* vol_dev, float* scale_dev);
 
+/* ---------------- autotuner and batched form ----------------
+ * No counterpart in the reference, which runs one stack with one fixed
+ * kernel configuration per run (main.cpp:311-545). */
+
+/* Times the tiled FP32 kernel's configurations (CTA depth 8 with raw staged
+ * in shared memory or read from global memory, depth 4) on a 128x128x64 probe
+ * of d's patch/search class, applies the fastest to d and caches the choice
+ * per process (and in the file named by the INLM_AUTOTUNE_CACHE environment
+ * variable when set). Results do not change: every configuration rounds each
+ * voxel identically. report (nullable) gets the timings. */
+int inlm_autotune(inlm_denoiser* d, char* report, size_t len);
+
+typedef struct inlm_batch inlm_batch;
+
+/* n volumes of different sizes and radii filtered together: shapes holds
+ * {nx, ny, nz} per volume, params one inlm_params per volume (plain FP32,
+ * noise mode global, z-adaptive or manual, one device). Each iteration of all
+ * volumes runs as one persistent kernel over their tiles (heaviest tiles
+ * first; tile configurations from the autotuner; volumes whose patch shape has
+ * no batched body get their own launch), and the whole schedule (noise
+ * estimates, padding, iterations) is captured once in a CUDA graph. At most 24
+ * batched volumes. */
+int inlm_batch_create(int n, const int* shapes, const inlm_params* params, inlm_batch** out);
+int inlm_batch_destroy(inlm_batch* b);
+/* Runs the schedule of every volume (inlm_denoise semantics per volume):
+ * raws[v] / outs[v] are host pointers (on_device = 0) or device pointers;
+ * ms_out (nullable) gets the graph's device time. */
+int inlm_batch_run(inlm_batch* b, const float* const* raws, float* const* outs, int on_device,
+                   float* ms_out);
+int inlm_batch_describe(inlm_batch* b, char* buf, size_t len);
+
 /* ---------------- host-only helpers (no device needed) ---------------- */
 
 /* Geometry of a parameter set (setup_searchspace / setup_patchspace /

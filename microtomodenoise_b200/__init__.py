@@ -25,7 +25,7 @@ import numpy as np
 from . import _lib
 from ._lib import InlmError, InlmParams, NOISE_MODES, PRECISIONS
 
-__all__ = ["DenoiseParameters", "IterativeNLM_GPU", "NoiseLevel", "denoise", "InlmError"]
+__all__ = ["DenoiseParameters", "IterativeNLM_GPU", "NoiseLevel", "Batch", "denoise", "InlmError"]
 
 
 @dataclass
@@ -193,6 +193,13 @@ class IterativeNLM_GPU:
         _lib.check(_lib.load().inlm_describe(self._h, buf, 512), "describe")
         return buf.value.decode()
 
+    def autotune(self) -> str:
+        """Chooses the tiled FP32 kernel configuration by timing (results unchanged)."""
+        self._need()
+        buf = C.create_string_buffer(512)
+        _lib.check(_lib.load().inlm_autotune(self._h, buf, 512), "autotune")
+        return buf.value.decode()
+
     def n_search_offsets(self) -> int:
         """Number of search offsets S of the configured geometry."""
         self._need()
@@ -297,6 +304,65 @@ class NoiseLevel:
     def close(self):
         if self._h:
             _lib.load().inlm_noise_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many volumes of different sizes and radii filtered together: one
+    persistent kernel per iteration over all their tiles, the whole schedule
+    replayed as a CUDA graph (inlm_batch_*). Plain FP32 filter; every volume's
+    result equals its single-volume run."""
+
+    def __init__(self, shapes_zyx, params):
+        L = _lib.load()
+        n = len(shapes_zyx)
+        if isinstance(params, DenoiseParameters):
+            params = [params] * n
+        assert len(params) == n
+        self.shapes = [tuple(int(v) for v in s) for s in shapes_zyx]
+        sh = (C.c_int * (3 * n))()
+        for i, (nz, ny, nx) in enumerate(self.shapes):
+            sh[3 * i:3 * i + 3] = [nx, ny, nz]
+        ps = (InlmParams * n)(*[p.to_c() for p in params])
+        self._h = C.c_void_p(None)
+        _lib.check(L.inlm_batch_create(n, sh, ps, C.byref(self._h)), "batch_create")
+        self.n = n
+        self.last_ms = None
+
+    def run(self, raws, outs=None, on_device: bool = False):
+        """raws: list of float32 arrays (host) or device pointers (on_device)."""
+        n = self.n
+        if on_device:
+            rp = (C.c_void_p * n)(*raws)
+            op = (C.c_void_p * n)(*outs)
+        else:
+            raws = [_f32c(r) for r in raws]
+            for r, s in zip(raws, self.shapes):
+                assert r.shape == s
+            if outs is None:
+                outs = [np.empty(s, np.float32) for s in self.shapes]
+            rp = (C.c_void_p * n)(*[r.ctypes.data for r in raws])
+            op = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        ms = C.c_float(0)
+        _lib.check(_lib.load().inlm_batch_run(self._h, rp, op, int(on_device), C.byref(ms)),
+                   "batch_run")
+        self.last_ms = ms.value
+        return outs
+
+    def describe(self) -> str:
+        buf = C.create_string_buffer(8192)
+        _lib.check(_lib.load().inlm_batch_describe(self._h, buf, 8192), "batch_describe")
+        return buf.value.decode()
+
+    def close(self):
+        if self._h:
+            _lib.load().inlm_batch_destroy(self._h)
             self._h = C.c_void_p(None)
 
     def __del__(self):

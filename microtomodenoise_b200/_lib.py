@@ -36,6 +36,8 @@ EXPORTS = (
     "inlm_proposal_set_params", "inlm_proposal_get_params", "inlm_proposal_logits",
     "inlm_proposal_train", "inlm_proposal_select", "inlm_attach_proposal", "inlm_proposal_stats",
     "inlm_weight_map", "inlm_net_input",
+    "inlm_autotune", "inlm_batch_create", "inlm_batch_destroy", "inlm_batch_run",
+    "inlm_batch_describe",
 )
 
 
@@ -125,6 +127,11 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.inlm_proposal_stats.argtypes = [vp, C.c_int64 * 5]
     L.inlm_weight_map.argtypes = [vp, vp]
     L.inlm_net_input.argtypes = [vp, vp, vp]
+    L.inlm_autotune.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.inlm_batch_create.argtypes = [C.c_int, vp, vp, C.POINTER(vp)]
+    L.inlm_batch_destroy.argtypes = [vp]
+    L.inlm_batch_run.argtypes = [vp, vp, vp, C.c_int, C.POINTER(C.c_float)]
+    L.inlm_batch_describe.argtypes = [vp, C.c_char_p, C.c_size_t]
     for name in EXPORTS:
         if name not in ("inlm_last_error", "inlm_default_params"):
             getattr(L, name).restype = C.c_int

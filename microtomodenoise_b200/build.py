@@ -41,6 +41,7 @@ LIB_SOURCES = [
     "api.cu",
     "proposal.cu",
     "api_proposal.cu",
+    "api_batch.cu",
     "geometry.cpp",
     "sampling.cpp",
 ]

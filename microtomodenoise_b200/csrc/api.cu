@@ -354,10 +354,13 @@ static void denoiser_free(inlm_denoiser* d) {
     if (d->own_stream && d->stream) cudaStreamDestroy(d->stream);
 }
 
-static int choose_tile_config(inlm_denoiser* d) {
+// Tiled FP32 configuration for one candidate (CTA depth tz, raw staged in
+// shared memory or read from global): tables, kernel arguments, TMA map.
+// *ok = false when the candidate does not apply or does not fit.
+int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     const Geometry& g = d->geo;
     const int* pr = g.patch_radius;
-    d->use_tile = false;
+    *ok = false;
     if (!tile_kernel_available(pr[0], pr[1], pr[2])) return INLM_OK;
     if (d->p.nslices / 2 < pr[2]) return INLM_OK;           // z-clipped patch
     if ((int)g.taps.size() > kMaxTaps) return INLM_OK;
@@ -369,8 +372,9 @@ static int choose_tile_config(inlm_denoiser* d) {
         if (order[3 * t] != g.taps[t].x || order[3 * t + 1] != g.taps[t].y ||
             order[3 * t + 2] != g.taps[t].z)
             return INLM_OK;
+    if (!((tz == 8) || (tz == 4 && !raw_smem))) return INLM_OK;
 
-    TileArgs& a = d->targs;
+    TileArgs a{};
     a.nx = d->shape[0];
     a.ny = d->shape[1];
     a.nz = d->shape[2];
@@ -388,26 +392,16 @@ static int choose_tile_config(inlm_denoiser* d) {
     a.rbx = (pr[0] + kTX + 2 * a.sxr + 3) / 4 * 4;
     a.rby = kTY + 2 * a.syr;
     for (int t = 0; t < nt; t++) a.w[t] = g.weights[t];
+    a.pbz = tz + 2 * a.pz;
+    a.rbz = tz + 2 * a.szc;
+    if (a.pbx > 256 || a.pby > 256 || a.pbz > 256) return INLM_OK;
+    if ((long long)a.pbx * a.pby * a.pbz >= 65536) return INLM_OK;  // 16-bit index table
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
-    const struct {
-        int tz;
-        bool raw;
-    } cands[] = {{8, true}, {8, false}, {4, false}};
-    for (auto c : cands) {
-        a.pbz = c.tz + 2 * a.pz;
-        a.rbz = c.tz + 2 * a.szc;
-        if (a.pbx > 256 || a.pby > 256 || a.pbz > 256) continue;
-        if ((long long)a.pbx * a.pby * a.pbz >= 65536) continue;  // 16-bit index table
-        TileConfig tc{pr[0], pr[1], pr[2], c.tz, c.raw, 0};
-        size_t sm = tile_smem_bytes(tc, a);
-        if (sm == 0 || sm > (size_t)smem_max) continue;
-        tc.smem_bytes = sm;
-        d->tcfg = tc;
-        d->use_tile = true;
-        break;
-    }
-    if (!d->use_tile) return INLM_OK;
+    TileConfig tc{pr[0], pr[1], pr[2], tz, raw_smem, 0};
+    size_t sm = tile_smem_bytes(tc, a);
+    if (sm == 0 || sm > (size_t)smem_max) return INLM_OK;
+    tc.smem_bytes = sm;
     a.tiles_x = (d->shape[0] + kTX - 1) / kTX;
     a.tiles_y = (d->shape[1] + kTY - 1) / kTY;
     // search deltas inside the shared-memory boxes (raw: box or global)
@@ -417,10 +411,10 @@ static int choose_tile_config(inlm_denoiser* d) {
     for (int s = 0; s < a.S; s++) {
         const Offset3& o = g.search[s];
         dl[s].x = o.z * pplane + o.y * a.pbx + o.x;
-        dl[s].y = d->tcfg.raw_smem ? o.z * rplane + o.y * rpx + o.x
-                                   : (int)(o.z * d->pitch_z + o.y * d->pitch_y + o.x);
+        dl[s].y = raw_smem ? o.z * rplane + o.y * rpx + o.x
+                           : (int)(o.z * d->pitch_z + o.y * d->pitch_y + o.x);
     }
-    CUDA_TRY(dalloc(&d->d_search_delta, a.S));
+    if (!d->d_search_delta) CUDA_TRY(dalloc(&d->d_search_delta, a.S));
     CUDA_TRY(cudaMemcpy(d->d_search_delta, dl.data(), a.S * sizeof(int2), cudaMemcpyHostToDevice));
     a.search_delta = d->d_search_delta;
     a.raw_pad = d->d_raw_pad;
@@ -431,6 +425,26 @@ static int choose_tile_config(inlm_denoiser* d) {
                            a.pbx, a.pby, a.pbz);
     if (rc) return rc;
     d->tm_raw = d->tm_prev;  // raw is staged with plain loads; the map is unused
+    d->targs = a;
+    d->tcfg = tc;
+    d->use_tile = true;
+    *ok = true;
+    return INLM_OK;
+}
+
+// Default choice (before any autotuning): the first candidate that fits.
+static int choose_tile_config(inlm_denoiser* d) {
+    d->use_tile = false;
+    const struct {
+        int tz;
+        bool raw;
+    } cands[] = {{8, true}, {8, false}, {4, false}};
+    for (auto c : cands) {
+        bool ok = false;
+        int rc = tile_config_try(d, c.tz, c.raw, &ok);
+        if (rc) return rc;
+        if (ok) return INLM_OK;
+    }
     return INLM_OK;
 }
 
@@ -683,7 +697,7 @@ extern "C" int inlm_set_stream(inlm_denoiser* d, void* stream) {
     return INLM_OK;
 }
 
-static int upload_sigma_device(inlm_denoiser* d) {
+int inlm::upload_sigma_device(inlm_denoiser* d) {
     CUDA_TRY(launch_sigma_to_mult(d->d_sigma, d->p.beta, d->d_mult, d->shape[2], d->stream));
     d->launches++;
     d->sigma_set = true;
@@ -731,7 +745,7 @@ int inlm::launch_filter(inlm_denoiser* d) {
 }
 
 // Pads the unpadded volume `src` (device) into the FP16 padded buffer `dst`.
-static int pad_into_half(inlm_denoiser* d, const float* src, void* dst) {
+int inlm::pad_into_half(inlm_denoiser* d, const float* src, void* dst) {
     const Geometry& g = d->geo;
     CUDA_TRY(launch_pad_reflective_half(src, d->shape[0], d->shape[1], d->shape[2], dst, g.pad[0],
                                         g.pad[1], g.pad[2], d->pitch_y, d->pitch_z, d->stream));
@@ -740,7 +754,7 @@ static int pad_into_half(inlm_denoiser* d, const float* src, void* dst) {
 }
 
 // Pads the unpadded volume `src` (device) into the padded buffer `dst`.
-static int pad_into(inlm_denoiser* d, const float* src, float* dst) {
+int inlm::pad_into(inlm_denoiser* d, const float* src, float* dst) {
     const Geometry& g = d->geo;
     CUDA_TRY(launch_pad_reflective(src, d->shape[0], d->shape[1], d->shape[2], dst, g.pad[0],
                                    g.pad[1], g.pad[2], d->pitch_y, d->pitch_z, d->stream));
@@ -849,7 +863,7 @@ extern "C" int inlm_get_result_device(inlm_denoiser* d, float* out_dev) {
 }
 
 // Noise estimate of a device volume into d->d_sigma (or sigma0 buffer).
-static int estimate_into(inlm_denoiser* d, const float* vol_dev, float* d_dst, std::vector<float>* host_copy) {
+int inlm::estimate_into(inlm_denoiser* d, const float* vol_dev, float* d_dst, std::vector<float>* host_copy) {
     if (!d->noise) return fail(INLM_ERR_ARG, "volume too small for the noise patch");
     std::vector<float> hs;
     bool on_host = false;

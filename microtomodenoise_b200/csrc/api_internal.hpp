@@ -182,6 +182,14 @@ namespace inlm {
 void noise_free(inlm_noise* n);
 int launch_filter(inlm_denoiser* d);
 int check_device_error(inlm_denoiser* d);
+int tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok);
+int upload_sigma_device(inlm_denoiser* d);
+int pad_into(inlm_denoiser* d, const float* src, float* dst);
+int pad_into_half(inlm_denoiser* d, const float* src, void* dst);
+// Noise estimate of a device volume into d_dst (nz floats, device); host_copy
+// (nullable) gets a host copy after a stream synchronisation.
+int estimate_into(inlm_denoiser* d, const float* vol_dev, float* d_dst,
+                  std::vector<float>* host_copy);
 // Runs the attached proposal on the padded previous iterate and points the
 // filter's plan at its per-CTA lists (api_proposal.cu).
 int proposal_enqueue(inlm_denoiser* d);

@@ -117,13 +117,16 @@ __device__ __forceinline__ void accumulate_rows(const float* __restrict__ D, int
     }
 }
 
+// One tile (TX x TY x TZ voxels at tile coordinates bx, by, bz) of the exact
+// filter, run by a CTA of 32*TZ threads; shared by the per-volume kernel and
+// the persistent batch kernel. smem holds the mbarrier (initialised by the
+// caller) at offset 0; the prev-box TMA completes phase `parity` of it.
+// Returns false (uniformly over the CTA) when the TMA wait ran out.
 template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
-__global__ void __launch_bounds__(32 * TZ, 1)
-    nlm_tile_f32_kernel(const __grid_constant__ CUtensorMap tm_prev,
-                        const __grid_constant__ CUtensorMap tm_raw,
-                        const __grid_constant__ TileArgs a) {
+__device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const TileArgs& a, int bx,
+                                              int by, int bz, unsigned char* smem,
+                                              uint32_t parity) {
     using G = TileGeom<RX, RY, RZ, TZ>;
-    extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
     float* prevb = reinterpret_cast<float*>(smem + 128);
     const int pplane = a.pbx * a.pby;
@@ -140,21 +143,14 @@ __global__ void __launch_bounds__(32 * TZ, 1)
     float* const D0 = D;
 
     const int tid = threadIdx.x;
-    const int X0 = blockIdx.x * kTX;
-    const int Y0 = blockIdx.y * kTY;
-    const int Z0 = blockIdx.z * TZ;
+    const int X0 = bx * kTX;
+    const int Y0 = by * kTY;
+    const int Z0 = bz * TZ;
 
-    if (tid == 0) {
-        prefetch_tmap(&tm_prev);
-        if (RAW_SMEM) prefetch_tmap(&tm_raw);
-        mbar_init(bar, 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
     if (tid == 0) {
         mbar_arrive_expect_tx(bar, (uint32_t)PB * 4u);
         // prev box starts at the tile origin in padded coordinates (x aligned to 32)
-        tma_load_3d(prevb, &tm_prev, X0, Y0, Z0, bar);
+        tma_load_3d(prevb, tm_prev, X0, Y0, Z0, bar);
     }
     if (RAW_SMEM) {
         // raw over tile + search halo, coalesced rows re-pitched while the
@@ -191,9 +187,10 @@ __global__ void __launch_bounds__(32 * TZ, 1)
         qdi[k] = p * G::DPLANE + r * G::DP + c;
     }
 
-    if (!mbar_wait_bounded(bar, 0)) {
-        set_error(a.err, DEV_TMA_TIMEOUT);
-        return;
+    const bool arrived = mbar_wait_bounded(bar, parity);
+    if (!__syncthreads_and(arrived)) {
+        if (tid == 0) set_error(a.err, DEV_TMA_TIMEOUT);
+        return false;
     }
     f32x2 qog[NQ];
 #pragma unroll
@@ -317,6 +314,67 @@ __global__ void __launch_bounds__(32 * TZ, 1)
             }
         }
     }
+    return true;
+}
+
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
+__global__ void __launch_bounds__(32 * TZ, 1)
+    nlm_tile_f32_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (threadIdx.x == 0) {
+        prefetch_tmap(&tm_prev);
+        mbar_init(reinterpret_cast<uint64_t*>(smem), 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    tile_f32_body<RX, RY, RZ, TZ, RAW_SMEM>(&tm_prev, a, blockIdx.x, blockIdx.y, blockIdx.z, smem, 0);
+}
+
+// Persistent batch kernel: CTAs take (volume, tile) items from a counter
+// until the batch is done; each volume runs the body of its patch shape and
+// tile configuration (kind). Items are numbered volume by volume in the order
+// the host gives (heaviest tiles first), tiles x-fastest within a volume.
+template <int RX, int RY, int RZ, bool RAW_SMEM>
+__device__ __forceinline__ bool batch_item(const BatchParams& bp, int v, int local,
+                                           unsigned char* smem, uint32_t parity) {
+    const TileArgs& a = bp.args[v];
+    const int bx = local % a.tiles_x;
+    const int rest = local / a.tiles_x;
+    const int by = rest % a.tiles_y;
+    const int bz = rest / a.tiles_y;
+    return tile_f32_body<RX, RY, RZ, 8, RAW_SMEM>(&bp.maps[v], a, bx, by, bz, smem, parity);
+}
+
+static_assert(sizeof(BatchParams) <= 32764, "batch parameter block exceeds the kernel parameter limit");
+
+// One persistent kernel per patch shape R and raw placement (a kernel mixing
+// bodies would carry the largest one's registers, shared memory and code for
+// every tile); volumes of any size and search radius. Radius 1 keeps to 128
+// registers so two CTAs fit an SM, as its per-volume kernel does.
+template <int R, bool RAW_SMEM>
+__global__ void __launch_bounds__(256, R == 1 ? 2 : 1)
+    nlm_batch_f32_kernel(const __grid_constant__ BatchParams bp) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_item;
+    if (threadIdx.x == 0) {
+        for (int v = 0; v < bp.n; v++) prefetch_tmap(&bp.maps[v]);
+        mbar_init(reinterpret_cast<uint64_t*>(smem), 1);
+        fence_mbar_init();
+    }
+    uint32_t parity = 0;
+    for (;;) {
+        __syncthreads();  // the previous item's shared memory is free
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(bp.counter, 1u);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= bp.item_begin[bp.n]) break;
+        int v = 0;
+        while (v + 1 < bp.n && item >= bp.item_begin[v + 1]) v++;
+        const int local = item - bp.item_begin[v];
+        const bool ok = batch_item<R, R, R, RAW_SMEM>(bp, v, local, smem, parity);
+        if (!ok) break;  // uniform over the CTA; the error flag is set
+        parity ^= 1u;
+    }
 }
 
 // ---- generic exact kernel: any patch shape, one thread per voxel ----
@@ -416,11 +474,55 @@ static size_t smem_bytes_for(const TileArgs& a) {
 template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
 static cudaError_t launch_inst(const CUtensorMap* tmp, const CUtensorMap* tmr, const TileArgs& a,
                                int tiles_z, size_t smem, cudaStream_t st) {
+    (void)tmr;
     auto kern = nlm_tile_f32_kernel<RX, RY, RZ, TZ, RAW_SMEM>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
-    kern<<<grid, 32 * TZ, smem, st>>>(*tmp, *tmr, a);
+    kern<<<grid, 32 * TZ, smem, st>>>(*tmp, a);
+    return cudaGetLastError();
+}
+
+int batch_kind(const TileConfig& c) {
+    if (c.tz != 8) return -1;
+    if (c.rx == 1 && c.ry == 1 && c.rz == 1) return c.raw_smem ? kBatchP111Smem : kBatchP111Glob;
+    if (c.rx == 2 && c.ry == 2 && c.rz == 2) return c.raw_smem ? kBatchP222Smem : kBatchP222Glob;
+    if (c.rx == 3 && c.ry == 3 && c.rz == 3) return c.raw_smem ? kBatchP333Smem : kBatchP333Glob;
+    return -1;
+}
+
+template <int R, bool RAW>
+static cudaError_t batch_setup_r(size_t smem, int* ctas_per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(nlm_batch_f32_kernel<R, RAW>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, nlm_batch_f32_kernel<R, RAW>,
+                                                         256, smem);
+}
+
+cudaError_t batch_kernel_setup(int kind, size_t smem, int* ctas_per_sm) {
+    switch (kind) {
+        case kBatchP111Smem: return batch_setup_r<1, true>(smem, ctas_per_sm);
+        case kBatchP111Glob: return batch_setup_r<1, false>(smem, ctas_per_sm);
+        case kBatchP222Smem: return batch_setup_r<2, true>(smem, ctas_per_sm);
+        case kBatchP222Glob: return batch_setup_r<2, false>(smem, ctas_per_sm);
+        case kBatchP333Smem: return batch_setup_r<3, true>(smem, ctas_per_sm);
+        case kBatchP333Glob: return batch_setup_r<3, false>(smem, ctas_per_sm);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_batch_kernel(int kind, const BatchParams& bp, int ctas, size_t smem,
+                                cudaStream_t st) {
+    switch (kind) {
+        case kBatchP111Smem: nlm_batch_f32_kernel<1, true><<<ctas, 256, smem, st>>>(bp); break;
+        case kBatchP111Glob: nlm_batch_f32_kernel<1, false><<<ctas, 256, smem, st>>>(bp); break;
+        case kBatchP222Smem: nlm_batch_f32_kernel<2, true><<<ctas, 256, smem, st>>>(bp); break;
+        case kBatchP222Glob: nlm_batch_f32_kernel<2, false><<<ctas, 256, smem, st>>>(bp); break;
+        case kBatchP333Smem: nlm_batch_f32_kernel<3, true><<<ctas, 256, smem, st>>>(bp); break;
+        case kBatchP333Glob: nlm_batch_f32_kernel<3, false><<<ctas, 256, smem, st>>>(bp); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

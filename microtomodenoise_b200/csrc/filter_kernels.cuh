@@ -69,6 +69,32 @@ cudaError_t launch_sigma_to_mult(const float* sigma, float beta, float* mult, in
                                  cudaStream_t st);
 cudaError_t launch_sigma_blend(const float* sigma0, float* sigma1, float alpha, int nz,
                                cudaStream_t st);
+// ---- persistent batch kernel (exact FP32 tiles of many volumes) ----
+constexpr int kBatchMax = 24;  // volumes per launch (the kernel parameter block holds them all)
+enum BatchKind : int {
+    kBatchP111Smem = 0,
+    kBatchP111Glob = 1,
+    kBatchP222Smem = 2,
+    kBatchP222Glob = 3,
+    kBatchP333Smem = 4,
+    kBatchP333Glob = 5,
+};
+struct BatchParams {
+    CUtensorMap maps[kBatchMax];     // prev-box maps (64-byte aligned, first)
+    TileArgs args[kBatchMax];
+    int kind[kBatchMax];
+    int item_begin[kBatchMax + 1];   // tile items of volume v: [item_begin[v], item_begin[v+1])
+    int n;
+    unsigned* counter;               // zeroed before each launch
+};
+// Batch body of a tile configuration (tz 8, patch (1,1,1) (2,2,2) (3,3,3)), or
+// -1: one persistent kernel per kind (patch shape kind / 2, raw placement
+// kind % 2: 0 shared memory, 1 global).
+int batch_kind(const TileConfig& c);
+cudaError_t batch_kernel_setup(int kind, size_t smem, int* ctas_per_sm);
+cudaError_t launch_batch_kernel(int kind, const BatchParams& bp, int ctas, size_t smem,
+                                cudaStream_t st);
+
 // Compile-time tap rows of an instantiation, flattened as (x,y,z) triples in
 // the order the kernel accumulates them; used to check host/device agreement.
 int tile_kernel_tap_order(int rx, int ry, int rz, int* xyz, int max_taps);
