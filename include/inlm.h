@@ -299,6 +299,28 @@ int inlm_batch_run(inlm_batch* b, const float* const* raws, float* const* outs, 
                    float* ms_out);
 int inlm_batch_describe(inlm_batch* b, char* buf, size_t len);
 
+/* ---------------- z-slab streaming ----------------
+ * replaces IterativeNLM_GPU::Run_GaussianNoise_GPUBlocks (iternlm_gpu.h:31-32,
+ * iternlm_gpu.cu:1887-2115) for volumes held in host memory. */
+
+/* The inlm_denoise schedule for a volume that stays in host memory (raw_host,
+ * out_host: nx*ny*nz floats each; page-locked here for the call when they are
+ * not already). Every iteration walks the volume in z-slabs of slab_depth
+ * slices (rounded up to a multiple of 8), each filtered on the device as a
+ * sub-volume with a halo of max(8, z padding rounded up to 8) slices (16 or
+ * more with a proposal) on two alternating streams, so one slab's copies
+ * overlap another's kernels; noise estimates gather each sample's patch std
+ * from the slab holding it. Results equal inlm_denoise's bit for bit in every
+ * form. p->precision selects the form; net (nullable, FP16 forms) attaches a
+ * learned proposal with k offsets per tile and fallback below min_mass.
+ * Noise modes: global, z-adaptive, manual. sigma0_out / sigma1_out (nullable,
+ * host, nz floats) receive the estimates; stats (nullable, 6 doubles) =
+ * {device ms, host-to-device bytes, device-to-host bytes, slabs, halo, slab
+ * depth}. Needs one extra host volume (page-locked) for the iterations. */
+int inlm_stream_denoise(const int shape[3], const inlm_params* p, const float* raw_host,
+                        float* out_host, int slab_depth, inlm_proposal* net, int k, float min_mass,
+                        float* sigma0_out, float* sigma1_out, double* stats);
+
 /* ---------------- host-only helpers (no device needed) ---------------- */
 
 /* Geometry of a parameter set (setup_searchspace / setup_patchspace /

@@ -25,7 +25,8 @@ import numpy as np
 from . import _lib
 from ._lib import InlmError, InlmParams, NOISE_MODES, PRECISIONS
 
-__all__ = ["DenoiseParameters", "IterativeNLM_GPU", "NoiseLevel", "Batch", "denoise", "InlmError"]
+__all__ = ["DenoiseParameters", "IterativeNLM_GPU", "NoiseLevel", "Batch", "denoise",
+           "stream_denoise", "InlmError"]
 
 
 @dataclass
@@ -370,6 +371,29 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def stream_denoise(raw: np.ndarray, params: DenoiseParameters, slab_depth: int = 64,
+                   net=None, k: int = 256, min_mass: float = 0.95, out: Optional[np.ndarray] = None):
+    """The denoise schedule for a host-resident volume, filtered in z-slabs
+    (inlm_stream_denoise). Returns (result, sigma0, sigma1, stats) with stats =
+    {ms, h2d_bytes, d2h_bytes, slabs, halo, slab_depth}."""
+    raw = _f32c(raw)
+    if out is None:
+        out = np.empty(raw.shape, np.float32)
+    nz = raw.shape[0]
+    s0 = np.zeros(nz, np.float32)
+    s1 = np.zeros(nz, np.float32)
+    st = np.zeros(6, np.float64)
+    cp = params.to_c()
+    rc = _lib.load().inlm_stream_denoise(_shape_c(raw.shape), C.byref(cp), raw.ctypes.data,
+                                         out.ctypes.data, int(slab_depth),
+                                         net._h if net is not None else None, int(k),
+                                         float(min_mass), s0.ctypes.data, s1.ctypes.data,
+                                         st.ctypes.data)
+    _lib.check(rc, "stream_denoise")
+    keys = ("ms", "h2d_bytes", "d2h_bytes", "slabs", "halo", "slab_depth")
+    return out, s0, s1, dict(zip(keys, st.tolist()))
 
 
 def denoise(raw: np.ndarray, params: Optional[DenoiseParameters] = None):

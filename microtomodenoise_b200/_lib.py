@@ -37,7 +37,7 @@ EXPORTS = (
     "inlm_proposal_train", "inlm_proposal_select", "inlm_attach_proposal", "inlm_proposal_stats",
     "inlm_weight_map", "inlm_net_input",
     "inlm_autotune", "inlm_batch_create", "inlm_batch_destroy", "inlm_batch_run",
-    "inlm_batch_describe",
+    "inlm_batch_describe", "inlm_stream_denoise",
 )
 
 
@@ -132,6 +132,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.inlm_batch_destroy.argtypes = [vp]
     L.inlm_batch_run.argtypes = [vp, vp, vp, C.c_int, C.POINTER(C.c_float)]
     L.inlm_batch_describe.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.inlm_stream_denoise.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp,
+                                      C.c_int, C.c_float, vp, vp, vp]
     for name in EXPORTS:
         if name not in ("inlm_last_error", "inlm_default_params"):
             getattr(L, name).restype = C.c_int

@@ -42,6 +42,7 @@ LIB_SOURCES = [
     "proposal.cu",
     "api_proposal.cu",
     "api_batch.cu",
+    "api_stream.cu",
     "geometry.cpp",
     "sampling.cpp",
 ]

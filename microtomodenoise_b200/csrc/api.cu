@@ -166,6 +166,83 @@ extern "C" int inlm_noise_destroy(inlm_noise* n) {
 
 // Runs the estimate for a device stack (pitches in elements); the result stays
 // in n->d_sigma. Host-side decisions (manual, semimanual) fill host_sigma.
+// Draws the sample positions on the first call and uploads the EM windows of
+// the mode (z-adaptive: one per slice; global: one); *nwin gets their count
+// (0 for the manual modes), *first whether the samples were drawn now.
+int inlm::noise_prepare(inlm_noise* n, const inlm_params* p, int* nwin, bool* first_out) {
+    const int nz = n->shape[2];
+    const int mode = p->noise_mode;
+    const bool first = n->samples.empty();
+    if (first_out) *first_out = first;
+    *nwin = 0;
+    if (first) {
+        n->samples = draw_noise_samples(n->shape, n->n_samples, n->patchsize,
+                                        p->circular_mask_diameter, n->seed);
+        CUDA_TRY(cudaMemcpyAsync(n->d_samples, n->samples.data(), n->samples.size() * 8,
+                                 cudaMemcpyHostToDevice, n->stream));
+        CUDA_TRY(cudaStreamSynchronize(n->stream));  // the host vector may be replaced later
+    }
+    const long long ns = (long long)n->samples.size();
+    if (mode == INLM_NOISE_ZADAPTIVE) {
+        if (n->zwindow_cached != p->zwindow || first) {
+            std::vector<int> st, en;
+            noise_zwindows(n->samples, n->shape, p->zwindow, st, en);
+            std::vector<int2> w(nz);
+            std::vector<long long> off(nz);
+            long long total = 0;
+            for (int z = 0; z < nz; z++) {
+                w[z] = make_int2(st[z], en[z]);
+                off[z] = total;
+                total += std::max(0, en[z] - st[z] + 1);
+            }
+            if ((size_t)total > n->assign_cap) {
+                cudaFree(n->d_assign);
+                n->d_assign = nullptr;
+                n->assign_cap = 0;
+                CUDA_TRY(dalloc(&n->d_assign, (size_t)total));
+                n->assign_cap = (size_t)total;
+            }
+            CUDA_TRY(cudaMemcpyAsync(n->d_windows, w.data(), nz * sizeof(int2),
+                                     cudaMemcpyHostToDevice, n->stream));
+            CUDA_TRY(cudaMemcpyAsync(n->d_scratch_off, off.data(), nz * 8, cudaMemcpyHostToDevice,
+                                     n->stream));
+            CUDA_TRY(cudaStreamSynchronize(n->stream));  // host vectors go out of scope
+            n->zwindow_cached = p->zwindow;
+        }
+        *nwin = nz;
+    } else if (mode == INLM_NOISE_GLOBAL) {
+        if (n->zwindow_cached != -2) {
+            int2 w = make_int2(0, (int)ns - 1);
+            long long off = 0;
+            if ((size_t)ns > n->assign_cap) {
+                cudaFree(n->d_assign);
+                n->d_assign = nullptr;
+                n->assign_cap = 0;
+                CUDA_TRY(dalloc(&n->d_assign, (size_t)ns));
+                n->assign_cap = (size_t)ns;
+            }
+            CUDA_TRY(cudaMemcpyAsync(n->d_windows, &w, sizeof w, cudaMemcpyHostToDevice, n->stream));
+            CUDA_TRY(cudaMemcpyAsync(n->d_scratch_off, &off, 8, cudaMemcpyHostToDevice, n->stream));
+            CUDA_TRY(cudaStreamSynchronize(n->stream));
+            n->zwindow_cached = -2;
+        }
+        *nwin = 1;
+    }
+    return INLM_OK;
+}
+
+// EM over the patch stds in n->d_patchstd and the per-slice sigma into
+// n->d_sigma (device work only).
+int inlm::noise_em_finish(inlm_noise* n, const inlm_params* p, int nwin) {
+    CUDA_TRY(launch_noise_em(n->d_patchstd, n->d_windows, nwin, n->d_scratch_off, n->d_assign,
+                             n->d_mean, n->d_sd, n->stream));
+    CUDA_TRY(launch_noise_finalize(n->d_mean, n->d_sd, n->shape[2],
+                                   p->noise_mode == INLM_NOISE_ZADAPTIVE ? 1 : 0, p->stds_from_mean,
+                                   n->d_sigma, n->stream));
+    n->ncalls++;
+    return INLM_OK;
+}
+
 static int noise_estimate_device(inlm_noise* n, inlm_params* p, const float* d_stack,
                                  long long pitch_y, long long pitch_z, std::vector<float>* host_sigma,
                                  bool* sigma_on_host) {
@@ -182,13 +259,10 @@ static int noise_estimate_device(inlm_noise* n, inlm_params* p, const float* d_s
     }
     if (mode != INLM_NOISE_ZADAPTIVE && mode != INLM_NOISE_GLOBAL && mode != INLM_NOISE_SEMIMANUAL)
         return fail(INLM_ERR_ARG, "unknown noise mode %d", mode);
-    bool first = n->samples.empty();
-    if (first) {
-        n->samples = draw_noise_samples(n->shape, n->n_samples, n->patchsize,
-                                        p->circular_mask_diameter, n->seed);
-        CUDA_TRY(cudaMemcpyAsync(n->d_samples, n->samples.data(), n->samples.size() * 8,
-                                 cudaMemcpyHostToDevice, n->stream));
-    }
+    int nwin = 0;
+    bool first = false;
+    int rc = noise_prepare(n, p, &nwin, &first);
+    if (rc) return rc;
     const long long ns = (long long)n->samples.size();
     CUDA_TRY(launch_noise_patchstd(d_stack, pitch_y, pitch_z, n->shape[0],
                                    (long long)n->shape[0] * n->shape[1], n->d_samples, ns,
@@ -218,58 +292,7 @@ static int noise_estimate_device(inlm_noise* n, inlm_params* p, const float* d_s
         n->ncalls++;
         return INLM_OK;
     }
-    int nwin;
-    if (mode == INLM_NOISE_ZADAPTIVE) {
-        if (n->zwindow_cached != p->zwindow || first) {
-            std::vector<int> st, en;
-            noise_zwindows(n->samples, n->shape, p->zwindow, st, en);
-            std::vector<int2> w(nz);
-            std::vector<long long> off(nz);
-            long long total = 0;
-            for (int z = 0; z < nz; z++) {
-                w[z] = make_int2(st[z], en[z]);
-                off[z] = total;
-                total += std::max(0, en[z] - st[z] + 1);
-            }
-            if ((size_t)total > n->assign_cap) {
-                cudaFree(n->d_assign);
-                n->d_assign = nullptr;
-                n->assign_cap = 0;
-                CUDA_TRY(dalloc(&n->d_assign, (size_t)total));
-                n->assign_cap = (size_t)total;
-            }
-            CUDA_TRY(cudaMemcpyAsync(n->d_windows, w.data(), nz * sizeof(int2),
-                                     cudaMemcpyHostToDevice, n->stream));
-            CUDA_TRY(cudaMemcpyAsync(n->d_scratch_off, off.data(), nz * 8, cudaMemcpyHostToDevice,
-                                     n->stream));
-            CUDA_TRY(cudaStreamSynchronize(n->stream));  // host vectors go out of scope
-            n->zwindow_cached = p->zwindow;
-        }
-        nwin = nz;
-    } else {
-        if (n->zwindow_cached != -2) {
-            int2 w = make_int2(0, (int)ns - 1);
-            long long off = 0;
-            if ((size_t)ns > n->assign_cap) {
-                cudaFree(n->d_assign);
-                n->d_assign = nullptr;
-                n->assign_cap = 0;
-                CUDA_TRY(dalloc(&n->d_assign, (size_t)ns));
-                n->assign_cap = (size_t)ns;
-            }
-            CUDA_TRY(cudaMemcpyAsync(n->d_windows, &w, sizeof w, cudaMemcpyHostToDevice, n->stream));
-            CUDA_TRY(cudaMemcpyAsync(n->d_scratch_off, &off, 8, cudaMemcpyHostToDevice, n->stream));
-            CUDA_TRY(cudaStreamSynchronize(n->stream));
-            n->zwindow_cached = -2;
-        }
-        nwin = 1;
-    }
-    CUDA_TRY(launch_noise_em(n->d_patchstd, n->d_windows, nwin, n->d_scratch_off, n->d_assign,
-                             n->d_mean, n->d_sd, n->stream));
-    CUDA_TRY(launch_noise_finalize(n->d_mean, n->d_sd, nz, mode == INLM_NOISE_ZADAPTIVE ? 1 : 0,
-                                   p->stds_from_mean, n->d_sigma, n->stream));
-    n->ncalls++;
-    return INLM_OK;
+    return noise_em_finish(n, p, nwin);
 }
 
 extern "C" int inlm_noise_estimate(inlm_noise* n, inlm_params* p, const float* stack,

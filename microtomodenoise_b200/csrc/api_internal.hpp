@@ -190,6 +190,11 @@ int pad_into_half(inlm_denoiser* d, const float* src, void* dst);
 // (nullable) gets a host copy after a stream synchronisation.
 int estimate_into(inlm_denoiser* d, const float* vol_dev, float* d_dst,
                   std::vector<float>* host_copy);
+// Parts of a device noise estimate (global / z-adaptive): sample draw and EM
+// windows, then patch stds into n->d_patchstd (by the caller), then EM and
+// per-slice sigma into n->d_sigma.
+int noise_prepare(inlm_noise* n, const inlm_params* p, int* nwin, bool* first);
+int noise_em_finish(inlm_noise* n, const inlm_params* p, int nwin);
 // Runs the attached proposal on the padded previous iterate and points the
 // filter's plan at its per-CTA lists (api_proposal.cu).
 int proposal_enqueue(inlm_denoiser* d);

@@ -1,0 +1,310 @@
+// z-slab streaming of a host-resident volume (include/inlm.h). The reference
+// streams volumes that do not fit its GPUs in blocks of slices
+// (IterativeNLM_GPU::Run_GaussianNoise_GPUBlocks, Denoiser/iternlm_gpu.cu:
+// 1887-2115); here the volume stays in host memory and every iteration walks
+// it in z-slabs:
+//   * slab [z0, z1) is filtered as the sub-volume [z0 - h, z1 + h) (h >= the
+//     filter's z padding, clipped at the volume's faces), so every voxel of
+//     the slab reads exactly the values the whole-volume filter reads; the
+//     faces of the sub-volume pad like the whole volume's only where they are
+//     the volume's own faces;
+//   * h and the slab starts are multiples of 8, so the FP16 form's tiles and
+//     the learned proposal's 8^3 tiles fall where they fall in the whole
+//     volume, and h >= 16 with a proposal (its 15-voxel receptive field);
+//   * two denoisers per sub-volume depth alternate on their own streams, so
+//     one slab's copies overlap the other's kernels;
+//   * the noise estimates take each sample's patch std from the slab holding
+//     it (on the device, right after the slab's filter for sigma1) and run the
+//     EM once over all samples.
+// Results equal the in-memory schedule (inlm_denoise) bit for bit.
+#include <map>
+
+#include "api_internal.hpp"
+#include "noise_kernels.cuh"
+
+using namespace inlm;
+
+namespace {
+
+struct SlabPair {
+    inlm_denoiser* d[2] = {nullptr, nullptr};
+    float* stage[2] = {nullptr, nullptr};  // unpadded raw sub-volume
+};
+
+struct StreamJob {
+    int shape[3];
+    long long plane = 0;
+    std::map<int, SlabPair> pairs;  // by sub-volume depth
+    inlm_noise* noise = nullptr;
+    float* d_sig0 = nullptr;  // sigma0 per slice
+    float* d_sig = nullptr;   // sigma of the current iteration
+    float* tmp_host = nullptr;
+    bool reg_raw = false, reg_out = false;
+    const float* raw_host = nullptr;
+    float* out_host = nullptr;
+    cudaStream_t main = nullptr;
+
+    ~StreamJob() {
+        for (auto& kv : pairs)
+            for (int j = 0; j < 2; j++) {
+                if (kv.second.d[j]) inlm_denoiser_destroy(kv.second.d[j]);
+                cudaFree(kv.second.stage[j]);
+            }
+        if (noise) inlm_noise_destroy(noise);
+        cudaFree(d_sig0);
+        cudaFree(d_sig);
+        if (tmp_host) cudaFreeHost(tmp_host);
+        if (reg_raw) cudaHostUnregister(const_cast<float*>(raw_host));
+        if (reg_out) cudaHostUnregister(out_host);
+        if (main) cudaStreamDestroy(main);
+    }
+};
+
+int round_up8(int v) { return (v + 7) / 8 * 8; }
+
+// Sample index range [i0, i1) of slices [z0, z1) (samples are sorted).
+void sample_range(const std::vector<long long>& s, long long plane, int z0, int z1, long long* i0,
+                  long long* i1) {
+    *i0 = std::lower_bound(s.begin(), s.end(), (long long)z0 * plane) - s.begin();
+    *i1 = std::lower_bound(s.begin(), s.end(), (long long)z1 * plane) - s.begin();
+}
+
+int get_pair(StreamJob& J, const inlm_params& p, int depth, inlm_proposal* net, int k,
+             float min_mass, SlabPair** out) {
+    auto it = J.pairs.find(depth);
+    if (it != J.pairs.end()) {
+        *out = &it->second;
+        return INLM_OK;
+    }
+    SlabPair& sp = J.pairs[depth];
+    inlm_params q = p;
+    q.n_samples = 0;  // the job's own noise handle covers the whole volume
+    const int sh[3] = {J.shape[0], J.shape[1], depth};
+    for (int j = 0; j < 2; j++) {
+        int rc = inlm_denoiser_create(sh, &q, &sp.d[j]);
+        if (rc) return rc;
+        CUDA_TRY(dalloc(&sp.stage[j], (size_t)J.plane * depth));
+        if (net) {
+            rc = inlm_attach_proposal(sp.d[j], net, k, min_mass);
+            if (rc) return rc;
+        }
+    }
+    *out = &sp;
+    return INLM_OK;
+}
+
+}  // namespace
+
+extern "C" int inlm_stream_denoise(const int shape[3], const inlm_params* p, const float* raw_host,
+                                   float* out_host, int slab_depth, inlm_proposal* net, int k,
+                                   float min_mass, float* sigma0_out, float* sigma1_out,
+                                   double* stats) {
+    if (!shape || !p || !raw_host || !out_host) return fail(INLM_ERR_ARG, "null argument");
+    if (slab_depth < 1) return fail(INLM_ERR_ARG, "slab depth must be >= 1");
+    if (p->noise_mode != INLM_NOISE_GLOBAL && p->noise_mode != INLM_NOISE_ZADAPTIVE &&
+        p->noise_mode != INLM_NOISE_MANUAL)
+        return fail(INLM_ERR_UNSUPPORTED, "streamed noise modes are global, z-adaptive and manual");
+    if (p->maxiterations < 1) return fail(INLM_ERR_ARG, "maxiterations < 1");
+    if (net && p->precision == INLM_PRECISION_F32)
+        return fail(INLM_ERR_UNSUPPORTED, "the proposal drives the FP16 form");
+    const bool manual = p->noise_mode == INLM_NOISE_MANUAL;
+    CUDA_TRY(cudaSetDevice(p->device_id));
+    StreamJob J;
+    for (int i = 0; i < 3; i++) J.shape[i] = shape[i];
+    J.plane = (long long)shape[0] * shape[1];
+    J.raw_host = raw_host;
+    J.out_host = out_host;
+    const int nz = shape[2];
+    const long long nvox = J.plane * nz;
+    CUDA_TRY(cudaStreamCreateWithFlags(&J.main, cudaStreamNonBlocking));
+
+    // halo and slab grid
+    const int pz = std::min(p->nslices / 2, p->search_radius[2]) + p->patch_radius[2];
+    int halo = round_up8(std::max(pz, 1));
+    if (net) halo = std::max(halo, 16);
+    const int sd = round_up8(slab_depth);
+    std::vector<int> z0s;
+    for (int z = 0; z < nz; z += sd) z0s.push_back(z);
+
+    // host buffers: page-locked for asynchronous copies
+    cudaError_t e = cudaHostRegister(const_cast<float*>(raw_host), nvox * 4, cudaHostRegisterPortable);
+    if (e == cudaSuccess) J.reg_raw = true;
+    else cudaGetLastError();  // already page-locked (or not registrable): copies still work
+    e = cudaHostRegister(out_host, nvox * 4, cudaHostRegisterPortable);
+    if (e == cudaSuccess) J.reg_out = true;
+    else cudaGetLastError();
+    if (p->maxiterations > 1) CUDA_TRY(cudaMallocHost(&J.tmp_host, nvox * 4));
+
+    CUDA_TRY(dalloc(&J.d_sig0, nz));
+    CUDA_TRY(dalloc(&J.d_sig, nz));
+    int nwin = 0;
+    if (!manual) {
+        int rc = inlm_noise_create(shape, p->n_samples, p->noise_patchsize, p->noise_seed,
+                                   p->device_id, &J.noise);
+        if (rc) return rc;
+        cudaStreamDestroy(J.noise->stream);
+        J.noise->stream = J.main;
+        J.noise->own_stream = false;
+        rc = noise_prepare(J.noise, p, &nwin, nullptr);
+        if (rc) return rc;
+    }
+    double h2d = 0, d2h = 0;
+    cudaEvent_t t0, t1;
+    CUDA_TRY(cudaEventCreate(&t0));
+    CUDA_TRY(cudaEventCreate(&t1));
+    CUDA_TRY(cudaEventRecord(t0, J.main));
+
+    auto sync_all = [&]() -> int {
+        for (auto& kv : J.pairs)
+            for (int j = 0; j < 2; j++) CUDA_TRY(cudaStreamSynchronize(kv.second.d[j]->stream));
+        CUDA_TRY(cudaStreamSynchronize(J.main));
+        return INLM_OK;
+    };
+    // patch stds of the samples in slices [z0, z1) of a device slab holding
+    // slices from zb on, on stream st
+    auto slab_patchstd = [&](const float* slab, int zb, int z0, int z1, cudaStream_t st) -> int {
+        long long i0, i1;
+        sample_range(J.noise->samples, J.plane, z0, z1, &i0, &i1);
+        CUDA_TRY(launch_noise_patchstd(slab, shape[0], J.plane, shape[0], J.plane,
+                                       J.noise->d_samples + i0, i1 - i0, J.noise->patchsize,
+                                       J.noise->d_patchstd + i0, st, zb));
+        return INLM_OK;
+    };
+
+    // sigma0 (main.cpp:327-351): the raw volume's samples, slab by slab
+    std::vector<float> s0h(nz), s1h(nz);
+    if (manual) {
+        std::vector<float> v(nz, p->sigma[0]);
+        CUDA_TRY(cudaMemcpy(J.d_sig0, v.data(), nz * 4, cudaMemcpyHostToDevice));
+    } else {
+        int s = 0;
+        for (int z0 : z0s) {
+            const int z1 = std::min(nz, z0 + sd);
+            SlabPair* sp;
+            int rc = get_pair(J, *p, std::min(nz, z1 + halo) - std::max(0, z0 - halo), net, k,
+                              min_mass, &sp);
+            if (rc) return rc;
+            const int j = s++ & 1;
+            cudaStream_t st = sp->d[j]->stream;
+            CUDA_TRY(cudaMemcpyAsync(sp->stage[j], raw_host + z0 * J.plane, (z1 - z0) * J.plane * 4,
+                                     cudaMemcpyHostToDevice, st));
+            h2d += (z1 - z0) * J.plane * 4.0;
+            rc = slab_patchstd(sp->stage[j], z0, z0, z1, st);
+            if (rc) return rc;
+        }
+        int rc = sync_all();
+        if (rc) return rc;
+        rc = noise_em_finish(J.noise, p, nwin);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(J.d_sig0, J.noise->d_sigma, nz * 4, cudaMemcpyDeviceToDevice, J.main));
+    }
+    CUDA_TRY(cudaMemcpyAsync(J.d_sig, J.d_sig0, nz * 4, cudaMemcpyDeviceToDevice, J.main));
+    CUDA_TRY(cudaMemcpyAsync(s0h.data(), J.d_sig0, nz * 4, cudaMemcpyDeviceToHost, J.main));
+    CUDA_TRY(cudaStreamSynchronize(J.main));
+
+    const int maxit = p->maxiterations;
+    const float* prev_host = raw_host;
+    for (int it = 1; it <= maxit; it++) {
+        // the last iteration writes the caller's buffer
+        float* next_host = ((maxit - it) % 2 == 0) ? out_host : J.tmp_host;
+        const bool estimate = (it == 1 && maxit > 1) || (it > 1 && p->continuous_estimate && maxit > it + 1);
+        int s = 0;
+        for (int z0 : z0s) {
+            const int z1 = std::min(nz, z0 + sd);
+            const int a = std::max(0, z0 - halo), b = std::min(nz, z1 + halo);
+            SlabPair* sp;
+            int rc = get_pair(J, *p, b - a, net, k, min_mass, &sp);
+            if (rc) return rc;
+            const int j = s++ & 1;
+            inlm_denoiser* d = sp->d[j];
+            cudaStream_t st = d->stream;
+            const size_t sub = (size_t)(b - a) * J.plane * 4;
+            // the sub-volume's sigma slice and multiplier
+            CUDA_TRY(cudaStreamWaitEvent(st, t0, 0));
+            CUDA_TRY(cudaMemcpyAsync(d->d_sigma, J.d_sig + a, (b - a) * 4, cudaMemcpyDeviceToDevice, st));
+            rc = upload_sigma_device(d);
+            if (rc) return rc;
+            CUDA_TRY(cudaMemcpyAsync(sp->stage[j], raw_host + a * J.plane, sub, cudaMemcpyHostToDevice, st));
+            h2d += sub;
+            if (it > 1) {
+                CUDA_TRY(cudaMemcpyAsync(d->d_next, prev_host + a * J.plane, sub, cudaMemcpyHostToDevice, st));
+                h2d += sub;
+            }
+            if (d->use_fast) {
+                rc = pad_into_half(d, sp->stage[j], d->d_raw_h);
+                if (rc) return rc;
+                if (it == 1) {
+                    CUDA_TRY(cudaMemcpyAsync(d->d_prev_h, d->d_raw_h, d->pitch_z * d->nzp * 2,
+                                             cudaMemcpyDeviceToDevice, st));
+                } else {
+                    rc = pad_into_half(d, d->d_next, d->d_prev_h);
+                    if (rc) return rc;
+                }
+                if (d->prop.net) {
+                    rc = proposal_enqueue(d);
+                    if (rc) return rc;
+                }
+            } else {
+                rc = pad_into(d, sp->stage[j], d->d_raw_pad);
+                if (rc) return rc;
+                if (it == 1) {
+                    CUDA_TRY(cudaMemcpyAsync(d->d_prev_pad, d->d_raw_pad, d->pitch_z * d->nzp * 4,
+                                             cudaMemcpyDeviceToDevice, st));
+                } else {
+                    rc = pad_into(d, d->d_next, d->d_prev_pad);
+                    if (rc) return rc;
+                }
+            }
+            rc = launch_filter(d);
+            if (rc) return rc;
+            d->last_iter = it;
+            CUDA_TRY(cudaMemcpyAsync(next_host + z0 * J.plane, d->d_next + (z0 - a) * J.plane,
+                                     (z1 - z0) * J.plane * 4, cudaMemcpyDeviceToHost, st));
+            d2h += (z1 - z0) * J.plane * 4.0;
+            if (estimate && !manual) {
+                rc = slab_patchstd(d->d_next, a, z0, z1, st);
+                if (rc) return rc;
+            }
+        }
+        int rc = sync_all();
+        if (rc) return rc;
+        for (auto& kv : J.pairs)
+            for (int j = 0; j < 2; j++) {
+                rc = check_device_error(kv.second.d[j]);
+                if (rc) return rc;
+            }
+        if (estimate) {
+            // sigma1 on this result, blended with sigma0 (main.cpp:422-448, 517-544)
+            if (manual) {
+                std::vector<float> v(nz, p->sigma[1]);
+                CUDA_TRY(cudaMemcpy(J.d_sig, v.data(), nz * 4, cudaMemcpyHostToDevice));
+            } else {
+                rc = noise_em_finish(J.noise, p, nwin);
+                if (rc) return rc;
+                CUDA_TRY(cudaMemcpyAsync(J.d_sig, J.noise->d_sigma, nz * 4, cudaMemcpyDeviceToDevice,
+                                         J.main));
+            }
+            if (it == 1) CUDA_TRY(cudaMemcpyAsync(s1h.data(), J.d_sig, nz * 4, cudaMemcpyDeviceToHost, J.main));
+            CUDA_TRY(launch_sigma_blend(J.d_sig0, J.d_sig, p->alpha, nz, J.main));
+            CUDA_TRY(cudaStreamSynchronize(J.main));
+        }
+        prev_host = next_host;
+    }
+    CUDA_TRY(cudaEventRecord(t1, J.main));
+    CUDA_TRY(cudaEventSynchronize(t1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (sigma0_out) std::memcpy(sigma0_out, s0h.data(), nz * 4);
+    if (sigma1_out && maxit > 1) std::memcpy(sigma1_out, s1h.data(), nz * 4);
+    if (stats) {
+        stats[0] = ms;
+        stats[1] = h2d;
+        stats[2] = d2h;
+        stats[3] = (double)z0s.size();
+        stats[4] = halo;
+        stats[5] = sd;
+    }
+    return INLM_OK;
+}

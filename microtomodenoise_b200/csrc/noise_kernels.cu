@@ -22,11 +22,14 @@ __global__ void __launch_bounds__(256) noise_patchstd_kernel(const float* __rest
                                                              int nx, long long nslice,
                                                              const long long* __restrict__ samples,
                                                              long long n, int patchsize,
-                                                             float* __restrict__ out) {
+                                                             float* __restrict__ out, int z_base) {
     long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (s >= n) return;
     long long idx = samples[s];
+    // stack holds slices z_base.. (a z-slab of the volume, or all of it)
     int z0 = (int)(idx / nslice);
+    idx -= (long long)z_base * nslice;
+    z0 -= z_base;
     int y0 = (int)((idx - z0 * nslice) / nx);
     int x0 = (int)(idx - z0 * nslice - (long long)y0 * nx);
     const int patchlength = patchsize * patchsize;
@@ -399,10 +402,11 @@ __global__ void noise_finalize_kernel(float* __restrict__ mean, float* __restric
 
 cudaError_t launch_noise_patchstd(const float* stack, long long pitch_y, long long pitch_z, int nx,
                                   long long nslice, const long long* samples, long long n,
-                                  int patchsize, float* out, cudaStream_t st) {
+                                  int patchsize, float* out, cudaStream_t st, int z_base) {
+    if (n <= 0) return cudaSuccess;
     if (n <= 0) return cudaSuccess;
     noise_patchstd_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
-        stack, pitch_y, pitch_z, nx, nslice, samples, n, patchsize, out);
+        stack, pitch_y, pitch_z, nx, nslice, samples, n, patchsize, out, z_base);
     return cudaGetLastError();
 }
 

@@ -4,9 +4,10 @@
 
 namespace inlm {
 
+// stack holds slices z_base.. of the volume (a z-slab; 0 = the whole volume).
 cudaError_t launch_noise_patchstd(const float* stack, long long pitch_y, long long pitch_z, int nx,
                                   long long nslice, const long long* samples, long long n,
-                                  int patchsize, float* out, cudaStream_t st);
+                                  int patchsize, float* out, cudaStream_t st, int z_base = 0);
 // windows[w] = inclusive sample range; scratch_off[w] = byte offset of the
 // window's assignment array inside scratch.
 cudaError_t launch_noise_em(const float* values, const int2* windows, int n_windows,

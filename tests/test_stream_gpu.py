@@ -1,0 +1,65 @@
+"""z-slab streaming of host-resident volumes: every form must equal the
+in-memory schedule (inlm_denoise) bit for bit, whatever the slab depth,
+because each slab is filtered as a sub-volume whose halo covers every value
+its voxels read (and, for the FP16 and learned forms, whose tiles sit where
+the whole volume's do)."""
+import numpy as np
+import pytest
+
+from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, stream_denoise, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def in_memory(raw, p, net=None, k=0, min_mass=0.0):
+    g = IterativeNLM_GPU()
+    g.configure_device(raw.shape, p)
+    if net is not None:
+        g.attach_proposal(net, k, min_mass)
+    out, s0, s1 = g.denoise(raw)
+    g.free_device()
+    return out, s0, s1
+
+
+@pytest.mark.parametrize("mode,slab,prec", [
+    ("z-adaptive", 8, "f32"), ("global", 16, "f32"), ("manual", 24, "f32"),
+    ("z-adaptive", 8, "f16"), ("global", 64, "f16"),
+])
+def test_stream_equals_in_memory(gpu, mode, slab, prec):
+    raw = synth.small_case((44, 40, 56), seed=21)
+    p = DenoiseParameters(radius_patchspace=(2, 2, 2), radius_searchspace=(3, 3, 3),
+                          noise_mode=mode, zwindow=10, sigma=(0.06, 0.05), noise_seed=3,
+                          precision=prec)
+    want, w0, w1 = in_memory(raw, p)
+    got, s0, s1, st = stream_denoise(raw, p, slab_depth=slab)
+    print(mode, prec, st)
+    assert st["slabs"] == -(-44 // st["slab_depth"])
+    if mode != "manual":
+        assert np.array_equal(s0, w0) and np.array_equal(s1, w1)
+    assert np.array_equal(got, want)
+
+
+def test_stream_continuous_estimate(gpu):
+    raw = synth.small_case((30, 36, 40), seed=4)
+    p = DenoiseParameters(radius_patchspace=(1, 1, 1), radius_searchspace=(2, 2, 2),
+                          noise_mode="global", continuous_estimate=True, noise_seed=9)
+    want, _, _ = in_memory(raw, p)
+    got, _, _, _ = stream_denoise(raw, p, slab_depth=8)
+    assert np.array_equal(got, want)
+
+
+def test_stream_learned_proposal(gpu, port):
+    from microtomodenoise_b200.proposal import ProposalNet
+    from oracle.oracle import FilterParams
+    from test_proposal_gpu import rand_params
+    raw = synth.small_case((48, 40, 48), seed=8)
+    p = DenoiseParameters(radius_patchspace=(1, 1, 1), radius_searchspace=(3, 3, 3),
+                          noise_mode="global", noise_seed=2, precision="f16")
+    S = len(port.search_offsets(FilterParams(search_radius=(3, 3, 3), patch_radius=(1, 1, 1))))
+    net = ProposalNet(S)
+    net.set_params(rand_params(S, 12))
+    want, _, _ = in_memory(raw, p, net, 40, 0.0)
+    got, _, _, st = stream_denoise(raw, p, slab_depth=8, net=net, k=40, min_mass=0.0)
+    assert st["halo"] >= 16
+    assert np.array_equal(got, want)
+    net.close()
