@@ -20,9 +20,11 @@ Multi-GPU (torchrun): each rank denoises its own volume (independent jobs,
 weak scaling, no data-path collective); time = max over ranks.
 
 ``forms`` (rank 0, one GPU): the same whole job in the FP16-storage form and
-in the learned-proposal + FP16 form (k = 128 of 514 offsets per 8^3 tile
-without fallback; and k = 256 with fallback to full search below 0.95
-predicted kept mass, which fires on every tile of this volume), each with
+in the learned-proposal + FP16 form (k = 112 of 514 offsets per 8^3 tile
+without fallback, the fastest k measured within 0.1 dB of the FP64 oracle's
+PSNR against the clean phantom with margin; and k = 256 with fallback to full
+search below 0.95 predicted kept mass, which fires on every tile of this
+volume), each with
 its speed-up over the plain FP32 job, the proposal's fallback fraction and
 evaluated-offset fraction, and its accuracy: max-abs error and PSNR against
 the FP64 full-search oracle on two sub-blocks (a corner and a central 40^3
@@ -264,7 +266,7 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
 
     net = ProposalNet.load(default_weights(PR, SR), device=local)
     forms = [("f32", "f32", None), ("fp16", "f16", None),
-             ("learned_fp16", "f16", (128, 0.0)), ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
+             ("learned_fp16", "f16", (112, 0.0)), ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
     raw_dev = torch.from_numpy(vol).cuda()
     out_dev = torch.empty_like(raw_dev)
     vox = float(np.prod(vol.shape))
@@ -406,6 +408,93 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_large_workload(args):
+    """One-step measurements of the two large workloads (rank 0, one GPU):
+
+    learned1024: float32 1024x1024x512 grain pack (noise 0.05 blurred 1, no
+      rings), patch r3 search r7 (1326 offsets), 4 iterations, global noise:
+      the whole job in plain FP32, FP16 full search, and learned + FP16 with
+      k = 256 per 8^3 tile (fallback below 0.95 predicted kept mass, and none).
+    stream2048: a 2048x2048xZ slab stack (Z = --stream-depth) of the grain pack
+      with noise sigma drifting 0.02 -> 0.08 along z (blur 1) and rings of
+      amplitude 0.03, z-adaptive noise, patch r3 search r7, 4 iterations, held
+      in host memory and streamed in z-slabs of 64 slices (inlm_stream_denoise):
+      plain FP32 and learned + FP16 (k = 256, no fallback).
+    PSNR against the clean phantom over the whole volume for every form."""
+    import torch
+    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, stream_denoise, synth
+    from microtomodenoise_b200.proposal import ProposalNet, default_weights
+    pr, sr = (3, 3, 3), (7, 7, 7)
+    net = ProposalNet.load(default_weights(pr, sr))
+    res = {"workload": args.workload, "forms": {}}
+    t = time.time()
+    if args.workload == "learned1024":
+        shape = (512, 1024, 1024)
+        vol, clean = synth.grain_pack_volume(shape, noise_std=0.05, noise_blur=1.0, ring_amp=0.0,
+                                             seed=0, return_clean=True)
+    else:
+        shape = (args.stream_depth, 2048, 2048)
+        vol, clean = synth.grain_pack_volume(shape, noise_blur=1.0, ring_amp=0.03,
+                                             sigma_drift=(0.02, 0.08), seed=0, return_clean=True)
+    log(f"generated {shape} in {time.time() - t:.1f}s")
+    vox = float(np.prod(shape)) * ITERS
+    res["config"] = {"shape_xyz": [shape[2], shape[1], shape[0]], "patch_radius": 3,
+                     "search_radius": 7, "offsets": 1326, "iterations": ITERS}
+    forms = [("f32", "f32", None), ("fp16", "f16", None), ("learned_fp16_k256_mass095", "f16", (256, 0.95)),
+             ("learned_fp16_k256", "f16", (256, 0.0))]
+    if args.workload == "stream2048":
+        forms = [("f32", "f32", None), ("learned_fp16_k256", "f16", (256, 0.0))]
+    ref_psnr = None
+    for name, prec, prop in forms:
+        dp = DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, maxiterations=ITERS,
+                               alpha=0.5, noise_seed=0, precision=prec,
+                               noise_mode="global" if args.workload == "learned1024" else "z-adaptive")
+        if args.workload == "learned1024":
+            g = IterativeNLM_GPU()
+            g.configure_device(shape, dp)
+            if prop:
+                g.attach_proposal(net, prop[0], prop[1])
+            raw = torch.from_numpy(vol).cuda()
+            out = torch.empty_like(raw)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            g.denoise(raw.data_ptr(), on_device=True, out=out.data_ptr())
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            r = {"ms_per_job": ms, "value": vox / (ms / 1e3), "unit": "voxel-iter/s", "kernel": g.describe()}
+            if prop:
+                st = g.proposal_stats()
+                r.update({"k": prop[0], "min_mass": prop[1],
+                          "fallback_fraction": st["fallback_tiles"] / max(st["tiles"], 1),
+                          "fraction_evaluated": st["fraction_evaluated"]})
+            o = out.cpu().numpy()
+            g.free_device()
+            del raw, out
+        else:
+            o, _, _, st = stream_denoise(vol, dp, slab_depth=64, net=net if prop else None,
+                                         k=prop[0] if prop else 0, min_mass=prop[1] if prop else 0.0)
+            ms = st["ms"]
+            r = {"ms_per_job": ms, "value": vox / (ms / 1e3), "unit": "voxel-iter/s",
+                 "h2d_bytes": st["h2d_bytes"], "d2h_bytes": st["d2h_bytes"], "slabs": st["slabs"],
+                 "halo": st["halo"]}
+            if prop:
+                r.update({"k": prop[0], "min_mass": prop[1]})
+        r["psnr_vs_clean_db"] = psnr(o, clean)
+        if name == "f32":
+            ref_psnr = r["psnr_vs_clean_db"]
+        r["delta_vs_f32_db"] = r["psnr_vs_clean_db"] - ref_psnr
+        res["forms"][name] = r
+        log(f"{name}: {r}")
+    f32 = res["forms"]["f32"]["ms_per_job"]
+    for v in res["forms"].values():
+        v["speedup_vs_f32"] = f32 / v["ms_per_job"]
+    net.close()
+    print(json.dumps(res), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -417,6 +506,11 @@ def main():
     ap.add_argument("--form-steps", type=int, default=2)
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--workload", default="grain512",
+                    choices=["grain512", "learned1024", "stream2048"],
+                    help="grain512: the headline bench line; the others: one-step "
+                         "measurements of the large workloads (see run_large_workload)")
+    ap.add_argument("--stream-depth", type=int, default=128)
     ap.add_argument("--shape", default="512,512,512",
                     help="nz,ny,nx of the volume (smaller shapes only for profiling runs)")
     args = ap.parse_args()
@@ -430,6 +524,12 @@ def main():
     SHAPE = tuple(int(v) for v in args.shape.split(","))
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.workload != "grain512":
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            run_large_workload(args)
         return
 
     import torch

@@ -1,0 +1,37 @@
+"""Small cases of the filter kernels for ncu captures (one GPU, a few GB).
+
+    python -m microtomodenoise_b200.profile_case fast
+        two iterations of a 512x512x64 grain pack, patch r2 search r5, FP16
+        form: iteration 1 with the shipped proposal (k = 112 per 8^3 tile, the
+        one-tile-per-CTA kernel), iteration 2 full search (the 32-wide kernel).
+"""
+from __future__ import annotations
+
+import sys
+
+import numpy as np
+
+
+def fast_case():
+    import torch
+    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, synth
+    from microtomodenoise_b200.proposal import ProposalNet, default_weights
+    vol = synth.grain_pack_volume((64, 512, 512), seed=0)
+    raw = torch.from_numpy(vol).cuda()
+    net = ProposalNet.load(default_weights((2, 2, 2), (5, 5, 5)))
+    g = IterativeNLM_GPU()
+    g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=(2, 2, 2),
+                                                    radius_searchspace=(5, 5, 5), precision="f16"))
+    g.set_sigma(np.full(64, 0.14, np.float32))
+    g.attach_proposal(net, 112, 0.0)
+    g.Run_GaussianNoise_device(1, raw.data_ptr())
+    g.attach_proposal(None)
+    g.Run_GaussianNoise_device(2)
+    torch.cuda.synchronize()
+    print("ok", g.describe())
+    g.free_device()
+    net.close()
+
+
+if __name__ == "__main__":
+    {"fast": fast_case}[sys.argv[1] if len(sys.argv) > 1 else "fast"]()
