@@ -20,9 +20,9 @@ Multi-GPU (torchrun): each rank denoises its own volume (independent jobs,
 weak scaling, no data-path collective); time = max over ranks.
 
 ``forms`` (rank 0, one GPU): the same whole job in the FP16-storage form and
-in the learned-proposal + FP16 form (k = 112 of 514 offsets per 8^3 tile
+in the learned-proposal + FP16 form (k = 104 of 514 offsets per 8^3 tile
 without fallback, the fastest k measured within 0.1 dB of the FP64 oracle's
-PSNR against the clean phantom with margin; and k = 256 with fallback to full
+PSNR against the clean phantom; and k = 256 with fallback to full
 search below 0.95 predicted kept mass, which fires on every tile of this
 volume), each with
 its speed-up over the plain FP32 job, the proposal's fallback fraction and
@@ -266,7 +266,7 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
 
     net = ProposalNet.load(default_weights(PR, SR), device=local)
     forms = [("f32", "f32", None), ("fp16", "f16", None),
-             ("learned_fp16", "f16", (112, 0.0)), ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
+             ("learned_fp16", "f16", (104, 0.0)), ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
     raw_dev = torch.from_numpy(vol).cuda()
     out_dev = torch.empty_like(raw_dev)
     vox = float(np.prod(vol.shape))

@@ -74,11 +74,13 @@ class InlmError(RuntimeError):
 _lib = None
 
 
-def load(path: str = LIB_PATH) -> C.CDLL:
-    """Loads libinlm.so once; raises if it has not been built."""
+def load(path: str = "") -> C.CDLL:
+    """Loads libinlm.so once (the in-tree build, or the file INLM_LIB names);
+    raises if it has not been built."""
     global _lib
     if _lib is not None:
         return _lib
+    path = path or os.environ.get("INLM_LIB", LIB_PATH)
     if not os.path.exists(path):
         raise ImportError(
             f"{path} is missing: build it with `python -m microtomodenoise_b200.build` "

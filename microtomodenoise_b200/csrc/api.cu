@@ -377,6 +377,30 @@ static void denoiser_free(inlm_denoiser* d) {
     if (d->own_stream && d->stream) cudaStreamDestroy(d->stream);
 }
 
+// Plane pitch (floats) of the raw box: the smallest padding of rpx * rby for
+// which the phase-B raw reads of a warp (8 rows j, 4 planes, one column) fall
+// in distinct banks.
+static int raw_plane_pitch(int rpx, int rby) {
+    const int base = rpx * rby;
+    for (int pad = 0; pad < 32; pad++) {
+        const int pl = base + pad;
+        bool ok = true;
+        for (int col = 0; col < 8 && ok; col++) {
+            unsigned used = 0;
+            for (int l = 0; l < 32; l++) {
+                const unsigned bank = (unsigned)((l >> 3) * pl + (l & 7) * rpx + col) % 32u;
+                if (used & (1u << bank)) {
+                    ok = false;
+                    break;
+                }
+                used |= 1u << bank;
+            }
+        }
+        if (ok) return pl;
+    }
+    return base;
+}
+
 // Tiled FP32 configuration for one candidate (CTA depth tz, raw staged in
 // shared memory or read from global): tables, kernel arguments, TMA map.
 // *ok = false when the candidate does not apply or does not fit.
@@ -419,6 +443,7 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     a.rbz = tz + 2 * a.szc;
     if (a.pbx > 256 || a.pby > 256 || a.pbz > 256) return INLM_OK;
     if ((long long)a.pbx * a.pby * a.pbz >= 65536) return INLM_OK;  // 16-bit index table
+    a.rplane = raw_plane_pitch(a.rbx + 1, a.rby);
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
     TileConfig tc{pr[0], pr[1], pr[2], tz, raw_smem, 0};
@@ -430,7 +455,7 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     // search deltas inside the shared-memory boxes (raw: box or global)
     std::vector<int2> dl(a.S);
     const int rpx = a.rbx + 1;  // odd shared-memory row pitch of the raw box
-    const int pplane = a.pbx * a.pby, rplane = rpx * a.rby;
+    const int pplane = a.pbx * a.pby, rplane = a.rplane;
     for (int s = 0; s < a.S; s++) {
         const Offset3& o = g.search[s];
         dl[s].x = o.z * pplane + o.y * a.pbx + o.x;

@@ -327,7 +327,8 @@ __global__ void __launch_bounds__(TX * TZ * 8 / FastThreads<TX>::VPT, TX == 32 ?
                     // Pade[3/3] of exp in Horner form, FMA
                     const float num = fmaf(fmaf(x + 12.f, x, 60.f), x, 120.f);
                     const float den = fmaf(fmaf(12.f - x, x, -60.f), x, 120.f);
-                    const float w = (x > -3.56648f) ? __fdividef(num, den) : 0.0f;
+                    const float q = __fdividef(num, den);  // formed, then selected
+                    const float w = (x > -3.56648f) ? q : 0.0f;
                     if constexpr (MASS) {
                         part = fmaf(w, inv[r], part);
                     } else {

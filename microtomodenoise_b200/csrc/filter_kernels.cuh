@@ -24,6 +24,8 @@ struct TileArgs {
     const int2* __restrict__ search_delta;  // (prev-box delta, raw delta) per offset
     int pbx, pby, pbz;            // prev box (shared memory) extents
     int rbx, rby, rbz;            // raw box extents (raw staged in shared memory)
+    int rplane;                   // raw box plane pitch (floats): rows of rbx + 1, padded so a
+                                  // warp's 8 rows x 4 planes hit distinct banks
     const float* __restrict__ raw_pad;   // padded raw (global) for the raw-global form
     long long gpitch_y, gpitch_z;        // padded global pitches (elements)
     float* __restrict__ out;      // unpadded result
