@@ -45,6 +45,7 @@ extern "C" {
 #define INLM_ERR_STATE -5      /* call out of order (e.g. iteration 2 before 1) */
 #define INLM_ERR_TIMEOUT -6    /* a bounded device wait ran out */
 #define INLM_ERR_UNSUPPORTED -7
+#define INLM_ERR_IO -8         /* file missing, unreadable or not a TIFF */
 
 /* noise estimation modes (denoise_parameters.h:22) */
 #define INLM_NOISE_ZADAPTIVE 0
@@ -334,6 +335,42 @@ int inlm_geometry(const inlm_params* p, int nz, int* search_xyz, int* n_search, 
  * sequence of srand(seed), sorted ascending. */
 int inlm_noise_draw_samples(const int shape[3], uint64_t n_samples, int patchsize,
                             int circular_mask_diameter, unsigned int seed, int64_t* out);
+
+/* ---------------- resume ---------------- */
+
+/* Installs a finished iteration's result read back from disk instead of
+ * computing it: the --resume branch of IterativeNLM_GPU::Run_GaussianNoise
+ * (iternlm_gpu.cu:1665-1697), which uploads the saved result and, for
+ * iteration 1, still prepares the raw volume. result_host holds nx*ny*nz
+ * floats; raw_host is required when iter == 1 and ignored otherwise. */
+int inlm_set_result(inlm_denoiser* d, int iter, const float* result_host, const float* raw_host);
+
+/* ---------------- TIFF sequence IO (hdcom::HdCommunication) ----------------
+ * Uncompressed baseline TIFF without libtiff: greyscale slices of 8, 16 or 32
+ * bits per sample (and 64-bit float), in strips, either byte order. path is a
+ * directory of .tif / .tiff slice files, taken in sorted name order, or one
+ * .tif / .tiff file whose pages are the slices (an ImageJ stack stored as one
+ * directory with "images=N" included). Compressed, tiled and multi-sample
+ * files return INLM_ERR_UNSUPPORTED; missing paths INLM_ERR_IO. */
+
+/* GetFilelist_And_ImageSequenceDimensions (Geometry/hdcommunication.cpp:51):
+ * shape receives {width, height, slices}; samples_per_pixel (nullable) the
+ * first slice's samples per pixel. */
+int inlm_tiff_shape(const char* path, int shape[3], int* samples_per_pixel);
+
+/* Get3DTifSequence_32bitPointer (hdcommunication.cpp:975, :1022) and
+ * GetTif_unknowndim_32bit (:106): slices first_slice..last_slice (inclusive,
+ * clamped to the stack; -1, -1 = all) into out, x fastest; n_out is the
+ * number of floats out holds. Integer samples convert by value (8- and
+ * 16-bit unsigned as the reference reads them), IEEE samples as stored. */
+int inlm_tiff_read(const char* path, int first_slice, int last_slice, float* out, uint64_t n_out);
+
+/* SaveTifSequence_32bit / SaveTifSequence_as16bit (hdcommunication.cpp:1576,
+ * :1602): shape[2] slices written as dir/<name><z0+i, 4 digits>.tif, dir
+ * created as needed; 32-bit IEEE float, or with as_16bit unsigned 16-bit after
+ * min(max(0, round(v)), 65535) (:1472). Strips of max(1, 2048 / width) rows. */
+int inlm_tiff_write_sequence(const float* image, const int shape[3], int z0, const char* dir,
+                             const char* name, int as_16bit);
 
 #ifdef __cplusplus
 }

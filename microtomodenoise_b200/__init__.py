@@ -152,6 +152,24 @@ class IterativeNLM_GPU:
         _lib.check(_lib.load().inlm_get_result(self._h, out.ctypes.data), "get_result")
         return out
 
+    def set_result(self, iteration: int, result: np.ndarray,
+                   instack: Optional[np.ndarray] = None) -> None:
+        """--resume: installs a finished iteration read back from disk in place
+        of computing it (iternlm_gpu.cu:1665-1697); iteration 1 also needs the
+        raw stack, which is prepared as a computed iteration 1 would."""
+        self._need()
+        result = _f32c(result)
+        assert result.shape == self.shape
+        ptr = None
+        if iteration == 1:
+            if instack is None:
+                raise ValueError("iteration 1 needs the raw stack")
+            instack = _f32c(instack)
+            assert instack.shape == self.shape
+            ptr = instack.ctypes.data
+        _lib.check(_lib.load().inlm_set_result(self._h, int(iteration), result.ctypes.data, ptr),
+                   "set_result")
+
     def get_result_device(self, out_dev_ptr: int) -> None:
         self._need()
         _lib.check(_lib.load().inlm_get_result_device(self._h, out_dev_ptr), "get_result_device")

@@ -19,6 +19,7 @@ ERRORS = {
     -5: "INLM_ERR_STATE",
     -6: "INLM_ERR_TIMEOUT",
     -7: "INLM_ERR_UNSUPPORTED",
+    -8: "INLM_ERR_IO",
 }
 NOISE_MODES = {"z-adaptive": 0, "auto": 0, "global": 1, "manual": 2, "semimanual": 3}
 PRECISIONS = {"f32": 0, "f16": 1, "f16_df32": 2}
@@ -37,7 +38,8 @@ EXPORTS = (
     "inlm_proposal_train", "inlm_proposal_select", "inlm_attach_proposal", "inlm_proposal_stats",
     "inlm_weight_map", "inlm_net_input",
     "inlm_autotune", "inlm_batch_create", "inlm_batch_destroy", "inlm_batch_run",
-    "inlm_batch_describe", "inlm_stream_denoise",
+    "inlm_batch_describe", "inlm_stream_denoise", "inlm_set_result",
+    "inlm_tiff_shape", "inlm_tiff_read", "inlm_tiff_write_sequence",
 )
 
 
@@ -136,6 +138,10 @@ def load(path: str = "") -> C.CDLL:
     L.inlm_batch_describe.argtypes = [vp, C.c_char_p, C.c_size_t]
     L.inlm_stream_denoise.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp,
                                       C.c_int, C.c_float, vp, vp, vp]
+    L.inlm_set_result.argtypes = [vp, C.c_int, vp, vp]
+    L.inlm_tiff_shape.argtypes = [C.c_char_p, C.c_int * 3, C.POINTER(C.c_int)]
+    L.inlm_tiff_read.argtypes = [C.c_char_p, C.c_int, C.c_int, vp, C.c_uint64]
+    L.inlm_tiff_write_sequence.argtypes = [vp, C.c_int * 3, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
     for name in EXPORTS:
         if name not in ("inlm_last_error", "inlm_default_params"):
             getattr(L, name).restype = C.c_int

@@ -45,6 +45,7 @@ LIB_SOURCES = [
     "api_stream.cu",
     "geometry.cpp",
     "sampling.cpp",
+    "tiff_io.cpp",
 ]
 
 
@@ -101,7 +102,7 @@ def build_cli(force: bool = False) -> str:
         return ""
     deps = [src, LIB, os.path.join(CSRC, "iternlm.hpp")]
     if force or _newer(CLI, [d for d in deps if os.path.exists(d)]):
-        _run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC,
+        _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC,
               src, "-o", CLI, "-L" + LIBDIR, "-linlm", "-Wl,-rpath,$ORIGIN"])
     return CLI
 

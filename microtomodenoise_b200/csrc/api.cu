@@ -900,6 +900,27 @@ extern "C" int inlm_get_result(inlm_denoiser* d, float* out_host) {
     return check_device_error(d);
 }
 
+extern "C" int inlm_set_result(inlm_denoiser* d, int iter, const float* result_host,
+                               const float* raw_host) {
+    if (!d || !result_host) return fail(INLM_ERR_ARG, "null argument");
+    if (iter < 1) return fail(INLM_ERR_ARG, "iteration must be >= 1");
+    if (iter > 1 && d->last_iter < 1) return fail(INLM_ERR_STATE, "iteration %d before iteration 1", iter);
+    CUDA_TRY(cudaSetDevice(d->device));
+    const long long nvox = (long long)d->shape[0] * d->shape[1] * d->shape[2];
+    if (iter == 1) {
+        if (!raw_host) return fail(INLM_ERR_ARG, "iteration 1 needs the raw volume");
+        // raw is padded once and kept, as prepare_iteration1 does
+        CUDA_TRY(cudaMemcpyAsync(d->d_next, raw_host, nvox * 4, cudaMemcpyHostToDevice, d->stream));
+        const int rc = d->use_fast ? pad_into_half(d, d->d_next, d->d_raw_h)
+                                   : pad_into(d, d->d_next, d->d_raw_pad);
+        if (rc) return rc;
+    }
+    CUDA_TRY(cudaMemcpyAsync(d->d_next, result_host, nvox * 4, cudaMemcpyHostToDevice, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    d->last_iter = iter;
+    return check_device_error(d);
+}
+
 extern "C" int inlm_get_result_device(inlm_denoiser* d, float* out_dev) {
     if (!d || !out_dev) return fail(INLM_ERR_ARG, "null argument");
     if (d->last_iter < 1) return fail(INLM_ERR_STATE, "no iteration has run");

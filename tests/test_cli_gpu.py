@@ -1,0 +1,123 @@
+"""The iterNLM command line end to end on the GPU: TIFF slices in, the
+reference driver's schedule (main.cpp:311-545) through the C++ shim and the
+C ABI, TIFF slices and noise files out; results checked bit for bit against
+the oracle (manual sigma) and against the library's own whole-job call
+(estimated sigma)."""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, synth, tiffio
+from oracle.oracle import FilterParams
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "microtomodenoise_b200", "lib", "iterNLM")
+
+
+def _cli(*args):
+    r = subprocess.run([CLI, *map(str, args)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r.stdout
+
+
+@pytest.fixture()
+def stack(tmp_path):
+    vol = synth.spheres_volume((12, 40, 48), n_spheres=6, rmin=3, rmax=9, seed=4)
+    tiffio.save_stack(vol, str(tmp_path / "in"), "slice")
+    return vol, tmp_path
+
+
+def test_cli_manual_sigma_matches_oracle(gpu, port, stack):
+    vol, tmp = stack
+    out = tmp / "out"
+    log = _cli("-i", tmp / "in", "-o", out, "-iter", 2, "-search", 3, "-patch", 1, "-noise", "manual",
+               "-sigma0", 0.05, "-sigma1", 0.03, "-alpha", 0.5)
+    assert "iteration 2 took" in log
+    it1 = tiffio.read_stack(str(out / "denoise-iteration01"))
+    it2 = tiffio.read_stack(str(out / "denoise-iteration02"))
+    p = FilterParams(search_radius=(3, 3, 3), patch_radius=(1, 1, 1))
+    s0 = np.full(12, 0.05, np.float32)
+    blend = (np.float32(0.5) * s0 + np.float32(0.5) * np.full(12, 0.03, np.float32)).astype(np.float32)
+    assert np.array_equal(it1, port.denoise_f32(vol, p, s0[None]))
+    assert np.array_equal(it2, port.denoise_f32(vol, p, np.stack([s0, blend])))
+    # noise files: "n,value" per slice
+    rows = (out / "noise_vs_slice00.csv").read_text().splitlines()
+    assert len(rows) == 12 and rows[0] == "0,0.05"
+    assert os.path.exists(tmp / "logfile.txt")
+
+
+def test_cli_estimated_noise_equals_library_whole_job(gpu, stack):
+    vol, tmp = stack
+    out = tmp / "out"
+    _cli("-i", tmp / "in", "-o", out, "-iter", 3, "-search", 3, "-patch", 2, "-noise", "global",
+         "-nsamples", 20000, "-seed", 5)
+    got = tiffio.read_stack(str(out / "denoise-iteration03"))
+    dp = DenoiseParameters(radius_searchspace=(3, 3, 3), radius_patchspace=(2, 2, 2),
+                           noise_mode="global", n_samples=20000, noise_seed=5, maxiterations=3)
+    g = IterativeNLM_GPU()
+    g.configure_device(vol.shape, dp)
+    want, s0, s1 = g.denoise(vol)
+    g.free_device()
+    assert np.array_equal(got, want)
+    csv0 = np.array([float(r.split(",")[1]) for r in (out / "noise_vs_slice00.csv").read_text().split()])
+    assert np.allclose(csv0, s0, rtol=1e-5)
+
+
+def test_cli_16bit_cleanup_and_slice_range(gpu, port, tmp_path):
+    vol = synth.spheres_volume((10, 32, 36), n_spheres=5, rmin=3, rmax=8, seed=6) * 1000.0
+    tiffio.save_stack(vol.astype(np.float32), str(tmp_path / "in"), "s")
+    out = tmp_path / "out"
+    _cli("-i", tmp_path / "in", "-o", out, "-iter", 2, "-search", 2, "-patch", 1, "-noise", "manual",
+         "-sigma", 40, "-fs", 2, "-ls", 6, "--16bit", "--cleanup")
+    names = sorted(n for n in os.listdir(out) if n.endswith(".tif"))
+    assert names == [f"denoised{z:04d}.tif" for z in range(2, 7)]
+    assert not any(n.startswith("denoise-iteration") for n in os.listdir(out))
+    got = tiffio.read_stack(str(out))
+    sub = vol[2:7].astype(np.float32)
+    p = FilterParams(search_radius=(2, 2, 2), patch_radius=(1, 1, 1))
+    s = np.full(5, 40, np.float32)
+    want = port.denoise_f32(sub, p, np.stack([s, s]))
+    r = np.trunc(want.astype(np.float64) + np.copysign(0.5, want))
+    assert np.array_equal(got, np.clip(r, 0, 65535).astype(np.float32))
+
+
+def test_cli_resume_reads_finished_iterations(gpu, stack):
+    vol, tmp = stack
+    out = tmp / "out"
+    args = ["-i", tmp / "in", "-o", out, "-iter", 3, "-search", 3, "-patch", 1, "-noise", "global",
+            "-nsamples", 20000, "-seed", 9]
+    _cli(*args)
+    full = tiffio.read_stack(str(out / "denoise-iteration03"))
+    shutil.rmtree(out / "denoise-iteration03")
+    log = _cli(*args, "--resume")
+    assert "iteration 1 read in from disk" in log and "iteration 2 read in from disk" in log
+    assert "iteration 3 took" in log
+    assert np.array_equal(tiffio.read_stack(str(out / "denoise-iteration03")), full)
+
+
+def test_cli_fp16_form(gpu, stack):
+    """-precision f16 runs the FP16 storage form: the same result as the
+    library's FP16 form called directly (its accuracy is covered by the FP16
+    tests against the FP64 oracle)."""
+    vol, tmp = stack
+    out = tmp / "out"
+    _cli("-i", tmp / "in", "-o", out, "-iter", 2, "-search", 3, "-patch", 2, "-noise", "manual",
+         "-sigma", 0.05, "-precision", "f16")
+    got = tiffio.read_stack(str(out / "denoise-iteration02"))
+    g = IterativeNLM_GPU()
+    g.configure_device(vol.shape, DenoiseParameters(radius_searchspace=(3, 3, 3),
+                                                    radius_patchspace=(2, 2, 2), precision="f16"))
+    s = np.full(12, 0.05, np.float32)
+    g.set_sigma(s)
+    g.Run_GaussianNoise(1, vol)
+    g.Run_GaussianNoise(2)
+    want = g.get_result()
+    g.free_device()
+    assert np.array_equal(got, want)
