@@ -296,6 +296,7 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / args.form_steps
             kms, kn = g.filter_kernel_ms()
+            r["kernel"] = g.describe()  # after the runs: the proposal selects the per-tile kernel
             r.update({"value": vox * ITERS / (ms / 1e3), "unit": "voxel-iter/s",
                       "ms_per_step": ms, "steps": args.form_steps, "warmup": 1,
                       "speedup_vs_f32": vox * ITERS / (ms / 1e3) / value_f32,
