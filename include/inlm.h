@@ -345,6 +345,38 @@ int inlm_noise_draw_samples(const int shape[3], uint64_t n_samples, int patchsiz
  * floats; raw_host is required when iter == 1 and ignored otherwise. */
 int inlm_set_result(inlm_denoiser* d, int iter, const float* result_host, const float* raw_host);
 
+/* ---------------- z-slab sharding across GPUs ----------------
+ * Building blocks of the multi-GPU form of Run_GaussianNoise_GPUBlocks
+ * (iternlm_gpu.cu:1732-2115, which splits the stack in z across n_gpus):
+ * each rank filters its z-slab plus halos of its neighbours' slices, and the
+ * noise estimate gathers the per-sample patch stds of all ranks before one
+ * replicated EM. The exchange itself is the caller's (NCCL or any transport). */
+
+/* Copies slices z0..z0+n_slices-1 of the last result out of (get) or into
+ * (set) the denoiser; set overwrites them before the next iteration pads the
+ * result into its previous-iterate volume. dst / src are host pointers when
+ * on_device == 0 (the call returns when the copy is done), else device
+ * pointers (the copy is queued on the denoiser's stream). */
+int inlm_get_result_slices(inlm_denoiser* d, int z0, int n_slices, float* dst, int on_device);
+int inlm_set_result_slices(inlm_denoiser* d, int z0, int n_slices, const float* src, int on_device);
+
+/* get_patchstd (noiselevel.cpp:235-283) for the samples lying in slices
+ * z_base..z_base+n_slices-1 of the noise handle's stack, read from slab (those
+ * slices only, x fastest; host or device memory by on_device). Draws the
+ * sample positions on the first call. patchstd_host receives one value per
+ * drawn sample (n_values >= the count inlm_noise_samples reports): the
+ * slab's samples get their std, all others 0, so that a sum over ranks
+ * holding disjoint slabs yields every sample's std. */
+int inlm_noise_patchstd_slab(inlm_noise* n, const inlm_params* p, const float* slab, int on_device,
+                             int z_base, int n_slices, float* patchstd_host, uint64_t n_values);
+
+/* The rest of get_noiselevel (noiselevel.cpp:9-95) for given patch stds
+ * (host, one per drawn sample): the two-cluster EM of the mode, or the
+ * semimanual / manual choice, into sigma_out (nz floats, host). Each call
+ * counts as one estimate of the handle, as inlm_noise_estimate does. */
+int inlm_noise_estimate_from_patchstd(inlm_noise* n, inlm_params* p, const float* patchstd_host,
+                                      uint64_t n_values, float* sigma_out);
+
 /* ---------------- TIFF sequence IO (hdcom::HdCommunication) ----------------
  * Uncompressed baseline TIFF without libtiff: greyscale slices of 8, 16 or 32
  * bits per sample (and 64-bit float), in strips, either byte order. path is a

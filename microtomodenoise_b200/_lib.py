@@ -40,6 +40,8 @@ EXPORTS = (
     "inlm_autotune", "inlm_batch_create", "inlm_batch_destroy", "inlm_batch_run",
     "inlm_batch_describe", "inlm_stream_denoise", "inlm_set_result",
     "inlm_tiff_shape", "inlm_tiff_read", "inlm_tiff_write_sequence",
+    "inlm_get_result_slices", "inlm_set_result_slices", "inlm_noise_patchstd_slab",
+    "inlm_noise_estimate_from_patchstd",
 )
 
 
@@ -142,6 +144,11 @@ def load(path: str = "") -> C.CDLL:
     L.inlm_tiff_shape.argtypes = [C.c_char_p, C.c_int * 3, C.POINTER(C.c_int)]
     L.inlm_tiff_read.argtypes = [C.c_char_p, C.c_int, C.c_int, vp, C.c_uint64]
     L.inlm_tiff_write_sequence.argtypes = [vp, C.c_int * 3, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
+    L.inlm_get_result_slices.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int]
+    L.inlm_set_result_slices.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int]
+    L.inlm_noise_patchstd_slab.argtypes = [vp, C.POINTER(InlmParams), vp, C.c_int, C.c_int, C.c_int,
+                                           vp, C.c_uint64]
+    L.inlm_noise_estimate_from_patchstd.argtypes = [vp, C.POINTER(InlmParams), vp, C.c_uint64, vp]
     for name in EXPORTS:
         if name not in ("inlm_last_error", "inlm_default_params"):
             getattr(L, name).restype = C.c_int

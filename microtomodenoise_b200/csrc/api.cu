@@ -338,6 +338,95 @@ extern "C" int inlm_noise_patchstd(inlm_noise* n, float* out, uint64_t max_n) {
     return INLM_OK;
 }
 
+extern "C" int inlm_noise_patchstd_slab(inlm_noise* n, const inlm_params* p, const float* slab,
+                                        int on_device, int z_base, int n_slices, float* patchstd_host,
+                                        uint64_t n_values) {
+    if (!n || !p || !slab || !patchstd_host) return fail(INLM_ERR_ARG, "null argument");
+    const int nz = n->shape[2];
+    if (z_base < 0 || n_slices < 1 || z_base + n_slices > nz)
+        return fail(INLM_ERR_ARG, "slices %d..%d outside the stack of %d", z_base, z_base + n_slices - 1, nz);
+    CUDA_TRY(cudaSetDevice(n->device));
+    int nwin = 0;
+    int rc = noise_prepare(n, p, &nwin, nullptr);  // draws the samples on the first call
+    if (rc) return rc;
+    const uint64_t ns = n->samples.size();
+    if (n_values < ns) return fail(INLM_ERR_ARG, "patchstd_host holds %llu values, %llu samples drawn",
+                                   (unsigned long long)n_values, (unsigned long long)ns);
+    const long long plane = (long long)n->shape[0] * n->shape[1];
+    const float* d_slab = slab;
+    if (!on_device) {
+        if (!n->d_stack) CUDA_TRY(dalloc(&n->d_stack, plane * nz));
+        CUDA_TRY(cudaMemcpyAsync(n->d_stack, slab, plane * n_slices * 4, cudaMemcpyHostToDevice, n->stream));
+        d_slab = n->d_stack;
+    }
+    // samples are sorted by linear index: the slab's samples are one range
+    const long long i0 = std::lower_bound(n->samples.begin(), n->samples.end(), (long long)z_base * plane) -
+                         n->samples.begin();
+    const long long i1 = std::lower_bound(n->samples.begin(), n->samples.end(),
+                                          (long long)(z_base + n_slices) * plane) - n->samples.begin();
+    std::fill(patchstd_host, patchstd_host + ns, 0.0f);
+    if (i1 > i0) {
+        CUDA_TRY(launch_noise_patchstd(d_slab, n->shape[0], plane, n->shape[0], plane, n->d_samples + i0,
+                                       i1 - i0, n->patchsize, n->d_patchstd + i0, n->stream, z_base));
+        CUDA_TRY(cudaMemcpyAsync(patchstd_host + i0, n->d_patchstd + i0, (i1 - i0) * 4,
+                                 cudaMemcpyDeviceToHost, n->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(n->stream));
+    return INLM_OK;
+}
+
+extern "C" int inlm_noise_estimate_from_patchstd(inlm_noise* n, inlm_params* p, const float* patchstd_host,
+                                                 uint64_t n_values, float* sigma_out) {
+    if (!n || !p || !sigma_out) return fail(INLM_ERR_ARG, "null argument");
+    const int nz = n->shape[2];
+    if (p->noise_mode == INLM_NOISE_MANUAL) {
+        // noiselevel.cpp:84-91
+        std::fill(sigma_out, sigma_out + nz, p->sigma[n->ncalls > 0 ? 1 : 0]);
+        n->ncalls++;
+        return INLM_OK;
+    }
+    if (p->noise_mode != INLM_NOISE_ZADAPTIVE && p->noise_mode != INLM_NOISE_GLOBAL &&
+        p->noise_mode != INLM_NOISE_SEMIMANUAL)
+        return fail(INLM_ERR_ARG, "unknown noise mode %d", p->noise_mode);
+    if (!patchstd_host) return fail(INLM_ERR_ARG, "null patch stds");
+    if (n->samples.empty()) return fail(INLM_ERR_STATE, "no samples drawn: run inlm_noise_patchstd_slab first");
+    const uint64_t ns = n->samples.size();
+    if (n_values != ns)
+        return fail(INLM_ERR_ARG, "%llu patch stds for %llu samples", (unsigned long long)n_values,
+                    (unsigned long long)ns);
+    CUDA_TRY(cudaSetDevice(n->device));
+    if (p->noise_mode == INLM_NOISE_SEMIMANUAL) {
+        // noiselevel.cpp:62-79, as inlm_noise_estimate decides it
+        float v;
+        if (n->ncalls == 0) {
+            float best = 1e9f;
+            v = p->sigma[0];
+            for (uint64_t i = 0; i < ns; i++) {
+                const float d = std::fabs(patchstd_host[i] - v);
+                if (d < best) {
+                    best = d;
+                    n->ref_sample_semimanual = (long long)i;
+                }
+            }
+        } else {
+            v = patchstd_host[n->ref_sample_semimanual];
+            p->sigma[1] = v;
+        }
+        std::fill(sigma_out, sigma_out + nz, v);
+        n->ncalls++;
+        return INLM_OK;
+    }
+    int nwin = 0;
+    int rc = noise_prepare(n, p, &nwin, nullptr);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(n->d_patchstd, patchstd_host, ns * 4, cudaMemcpyHostToDevice, n->stream));
+    rc = noise_em_finish(n, p, nwin);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(sigma_out, n->d_sigma, nz * 4, cudaMemcpyDeviceToHost, n->stream));
+    CUDA_TRY(cudaStreamSynchronize(n->stream));
+    return INLM_OK;
+}
+
 // ---------------- denoiser handle ----------------
 
 static void denoiser_free(inlm_denoiser* d) {
@@ -919,6 +1008,35 @@ extern "C" int inlm_set_result(inlm_denoiser* d, int iter, const float* result_h
     CUDA_TRY(cudaStreamSynchronize(d->stream));
     d->last_iter = iter;
     return check_device_error(d);
+}
+
+static int result_slices(inlm_denoiser* d, int z0, int n_slices, const void* src, void* dst, bool to_result,
+                         int on_device) {
+    if (!d || !(to_result ? src : dst)) return fail(INLM_ERR_ARG, "null argument");
+    if (d->last_iter < 1) return fail(INLM_ERR_STATE, "no iteration has run");
+    if (z0 < 0 || n_slices < 0 || z0 + n_slices > d->shape[2])
+        return fail(INLM_ERR_ARG, "slices %d..%d outside 0..%d", z0, z0 + n_slices - 1, d->shape[2] - 1);
+    if (n_slices == 0) return INLM_OK;
+    CUDA_TRY(cudaSetDevice(d->device));
+    const size_t plane = (size_t)d->shape[0] * d->shape[1];
+    float* res = d->d_next + plane * z0;
+    const size_t bytes = plane * n_slices * 4;
+    const cudaMemcpyKind kind = to_result ? (on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice)
+                                          : (on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost);
+    CUDA_TRY(cudaMemcpyAsync(to_result ? (void*)res : dst, to_result ? src : (const void*)res, bytes, kind,
+                             d->stream));
+    // host copies complete before returning; device copies are ordered on the stream
+    if (!on_device) CUDA_TRY(cudaStreamSynchronize(d->stream));
+    return INLM_OK;
+}
+
+extern "C" int inlm_get_result_slices(inlm_denoiser* d, int z0, int n_slices, float* dst, int on_device) {
+    return result_slices(d, z0, n_slices, nullptr, dst, false, on_device);
+}
+
+extern "C" int inlm_set_result_slices(inlm_denoiser* d, int z0, int n_slices, const float* src,
+                                      int on_device) {
+    return result_slices(d, z0, n_slices, src, nullptr, true, on_device);
 }
 
 extern "C" int inlm_get_result_device(inlm_denoiser* d, float* out_dev) {
