@@ -27,7 +27,7 @@ the FP32 form. Requirements: every slab at least ``halo`` slices deep.
 from __future__ import annotations
 
 import ctypes as C
-from typing import List, Optional, Sequence, Tuple
+from typing import List, Optional, Tuple
 
 import numpy as np
 
@@ -130,13 +130,13 @@ class CudaSlabBackend:
         self.lo, self.own = z0 - self.a, z1 - z0
         self.hi = self.b - z1
         self.dev = torch.device("cuda", int(params.deviceID))
-        self.stream = torch.cuda.current_stream(self.dev)
+        # one stream for the denoiser and for every torch op on its buffers
+        self.stream = torch.cuda.Stream(device=self.dev)
         self.g = IterativeNLM_GPU()
         self.g.configure_device((self.b - self.a, ny, nx), params)
         self.g.set_stream(self.stream.cuda_stream)
         if proposal is not None:
             self.g.attach_proposal(*proposal)
-        self.plane = ny * nx
         self.raw = torch.empty((self.b - self.a, ny, nx), dtype=torch.float32, device=self.dev)
         self.buf = torch.empty((self.own, ny, nx), dtype=torch.float32, device=self.dev)
         L = _lib.load()
@@ -147,41 +147,46 @@ class CudaSlabBackend:
         _lib.check(L.inlm_noise_create(shape, int(params.n_samples), int(params.patchsize),
                                        self.cp.noise_seed, self.cp.device_id, C.byref(self.noise)),
                    "noise_create")
-        self.iter = 0
 
     # raw sub-volume: own slices from the caller, halos from the neighbours
     def set_raw(self, raw_own, raw_lo, raw_hi) -> None:
         r = self.raw
-        r[self.lo:self.lo + self.own].copy_(self.torch.as_tensor(np.ascontiguousarray(raw_own, np.float32)))
-        if self.lo:
-            r[:self.lo].copy_(raw_lo[-self.lo:])
-        if self.hi:
-            r[self.lo + self.own:].copy_(raw_hi[:self.hi])
-
-    def raw_edges(self, h: int):
-        own = self.raw[self.lo:self.lo + self.own]
-        return own[:h], own[-h:]
+        with self.torch.cuda.stream(self.stream):
+            r[self.lo:self.lo + self.own].copy_(
+                self.torch.as_tensor(np.ascontiguousarray(raw_own, np.float32)))
+            if self.lo:
+                r[:self.lo].copy_(raw_lo[-self.lo:])
+            if self.hi:
+                r[self.lo + self.own:].copy_(raw_hi[:self.hi])
+        self.stream.synchronize()
 
     def result_edges(self, h: int):
+        """The first and last h owned result slices (device tensors, complete
+        on return, so any stream may send them)."""
         t = self.torch
-        lo = t.empty((h,) + self.full[1:], dtype=t.float32, device=self.dev)
-        hi = t.empty_like(lo)
+        with t.cuda.stream(self.stream):
+            lo = t.empty((h,) + self.full[1:], dtype=t.float32, device=self.dev)
+            hi = t.empty_like(lo)
         _lib.check(self.L.inlm_get_result_slices(self.g._h, self.lo, h, lo.data_ptr(), 1), "get_slices")
         _lib.check(self.L.inlm_get_result_slices(self.g._h, self.lo + self.own - h, h, hi.data_ptr(), 1),
                    "get_slices")
+        self.stream.synchronize()
         return lo, hi
 
     def set_halos(self, recv_lo, recv_hi) -> None:
-        if self.lo:
-            src = recv_lo[-self.lo:].to(self.dev).contiguous()
-            _lib.check(self.L.inlm_set_result_slices(self.g._h, 0, self.lo, src.data_ptr(), 1), "set_slices")
-            self._keep = src
-        if self.hi:
-            src = recv_hi[:self.hi].to(self.dev).contiguous()
-            _lib.check(self.L.inlm_set_result_slices(self.g._h, self.lo + self.own, self.hi,
-                                                     src.data_ptr(), 1), "set_slices")
-            self._keep_hi = src
-        self.stream.synchronize()
+        keep = []
+        with self.torch.cuda.stream(self.stream):
+            if self.lo:
+                src = recv_lo[-self.lo:].to(self.dev).contiguous()
+                keep.append(src)
+                _lib.check(self.L.inlm_set_result_slices(self.g._h, 0, self.lo, src.data_ptr(), 1),
+                           "set_slices")
+            if self.hi:
+                src = recv_hi[:self.hi].to(self.dev).contiguous()
+                keep.append(src)
+                _lib.check(self.L.inlm_set_result_slices(self.g._h, self.lo + self.own, self.hi,
+                                                         src.data_ptr(), 1), "set_slices")
+        self.stream.synchronize()  # the sources may be freed after this
 
     def patchstd(self, source: str) -> np.ndarray:
         n = C.c_uint64(0)
@@ -263,7 +268,9 @@ class ZSlabJob:
 
     def run(self, raw_own: np.ndarray):
         """raw_own: this rank's slices [z0, z1) of the raw stack (host).
-        Returns (this rank's result slices, sigma0, sigma1) as host arrays."""
+        Returns (this rank's result slices, sigma0, sigma1) as host arrays,
+        sigma1 being the estimate on iteration 1's result before the alpha
+        blend (zeros for a single iteration), as inlm_denoise reports it."""
         p = self.params
         raw_own = np.ascontiguousarray(raw_own, np.float32)
         assert raw_own.shape == (self.z1 - self.z0,) + self.full[1:], raw_own.shape
@@ -276,18 +283,18 @@ class ZSlabJob:
         s0 = self._estimate("raw")
         self.be.set_sigma(s0)
         self.be.iterate(1)
-        s1 = s0
+        s1 = np.zeros_like(s0)
         if p.maxiterations > 1:
             self._swap_results()
-            s1 = self._blend(s0, self._estimate("result"))
-            self.be.set_sigma(s1)
+            s1 = self._estimate("result")
+            self.be.set_sigma(self._blend(s0, s1))
         for it in range(2, p.maxiterations + 1):
             self.be.iterate(it)
             if it < p.maxiterations:
                 self._swap_results()
             if p.continuous_estimate and p.maxiterations > it + 1:
-                s1 = self._blend(s0, self._estimate("result"))
-                self.be.set_sigma(s1)
+                self.be.set_sigma(self._blend(s0, self._estimate("result")))
+        # sigma1 as inlm_denoise reports it: the pre-blend estimate on iteration 1's result
         return self.be.result_own(), s0, s1
 
     def _blend(self, s0, s1):

@@ -98,8 +98,27 @@ def test_cli_resume_reads_finished_iterations(gpu, stack):
     shutil.rmtree(out / "denoise-iteration03")
     log = _cli(*args, "--resume")
     assert "iteration 1 read in from disk" in log and "iteration 2 read in from disk" in log
+    assert "Read in noise level 0 from file" in log and "Read in noise level 1 from file" in log
     assert "iteration 3 took" in log
-    assert np.array_equal(tiffio.read_stack(str(out / "denoise-iteration03")), full)
+    got = tiffio.read_stack(str(out / "denoise-iteration03"))
+    # a resumed run continues from the saved iterations and from the noise
+    # files, whose six significant digits (hdcommunication.cpp:1736-1746)
+    # round sigma: rebuild that continuation through the library
+    csv = lambda k: np.array([float(r.split(",")[1]) for r in
+                              (out / f"noise_vs_slice{k:02d}.csv").read_text().split()], np.float32)
+    s0c, s1c = csv(0), csv(1)
+    blend = (np.float32(0.5) * s0c + np.float32(0.5) * s1c).astype(np.float32)
+    g = IterativeNLM_GPU()
+    g.configure_device(vol.shape, DenoiseParameters(radius_searchspace=(3, 3, 3),
+                                                    radius_patchspace=(1, 1, 1)))
+    g.set_sigma(blend)
+    g.set_result(1, tiffio.read_stack(str(out / "denoise-iteration01")), vol)
+    g.set_result(2, tiffio.read_stack(str(out / "denoise-iteration02")))
+    g.Run_GaussianNoise(3)
+    want = g.get_result()
+    g.free_device()
+    assert np.array_equal(got, want)
+    assert np.max(np.abs(got - full)) < 1e-4  # and close to the uninterrupted run
 
 
 def test_cli_fp16_form(gpu, stack):
