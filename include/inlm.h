@@ -404,6 +404,54 @@ int inlm_tiff_read(const char* path, int first_slice, int last_slice, float* out
 int inlm_tiff_write_sequence(const float* image, const int shape[3], int z0, const char* dir,
                              const char* name, int as_16bit);
 
+/* ---------------- colour (2D RGB) path ----------------
+ * color_denoise::run_colorimage_denoising (Color/color_denoising.h:19-150) for
+ * one image: optional Anscombe transform 2 sqrt(v + 3/8) (colorspace.h:83-103),
+ * noise per channel (NoiseLevel::get_noiselevel_2D_RGB, noiselevel.cpp:96-191),
+ * optionally averaged over the channels, iterations of the three-channel
+ * filter (IterativeNLM_CPU::Run_GaussianNoise_3channels, iternlm_cpu.cpp:272;
+ * filterslice_3channels, :932-1075): one weight per search offset from the
+ * mean of the three channels' patch distances, or one per channel with
+ * independent_channels; the sigma of each later iteration is
+ * alpha * sigma + (1 - alpha) * (the estimate on the previous result). */
+typedef struct {
+    int stabilize_variance;    /* Anscombe transform (reference default 1; --nopoisson: 0) */
+    int independent_channels;  /* --independent */
+    int average_channelsigma;  /* one sigma for all channels (default 1; --noaverage: 0) */
+} inlm_color_params;
+
+/* Called after each iteration with that iteration's result as the reference
+ * saves it (inverse-transformed planes, host memory valid during the call).
+ * Passing a callback also reproduces what the reference does to its buffers
+ * around such a save under the transform (inverse, then forward again, in
+ * place), so results equal the reference run that saves every iteration
+ * (no --cleanup); pass NULL for the --cleanup run. */
+typedef void (*inlm_rgb_iteration_fn)(int iter, const float* r, const float* g, const float* b,
+                                      void* user);
+
+/* r, g, b: nx*ny host planes (values as read, 0..255 for 8-bit images);
+ * out_*: the final result, inverse-transformed, not clamped. p supplies the x
+ * and y search / patch radii, alpha, beta, maxiterations, the noise knobs
+ * (z-adaptive acts as global on one image; the reference driver passes
+ * n_samples = 2048), noise_seed and device_id; z radii and nslices are
+ * forced to 0 and 1. sigma_first / sigma_last (nullable, 3 floats) receive the
+ * initial estimate and the sigma of the last iteration. */
+int inlm_rgb_denoise(int nx, int ny, const inlm_params* p, const inlm_color_params* color,
+                     const float* r, const float* g, const float* b, float* out_r, float* out_g,
+                     float* out_b, inlm_rgb_iteration_fn on_iteration, void* user,
+                     float sigma_first[3], float sigma_last[3]);
+
+/* GetRGBTif_32bitChannels (hdcommunication.cpp:674): an 8- or 16-bit RGB(A)
+ * TIFF into three float planes (alpha ignored); shape receives {nx, ny}; with
+ * r = g = b = NULL only the shape is read. */
+int inlm_tiff_read_rgb(const char* file, int shape[2], float* r, float* g, float* b, uint64_t n_out);
+
+/* Save2DTifImage_RGB (hdcommunication.cpp:1487) of three float planes as
+ * dir/<name>.tif, 8-bit interleaved, each value as (uint8_t) min(255, v)
+ * (color_denoising.h:76-78), values below 0 as 0. */
+int inlm_tiff_write_rgb(const char* dir, const char* name, const float* r, const float* g,
+                        const float* b, int nx, int ny);
+
 #ifdef __cplusplus
 }
 #endif

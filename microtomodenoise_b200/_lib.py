@@ -41,8 +41,20 @@ EXPORTS = (
     "inlm_batch_describe", "inlm_stream_denoise", "inlm_set_result",
     "inlm_tiff_shape", "inlm_tiff_read", "inlm_tiff_write_sequence",
     "inlm_get_result_slices", "inlm_set_result_slices", "inlm_noise_patchstd_slab",
-    "inlm_noise_estimate_from_patchstd",
+    "inlm_noise_estimate_from_patchstd", "inlm_rgb_denoise", "inlm_tiff_read_rgb",
+    "inlm_tiff_write_rgb",
 )
+
+
+class InlmColorParams(C.Structure):
+    _fields_ = [
+        ("stabilize_variance", C.c_int),
+        ("independent_channels", C.c_int),
+        ("average_channelsigma", C.c_int),
+    ]
+
+
+RGB_ITERATION_FN = C.CFUNCTYPE(None, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
 
 
 class InlmParams(C.Structure):
@@ -149,6 +161,11 @@ def load(path: str = "") -> C.CDLL:
     L.inlm_noise_patchstd_slab.argtypes = [vp, C.POINTER(InlmParams), vp, C.c_int, C.c_int, C.c_int,
                                            vp, C.c_uint64]
     L.inlm_noise_estimate_from_patchstd.argtypes = [vp, C.POINTER(InlmParams), vp, C.c_uint64, vp]
+    L.inlm_rgb_denoise.argtypes = [C.c_int, C.c_int, C.POINTER(InlmParams), C.POINTER(InlmColorParams),
+                                   vp, vp, vp, vp, vp, vp, RGB_ITERATION_FN, vp, C.c_float * 3,
+                                   C.c_float * 3]
+    L.inlm_tiff_read_rgb.argtypes = [C.c_char_p, C.c_int * 2, vp, vp, vp, C.c_uint64]
+    L.inlm_tiff_write_rgb.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, C.c_int, C.c_int]
     for name in EXPORTS:
         if name not in ("inlm_last_error", "inlm_default_params"):
             getattr(L, name).restype = C.c_int

@@ -43,6 +43,8 @@ LIB_SOURCES = [
     "api_proposal.cu",
     "api_batch.cu",
     "api_stream.cu",
+    "color_kernels.cu",
+    "api_color.cu",
     "geometry.cpp",
     "sampling.cpp",
     "tiff_io.cpp",

@@ -7,7 +7,9 @@
 // Output: <outdir>/denoise-iterationNN/denoised####.tif per iteration (only
 // the last one, written to <outdir> itself, with --cleanup),
 // <outdir>/noise_vs_sliceNN.csv, and a run record appended to logfile.txt one
-// level above <outdir>. Not built: the CPU filter (-gpus 0) and --color.
+// level above <outdir>; with --color, <outdir>/<image>_denoised.tif per RGB
+// image (and <outdir>/denoise_iterations/<image>_iterNN.tif without
+// --cleanup). Not built: the CPU filter (-gpus 0).
 // Additions: -precision f32|f16, -seed N (noise sample draw), -slab N
 // (z-slab depth when the stack does not fit on the device).
 #include <sys/stat.h>
@@ -58,6 +60,76 @@ float* read_iteration(const string& dir, int first, int last, int shape[3]) {
         }
     }
     return out;
+}
+
+struct ColorSave {
+    string dir, name;
+    int nx, ny;
+    int status;
+};
+
+// saves one iteration of the colour job (color_denoising.h:73-84)
+void save_color_iteration(int iter, const float* r, const float* g, const float* b, void* user) {
+    ColorSave* s = static_cast<ColorSave*>(user);
+    const int rc = inlm_tiff_write_rgb(s->dir.c_str(), (s->name + "_iter" + hdcom::zfill_int2string(iter, 2)).c_str(),
+                                       r, g, b, s->nx, s->ny);
+    if (rc != INLM_OK) s->status = protocol::report(rc, "saving iteration");
+}
+
+// The colour driver (color_denoise::run_colorimage_denoising,
+// Color/color_denoising.h:19-150): every RGB image of the input, 2D, on the GPU.
+int run_color(const string& inpath, const string& outpath, protocol::DenoiseParameters& params) {
+    std::vector<string> files;
+    const bool single = inpath.size() >= 3 && (inpath.substr(inpath.size() - 3) == "tif" ||
+                                               (inpath.size() >= 4 && inpath.substr(inpath.size() - 4) == "tiff"));
+    if (single) {
+        files.push_back(inpath);
+    } else {
+        std::error_code ec;
+        for (const auto& e : std::filesystem::directory_iterator(inpath, ec)) {
+            const string f = e.path().string();
+            if ((f.size() > 4 && f.substr(f.size() - 4) == ".tif") || (f.size() > 5 && f.substr(f.size() - 5) == ".tiff"))
+                files.push_back(f);
+        }
+        std::sort(files.begin(), files.end());
+    }
+    // the colour driver's fixed settings (color_denoising.h:25-28)
+    params.radius_patchspace[2] = 0;
+    params.radius_searchspace[2] = 0;
+    params.nslices = 1;
+    params.noiselevel.n_samples = 2048;
+    const inlm_params q = protocol::to_inlm(params);
+    const inlm_color_params cp = {params.color.stabilize_variance ? 1 : 0, params.color.independent_channels ? 1 : 0,
+                                  params.color.average_channelsigma ? 1 : 0};
+    for (const string& file : files) {
+        cout << "--------------------------------------" << endl;
+        const size_t slash = file.rfind('/');
+        string name = file.substr(slash == string::npos ? 0 : slash + 1);
+        name = name.substr(0, name.rfind('.'));
+        cout << "image: " << name << endl;
+        int shape[2];
+        if (protocol::report(inlm_tiff_read_rgb(file.c_str(), shape, nullptr, nullptr, nullptr, 0), "reading image"))
+            return -1;
+        const size_t n = (size_t)shape[0] * shape[1];
+        std::vector<float> in(3 * n), out(3 * n);
+        if (protocol::report(inlm_tiff_read_rgb(file.c_str(), shape, in.data(), in.data() + n, in.data() + 2 * n, n),
+                             "reading image"))
+            return -1;
+        ColorSave save{outpath + "/denoise_iterations/", name, shape[0], shape[1], INLM_OK};
+        float s_first[3], s_last[3];
+        const int rc = inlm_rgb_denoise(shape[0], shape[1], &q, &cp, in.data(), in.data() + n, in.data() + 2 * n,
+                                        out.data(), out.data() + n, out.data() + 2 * n,
+                                        params.io.cleanup ? nullptr : save_color_iteration, &save, s_first, s_last);
+        if (protocol::report(rc, "rgb_denoise") || save.status) return -2;
+        cout << "initial noise level: " << s_first[0] << ", " << s_first[1] << ", " << s_first[2] << endl;
+        cout << "final noise level: " << s_last[0] << ", " << s_last[1] << ", " << s_last[2] << endl;
+        if (protocol::report(inlm_tiff_write_rgb(outpath.c_str(), (name + "_denoised").c_str(), out.data(),
+                                                 out.data() + n, out.data() + 2 * n, shape[0], shape[1]),
+                             "saving image"))
+            return -1;
+    }
+    cout << "--------------------------------------" << endl;
+    return 0;
 }
 
 }  // namespace
@@ -168,8 +240,12 @@ int main(int argc, char* argv[]) {
         cout << "Error! No tif-file in directory! Please provide a valid input with the -i argument" << endl;
         return -1;
     }
-    if (params.io.rgb || is_rgb) {
-        cout << "Error! The RGB denoiser (--color) is not part of this build" << endl;
+    if (params.io.rgb) {
+        cout << "Switching to RGB-Denoiser!" << endl;
+        return run_color(inpath, outpath, params);
+    }
+    if (is_rgb) {
+        cout << "Error! RGB input: run with --color" << endl;
         return -1;
     }
     if (params.gpu.n_gpus <= 0) {

@@ -365,6 +365,117 @@ int write_slice(const std::string& file, const float* image, uint32_t width, uin
     return INLM_OK;
 }
 
+// An RGB(A) page as three float planes: 8- or 16-bit unsigned samples,
+// interleaved (planar configuration 1); alpha is ignored
+// (GetRGBTif_32bitChannels, hdcommunication.cpp:674-795).
+int read_page_rgb(const std::string& file, const PageInfo& p, float* r, float* g, float* b) {
+    if (p.width == 0 || p.height == 0) return fail(INLM_ERR_IO, "%s: missing image size", file.c_str());
+    if (p.tiled || p.compression != 1)
+        return fail(INLM_ERR_UNSUPPORTED, "%s: tiled or compressed TIFF is not supported", file.c_str());
+    if ((p.samples != 3 && p.samples != 4) || p.planar != 1)
+        return fail(INLM_ERR_UNSUPPORTED, "%s: %u samples per pixel, planar %u (RGB or RGBA, interleaved)",
+                    file.c_str(), p.samples, p.planar);
+    if ((p.bits != 8 && p.bits != 16) || p.sample_format == 3 || p.sample_format == 2)
+        return fail(INLM_ERR_UNSUPPORTED, "%s: %u-bit RGB samples (8- or 16-bit unsigned only)", file.c_str(),
+                    p.bits);
+    if (p.strip_offsets.empty()) return fail(INLM_ERR_IO, "%s: no strip offsets", file.c_str());
+    File f(file, "rb");
+    if (!f.f) return fail(INLM_ERR_IO, "cannot open %s", file.c_str());
+    const uint32_t bps = p.bits / 8;
+    const uint64_t row_bytes = (uint64_t)p.width * p.samples * bps;
+    const uint32_t rps = p.rows_per_strip;
+    const uint64_t n_strips = (p.height + rps - 1) / rps;
+    if (p.strip_offsets.size() < n_strips) return fail(INLM_ERR_IO, "%s: too few strips", file.c_str());
+    std::vector<uint8_t> buf;
+    for (uint64_t s = 0; s < n_strips; s++) {
+        const uint32_t y0 = (uint32_t)(s * rps);
+        const uint32_t rows = std::min<uint32_t>(rps, p.height - y0);
+        const uint64_t need = rows * row_bytes;
+        if (s < p.strip_bytes.size() && p.strip_bytes[s] < need)
+            return fail(INLM_ERR_IO, "%s: short strip %llu", file.c_str(), (unsigned long long)s);
+        buf.resize(need);
+        if (!f.read_at(p.strip_offsets[s], buf.data(), need))
+            return fail(INLM_ERR_IO, "%s: truncated strip %llu", file.c_str(), (unsigned long long)s);
+        for (uint32_t yy = 0; yy < rows; yy++) {
+            const uint8_t* row = buf.data() + yy * row_bytes;
+            const uint64_t o = (uint64_t)(y0 + yy) * p.width;
+            for (uint32_t x = 0; x < p.width; x++) {
+                const uint8_t* px = row + (uint64_t)x * p.samples * bps;
+                float v[3];
+                for (int c = 0; c < 3; c++)
+                    v[c] = bps == 1 ? (float)px[c] : (float)load_sample<uint16_t>(px + 2 * c, p.big_endian);
+                r[o + x] = v[0];
+                g[o + x] = v[1];
+                b[o + x] = v[2];
+            }
+        }
+    }
+    return INLM_OK;
+}
+
+// 8-bit RGB slice (Save2DTifImage_RGB, hdcommunication.cpp:1487-1547):
+// interleaved, photometric RGB, strips of max(1, 2048 / width) rows.
+int write_rgb(const std::string& file, const uint8_t* rgb, uint32_t width, uint32_t height) {
+    uint32_t rps = 2048 / width;
+    if (rps == 0) rps = 1;
+    if (rps > height) rps = height;
+    const uint64_t row_bytes = 3ull * width;
+    const uint32_t n_strips = (height + rps - 1) / rps;
+    const uint64_t data_bytes = row_bytes * height;
+    if (8 + data_bytes + 4096 + 8ull * n_strips > 0xffffffffull)
+        return fail(INLM_ERR_UNSUPPORTED, "%s: image too large for classic TIFF", file.c_str());
+    const uint32_t data_off = 8;
+    uint32_t ifd_off = (uint32_t)(data_off + data_bytes);
+    ifd_off += ifd_off & 1;
+    const uint16_t n_tags = 11;
+    const uint32_t bits_off = ifd_off + 2 + n_tags * 12 + 4;  // BitsPerSample: 3 SHORTs
+    const uint32_t arrays_off = bits_off + 6 + 2;
+    std::vector<uint8_t> out;
+    out.reserve(arrays_off + 8ull * n_strips);
+    out.push_back('I');
+    out.push_back('I');
+    put16(out, 42);
+    put32(out, ifd_off);
+    out.insert(out.end(), rgb, rgb + data_bytes);
+    while (out.size() < ifd_off) out.push_back(0);
+    auto entry = [&](uint16_t tag, uint16_t type, uint32_t count, uint32_t value) {
+        put16(out, tag);
+        put16(out, type);
+        put32(out, count);
+        if (type == 3 && count == 1) {
+            put16(out, (uint16_t)value);
+            put16(out, 0);
+        } else {
+            put32(out, value);
+        }
+    };
+    const uint32_t off_array = arrays_off, cnt_array = arrays_off + 4 * n_strips;
+    put16(out, n_tags);
+    entry(256, 4, 1, width);
+    entry(257, 4, 1, height);
+    entry(258, 3, 3, bits_off);
+    entry(259, 3, 1, 1);
+    entry(262, 3, 1, 2);  // RGB
+    entry(273, 4, n_strips, n_strips == 1 ? data_off : off_array);
+    entry(277, 3, 1, 3);
+    entry(278, 4, 1, rps);
+    entry(279, 4, n_strips, n_strips == 1 ? (uint32_t)data_bytes : cnt_array);
+    entry(284, 3, 1, 1);
+    entry(339, 3, 1, 1);
+    put32(out, 0);
+    for (int c = 0; c < 3; c++) put16(out, 8);
+    put16(out, 0);  // pad to a word boundary
+    if (n_strips > 1) {
+        for (uint32_t s = 0; s < n_strips; s++) put32(out, (uint32_t)(data_off + (uint64_t)s * rps * row_bytes));
+        for (uint32_t s = 0; s < n_strips; s++) put32(out, (uint32_t)(std::min(rps, height - s * rps) * row_bytes));
+    }
+    File f(file, "wb");
+    if (!f.f) return fail(INLM_ERR_IO, "cannot write %s", file.c_str());
+    if (std::fwrite(out.data(), 1, out.size(), f.f) != out.size())
+        return fail(INLM_ERR_IO, "short write to %s", file.c_str());
+    return INLM_OK;
+}
+
 namespace {
 
 // What one path holds: slice files, or the pages of one file.
@@ -531,4 +642,42 @@ extern "C" int inlm_tiff_write_sequence(const float* image, const int shape[3], 
         return tiff::write_slice(base + id + ".tif", image + i * nslice, (uint32_t)shape[0],
                                  (uint32_t)shape[1], as_16bit != 0);
     });
+}
+
+extern "C" int inlm_tiff_read_rgb(const char* file, int shape[2], float* r, float* g, float* b,
+                                  uint64_t n_out) {
+    if (!file || !shape) return fail(INLM_ERR_ARG, "null argument");
+    std::vector<tiff::PageInfo> pages;
+    int rc = tiff::read_pages(file, pages);
+    if (rc) return rc;
+    const tiff::PageInfo& p = pages[0];
+    shape[0] = (int)p.width;
+    shape[1] = (int)p.height;
+    if (!r && !g && !b) return INLM_OK;  // size query
+    if (!r || !g || !b) return fail(INLM_ERR_ARG, "null channel plane");
+    if (n_out < (uint64_t)p.width * p.height)
+        return fail(INLM_ERR_ARG, "planes hold %llu values, %llu needed", (unsigned long long)n_out,
+                    (unsigned long long)p.width * p.height);
+    return tiff::read_page_rgb(file, p, r, g, b);
+}
+
+extern "C" int inlm_tiff_write_rgb(const char* dir, const char* name, const float* r, const float* g,
+                                   const float* b, int nx, int ny) {
+    if (!dir || !name || !r || !g || !b) return fail(INLM_ERR_ARG, "null argument");
+    if (nx <= 0 || ny <= 0) return fail(INLM_ERR_ARG, "bad image size %dx%d", nx, ny);
+    std::error_code ec;
+    std::filesystem::create_directories(dir, ec);
+    if (ec) return fail(INLM_ERR_IO, "cannot create %s: %s", dir, ec.message().c_str());
+    const uint64_t n = (uint64_t)nx * ny;
+    std::vector<uint8_t> rgb(3 * n);
+    const float* ch[3] = {r, g, b};
+    for (uint64_t i = 0; i < n; i++)
+        for (int c = 0; c < 3; c++) {
+            // (uint8_t) std::min(255.f, v) (color_denoising.h:76-78): NaN gives
+            // 255, values truncate toward zero; below zero gives 0
+            const float v = ch[c][i];
+            const float t = (v < 255.f) ? v : 255.f;
+            rgb[3 * i + c] = (t > 0.f) ? (uint8_t)t : 0;
+        }
+    return tiff::write_rgb(std::string(dir) + "/" + name + ".tif", rgb.data(), (uint32_t)nx, (uint32_t)ny);
 }

@@ -872,3 +872,105 @@ void ora_weight_mass_f64(const float* prev, const int shape[3], const ora_params
     }
     free(wt); free(soff); free(prevd); free(prev_pad);
 }
+
+/* ---- colour path ---- */
+
+void ora_filter_rgb(const float* const raw[3], const float* const prev[3], int nx, int ny,
+                    const ora_params* p2d, const float mult[3], int independent, float* const out[3]) {
+    /* IterativeNLM_CPU::filterslice_3channels (iternlm_cpu.cpp:932-1075) on one
+     * 2D image: p2d has z radii 0 and nslices 1; the weights are
+     * setup_distweight's (iternlm_prepare.cpp:204-262) for a one-slice stack. */
+    int pad[3];
+    ora_padding(p2d, pad);
+    const int shape[3] = {nx, ny, 1};
+    long long nxp = nx + 2 * pad[0], nyp = ny + 2 * pad[1];
+    static int sdx[ORA_MAXS], sdy[ORA_MAXS], sdz[ORA_MAXS];
+    int pdx[ORA_MAXP], pdy[ORA_MAXP], pdz[ORA_MAXP];
+    float w[ORA_MAXP];
+    int ns = ora_search_offsets(p2d, sdx, sdy, sdz, ORA_MAXS);
+    int np = ora_patch_taps(p2d, pdx, pdy, pdz, ORA_MAXP);
+    ora_distweight(p2d, 1, w, ORA_MAXP);
+    float* rp[3];
+    float* pp[3];
+    for (int c = 0; c < 3; c++) {
+        rp[c] = (float*)malloc(sizeof(float) * nxp * nyp);
+        pp[c] = (float*)malloc(sizeof(float) * nxp * nyp);
+        ora_pad_reflective(raw[c], shape, pad, rp[c]);
+        ora_pad_reflective(prev[c], shape, pad, pp[c]);
+    }
+#pragma omp parallel for schedule(dynamic)
+    for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+            long long i0 = (y + pad[1]) * nxp + (x + pad[0]);
+            float fv[3] = {0.f, 0.f, 0.f}, fw[3] = {0.f, 0.f, 0.f}, mw[3] = {0.f, 0.f, 0.f};
+            for (int s = 0; s < ns; s++) {
+                long long i1 = i0 + sdy[s] * nxp + sdx[s];
+                float d[3] = {0.f, 0.f, 0.f};
+                for (int q = 0; q < np; q++) {
+                    long long po = pdy[q] * nxp + pdx[q];
+                    for (int c = 0; c < 3; c++) {
+                        float t = pp[c][i1 + po] - pp[c][i0 + po];
+                        float sq = t * t;
+                        float term = sq * w[q];
+                        d[c] = d[c] + term;
+                    }
+                }
+                for (int c = 0; c < 3; c++) d[c] = d[c] * mult[c];
+                if (!independent) {
+                    float sum = d[0] + d[1];
+                    sum = sum + d[2];
+                    float ds = sum / 3.f;
+                    float wt = (ds > PADE_CUTOFF) ? pade_f32(ds) : 0.0f;
+                    for (int c = 0; c < 3; c++) {
+                        float prod = wt * rp[c][i1];
+                        fv[c] = fv[c] + prod;
+                    }
+                    fw[0] = fw[0] + wt;
+                    if (wt > mw[0]) mw[0] = wt;
+                } else {
+                    for (int c = 0; c < 3; c++) {
+                        float wt = (d[c] > PADE_CUTOFF) ? pade_f32(d[c]) : 0.0f;
+                        float prod = wt * rp[c][i1];
+                        fv[c] = fv[c] + prod;
+                        fw[c] = fw[c] + wt;
+                        if (wt > mw[c]) mw[c] = wt;
+                    }
+                }
+            }
+            long long o = (long long)y * nx + x;
+            for (int c = 0; c < 3; c++) {
+                float r0 = rp[c][i0];
+                if (!independent) {
+                    if (mw[0] > 0.0f) {
+                        float prod = mw[0] * r0;
+                        float num = fv[c] + prod;
+                        float den = fw[0] + mw[0];
+                        out[c][o] = num / den;
+                    } else {
+                        out[c][o] = r0;
+                    }
+                } else {
+                    out[c][o] = (mw[c] > 0.0f) ? fv[c] / fw[c] : r0;
+                }
+            }
+        }
+    for (int c = 0; c < 3; c++) {
+        free(rp[c]);
+        free(pp[c]);
+    }
+}
+
+void ora_anscombe(float* v, int64_t n, int inverse) {
+    /* colorspace.h:83-125: 2 sqrt(v + 3/8), and (v/2)^2 - 3/8 */
+    for (int64_t i = 0; i < n; i++) {
+        float r = v[i];
+        if (inverse) {
+            float h = r / 2.f;
+            float sq = h * h;
+            v[i] = sq - 3.f / 8.f;
+        } else {
+            float s = sqrtf(r + 3.f / 8.f);
+            v[i] = 2.f * s;
+        }
+    }
+}

@@ -140,6 +140,11 @@ void ora_noise_from_patchstd(const float* patchstd, const int64_t* samples, int6
                              const int shape[3], int mode, int zwindow, float stds_from_mean,
                              int f64acc, float* sigma);
 
+/* colour path: the three-channel 2D filter and the Anscombe transforms */
+void ora_filter_rgb(const float* const raw[3], const float* const prev[3], int nx, int ny,
+                    const ora_params* p2d, const float mult[3], int independent, float* const out[3]);
+void ora_anscombe(float* v, int64_t n, int inverse);
+
 #ifdef __cplusplus
 }
 #endif

@@ -109,6 +109,9 @@ class Port:
         L.ora_fill_empty_slices.argtypes = [_f32p, _f32p, C.c_int]
         L.ora_noise_from_patchstd.argtypes = [_f32p, _i64p, C.c_int64, C.c_int * 3, C.c_int,
                                               C.c_int, C.c_float, C.c_int, _f32p]
+        L.ora_filter_rgb.argtypes = [C.c_void_p * 3, C.c_void_p * 3, C.c_int, C.c_int,
+                                     C.POINTER(_CParams), C.c_float * 3, C.c_int, C.c_void_p * 3]
+        L.ora_anscombe.argtypes = [_f32p, C.c_int64, C.c_int]
 
     # ---- geometry ----
     def padding(self, p: FilterParams):
@@ -220,6 +223,25 @@ class Port:
                                  sig.shape[0], out.ravel())
         return out
 
+    # ---- colour path ----
+    def filter_rgb(self, raw3, prev3, p: FilterParams, mult3, independent: bool = False):
+        """One three-channel 2D iteration (filterslice_3channels); raw3 / prev3:
+        three (ny, nx) planes; p with z radii 0 and nslices 1."""
+        raw3 = [np.ascontiguousarray(a, np.float32) for a in raw3]
+        prev3 = [np.ascontiguousarray(a, np.float32) for a in prev3]
+        ny, nx = raw3[0].shape
+        out = [np.empty((ny, nx), np.float32) for _ in range(3)]
+        ptr = lambda arrs: (C.c_void_p * 3)(*[a.ctypes.data for a in arrs])
+        self.lib.ora_filter_rgb(ptr(raw3), ptr(prev3), nx, ny, C.byref(_cparams(p)),
+                                (C.c_float * 3)(*[float(m) for m in mult3]), int(bool(independent)),
+                                ptr(out))
+        return out
+
+    def anscombe(self, v: np.ndarray, inverse: bool = False) -> np.ndarray:
+        out = np.ascontiguousarray(v, np.float32).copy()
+        self.lib.ora_anscombe(out.ravel(), out.size, int(bool(inverse)))
+        return out
+
     # ---- noise ----
     def rand_sequence(self, seed: int, n: int) -> np.ndarray:
         st = C.create_string_buffer(256)
@@ -290,6 +312,25 @@ class _RefNoiseParams(C.Structure):
     ]
 
 
+class _RefRgbParams(C.Structure):
+    _fields_ = [
+        ("alpha", C.c_float),
+        ("maxiterations", C.c_int),
+        ("mode", C.c_char_p),
+        ("sigma", C.c_float * 2),
+        ("n_samples", C.c_ulonglong),
+        ("patchsize", C.c_int),
+        ("stds_from_mean", C.c_float),
+        ("continuous_estimate", C.c_int),
+        ("circular_mask_diameter", C.c_int),
+        ("seed", C.c_uint),
+        ("stabilize_variance", C.c_int),
+        ("independent_channels", C.c_int),
+        ("average_channelsigma", C.c_int),
+        ("keep_iterations", C.c_int),
+    ]
+
+
 def reference_available() -> bool:
     return os.path.exists(REF_SO)
 
@@ -319,6 +360,10 @@ class Reference:
         L.ref_noise_destroy.argtypes = [C.c_void_p]
         L.ref_patchstd.argtypes = [_f32p, C.c_int * 3, _i64p, C.c_longlong, C.c_int, _f32p]
         L.ref_create2clusters.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p]
+        L.ref_rgb_job.restype = C.c_int
+        L.ref_rgb_job.argtypes = [_f32p, _f32p, _f32p, C.c_int, C.c_int, C.POINTER(_RefParams),
+                                  C.POINTER(_RefRgbParams), _f32p, _f32p, _f32p, C.c_void_p,
+                                  C.c_float * 3, C.c_float * 3]
 
     def denoise(self, raw: np.ndarray, p: FilterParams, sigmas: np.ndarray, n_threads: int = 0,
                 all_iters: bool = False):
@@ -368,6 +413,27 @@ class Reference:
         out = np.zeros(2, np.float32)
         self.lib.ref_create2clusters(values, len(values), first, last, out)
         return float(out[0]), float(out[1])
+
+    def rgb_job(self, rgb, p: FilterParams, alpha=0.5, maxiterations=4, mode="global",
+                sigma=(0.0, 0.0), n_samples=2048, patchsize=15, stds_from_mean=1.0,
+                continuous=False, mask=0, seed=0, stabilize=True, independent=False,
+                average=True, keep_iterations=True):
+        """The colour driver's job on one image (color_denoising.h:19-150) with
+        the reference's own transforms, noise estimate and three-channel
+        filter. rgb: three (ny, nx) planes. Returns (final planes, per-iteration
+        saved planes or None, sigma_first, sigma_last)."""
+        r, g, b = (np.ascontiguousarray(a, np.float32) for a in rgb)
+        ny, nx = r.shape
+        cp = _RefRgbParams(alpha, maxiterations, mode.encode(), (C.c_float * 2)(*sigma), n_samples,
+                           patchsize, stds_from_mean, int(continuous), mask, seed, int(stabilize),
+                           int(independent), int(average), int(keep_iterations))
+        rp = _RefParams(*[getattr(_cparams(p), f) for f, _ in _CParams._fields_])
+        out = [np.empty((ny, nx), np.float32) for _ in range(3)]
+        its = np.empty((maxiterations, 3, ny, nx), np.float32) if keep_iterations else None
+        s0, s1 = (C.c_float * 3)(), (C.c_float * 3)()
+        self.lib.ref_rgb_job(r, g, b, nx, ny, C.byref(rp), C.byref(cp), out[0], out[1], out[2],
+                             its.ctypes.data if its is not None else None, s0, s1)
+        return out, its, np.array(s0[:], np.float32), np.array(s1[:], np.float32)
 
 
 class _RefNoiseSession:

@@ -39,6 +39,7 @@
 #include "Denoiser/iternlm_prepare.h"
 #include "Noise/noiselevel.h"
 #undef private
+#include "Color/colorspace.h"
 
 extern "C" {
 
@@ -235,6 +236,115 @@ void ref_create2clusters(const float* values, int n, int first, int last, float*
     std::pair<float, float> r = nl.create2clusters(const_cast<float*>(values), n, first, last);
     mean_std[0] = r.first;
     mean_std[1] = r.second;
+}
+
+// ---- colour path (Color/color_denoising.h:19-150) ----
+
+struct ref_rgb_params {
+    float alpha;
+    int maxiterations;
+    const char* mode;
+    float sigma[2];
+    unsigned long long n_samples;
+    int patchsize;
+    float stds_from_mean;
+    int continuous_estimate;
+    int circular_mask_diameter;
+    unsigned int seed;
+    int stabilize_variance;
+    int independent_channels;
+    int average_channelsigma;
+    int keep_iterations;  // the run without --cleanup: every iteration is saved
+};
+
+// The colour driver's schedule for one image with the reference's own
+// pieces (colorspace.h transforms, NoiseLevel::get_noiselevel_2D_RGB,
+// IterativeNLM_CPU::Run_GaussianNoise_3channels); file IO left out. With
+// keep_iterations, iter_out (nullable, maxiterations x 3 x nx*ny) receives
+// each iteration's planes as they would be saved (before the uint8 cast),
+// and the buffers go through the same inverse/forward transform the saves
+// apply. out_*: the final planes before the uint8 cast.
+int ref_rgb_job(const float* r, const float* g, const float* b, int nx, int ny, const ref_params* rp,
+                const ref_rgb_params* cp, float* out_r, float* out_g, float* out_b, float* iter_out,
+                float* sigma_first, float* sigma_last) {
+    protocol::DenoiseParameters params;
+    fill_params(&params, rp);
+    params.radius_patchspace[2] = 0;
+    params.radius_searchspace[2] = 0;
+    params.nslices = 1;
+    params.alpha = cp->alpha;
+    params.maxiterations = cp->maxiterations;
+    params.noiselevel.mode = cp->mode;
+    params.noiselevel.sigma[0] = cp->sigma[0];
+    params.noiselevel.sigma[1] = cp->sigma[1];
+    params.noiselevel.n_samples = cp->n_samples;
+    params.noiselevel.patchsize = cp->patchsize;
+    params.noiselevel.stds_from_mean = cp->stds_from_mean;
+    params.noiselevel.continuous_estimate = cp->continuous_estimate != 0;
+    params.noiselevel.circular_mask_diameter = cp->circular_mask_diameter;
+    params.color.stabilize_variance = cp->stabilize_variance != 0;
+    params.color.independent_channels = cp->independent_channels != 0;
+    params.color.average_channelsigma = cp->average_channelsigma != 0;
+    params.io.cleanup = cp->keep_iterations == 0;
+
+    int shape[3] = {nx, ny, 1};
+    const long long n = (long long)nx * ny;
+    float* R = (float*)malloc(n * 4);
+    float* G = (float*)malloc(n * 4);
+    float* B = (float*)malloc(n * 4);
+    std::memcpy(R, r, n * 4);
+    std::memcpy(G, g, n * 4);
+    std::memcpy(B, b, n * 4);
+    std::streambuf* saved_buf = std::cout.rdbuf();
+    std::ostringstream sink;
+    std::cout.rdbuf(sink.rdbuf());
+
+    if (params.color.stabilize_variance) color::anscombe_transform(R, G, B, shape);
+    denoise::IterativeNLM_CPU nlm;
+    std::vector<float*> raw = {R, G, B};
+    std::vector<float*> res;
+    noise::NoiseLevel noise(params.noiselevel.n_samples, params.noiselevel.patchsize, shape);
+    srand(cp->seed);
+    int saved_threads = omp_get_max_threads();
+    omp_set_num_threads(1);  // the first estimate draws the samples
+    std::vector<float> s0 = noise.get_noiselevel_2D_RGB(R, G, B, &params);
+    omp_set_num_threads(saved_threads);
+    auto average = [&](std::vector<float>& s) {
+        if (params.color.average_channelsigma) s[0] = s[1] = s[2] = (s[0] + s[1] + s[2]) / 3.f;
+    };
+    auto blend = [&](const std::vector<float>& s1) {
+        for (int c = 0; c < 3; c++) s0[c] = params.alpha * s0[c] + (1.f - params.alpha) * s1[c];
+    };
+    average(s0);
+    if (sigma_first)
+        for (int c = 0; c < 3; c++) sigma_first[c] = s0[c];
+    auto save = [&](int iter) {
+        if (params.io.cleanup) return;
+        if (params.color.stabilize_variance) color::inverse_anscombe_transform(res[0], res[1], res[2], shape);
+        if (iter_out)
+            for (int c = 0; c < 3; c++)
+                std::memcpy(iter_out + ((long long)(iter - 1) * 3 + c) * n, res[c], n * 4);
+        if (params.color.stabilize_variance) color::anscombe_transform(res[0], res[1], res[2], shape);
+    };
+    for (int iter = 1; iter <= params.maxiterations; iter++) {
+        nlm.Run_GaussianNoise_3channels(iter, raw, res, s0, shape, &params);
+        save(iter);
+        if ((iter == 1 && params.maxiterations > 1) || (iter > 1 && params.noiselevel.continuous_estimate)) {
+            std::vector<float> s1 = noise.get_noiselevel_2D_RGB(res[0], res[1], res[2], &params);
+            average(s1);
+            blend(s1);
+        }
+    }
+    if (sigma_last)
+        for (int c = 0; c < 3; c++) sigma_last[c] = s0[c];
+    if (params.color.stabilize_variance) color::inverse_anscombe_transform(res[0], res[1], res[2], shape);
+    std::cout.rdbuf(saved_buf);
+    std::memcpy(out_r, res[0], n * 4);
+    std::memcpy(out_g, res[1], n * 4);
+    std::memcpy(out_b, res[2], n * 4);
+    for (float* q : raw) free(q);
+    for (float* q : res) free(q);
+    return 0;
 }
 
 }  // extern "C"

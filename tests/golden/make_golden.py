@@ -17,6 +17,11 @@ Fixtures:
   config1.json       the 128x128x64 spheres workload (p1, s5, 4 iterations,
                      global noise): reference sigma0/sigma1, sha256 of every
                      iterate and 256 sampled voxels per iterate.
+  rgb_small.npz      the colour path (color_denoising.h) on a seeded 48x64 RGB
+                     image: final and per-iteration planes and both sigma
+                     triples for the cases in RGB_CASES.
+
+    python tests/golden/make_golden.py rgb     # only rgb_small.npz
 """
 from __future__ import annotations
 
@@ -60,7 +65,52 @@ def config1_volume() -> np.ndarray:
                                 noise_blur=1.0, seed=0)
 
 
+def rgb_image() -> list:
+    """A seeded 8-bit RGB test image: smooth colour gradients, a few disks and
+    Poisson counts, as three float planes."""
+    rng = np.random.default_rng(5)
+    ny, nx = 48, 64
+    y, x = np.mgrid[0:ny, 0:nx].astype(np.float32)
+    base = [40 + 2.0 * x, 60 + 3.0 * y, 120 + 40 * np.sin(x / 9.0) * np.cos(y / 7.0)]
+    for cy, cx, r, v in ((14, 18, 7, 200.0), (30, 44, 9, 30.0), (36, 12, 5, 150.0)):
+        m = (y - cy) ** 2 + (x - cx) ** 2 <= r * r
+        for c in range(3):
+            base[c] = np.where(m, v - 40 * c, base[c])
+    return [np.clip(rng.poisson(np.clip(b, 1, 250)), 0, 255).astype(np.float32) for b in base]
+
+
+# name: (search xy, patch xy, iterations, mode, sigma, independent, stabilize, average,
+#        continuous, keep_iterations)
+RGB_CASES = {
+    "manual_joint": ((4, 4), (1, 1), 3, "manual", (1.2, 0.9), False, True, True, False, True),
+    "manual_indep_raw": ((3, 5), (2, 1), 2, "manual", (18.0, 12.0), True, False, True, False, False),
+    "global_joint": ((5, 5), (1, 1), 3, "global", (0.0, 0.0), False, True, True, False, True),
+    "global_noavg_cont": ((4, 4), (2, 2), 4, "global", (0.0, 0.0), False, True, False, True, False),
+    "semimanual": ((4, 4), (1, 1), 3, "semimanual", (1.0, 0.0), False, True, True, False, True),
+}
+
+
+def make_rgb(ref) -> None:
+    img = rgb_image()
+    out = {"image": np.stack(img)}
+    for name, (sr, pr, iters, mode, sig, indep, stab, avg, cont, keep) in RGB_CASES.items():
+        p = FilterParams(search_radius=(sr[0], sr[1], 0), patch_radius=(pr[0], pr[1], 0), nslices=1)
+        fin, its, s_first, s_last = ref.rgb_job(img, p, maxiterations=iters, mode=mode, sigma=sig,
+                                                seed=3, stabilize=stab, independent=indep,
+                                                average=avg, continuous=cont, keep_iterations=keep)
+        out[name + "/final"] = np.stack(fin)
+        if its is not None:
+            out[name + "/iterations"] = its
+        out[name + "/sigma_first"] = s_first
+        out[name + "/sigma_last"] = s_last
+    np.savez_compressed(os.path.join(HERE, "rgb_small.npz"), **out)
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "rgb":
+        make_rgb(Reference())
+        print("rgb_small.npz written to", HERE)
+        return
     ref = Reference()
     # ---- filter ----
     raw = small_filter_volume()
@@ -134,6 +184,7 @@ def main():
     }
     with open(os.path.join(HERE, "config1.json"), "w") as f:
         json.dump(cfg, f, indent=1)
+    make_rgb(ref)
     print("golden fixtures written to", HERE)
 
 
