@@ -19,7 +19,9 @@ exceed L2 (126 MB) between steps.
 Multi-GPU (torchrun): each rank denoises its own volume (independent jobs,
 weak scaling, no data-path collective); time = max over ranks.
 
-``forms`` (rank 0, one GPU): the same whole job in the FP16-storage form and
+``forms`` (rank 0, one GPU): the same whole job in the fused FP32 form
+(fused multiply-adds, within 1e-4 relative of the reference except at
+weights that cross the Pade cutoff), the FP16-storage form and
 in the learned-proposal + FP16 form (k = 104 of 514 offsets per 8^3 tile
 without fallback, the fastest k measured within 0.1 dB of the FP64 oracle's
 PSNR against the clean phantom; and k = 256 with fallback to full
@@ -265,7 +267,7 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
     from oracle.oracle import FilterParams, Port
 
     net = ProposalNet.load(default_weights(PR, SR), device=local)
-    forms = [("f32", "f32", None), ("fp16", "f16", None),
+    forms = [("f32", "f32", None), ("f32_fused", "f32_fma", None), ("fp16", "f16", None),
              ("learned_fp16", "f16", (104, 0.0)), ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
     raw_dev = torch.from_numpy(vol).cuda()
     out_dev = torch.empty_like(raw_dev)
@@ -443,6 +445,10 @@ def run_large_workload(args):
                      "search_radius": 7, "offsets": 1326, "iterations": ITERS}
     forms = [("f32", "f32", None), ("fp16", "f16", None), ("learned_fp16_k256_mass095", "f16", (256, 0.95)),
              ("learned_fp16_k256", "f16", (256, 0.0))]
+    if args.k_list:
+        # a sweep of k (no fallback) beside plain FP32 and FP16 full search
+        forms = [("f32", "f32", None), ("fp16", "f16", None)] + [
+            (f"learned_fp16_k{k}", "f16", (k, 0.0)) for k in (int(v) for v in args.k_list.split(","))]
     if args.workload == "stream2048":
         forms = [("f32", "f32", None), ("learned_fp16_k256", "f16", (256, 0.0))]
     ref_psnr = None
@@ -512,6 +518,8 @@ def main():
                     help="grain512: the headline bench line; the others: one-step "
                          "measurements of the large workloads (see run_large_workload)")
     ap.add_argument("--stream-depth", type=int, default=128)
+    ap.add_argument("--k-list", default="",
+                    help="learned1024: comma-separated k values to sweep (no fallback)")
     ap.add_argument("--shape", default="512,512,512",
                     help="nz,ny,nx of the volume (smaller shapes only for profiling runs)")
     args = ap.parse_args()

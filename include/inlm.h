@@ -57,6 +57,9 @@ extern "C" {
 #define INLM_PRECISION_F32 0   /* FP32, bit-identical to the reference CPU filter */
 #define INLM_PRECISION_F16 1   /* FP16 volumes and squared-difference planes, FP32 accumulation */
 #define INLM_PRECISION_F16_DF32 2 /* FP16 volumes, FP32 squared-difference planes */
+#define INLM_PRECISION_F32_FMA 3  /* FP32 volumes, patch taps and Pade fused (FFMA), fast
+                                     division: within a stated tolerance of the reference,
+                                     not bit-identical */
 
 /* patch-weight table */
 #define INLM_WEIGHTS_CPU 0        /* the table the reference CPU filter applies (default) */

@@ -22,7 +22,7 @@ ERRORS = {
     -8: "INLM_ERR_IO",
 }
 NOISE_MODES = {"z-adaptive": 0, "auto": 0, "global": 1, "manual": 2, "semimanual": 3}
-PRECISIONS = {"f32": 0, "f16": 1, "f16_df32": 2}
+PRECISIONS = {"f32": 0, "f16": 1, "f16_df32": 2, "f32_fma": 3}
 
 # Every entry point include/inlm.h declares.
 EXPORTS = (

@@ -509,6 +509,8 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
             order[3 * t + 2] != g.taps[t].z)
             return INLM_OK;
     if (!((tz == 8) || (tz == 4 && !raw_smem))) return INLM_OK;
+    const bool fused = d->p.precision == INLM_PRECISION_F32_FMA;
+    if (fused && tz != 8) return INLM_OK;  // the fused form is instantiated at CTA depth 8
 
     TileArgs a{};
     a.nx = d->shape[0];
@@ -535,7 +537,7 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     a.rplane = raw_plane_pitch(a.rbx + 1, a.rby);
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
-    TileConfig tc{pr[0], pr[1], pr[2], tz, raw_smem, 0};
+    TileConfig tc{pr[0], pr[1], pr[2], tz, raw_smem, 0, fused};
     size_t sm = tile_smem_bytes(tc, a);
     if (sm == 0 || sm > (size_t)smem_max) return INLM_OK;
     tc.smem_bytes = sm;
@@ -693,7 +695,7 @@ extern "C" int inlm_denoiser_create(const int shape[3], const inlm_params* p, in
     }
     if (p->nslices < 1) return fail(INLM_ERR_ARG, "nslices must be >= 1");
     const bool f16 = p->precision == INLM_PRECISION_F16 || p->precision == INLM_PRECISION_F16_DF32;
-    if (p->precision != INLM_PRECISION_F32 && !f16)
+    if (p->precision != INLM_PRECISION_F32 && p->precision != INLM_PRECISION_F32_FMA && !f16)
         return fail(INLM_ERR_ARG, "unknown precision %d", p->precision);
 
     inlm_denoiser* d = new inlm_denoiser();
@@ -1162,8 +1164,9 @@ extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
     }
     else if (d->use_tile)
         snprintf(buf, len,
-                 "nlm_tile_f32<%d,%d,%d> tz=%d raw_%s smem=%zu S=%zu P=%zu weights=%s pad=%d,%d,%d",
-                 d->tcfg.rx, d->tcfg.ry, d->tcfg.rz, d->tcfg.tz, d->tcfg.raw_smem ? "smem" : "global",
+                 "nlm_tile_f32%s<%d,%d,%d> tz=%d raw_%s smem=%zu S=%zu P=%zu weights=%s pad=%d,%d,%d",
+                 d->tcfg.fused ? "_fused" : "", d->tcfg.rx, d->tcfg.ry, d->tcfg.rz, d->tcfg.tz,
+                 d->tcfg.raw_smem ? "smem" : "global",
                  d->tcfg.smem_bytes, g.search.size(), g.taps.size(),
                  g.specialised && d->p.weight_table == INLM_WEIGHTS_CPU ? "cpu-table" : "distweight",
                  g.pad[0], g.pad[1], g.pad[2]);

@@ -58,6 +58,12 @@ __device__ __forceinline__ f32x2 mul2_to_mul(f32x2 a, f32x2 b) {
     asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
     return d;
 }
+// Fused pair a*b + c, one rounding per lane (FFMA2): the fused FP32 form only.
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
 __device__ __forceinline__ f32x2 pack2(float lo, float hi) {
     f32x2 d;
     asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
@@ -93,7 +99,7 @@ __device__ __forceinline__ void load_window(const float* __restrict__ rowp, floa
 // Patch sums of NO offsets at once (D planes D0 + o*DSZ): the same operations
 // as one offset's patch sum on each, interleaved row by row so a thread has 4*NO
 // independent chains in flight.
-template <int RX, int RY, int RZ, int TZ, int NO, int RI>
+template <int RX, int RY, int RZ, int TZ, int NO, int RI, bool FUSED = false>
 __device__ __forceinline__ void accumulate_rows_n(const float* __restrict__ D0, int dsz, int rowoff,
                                                   f32x2 (&d)[NO][kVoxPerThread / 2],
                                                   const TileArgs& a) {
@@ -118,10 +124,20 @@ __device__ __forceinline__ void accumulate_rows_n(const float* __restrict__ D0, 
             for (int p = 0; p < kVoxPerThread / 2; p++) {
                 const int i = RX + 2 * p + xp;
 #pragma unroll
-                for (int o = 0; o < NO; o++) d[o][p] = add2(d[o][p], mul_pair(win[o][i], win[o][i + 1], w));
+                for (int o = 0; o < NO; o++) {
+                    if (!FUSED) {
+                        d[o][p] = add2(d[o][p], mul_pair(win[o][i], win[o][i + 1], w));
+                    } else if ((i & 1) == 0) {
+                        // an even window index is an aligned register pair
+                        d[o][p] = fma2(pack2(win[o][i], win[o][i + 1]), splat2(w), d[o][p]);
+                    } else {
+                        const float2 c = unpack2(d[o][p]);
+                        d[o][p] = pack2(__fmaf_rn(win[o][i], w, c.x), __fmaf_rn(win[o][i + 1], w, c.y));
+                    }
+                }
             }
         }
-        accumulate_rows_n<RX, RY, RZ, TZ, NO, RI + 1>(D0, dsz, rowoff, d, a);
+        accumulate_rows_n<RX, RY, RZ, TZ, NO, RI + 1, FUSED>(D0, dsz, rowoff, d, a);
     }
 }
 
@@ -130,7 +146,7 @@ __device__ __forceinline__ void accumulate_rows_n(const float* __restrict__ D0, 
 // three gave 0.3% more for 21 KB more shared memory at patch radius 2.
 constexpr int kOffGroup = 2;
 
-template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED = false>
 __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const TileArgs& a, int bx,
                                               int by, int bz, unsigned char* smem,
                                               uint32_t parity) {
@@ -236,7 +252,7 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
 #pragma unroll
     for (int r = 0; r < kVoxPerThread; r++) wmax[r] = 0.0f;
 
-    const f32x2 c12 = splat2(12.f), c120 = splat2(120.f);
+    const f32x2 c12 = splat2(12.f), c120 = splat2(120.f), c60 = splat2(60.f), cm60 = splat2(-60.f);
 
     // phase A for one offset: D = (prev(.+s) - prev(.))^2 over tile + patch halo
     auto phase_a = [&](float* Dw, int dlx) {
@@ -258,6 +274,24 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
             } else {
                 rsv = make_float2(__ldg(&a.raw_pad[gbase + dly + 2 * p]),
                                   __ldg(&a.raw_pad[gbase + dly + 2 * p + 1]));
+            }
+            if (FUSED) {
+                // the same Pade[3/3] in Horner form with fused pairs and a fast
+                // division: 120 + x(60 + x(12 + x)) over 120 + x(-60 + x(12 - x))
+                const f32x2 x = mul2_to_mul(dist[p], m2);
+                const float2 xs = unpack2(x);
+                const f32x2 num = fma2(x, fma2(x, add2(c12, x), c60), c120);
+                const f32x2 den = fma2(x, fma2(x, sub2(c12, x), cm60), c120);
+                const float2 nu = unpack2(num), de = unpack2(den);
+                const float q0 = __fdividef(nu.x, de.x), q1 = __fdividef(nu.y, de.y);
+                const float w0 = (xs.x > -3.56648f) ? q0 : 0.0f;
+                const float w1 = (xs.y > -3.56648f) ? q1 : 0.0f;
+                const f32x2 wp = pack2(w0, w1);
+                acc[p] = fma2(wp, pack2(rsv.x, rsv.y), acc[p]);
+                wsum[p] = add2(wsum[p], wp);
+                wmax[2 * p] = fmaxf(wmax[2 * p], w0);
+                wmax[2 * p + 1] = fmaxf(wmax[2 * p + 1], w1);
+                continue;
             }
             // Pade[3/3] (120 + 60x + 12x*x + x*x*x) / (120 - 60x + 12x*x - x*x*x):
             // products that feed the sums are scalar, the sums are paired
@@ -308,7 +342,7 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
                 for (int p = 0; p < NP; p++) d[o][p] = mul_pair(win[RX + 2 * p], win[RX + 2 * p + 1], w0);
             }
         }
-        accumulate_rows_n<RX, RY, RZ, TZ, NO, 0>(D0, DSZ, rowoff, d, a);
+        accumulate_rows_n<RX, RY, RZ, TZ, NO, 0, FUSED>(D0, DSZ, rowoff, d, a);
 #pragma unroll
         for (int o = 0; o < NO; o++)
             if (s + o < a.S) accumulate(d[o], dl[o].y);
@@ -341,7 +375,7 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
     return true;
 }
 
-template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED>
 __global__ void __launch_bounds__(32 * TZ, 1)
     nlm_tile_f32_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -351,7 +385,8 @@ __global__ void __launch_bounds__(32 * TZ, 1)
         fence_mbar_init();
     }
     __syncthreads();
-    tile_f32_body<RX, RY, RZ, TZ, RAW_SMEM>(&tm_prev, a, blockIdx.x, blockIdx.y, blockIdx.z, smem, 0);
+    tile_f32_body<RX, RY, RZ, TZ, RAW_SMEM, FUSED>(&tm_prev, a, blockIdx.x, blockIdx.y, blockIdx.z, smem,
+                                                  0);
 }
 
 // Persistent batch kernel: CTAs take (volume, tile) items from a counter
@@ -495,11 +530,11 @@ static size_t smem_bytes_for(const TileArgs& a) {
     return 128 + 4 * (pb + rb + kOffGroup * d);
 }
 
-template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM>
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED = false>
 static cudaError_t launch_inst(const CUtensorMap* tmp, const CUtensorMap* tmr, const TileArgs& a,
                                int tiles_z, size_t smem, cudaStream_t st) {
     (void)tmr;
-    auto kern = nlm_tile_f32_kernel<RX, RY, RZ, TZ, RAW_SMEM>;
+    auto kern = nlm_tile_f32_kernel<RX, RY, RZ, TZ, RAW_SMEM, FUSED>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
@@ -578,6 +613,11 @@ cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,
                                cudaStream_t st) {
 #define X(A, B, C)                                                                             \
     if (c.rx == A && c.ry == B && c.rz == C) {                                                 \
+        if (c.fused && c.tz == 8 && c.raw_smem)                                                \
+            return launch_inst<A, B, C, 8, true, true>(tm_prev, tm_raw, a, tiles_z, c.smem_bytes, st); \
+        if (c.fused && c.tz == 8 && !c.raw_smem)                                               \
+            return launch_inst<A, B, C, 8, false, true>(tm_prev, tm_raw, a, tiles_z, c.smem_bytes, st); \
+        if (c.fused) return cudaErrorInvalidConfiguration;                                     \
         if (c.tz == 8 && c.raw_smem)                                                           \
             return launch_inst<A, B, C, 8, true>(tm_prev, tm_raw, a, tiles_z, c.smem_bytes, st);  \
         if (c.tz == 8 && !c.raw_smem)                                                          \

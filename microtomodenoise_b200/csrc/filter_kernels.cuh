@@ -54,6 +54,7 @@ struct TileConfig {
     int tz;           // CTA depth (z-planes = warps)
     bool raw_smem;    // raw box staged in shared memory
     size_t smem_bytes;
+    bool fused = false;  // the fused FP32 form (FFMA taps, Horner Pade, fast division); tz 8 only
 };
 
 // Returns false when no tiled instantiation exists for the patch shape.

@@ -174,3 +174,31 @@ def test_512_cube_p2s5_sampled_voxels(gpu, port):
     # size-independent properties on the whole output
     assert np.isfinite(got).all()
     assert got.min() >= vol.min() - 1e-6 and got.max() <= vol.max() + 1e-6  # convex combination
+
+
+@pytest.mark.parametrize("pr,sr,shape", [((1, 1, 1), (3, 3, 3), (24, 40, 56)),
+                                         ((2, 2, 2), (3, 3, 3), (20, 33, 47)),
+                                         ((3, 3, 3), (2, 2, 2), (16, 40, 40)),
+                                         ((2, 2, 1), (4, 4, 4), (24, 48, 48))])
+def test_fused_form_tolerance(gpu, port, pr, sr, shape):
+    """precision="f32_fma": the tiled kernel with fused multiply-adds, a
+    Horner Pade and a fast division. Tolerance, written here: relative error
+    against the reference CPU filter at most 1e-4 on all but 1e-4 of the
+    voxels (a weight whose argument lands within rounding of the Pade cutoff
+    can switch between ~0.025 and 0, which moves that voxel further), and at
+    most 1e-5 for the median voxel."""
+    vol = synth.small_case(shape, seed=1)
+    sig = np.full(shape[0], 0.05, np.float32)
+    want = port.denoise_f32(vol, FilterParams(sr, pr), np.stack([sig, sig]))
+    g = IterativeNLM_GPU()
+    g.configure_device(shape, DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr,
+                                                precision="f32_fma"))
+    g.set_sigma(sig)
+    g.Run_GaussianNoise(1, vol)
+    g.Run_GaussianNoise(2)
+    got = g.get_result()
+    assert "fused" in g.describe()
+    g.free_device()
+    rel = np.abs(got.astype(np.float64) - want) / np.maximum(np.abs(want.astype(np.float64)), 1e-6)
+    assert float((rel > 1e-4).mean()) <= 1e-4, rel.max()
+    assert float(np.median(rel)) <= 1e-5
