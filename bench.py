@@ -502,6 +502,51 @@ def run_large_workload(args):
     print(json.dumps(res), flush=True)
 
 
+def run_rgb_workload(args):
+    """The colour path (--color) on a 4096x3072 RGB image (seeded gradients,
+    disks and shot noise; reference defaults: search radius 10, patch radius 1,
+    4 iterations, alpha 0.5, one noise estimate per channel from 2048 samples,
+    Anscombe transform, joint weights): the whole job through
+    color.rgb_denoise (host planes in and out), and the reference's own colour
+    job (oracle/_ref) on a 1024x768 crop on all host threads."""
+    import torch
+    from microtomodenoise_b200 import DenoiseParameters, synth
+    from microtomodenoise_b200.color import ColorParameters, rgb_denoise
+    ny, nx = 3072, 4096
+    img = synth.rgb_photo(ny, nx, seed=0)
+    dp = DenoiseParameters(radius_searchspace=(10, 10, 0), radius_patchspace=(1, 1, 0), nslices=1,
+                           maxiterations=ITERS, alpha=0.5, noise_mode="global", n_samples=2048,
+                           noise_seed=0)
+    cp = ColorParameters()
+    rgb_denoise([c[:256, :256] for c in img], dp, cp)  # warm-up
+    times = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        rgb_denoise(img, dp, cp)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t)
+    secs = min(times)
+    res = {"workload": "rgb 4096x3072, search r10, patch r1, 4 iterations, global noise (2048 samples), "
+                       "Anscombe, joint weights",
+           "ms_per_job": secs * 1e3, "value": ny * nx * ITERS / secs, "unit": "pixel-iter/s",
+           "e2e": "host planes in and out, host wall clock (min of steps)"}
+    from oracle.oracle import FilterParams, Reference, reference_available
+    if reference_available():
+        cy, cx = 768, 1024
+        crop = [np.ascontiguousarray(c[1000:1000 + cy, 1500:1500 + cx]) for c in img]
+        t = time.perf_counter()
+        Reference().rgb_job(crop, FilterParams(search_radius=(10, 10, 0), patch_radius=(1, 1, 0),
+                                               nslices=1), maxiterations=ITERS, mode="global",
+                            n_samples=2048, seed=0, keep_iterations=False)
+        csecs = time.perf_counter() - t
+        res["cpu_reference"] = {"value": cy * cx * ITERS / csecs, "unit": "pixel-iter/s",
+                                "cores": os.cpu_count(), "kind": "reference",
+                                "sample": f"{cx}x{cy} crop, whole colour job, {csecs:.1f}s"}
+        res["speedup_vs_cpu_reference"] = res["value"] / res["cpu_reference"]["value"]
+    print(json.dumps(res), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -514,7 +559,7 @@ def main():
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--workload", default="grain512",
-                    choices=["grain512", "learned1024", "stream2048"],
+                    choices=["grain512", "learned1024", "stream2048", "rgb4k"],
                     help="grain512: the headline bench line; the others: one-step "
                          "measurements of the large workloads (see run_large_workload)")
     ap.add_argument("--stream-depth", type=int, default=128)
@@ -538,7 +583,10 @@ def main():
         if rank == 0:
             import torch
             torch.cuda.set_device(local)
-            run_large_workload(args)
+            if args.workload == "rgb4k":
+                run_rgb_workload(args)
+            else:
+                run_large_workload(args)
         return
 
     import torch

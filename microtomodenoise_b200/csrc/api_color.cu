@@ -170,6 +170,16 @@ extern "C" int inlm_rgb_denoise(int nx, int ny, const inlm_params* params, const
     a.sx = p.search_radius[0];
     a.sy = p.search_radius[1];
     a.independent = color->independent_channels ? 1 : 0;
+    // the unrolled kernel when its compile-time tap order is the table's
+    a.tap_radius = 0;
+    if (p.patch_radius[0] == p.patch_radius[1] && p.patch_radius[0] >= 1) {
+        std::vector<int> order(2 * 64);
+        const int nt = rgb_tap_order(p.patch_radius[0], order.data(), 64);
+        bool same = nt == a.P;
+        for (int q = 0; same && q < nt; q++)
+            same = order[2 * q] == geo.taps[q].x && order[2 * q + 1] == geo.taps[q].y && geo.taps[q].z == 0;
+        if (same) a.tap_radius = p.patch_radius[0];
+    }
     if (rgb_smem_bytes(a) > 227u * 1024)
         return fail(INLM_ERR_UNSUPPORTED, "search + patch radius too large for the tile (%zu bytes)",
                     rgb_smem_bytes(a));

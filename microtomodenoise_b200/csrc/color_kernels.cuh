@@ -19,11 +19,16 @@ struct RgbArgs {
     int hx, hy;            // staged halo of prev: search + patch radius per axis
     int sx, sy;            // staged halo of raw: search radius per axis
     int independent;       // params.color.independent_channels
+    int tap_radius;        // r > 0: the unrolled kernel for patch radius (r, r) (tap order
+                           // checked by the host against the table); 0: the generic kernel
 };
 
 constexpr int kRgbTX = 32, kRgbTY = 8;
 
 size_t rgb_smem_bytes(const RgbArgs& a);
+// Tap order (dx, dy pairs) of the unrolled kernel for patch radius (r, r);
+// returns the tap count, or -1 when no such kernel exists.
+int rgb_tap_order(int r, int* dxdy, int max_taps);
 cudaError_t launch_rgb_filter(const RgbArgs& a, cudaStream_t st);
 // forward (2 sqrt(v + 3/8)) or inverse ((v/2)^2 - 3/8) Anscombe transform of n
 // values in place, colorspace.h:83-125

@@ -144,3 +144,23 @@ def small_case(shape=(16, 20, 24), seed=0, noise_std=0.05) -> np.ndarray:
     r = max(2.0, min(shape) / 4.0)
     return spheres_volume(shape, n_spheres=4, rmin=1.5, rmax=r, noise_std=noise_std,
                           noise_blur=1.0, seed=seed)
+
+
+def rgb_photo(ny: int = 3072, nx: int = 4096, n_disks: int = 60, seed: int = 0):
+    """A seeded 8-bit RGB test image: smooth colour gradients, random flat
+    disks and Poisson (shot) noise on the counts, as three float32 (ny, nx)
+    planes with integer values 0..255 (the colour path's input)."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:ny, 0:nx].astype(np.float32)
+    base = [40 + 150 * x / nx, 60 + 120 * y / ny,
+            120 + 50 * np.sin(x * (12.0 / nx)) * np.cos(y * (9.0 / ny))]
+    for _ in range(n_disks):
+        cy, cx = rng.uniform(0, ny), rng.uniform(0, nx)
+        r = rng.uniform(0.01, 0.06) * min(ny, nx)
+        col = rng.uniform(10, 245, 3)
+        y0, y1 = int(max(0, cy - r)), int(min(ny, cy + r + 1))
+        x0, x1 = int(max(0, cx - r)), int(min(nx, cx + r + 1))
+        m = (y[y0:y1, x0:x1] - cy) ** 2 + (x[y0:y1, x0:x1] - cx) ** 2 <= r * r
+        for c in range(3):
+            base[c][y0:y1, x0:x1] = np.where(m, col[c], base[c][y0:y1, x0:x1])
+    return [np.clip(rng.poisson(np.clip(b, 1, 250)), 0, 255).astype(np.float32) for b in base]
