@@ -22,9 +22,11 @@ weak scaling, no data-path collective); time = max over ranks.
 ``forms`` (rank 0, one GPU): the same whole job in the fused FP32 form
 (fused multiply-adds, within 1e-4 relative of the reference except at
 weights that cross the Pade cutoff), the FP16-storage form and
-in the learned-proposal + FP16 form (k = 104 of 514 offsets per 8^3 tile
-without fallback, the fastest k measured within 0.1 dB of the FP64 oracle's
-PSNR against the clean phantom; and k = 256 with fallback to full
+in the learned-proposal + FP16 form (k = 144 of 514 offsets per 32x8x8 block,
+the four 8^3 tiles' predictions summed, run by the full-width kernel, without
+fallback: the fastest setting measured within 0.1 dB of the FP64 oracle's
+PSNR against the clean phantom; k = 104 per 8^3 tile with the one-tile
+kernel; and k = 256 per tile with fallback to full
 search below 0.95 predicted kept mass, which fires on every tile of this
 volume), each with
 its speed-up over the plain FP32 job, the proposal's fallback fraction and
@@ -268,7 +270,11 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
 
     net = ProposalNet.load(default_weights(PR, SR), device=local)
     forms = [("f32", "f32", None), ("f32_fused", "f32_fma", None), ("fp16", "f16", None),
-             ("learned_fp16", "f16", (104, 0.0)), ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
+             ("learned_fp16", "f16", (144, 0.0, 4)), ("learned_fp16_pertile_k104", "f16", (104, 0.0, 1)),
+             ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
+    for item in filter(None, args.learned_extra.split(",")):
+        k, t = (int(v) for v in item.split("@"))
+        forms.append((f"learned_fp16_k{k}_t{t}", "f16", (k, 0.0, t)))
     raw_dev = torch.from_numpy(vol).cuda()
     out_dev = torch.empty_like(raw_dev)
     vox = float(np.prod(vol.shape))
@@ -282,7 +288,7 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
         g.configure_device(vol.shape, dp)
         g.set_stream(stream.cuda_stream)
         if prop:
-            g.attach_proposal(net, prop[0], prop[1])
+            g.attach_proposal(net, prop[0], prop[1], tiles_x=prop[2] if len(prop) > 2 else 1)
         r = {"kernel": g.describe()}
         if name != "f32":
             for _ in range(1):
@@ -306,6 +312,7 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
             if prop:
                 st = g.proposal_stats()
                 r.update({"k": prop[0], "min_mass": prop[1],
+                          "tiles_per_plan": prop[2] if len(prop) > 2 else 1,
                           "fallback_fraction": st["fallback_tiles"] / max(st["tiles"], 1),
                           "fraction_evaluated": st["fraction_evaluated"]})
         # accuracy run: the FP32 job's sigma schedule, fixed, for every form
@@ -563,6 +570,8 @@ def main():
                     help="grain512: the headline bench line; the others: one-step "
                          "measurements of the large workloads (see run_large_workload)")
     ap.add_argument("--stream-depth", type=int, default=128)
+    ap.add_argument("--learned-extra", default="",
+                    help="extra learned + FP16 forms in the headline run, k@tiles_per_plan[,...]")
     ap.add_argument("--k-list", default="",
                     help="learned1024: comma-separated k values to sweep (no fallback)")
     ap.add_argument("--shape", default="512,512,512",

@@ -261,8 +261,21 @@ int inlm_proposal_select(inlm_proposal* p, const float* vol_dev, const float* sc
  * later iteration runs the network on its previous iterate and evaluates the
  * selected offsets per 8^3 tile. */
 int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass);
-/* Last iteration of an attached proposal: stats = {tiles, fallback tiles,
- * offsets evaluated summed over filter CTAs, CTAs * S (full search), S}. */
+/* The same with one offset list per tiles_x 8^3 tiles along x: 1 (as above,
+ * one 8^3 tile per filter CTA), or 4: the offsets ranked by the sum of the
+ * four tiles' softmax probabilities, one list per 32 x 8 x 8 block, run by
+ * the full-width FP16 kernel (a coarser choice per offset, a faster kernel
+ * per offset; the predicted kept mass is the mean over the four tiles). */
+int inlm_attach_proposal_grouped(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass,
+                                 int tiles_x);
+/* inlm_proposal_select for groups of tiles_x 8^3 tiles along x: bitmap and
+ * pred_mass hold one entry per group, groups ordered z, y, x. */
+int inlm_proposal_select_grouped(inlm_proposal* p, const float* vol_dev, const float* scale_dev,
+                                 const int shape[3], int tiles_x, int k, float min_mass,
+                                 uint32_t* bitmap_dev, float* pred_mass_dev, int* n_fallback);
+/* Last iteration of an attached proposal: stats = {plan lists (tiles or
+ * groups), lists that fell back, offsets evaluated summed over filter CTAs,
+ * lists * S (full search), S}. */
 int inlm_proposal_stats(inlm_denoiser* d, int64_t stats[5]);
 /* Training targets: the last iteration's per-8^3-tile weight mass of every
  * search offset (full search, FP16 form), each voxel's offset weights divided

@@ -231,14 +231,16 @@ class IterativeNLM_GPU:
         _lib.check(_lib.load().inlm_tile_grid(self._h, ts, tc), "tile_grid")
         return tuple(ts), tuple(tc)
 
-    def attach_proposal(self, net, k: int = 256, min_mass: float = 0.95) -> None:
+    def attach_proposal(self, net, k: int = 256, min_mass: float = 0.95, tiles_x: int = 1) -> None:
         """Evaluates only each 8^3 tile's top-k offsets predicted by `net` (a
         proposal.ProposalNet), or every offset where the predicted kept mass
-        is below min_mass. net=None returns to full search. FP16 form only."""
+        is below min_mass. tiles_x = 4 ranks one list per 4 tiles along x
+        (32 x 8 x 8 blocks, the full-width kernel). net=None returns to full
+        search. FP16 form only."""
         self._need()
         h = net._h if net is not None else None
-        _lib.check(_lib.load().inlm_attach_proposal(self._h, h, int(k), float(min_mass)),
-                   "attach_proposal")
+        _lib.check(_lib.load().inlm_attach_proposal_grouped(self._h, h, int(k), float(min_mass),
+                                                            int(tiles_x)), "attach_proposal")
         self._proposal = net  # keep the network alive while attached
 
     def proposal_stats(self) -> dict:

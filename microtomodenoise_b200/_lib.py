@@ -42,7 +42,7 @@ EXPORTS = (
     "inlm_tiff_shape", "inlm_tiff_read", "inlm_tiff_write_sequence",
     "inlm_get_result_slices", "inlm_set_result_slices", "inlm_noise_patchstd_slab",
     "inlm_noise_estimate_from_patchstd", "inlm_rgb_denoise", "inlm_tiff_read_rgb",
-    "inlm_tiff_write_rgb",
+    "inlm_tiff_write_rgb", "inlm_attach_proposal_grouped", "inlm_proposal_select_grouped",
 )
 
 
@@ -142,6 +142,9 @@ def load(path: str = "") -> C.CDLL:
     L.inlm_proposal_select.argtypes = [vp, vp, vp, C.c_int * 3, C.c_int, C.c_float, vp, vp,
                                        C.POINTER(C.c_int)]
     L.inlm_attach_proposal.argtypes = [vp, vp, C.c_int, C.c_float]
+    L.inlm_attach_proposal_grouped.argtypes = [vp, vp, C.c_int, C.c_float, C.c_int]
+    L.inlm_proposal_select_grouped.argtypes = [vp, vp, vp, C.c_int * 3, C.c_int, C.c_int, C.c_float,
+                                               vp, vp, C.POINTER(C.c_int)]
     L.inlm_proposal_stats.argtypes = [vp, C.c_int64 * 5]
     L.inlm_weight_map.argtypes = [vp, vp]
     L.inlm_net_input.argtypes = [vp, vp, vp]

@@ -864,7 +864,11 @@ int inlm::launch_filter(inlm_denoiser* d) {
         CUDA_TRY(cudaEventCreate(&t.b));
     }
     CUDA_TRY(cudaEventRecord(t.a, d->stream));
-    if (d->use_fast && d->plan_active) {
+    if (d->use_fast && d->plan_active && d->plan_cta32) {
+        // per-CTA plans of the learned proposal at 4 tiles per plan: full-width CTAs
+        int tiles_z = (d->shape[2] + d->fcfg.tz - 1) / d->fcfg.tz;
+        CUDA_TRY(launch_fast_kernel(d->fcfg, &d->tm_prev_h, d->fargs_plan, tiles_z, d->stream));
+    } else if (d->use_fast && d->plan_active) {
         // per-tile plans: one 8^3 tile per CTA
         int tiles_z = (d->shape[2] + d->fcfg8.tz - 1) / d->fcfg8.tz;
         CUDA_TRY(launch_fast_kernel(d->fcfg8, &d->tm_prev_h8, d->fargs8, tiles_z, d->stream));
@@ -1154,12 +1158,13 @@ extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
     if (!d || !buf) return fail(INLM_ERR_ARG, "null argument");
     const Geometry& g = d->geo;
     if (d->use_fast) {
-        const FastConfig& c = d->plan_active ? d->fcfg8 : d->fcfg;
+        const FastConfig& c = (d->plan_active && !d->plan_cta32) ? d->fcfg8 : d->fcfg;
         snprintf(buf, len,
                  "nlm_tile_fast<%d,%d,%d> tx=%d tz=%d d_planes=%s smem=%zu S=%zu P=%zu plan=%s "
                  "pad=%d,%d,%d",
                  c.rx, c.ry, c.rz, c.tx, c.tz, c.d_half ? "f16" : "f32", c.smem_bytes,
-                 g.search.size(), g.taps.size(), d->plan_active ? "per-tile" : "full", g.pad[0],
+                 g.search.size(), g.taps.size(),
+                 d->plan_active ? (d->plan_cta32 ? "per-cta" : "per-tile") : "full", g.pad[0],
                  g.pad[1], g.pad[2]);
     }
     else if (d->use_tile)
@@ -1289,6 +1294,7 @@ extern "C" int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const in
         return fail(INLM_ERR_UNSUPPORTED, "offset plans need the FP16 form");
     if (d->prop.net) return fail(INLM_ERR_STATE, "a proposal network is attached; detach it first");
     CUDA_TRY(cudaSetDevice(d->device));
+    d->plan_cta32 = false;
     if (!start) {
         d->plan_active = false;
         d->fargs8.plan_start = nullptr;

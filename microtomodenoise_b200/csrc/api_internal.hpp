@@ -121,6 +121,8 @@ struct ProposalRun {
     int nwords = 0;
     long long n_tiles = 0;
     inlm::Dim3i t8{0, 0, 0};
+    int group = 1;         // 8^3 tiles per plan along x: 1, or 4 (the 32 x 8 x 8 CTA)
+    long long n_plan = 0;  // plan lists (tiles / groups)
     inlm::DevBuf a1, a2, a3, a4, bitmap, pmass, counters, scale, plan_start, plan_off;
 };
 
@@ -158,6 +160,8 @@ struct inlm_denoiser {
     CUtensorMap tm_prev_h8{};
     int2* d_search_delta8 = nullptr;
     bool plan_active = false;     // fargs8 carries a per-tile plan
+    bool plan_cta32 = false;      // ... or fargs_plan a per-32x8x8-CTA plan (proposal, group 4)
+    inlm::FastArgs fargs_plan{};
     int* d_plan_start = nullptr;  // per-tile offset lists set by inlm_set_offset_plan
     int* d_plan_off = nullptr;
     int plan_cap = 0;

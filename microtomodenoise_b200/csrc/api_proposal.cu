@@ -226,6 +226,33 @@ extern "C" int inlm_proposal_select(inlm_proposal* p, const float* vol, const fl
     return INLM_OK;
 }
 
+extern "C" int inlm_proposal_select_grouped(inlm_proposal* p, const float* vol, const float* scale,
+                                            const int shape[3], int tiles_x, int k, float min_mass,
+                                            uint32_t* bitmap, float* pred_mass, int* n_fallback) {
+    if (tiles_x == 1) return inlm_proposal_select(p, vol, scale, shape, k, min_mass, bitmap, pred_mass, n_fallback);
+    if (!p || !vol || !scale || !bitmap || !pred_mass) return fail(INLM_ERR_ARG, "null argument");
+    if (k < 1 || tiles_x < 1) return fail(INLM_ERR_ARG, "k and tiles_x must be >= 1");
+    int rc = check_shape(shape);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(p->device));
+    NetIn in;
+    rc = example_input(p, vol, scale, shape, &in);
+    if (rc) return rc;
+    CUDA_TRY(prop_levels_alloc(&p->a1, &p->a2, &p->a3, &p->a4, shape[0], shape[1], shape[2]));
+    CUDA_TRY(p->counters.ensure(16));
+    CUDA_TRY(cudaMemsetAsync(p->counters.p, 0, 16, p->stream));
+    CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, prop_acts(p), p->stream));
+    Dim3i lv[4];
+    net_levels(shape[0], shape[1], shape[2], lv);
+    CUDA_TRY(net_select_group(p->L, p->d_wb, p->d_w, p->a4.as<float>(), lv[3], tiles_x, k, min_mass, bitmap,
+                              (p->L.S + 31) / 32, pred_mass, p->counters.as<int>(), p->stream));
+    int cnt[4] = {0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpyAsync(cnt, p->counters.p, 16, cudaMemcpyDeviceToHost, p->stream));
+    CUDA_TRY(cudaStreamSynchronize(p->stream));
+    if (n_fallback) *n_fallback = cnt[0];
+    return INLM_OK;
+}
+
 // ---------------- denoiser side ----------------
 
 void inlm::proposal_release(inlm_denoiser* d) {
@@ -237,12 +264,18 @@ void inlm::proposal_release(inlm_denoiser* d) {
 }
 
 extern "C" int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass) {
+    return inlm_attach_proposal_grouped(d, p, k, min_mass, 1);
+}
+
+extern "C" int inlm_attach_proposal_grouped(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass,
+                                            int tiles_x) {
     if (!d) return fail(INLM_ERR_ARG, "null handle");
     CUDA_TRY(cudaSetDevice(d->device));
     CUDA_TRY(cudaStreamSynchronize(d->stream));
     if (!p) {
         if (d->prop.net) {
             d->plan_active = false;
+            d->plan_cta32 = false;
             d->fargs8.plan_start = nullptr;
             d->fargs8.plan_count = nullptr;
             d->fargs8.plan_offsets = nullptr;
@@ -250,6 +283,9 @@ extern "C" int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, f
         proposal_release(d);
         return INLM_OK;
     }
+    if (tiles_x != 1 && tiles_x != 4) return fail(INLM_ERR_ARG, "tiles_x must be 1 or 4");
+    if (tiles_x == 4 && (d->fcfg.tx != 32 || d->fcfg.tz != 8))
+        return fail(INLM_ERR_UNSUPPORTED, "no 32 x 8 x 8 FP16 kernel for this patch shape");
     if (!d->use_fast || !d->use_tile8)
         return fail(INLM_ERR_UNSUPPORTED, "the proposal drives the FP16 form only");
     if (d->plan_active && !d->prop.net)
@@ -267,11 +303,14 @@ extern "C" int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, f
     net_levels(d->shape[0], d->shape[1], d->shape[2], lv);
     r.t8 = lv[3];
     r.n_tiles = (long long)lv[3].x * lv[3].y * lv[3].z;
-    // one plan list per 8^3 tile = per CTA of the tx = 8 configuration
-    const long long n = r.n_tiles;
+    r.group = tiles_x;
+    // one plan list per 8^3 tile (a CTA of the tx = 8 configuration) or per
+    // group of 4 tiles along x (a CTA of the tx = 32 configuration)
+    r.n_plan = (long long)((lv[3].x + tiles_x - 1) / tiles_x) * lv[3].y * lv[3].z;
+    const long long n = r.n_plan;
     CUDA_TRY(prop_levels_alloc(&r.a1, &r.a2, &r.a3, &r.a4, d->shape[0], d->shape[1], d->shape[2]));
-    CUDA_TRY(r.bitmap.ensure((size_t)r.n_tiles * r.nwords * 4));
-    CUDA_TRY(r.pmass.ensure((size_t)r.n_tiles * 4));
+    CUDA_TRY(r.bitmap.ensure((size_t)n * r.nwords * 4));
+    CUDA_TRY(r.pmass.ensure((size_t)n * 4));
     CUDA_TRY(r.counters.ensure(16));
     CUDA_TRY(r.scale.ensure((size_t)d->shape[2] * 4));
     CUDA_TRY(r.plan_start.ensure((size_t)2 * n * 4));
@@ -306,16 +345,30 @@ int inlm::proposal_enqueue(inlm_denoiser* d) {
     NetActs act{r.a1.as<float>(), r.a2.as<float>(), r.a3.as<float>(), r.a4.as<float>()};
     CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, act, d->stream));
     CUDA_TRY(cudaMemsetAsync(r.counters.p, 0, 16, d->stream));
-    CUDA_TRY(net_select(p->L, p->d_wb, p->d_w, act.a4, (int)r.n_tiles, r.k, r.min_mass,
-                        r.bitmap.as<unsigned>(), r.nwords, r.pmass.as<float>(), r.counters.as<int>(),
-                        d->stream));
+    if (r.group == 1)
+        CUDA_TRY(net_select(p->L, p->d_wb, p->d_w, act.a4, (int)r.n_tiles, r.k, r.min_mass,
+                            r.bitmap.as<unsigned>(), r.nwords, r.pmass.as<float>(), r.counters.as<int>(),
+                            d->stream));
+    else
+        CUDA_TRY(net_select_group(p->L, p->d_wb, p->d_w, act.a4, r.t8, r.group, r.k, r.min_mass,
+                                  r.bitmap.as<unsigned>(), r.nwords, r.pmass.as<float>(),
+                                  r.counters.as<int>(), d->stream));
     int* ps = r.plan_start.as<int>();
-    CUDA_TRY(net_plan_tiles(r.bitmap.as<unsigned>(), r.nwords, r.n_tiles, p->L.S,
-                            r.plan_off.as<int>(), ps + r.n_tiles, r.counters.as<int>(), d->stream));
+    CUDA_TRY(net_plan_tiles(r.bitmap.as<unsigned>(), r.nwords, r.n_plan, p->L.S,
+                            r.plan_off.as<int>(), ps + r.n_plan, r.counters.as<int>(), d->stream));
     d->launches += 7;  // scale, 4 layers, select, plan
-    d->fargs8.plan_start = ps;
-    d->fargs8.plan_count = ps + r.n_tiles;
-    d->fargs8.plan_offsets = r.plan_off.as<int>();
+    if (r.group == 1) {
+        d->fargs8.plan_start = ps;
+        d->fargs8.plan_count = ps + r.n_plan;
+        d->fargs8.plan_offsets = r.plan_off.as<int>();
+        d->plan_cta32 = false;
+    } else {
+        d->fargs_plan = d->fargs;
+        d->fargs_plan.plan_start = ps;
+        d->fargs_plan.plan_count = ps + r.n_plan;
+        d->fargs_plan.plan_offsets = r.plan_off.as<int>();
+        d->plan_cta32 = true;
+    }
     d->plan_active = true;
     return INLM_OK;
 }
@@ -327,10 +380,10 @@ extern "C" int inlm_proposal_stats(inlm_denoiser* d, int64_t stats[5]) {
     int cnt[4] = {0, 0, 0, 0};
     CUDA_TRY(cudaMemcpyAsync(cnt, d->prop.counters.p, 16, cudaMemcpyDeviceToHost, d->stream));
     CUDA_TRY(cudaStreamSynchronize(d->stream));
-    stats[0] = d->prop.n_tiles;
+    stats[0] = d->prop.n_plan;
     stats[1] = cnt[0];
     stats[2] = cnt[1];
-    stats[3] = (int64_t)d->prop.n_tiles * d->fargs.S;
+    stats[3] = (int64_t)d->prop.n_plan * d->fargs.S;
     stats[4] = d->fargs.S;
     return INLM_OK;
 }

@@ -492,40 +492,12 @@ __device__ __forceinline__ unsigned order_key(float f) {
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-// One warp per tile: logits in the warp's shared-memory row, softmax
-// normaliser by shuffles, radix select of the K-th largest logit (8 bits per
-// pass, a warp-private 256-bin histogram), ties broken towards lower offsets;
-// offsets k = 32 i + lane are handled in rounds i, so a ballot of the kept
-// flags in round i is bitmap word i.
-constexpr int kSelWarps = 4;
-
-__global__ void __launch_bounds__(32 * kSelWarps)
-    net_select_kernel(const float* __restrict__ a4, long long n_tiles, int S,
-                      const __nv_bfloat16* __restrict__ Wh, const float* __restrict__ bh, int K,
-                      float min_mass, unsigned* __restrict__ bitmap, int nwords,
-                      float* __restrict__ pred_mass, int* counters) {
-    extern __shared__ unsigned sel_smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rowlen = (S + 3) / 4 * 4;
-    float* sl = reinterpret_cast<float*>(sel_smem) + warp * rowlen;
-    unsigned* hist = sel_smem + kSelWarps * rowlen + warp * 256;
-    const long long tile = blockIdx.x * (long long)kSelWarps + warp;
-    if (tile >= n_tiles) return;
-    float h[kNetC];
-    load16(a4 + tile * kNetC, h);
-    float m = -INFINITY;
-    for (int k = lane; k < S; k += 32) {
-        const float l = head_logit(Wh, bh, h, k);
-        sl[k] = l;
-        m = fmaxf(m, l);
-    }
-    const float M = warp_max(m);
-    float z = 0.f;
-    for (int k = lane; k < S; k += 32) z += expf(sl[k] - M);
-    const float Z = warp_sum(z);
-    __syncwarp();
-
-    const int Ke = min(max(K, 1), S);
+// Radix select over the values sl[0..S) of one warp: on return the kept set is
+// every key above *prefix plus the first *remaining keys equal to it in
+// offset order (the Ke largest values, ties towards lower offsets); 8 bits
+// per pass over a warp-private 256-bin histogram.
+__device__ __forceinline__ void warp_topk_threshold(const float* sl, int S, int Ke, unsigned* hist,
+                                                    int lane, unsigned* prefix_out, int* remaining_out) {
     unsigned prefix = 0, pmask = 0;
     int remaining = Ke;
     for (int shift = 24; shift >= 0; shift -= 8) {
@@ -573,8 +545,14 @@ __global__ void __launch_bounds__(32 * kSelWarps)
         remaining -= found_above;
         __syncwarp();
     }
-    // keys above the K-th are kept; of the keys equal to it, the first
-    // `remaining` in offset order
+    *prefix_out = prefix;
+    *remaining_out = remaining;
+}
+
+// Sum over the kept offsets of val(k), warp-reduced.
+template <class F>
+__device__ __forceinline__ float warp_kept_sum(const float* sl, int S, unsigned prefix, int remaining,
+                                               int lane, F val) {
     float kept = 0.f;
     int ties_before = 0;
     const int rounds = (S + 31) / 32;
@@ -586,11 +564,17 @@ __global__ void __launch_bounds__(32 * kSelWarps)
         const int rank = ties_before + __popc(tb & ((1u << lane) - 1u));
         const bool s = k < S && (key > prefix || (tie && rank < remaining));
         ties_before += __popc(tb);
-        if (s) kept += expf(sl[k] - M);
+        if (s) kept += val(k);
     }
-    kept = warp_sum(kept) / Z;
-    const bool fallback = !(kept >= min_mass);
-    ties_before = 0;
+    return warp_sum(kept);
+}
+
+// Kept flags as bitmap words (word i = offsets 32i .. 32i+31); every offset
+// under fallback.
+__device__ __forceinline__ void warp_write_bitmap(const float* sl, int S, unsigned prefix, int remaining,
+                                                  bool fallback, unsigned* out, int nwords, int lane) {
+    int ties_before = 0;
+    const int rounds = (S + 31) / 32;
     for (int i = 0; i < rounds; i++) {
         const int k = 32 * i + lane;
         const unsigned key = k < S ? order_key(sl[k]) : 0u;
@@ -600,10 +584,108 @@ __global__ void __launch_bounds__(32 * kSelWarps)
         ties_before += __popc(tb);
         const bool s = k < S && (fallback || key > prefix || (tie && rank < remaining));
         const unsigned word = __ballot_sync(0xffffffffu, s);
-        if (lane == 0 && i < nwords) bitmap[tile * nwords + i] = word;
+        if (lane == 0 && i < nwords) out[i] = word;
     }
+}
+
+// One warp per tile: logits in the warp's shared-memory row, softmax
+// normaliser by shuffles, radix select of the K-th largest logit (8 bits per
+// pass, a warp-private 256-bin histogram), ties broken towards lower offsets;
+// offsets k = 32 i + lane are handled in rounds i, so a ballot of the kept
+// flags in round i is bitmap word i.
+constexpr int kSelWarps = 4;
+
+__global__ void __launch_bounds__(32 * kSelWarps)
+    net_select_kernel(const float* __restrict__ a4, long long n_tiles, int S,
+                      const __nv_bfloat16* __restrict__ Wh, const float* __restrict__ bh, int K,
+                      float min_mass, unsigned* __restrict__ bitmap, int nwords,
+                      float* __restrict__ pred_mass, int* counters) {
+    extern __shared__ unsigned sel_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rowlen = (S + 3) / 4 * 4;
+    float* sl = reinterpret_cast<float*>(sel_smem) + warp * rowlen;
+    unsigned* hist = sel_smem + kSelWarps * rowlen + warp * 256;
+    const long long tile = blockIdx.x * (long long)kSelWarps + warp;
+    if (tile >= n_tiles) return;
+    float h[kNetC];
+    load16(a4 + tile * kNetC, h);
+    float m = -INFINITY;
+    for (int k = lane; k < S; k += 32) {
+        const float l = head_logit(Wh, bh, h, k);
+        sl[k] = l;
+        m = fmaxf(m, l);
+    }
+    const float M = warp_max(m);
+    float z = 0.f;
+    for (int k = lane; k < S; k += 32) z += expf(sl[k] - M);
+    const float Z = warp_sum(z);
+    __syncwarp();
+
+    const int Ke = min(max(K, 1), S);
+    unsigned prefix;
+    int remaining;
+    warp_topk_threshold(sl, S, Ke, hist, lane, &prefix, &remaining);
+    float kept = warp_kept_sum(sl, S, prefix, remaining, lane, [&](int k) { return expf(sl[k] - M); });
+    kept = kept / Z;
+    const bool fallback = !(kept >= min_mass);
+    warp_write_bitmap(sl, S, prefix, remaining, fallback, bitmap + tile * nwords, nwords, lane);
     if (lane == 0) {
         pred_mass[tile] = kept;
+        if (fallback) atomicAdd(&counters[0], 1);
+    }
+}
+
+// One warp per group of up to G consecutive 8^3 tiles along x (the 32 x 8 x 8
+// CTA of the full-width filter kernel for G = 4): each tile's softmax over the
+// offsets, summed over the group's tiles, ranked and cut at the top K (ties
+// towards lower offsets). The predicted kept mass is the mean over the tiles
+// of each tile's kept probability; below min_mass the group keeps everything.
+__global__ void __launch_bounds__(32 * kSelWarps)
+    net_select_group_kernel(const float* __restrict__ a4, int t8x, long long n_groups, int gx, int G,
+                            int S, const __nv_bfloat16* __restrict__ Wh, const float* __restrict__ bh,
+                            int K, float min_mass, unsigned* __restrict__ bitmap, int nwords,
+                            float* __restrict__ pred_mass, int* counters) {
+    extern __shared__ unsigned sel_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rowlen = (S + 3) / 4 * 4;
+    float* sc = reinterpret_cast<float*>(sel_smem) + warp * 2 * rowlen;
+    float* sl = sc + rowlen;
+    unsigned* hist = sel_smem + kSelWarps * 2 * rowlen + warp * 256;
+    const long long g = blockIdx.x * (long long)kSelWarps + warp;
+    if (g >= n_groups) return;
+    const long long row = g / gx;  // (z, y) tile row
+    const int gxi = (int)(g - row * gx);
+    for (int k = lane; k < S; k += 32) sc[k] = 0.f;
+    int ng = 0;
+    for (int j = 0; j < G; j++) {
+        const int tx = gxi * G + j;
+        if (tx >= t8x) break;
+        const long long tile = row * t8x + tx;
+        float h[kNetC];
+        load16(a4 + tile * kNetC, h);
+        float m = -INFINITY;
+        for (int k = lane; k < S; k += 32) {
+            const float l = head_logit(Wh, bh, h, k);
+            sl[k] = l;
+            m = fmaxf(m, l);
+        }
+        const float M = warp_max(m);
+        float z = 0.f;
+        for (int k = lane; k < S; k += 32) z += expf(sl[k] - M);
+        const float Z = warp_sum(z);
+        for (int k = lane; k < S; k += 32) sc[k] += expf(sl[k] - M) / Z;  // lane-owned entries
+        ng++;
+        __syncwarp();
+    }
+    const int Ke = min(max(K, 1), S);
+    unsigned prefix;
+    int remaining;
+    warp_topk_threshold(sc, S, Ke, hist, lane, &prefix, &remaining);
+    const float kept = warp_kept_sum(sc, S, prefix, remaining, lane, [&](int k) { return sc[k]; }) / ng;
+    const bool fallback = !(kept >= min_mass);
+    warp_write_bitmap(sc, S, prefix, remaining, fallback, bitmap + g * nwords, nwords, lane);
+    if (lane == 0) {
+        pred_mass[g] = kept;
         if (fallback) atomicAdd(&counters[0], 1);
     }
 }
@@ -813,6 +895,23 @@ cudaError_t net_select(const NetLayout& L, const __nv_bfloat16* wb, const float*
     const long long blocks = ((long long)n_tiles + kSelWarps - 1) / kSelWarps;
     net_select_kernel<<<(unsigned)blocks, 32 * kSelWarps, sm, st>>>(
         a4, n_tiles, L.S, wb + L.wh, wf + L.bh, K, min_mass, bitmap, nwords, pred_mass, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t net_select_group(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const float* a4,
+                             Dim3i t8, int G, int K, float min_mass, unsigned* bitmap, int nwords,
+                             float* pred_mass, int* counters, cudaStream_t st) {
+    const int gx = (t8.x + G - 1) / G;
+    const long long n_groups = (long long)gx * t8.y * t8.z;
+    if (n_groups <= 0) return cudaSuccess;
+    const size_t sm = (size_t)kSelWarps * (2 * ((L.S + 3) / 4 * 4) + 256) * 4;
+    cudaError_t e = cudaFuncSetAttribute(net_select_group_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    const long long blocks = (n_groups + kSelWarps - 1) / kSelWarps;
+    net_select_group_kernel<<<(unsigned)blocks, 32 * kSelWarps, sm, st>>>(
+        a4, t8.x, n_groups, gx, G, L.S, wb + L.wh, wf + L.bh, K, min_mass, bitmap, nwords, pred_mass,
+        counters);
     return cudaGetLastError();
 }
 

@@ -75,6 +75,11 @@ cudaError_t net_select(const NetLayout& L, const __nv_bfloat16* wb, const float*
 
 // Per 8^3 tile: its kept offsets in ascending order at plan_off[tile * S],
 // their number in plan_count[tile]; counters[1] += entries written.
+// Selection per group of G 8^3 tiles along x (t8: the 8^3 tile grid); bitmap
+// and pred_mass have one entry per group, groups ordered (z, y, x).
+cudaError_t net_select_group(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const float* a4,
+                             Dim3i t8, int G, int K, float min_mass, unsigned* bitmap, int nwords,
+                             float* pred_mass, int* counters, cudaStream_t st);
 cudaError_t net_plan_tiles(const unsigned* bitmap, int nwords, long long n_tiles, int S,
                            int* plan_off, int* plan_count, int* counters, cudaStream_t st);
 

@@ -165,20 +165,21 @@ class ProposalNet:
                    "proposal_train")
         return loss.value
 
-    def select(self, vol, scale, k: int, min_mass: float):
-        """(keep bitmap int32 [tiles, ceil(S/32)], predicted kept mass [tiles], fallback tiles)."""
+    def select(self, vol, scale, k: int, min_mass: float, tiles_x: int = 1):
+        """(keep bitmap int32 [lists, ceil(S/32)], predicted kept mass [lists],
+        fallback lists); one list per 8^3 tile, or per tiles_x tiles along x."""
         torch = _torch()
         nz, ny, nx = vol.shape
-        nt = int(np.prod(tiles8(vol.shape)))
+        tz, ty, tx = tiles8(vol.shape)
+        nt = (-(-tx // tiles_x)) * ty * tz
         nw = (self.S + 31) // 32
         bm = torch.zeros((nt, nw), dtype=torch.int32, device=vol.device)
         pm = torch.zeros(nt, dtype=torch.float32, device=vol.device)
         nfb = C.c_int(0)
         torch.cuda.synchronize(vol.device)
-        _lib.check(_lib.load().inlm_proposal_select(self._h, vol.data_ptr(), scale.data_ptr(),
-                                                    (C.c_int * 3)(nx, ny, nz), int(k),
-                                                    float(min_mass), bm.data_ptr(), pm.data_ptr(),
-                                                    C.byref(nfb)), "proposal_select")
+        _lib.check(_lib.load().inlm_proposal_select_grouped(
+            self._h, vol.data_ptr(), scale.data_ptr(), (C.c_int * 3)(nx, ny, nz), int(tiles_x), int(k),
+            float(min_mass), bm.data_ptr(), pm.data_ptr(), C.byref(nfb)), "proposal_select")
         return bm, pm, nfb.value
 
     def close(self) -> None:

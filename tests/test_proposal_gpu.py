@@ -170,12 +170,12 @@ def check_close(got, ref, what, psnr_min=50.0, outlier_frac=2e-3):
     assert float(np.mean(err > 3e-3)) <= outlier_frac
 
 
-def run_with_net(vol, pr, sr, sig, net, k, min_mass, record=False):
+def run_with_net(vol, pr, sr, sig, net, k, min_mass, record=False, tiles_x=1):
     g = IterativeNLM_GPU()
     g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr,
                                                     precision="f16"))
     if net is not None:
-        g.attach_proposal(net, k, min_mass)
+        g.attach_proposal(net, k, min_mass, tiles_x=tiles_x)
     keeps, stats, outs = [], [], []
     for it in range(sig.shape[0]):
         g.set_sigma(sig[it])
@@ -185,7 +185,7 @@ def run_with_net(vol, pr, sr, sig, net, k, min_mass, record=False):
             x = torch.empty(vol.shape, dtype=torch.float32, device="cuda")
             s = torch.empty(vol.shape[0], dtype=torch.float32, device="cuda")
             g.net_input(x.data_ptr(), s.data_ptr())
-            bm, _, _ = net.select(x, s, k, min_mass)
+            bm, _, _ = net.select(x, s, k, min_mass, tiles_x=tiles_x)
             keeps.append(bitmap_keep(bm, net.S))
             stats.append(g.proposal_stats())
     ts, tc = g.tile_grid()
@@ -308,4 +308,82 @@ def test_trained_net_gains_over_static_prior(gpu, port):
           f"trained {np.round(res['trained'], 2)} dB")
     assert np.mean(res["trained"]) > np.mean(res["prior"])
     base.close()
+    net.close()
+
+
+def group_scores(logits, shape, G=4):
+    """Sum of the tiles' softmax probabilities per group of G 8^3 tiles along
+    x (groups ordered z, y, x), float64; and each group's tile count."""
+    tx, ty, tz = (-(-int(n) // 8) for n in shape[::-1])
+    prob = po.softmax(np.asarray(logits, np.float64)).reshape(tz, ty, tx, -1)
+    gx = -(-tx // G)
+    sc = np.zeros((tz, ty, gx, prob.shape[-1]))
+    cnt = np.zeros((tz, ty, gx))
+    for x in range(tx):
+        sc[:, :, x // G] += prob[:, :, x]
+        cnt[:, :, x // G] += 1
+    return sc.reshape(-1, prob.shape[-1]), cnt.ravel()
+
+
+def expand_groups(keep_g, shape, G=4):
+    """Per-8^3-tile keep flags from per-group ones (every tile takes its group's)."""
+    tx, ty, tz = (-(-int(n) // 8) for n in shape[::-1])
+    gx = -(-tx // G)
+    kg = keep_g.reshape(tz, ty, gx, -1)
+    return np.stack([kg[:, :, x // G] for x in range(tx)], axis=2).reshape(tz * ty * tx, -1)
+
+
+@pytest.mark.parametrize("k", [1, 9, 30])
+def test_select_grouped_vs_oracle(gpu, k):
+    """Top-k of the summed softmax per 4 tiles along x: the kept set is a top-k
+    of the FP64 scores (up to float rounding between near-equal scores), the
+    predicted mass is the mean kept probability of the group's tiles."""
+    P = prop_mod()
+    S = 45
+    net = P.ProposalNet(S)
+    net.set_params(rand_params(S, 4))
+    shape = (17, 24, 40)  # 5 tiles along x: groups of 4 and of 1
+    ex, _ = example(shape, 9, S)
+    logits = net.logits(ex.vol, ex.scale).cpu().numpy().astype(np.float64)
+    sc, cnt = group_scores(logits, shape)
+    bm, pm, nfb = net.select(ex.vol, ex.scale, k, 0.0, tiles_x=4)
+    keep = bitmap_keep(bm, S)
+    assert keep.shape == sc.shape and nfb == 0
+    assert (keep.sum(axis=1) == k).all()
+    for g in range(sc.shape[0]):
+        kept, dropped = sc[g][keep[g]], sc[g][~keep[g]]
+        if len(dropped):
+            assert kept.min() >= dropped.max() - 1e-6
+        assert abs(float(pm.cpu().numpy()[g]) - kept.sum() / cnt[g]) < 1e-5
+    # threshold between two groups' masses: exactly those fall back
+    pmv = np.sort(pm.cpu().numpy())
+    i = len(pmv) // 2
+    while pmv[i] - pmv[i - 1] < 1e-4:
+        i += 1
+    thr = float(0.5 * (pmv[i] + pmv[i - 1]))
+    bm2, pm2, nfb2 = net.select(ex.vol, ex.scale, k, thr, tiles_x=4)
+    keep2 = bitmap_keep(bm2, S)
+    fb = pm.cpu().numpy() < thr
+    assert nfb2 == int(fb.sum()) and keep2[fb].all() and np.array_equal(keep2[~fb], keep[~fb])
+    net.close()
+
+
+def test_grouped_plans_vs_fp64_plan_oracle(gpu, port):
+    """tiles_x = 4: the full-width kernel runs each 32 x 8 x 8 block's list;
+    equal to the FP64 filter where every 8^3 tile evaluates its group's list."""
+    P = prop_mod()
+    vol = synth.small_case((16, 24, 72), seed=11)  # 9 tiles along x: groups of 4, 4, 1
+    pr, sr = (1, 1, 1), (3, 3, 3)
+    p = FilterParams(search_radius=sr, patch_radius=pr)
+    S = len(port.search_offsets(p))
+    net = P.ProposalNet(S)
+    net.set_params(rand_params(S, 5))
+    k = S // 3
+    sig = np.stack([np.full(vol.shape[0], 0.07, np.float32)] * 2)
+    got, keeps, stats, _ = run_with_net(vol, pr, sr, sig, net, k, 0.0, record=True, tiles_x=4)
+    for kp, st in zip(keeps, stats):
+        assert st["tiles"] == kp.shape[0] and st["fallback_tiles"] == 0
+        assert st["offsets_evaluated"] == k * kp.shape[0]
+    ref = port.denoise_f64_plan(vol, p, sig, (8, 8, 8), np.stack([expand_groups(kp, vol.shape) for kp in keeps]))
+    check_close(got[-1], ref, "grouped plan")
     net.close()
