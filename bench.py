@@ -453,9 +453,12 @@ def run_large_workload(args):
     forms = [("f32", "f32", None), ("fp16", "f16", None), ("learned_fp16_k256_mass095", "f16", (256, 0.95)),
              ("learned_fp16_k256", "f16", (256, 0.0))]
     if args.k_list:
-        # a sweep of k (no fallback) beside plain FP32 and FP16 full search
-        forms = [("f32", "f32", None), ("fp16", "f16", None)] + [
-            (f"learned_fp16_k{k}", "f16", (k, 0.0)) for k in (int(v) for v in args.k_list.split(","))]
+        # a sweep of k (no fallback; k@t: one list per t 8^3 tiles along x)
+        # beside plain FP32 and FP16 full search
+        forms = [("f32", "f32", None), ("fp16", "f16", None)]
+        for item in args.k_list.split(","):
+            k, _, t = item.partition("@")
+            forms.append((f"learned_fp16_k{k}" + (f"_t{t}" if t else ""), "f16", (int(k), 0.0, int(t or 1))))
     if args.workload == "stream2048":
         forms = [("f32", "f32", None), ("learned_fp16_k256", "f16", (256, 0.0))]
     ref_psnr = None
@@ -467,7 +470,7 @@ def run_large_workload(args):
             g = IterativeNLM_GPU()
             g.configure_device(shape, dp)
             if prop:
-                g.attach_proposal(net, prop[0], prop[1])
+                g.attach_proposal(net, prop[0], prop[1], tiles_x=prop[2] if len(prop) > 2 else 1)
             raw = torch.from_numpy(vol).cuda()
             out = torch.empty_like(raw)
             torch.cuda.synchronize()
