@@ -429,7 +429,7 @@ def run_large_workload(args):
       with noise sigma drifting 0.02 -> 0.08 along z (blur 1) and rings of
       amplitude 0.03, z-adaptive noise, patch r3 search r7, 4 iterations, held
       in host memory and streamed in z-slabs of 64 slices (inlm_stream_denoise):
-      plain FP32 and learned + FP16 (k = 256, no fallback).
+      plain FP32 and learned + FP16 (k = 896 per 32x8x8 block, no fallback).
     PSNR against the clean phantom over the whole volume for every form."""
     import torch
     from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, stream_denoise, synth
@@ -460,7 +460,7 @@ def run_large_workload(args):
             k, _, t = item.partition("@")
             forms.append((f"learned_fp16_k{k}" + (f"_t{t}" if t else ""), "f16", (int(k), 0.0, int(t or 1))))
     if args.workload == "stream2048":
-        forms = [("f32", "f32", None), ("learned_fp16_k256", "f16", (256, 0.0))]
+        forms = [("f32", "f32", None), ("learned_fp16_k896_t4", "f16", (896, 0.0, 4))]
     ref_psnr = None
     for name, prec, prop in forms:
         dp = DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, maxiterations=ITERS,
@@ -492,7 +492,8 @@ def run_large_workload(args):
             del raw, out
         else:
             o, _, _, st = stream_denoise(vol, dp, slab_depth=64, net=net if prop else None,
-                                         k=prop[0] if prop else 0, min_mass=prop[1] if prop else 0.0)
+                                         k=prop[0] if prop else 0, min_mass=prop[1] if prop else 0.0,
+                                         tiles_x=prop[2] if prop and len(prop) > 2 else 1)
             ms = st["ms"]
             r = {"ms_per_job": ms, "value": vox / (ms / 1e3), "unit": "voxel-iter/s",
                  "h2d_bytes": st["h2d_bytes"], "d2h_bytes": st["d2h_bytes"], "slabs": st["slabs"],

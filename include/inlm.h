@@ -337,6 +337,13 @@ int inlm_batch_describe(inlm_batch* b, char* buf, size_t len);
 int inlm_stream_denoise(const int shape[3], const inlm_params* p, const float* raw_host,
                         float* out_host, int slab_depth, inlm_proposal* net, int k, float min_mass,
                         float* sigma0_out, float* sigma1_out, double* stats);
+/* The same with the proposal's lists per tiles_x 8^3 tiles along x (1 or 4,
+ * as inlm_attach_proposal_grouped); slabs split z only, so the results equal
+ * the in-memory schedule with the same grouping. */
+int inlm_stream_denoise_grouped(const int shape[3], const inlm_params* p, const float* raw_host,
+                                float* out_host, int slab_depth, inlm_proposal* net, int k,
+                                float min_mass, int tiles_x, float* sigma0_out, float* sigma1_out,
+                                double* stats);
 
 /* ---------------- host-only helpers (no device needed) ---------------- */
 

@@ -394,9 +394,11 @@ class Batch:
 
 
 def stream_denoise(raw: np.ndarray, params: DenoiseParameters, slab_depth: int = 64,
-                   net=None, k: int = 256, min_mass: float = 0.95, out: Optional[np.ndarray] = None):
+                   net=None, k: int = 256, min_mass: float = 0.95, out: Optional[np.ndarray] = None,
+                   tiles_x: int = 1):
     """The denoise schedule for a host-resident volume, filtered in z-slabs
-    (inlm_stream_denoise). Returns (result, sigma0, sigma1, stats) with stats =
+    (inlm_stream_denoise_grouped; tiles_x as IterativeNLM_GPU.attach_proposal).
+    Returns (result, sigma0, sigma1, stats) with stats =
     {ms, h2d_bytes, d2h_bytes, slabs, halo, slab_depth}."""
     raw = _f32c(raw)
     if out is None:
@@ -406,11 +408,11 @@ def stream_denoise(raw: np.ndarray, params: DenoiseParameters, slab_depth: int =
     s1 = np.zeros(nz, np.float32)
     st = np.zeros(6, np.float64)
     cp = params.to_c()
-    rc = _lib.load().inlm_stream_denoise(_shape_c(raw.shape), C.byref(cp), raw.ctypes.data,
-                                         out.ctypes.data, int(slab_depth),
-                                         net._h if net is not None else None, int(k),
-                                         float(min_mass), s0.ctypes.data, s1.ctypes.data,
-                                         st.ctypes.data)
+    rc = _lib.load().inlm_stream_denoise_grouped(_shape_c(raw.shape), C.byref(cp), raw.ctypes.data,
+                                                 out.ctypes.data, int(slab_depth),
+                                                 net._h if net is not None else None, int(k),
+                                                 float(min_mass), int(tiles_x), s0.ctypes.data,
+                                                 s1.ctypes.data, st.ctypes.data)
     _lib.check(rc, "stream_denoise")
     keys = ("ms", "h2d_bytes", "d2h_bytes", "slabs", "halo", "slab_depth")
     return out, s0, s1, dict(zip(keys, st.tolist()))

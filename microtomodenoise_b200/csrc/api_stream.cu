@@ -43,6 +43,7 @@ struct StreamJob {
     const float* raw_host = nullptr;
     float* out_host = nullptr;
     cudaStream_t main = nullptr;
+    int tiles_x = 1;  // proposal lists per 8^3 tile (1) or per 32 x 8 x 8 block (4)
 
     ~StreamJob() {
         for (auto& kv : pairs)
@@ -85,7 +86,7 @@ int get_pair(StreamJob& J, const inlm_params& p, int depth, inlm_proposal* net, 
         if (rc) return rc;
         CUDA_TRY(dalloc(&sp.stage[j], (size_t)J.plane * depth));
         if (net) {
-            rc = inlm_attach_proposal(sp.d[j], net, k, min_mass);
+            rc = inlm_attach_proposal_grouped(sp.d[j], net, k, min_mass, J.tiles_x);
             if (rc) return rc;
         }
     }
@@ -99,7 +100,16 @@ extern "C" int inlm_stream_denoise(const int shape[3], const inlm_params* p, con
                                    float* out_host, int slab_depth, inlm_proposal* net, int k,
                                    float min_mass, float* sigma0_out, float* sigma1_out,
                                    double* stats) {
+    return inlm_stream_denoise_grouped(shape, p, raw_host, out_host, slab_depth, net, k, min_mass, 1,
+                                       sigma0_out, sigma1_out, stats);
+}
+
+extern "C" int inlm_stream_denoise_grouped(const int shape[3], const inlm_params* p,
+                                           const float* raw_host, float* out_host, int slab_depth,
+                                           inlm_proposal* net, int k, float min_mass, int tiles_x,
+                                           float* sigma0_out, float* sigma1_out, double* stats) {
     if (!shape || !p || !raw_host || !out_host) return fail(INLM_ERR_ARG, "null argument");
+    if (tiles_x != 1 && tiles_x != 4) return fail(INLM_ERR_ARG, "tiles_x must be 1 or 4");
     if (slab_depth < 1) return fail(INLM_ERR_ARG, "slab depth must be >= 1");
     if (p->noise_mode != INLM_NOISE_GLOBAL && p->noise_mode != INLM_NOISE_ZADAPTIVE &&
         p->noise_mode != INLM_NOISE_MANUAL)
@@ -110,6 +120,7 @@ extern "C" int inlm_stream_denoise(const int shape[3], const inlm_params* p, con
     const bool manual = p->noise_mode == INLM_NOISE_MANUAL;
     CUDA_TRY(cudaSetDevice(p->device_id));
     StreamJob J;
+    J.tiles_x = tiles_x;
     for (int i = 0; i < 3; i++) J.shape[i] = shape[i];
     J.plane = (long long)shape[0] * shape[1];
     J.raw_host = raw_host;

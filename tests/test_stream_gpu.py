@@ -11,11 +11,11 @@ from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, stream_de
 pytestmark = pytest.mark.gpu
 
 
-def in_memory(raw, p, net=None, k=0, min_mass=0.0):
+def in_memory(raw, p, net=None, k=0, min_mass=0.0, tiles_x=1):
     g = IterativeNLM_GPU()
     g.configure_device(raw.shape, p)
     if net is not None:
-        g.attach_proposal(net, k, min_mass)
+        g.attach_proposal(net, k, min_mass, tiles_x=tiles_x)
     out, s0, s1 = g.denoise(raw)
     g.free_device()
     return out, s0, s1
@@ -61,5 +61,23 @@ def test_stream_learned_proposal(gpu, port):
     want, _, _ = in_memory(raw, p, net, 40, 0.0)
     got, _, _, st = stream_denoise(raw, p, slab_depth=8, net=net, k=40, min_mass=0.0)
     assert st["halo"] >= 16
+    assert np.array_equal(got, want)
+    net.close()
+
+
+def test_stream_grouped_proposal(gpu, port):
+    """Per-32x8x8-block lists: slabs split z only, so the streamed job equals
+    the in-memory one with the same grouping."""
+    from microtomodenoise_b200.proposal import ProposalNet
+    from oracle.oracle import FilterParams
+    from test_proposal_gpu import rand_params
+    raw = synth.small_case((48, 40, 72), seed=8)
+    p = DenoiseParameters(radius_patchspace=(1, 1, 1), radius_searchspace=(3, 3, 3),
+                          noise_mode="global", noise_seed=2, precision="f16")
+    S = len(port.search_offsets(FilterParams(search_radius=(3, 3, 3), patch_radius=(1, 1, 1))))
+    net = ProposalNet(S)
+    net.set_params(rand_params(S, 12))
+    want, _, _ = in_memory(raw, p, net, 40, 0.0, tiles_x=4)
+    got, _, _, st = stream_denoise(raw, p, slab_depth=16, net=net, k=40, min_mass=0.0, tiles_x=4)
     assert np.array_equal(got, want)
     net.close()
