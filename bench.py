@@ -424,7 +424,8 @@ def run_large_workload(args):
     learned1024: float32 1024x1024x512 grain pack (noise 0.05 blurred 1, no
       rings), patch r3 search r7 (1326 offsets), 4 iterations, global noise:
       the whole job in plain FP32, FP16 full search, and learned + FP16 with
-      k = 256 per 8^3 tile (fallback below 0.95 predicted kept mass, and none).
+      k = 896 per 32x8x8 block (no fallback) and k = 256 per 8^3 tile with
+      fallback below 0.95 predicted kept mass.
     stream2048: a 2048x2048xZ slab stack (Z = --stream-depth) of the grain pack
       with noise sigma drifting 0.02 -> 0.08 along z (blur 1) and rings of
       amplitude 0.03, z-adaptive noise, patch r3 search r7, 4 iterations, held
@@ -450,8 +451,8 @@ def run_large_workload(args):
     vox = float(np.prod(shape)) * ITERS
     res["config"] = {"shape_xyz": [shape[2], shape[1], shape[0]], "patch_radius": 3,
                      "search_radius": 7, "offsets": 1326, "iterations": ITERS}
-    forms = [("f32", "f32", None), ("fp16", "f16", None), ("learned_fp16_k256_mass095", "f16", (256, 0.95)),
-             ("learned_fp16_k256", "f16", (256, 0.0))]
+    forms = [("f32", "f32", None), ("fp16", "f16", None), ("learned_fp16_k896_t4", "f16", (896, 0.0, 4)),
+             ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
     if args.k_list:
         # a sweep of k (no fallback; k@t: one list per t 8^3 tiles along x)
         # beside plain FP32 and FP16 full search
