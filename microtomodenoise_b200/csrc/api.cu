@@ -208,6 +208,7 @@ int inlm::noise_prepare(inlm_noise* n, const inlm_params* p, int* nwin, bool* fi
                                      n->stream));
             CUDA_TRY(cudaStreamSynchronize(n->stream));  // host vectors go out of scope
             n->zwindow_cached = p->zwindow;
+            n->mean_window = nz > 0 ? total / nz : 0;
         }
         *nwin = nz;
     } else if (mode == INLM_NOISE_GLOBAL) {
@@ -225,6 +226,7 @@ int inlm::noise_prepare(inlm_noise* n, const inlm_params* p, int* nwin, bool* fi
             CUDA_TRY(cudaMemcpyAsync(n->d_scratch_off, &off, 8, cudaMemcpyHostToDevice, n->stream));
             CUDA_TRY(cudaStreamSynchronize(n->stream));
             n->zwindow_cached = -2;
+            n->mean_window = ns;
         }
         *nwin = 1;
     }
@@ -235,7 +237,7 @@ int inlm::noise_prepare(inlm_noise* n, const inlm_params* p, int* nwin, bool* fi
 // n->d_sigma (device work only).
 int inlm::noise_em_finish(inlm_noise* n, const inlm_params* p, int nwin) {
     CUDA_TRY(launch_noise_em(n->d_patchstd, n->d_windows, nwin, n->d_scratch_off, n->d_assign,
-                             n->d_mean, n->d_sd, n->stream));
+                             n->d_mean, n->d_sd, n->stream, n->mean_window));
     CUDA_TRY(launch_noise_finalize(n->d_mean, n->d_sd, n->shape[2],
                                    p->noise_mode == INLM_NOISE_ZADAPTIVE ? 1 : 0, p->stds_from_mean,
                                    n->d_sigma, n->stream));

@@ -95,6 +95,7 @@ struct inlm_noise {
     float* d_sigma = nullptr;
     int ncalls = 0;
     long long ref_sample_semimanual = 0;
+    long long mean_window = 0;  // average samples per EM window (picks the EM's CTA size)
 };
 
 // Proposal network: FP32 master parameters, BF16 copy, Adam state, training

@@ -68,7 +68,9 @@ struct EmRed {
     long long n1, n2;
 };
 
-// Block-wide sum of (s1, s2, n1, n2) and OR of flag; result broadcast to all.
+// Block-wide sum of (s1, s2, n1, n2) and OR of flag; result broadcast to all
+// NT threads.
+template <int NT>
 __device__ __forceinline__ void block_reduce(EmRed& r, int& flag, EmRed* sh, int* shflag) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -86,7 +88,7 @@ __device__ __forceinline__ void block_reduce(EmRed& r, int& flag, EmRed* sh, int
     }
     __syncthreads();
     if (warp == 0) {
-        constexpr int NW = kEmThreads / 32;
+        constexpr int NW = NT / 32;
         EmRed t = (lane < NW) ? sh[lane] : EmRed{0.0, 0.0, 0, 0};
         int f = (lane < NW) ? shflag[lane] : 0;
 #pragma unroll
@@ -108,21 +110,22 @@ __device__ __forceinline__ void block_reduce(EmRed& r, int& flag, EmRed* sh, int
     __syncthreads();
 }
 
-// Two-cluster EM over values[fs..ls] by one CTA; asg[i] holds sample i's
-// cluster (-1 excluded, 0, 1). Writes out_mean[w], out_sd[w].
+// Two-cluster EM over values[fs..ls] by one CTA of NT threads; asg[i] holds
+// sample i's cluster (-1 excluded, 0, 1). Writes out_mean[w], out_sd[w].
+template <int NT>
 __device__ __forceinline__ void em_window(const float* __restrict__ values, int fs, int ls,
                                           signed char* __restrict__ asg, int w,
                                           float* __restrict__ out_mean,
                                           float* __restrict__ out_sd) {
-    __shared__ EmRed sh[kEmThreads / 32];
-    __shared__ int shflag[kEmThreads / 32];
-    __shared__ float shmin[kEmThreads / 32], shmax[kEmThreads / 32];
+    __shared__ EmRed sh[NT / 32];
+    __shared__ int shflag[NT / 32];
+    __shared__ float shmin[NT / 32], shmax[NT / 32];
     // assignments indexed by sample id
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     // min / max (noiselevel.cpp:384-390)
     float mn = 1e20f, mx = -1e20f;
-    for (int i = fs + tid; i <= ls; i += kEmThreads) {
+    for (int i = fs + tid; i <= ls; i += NT) {
         float v = values[i];
         mn = fminf(mn, v);
         mx = fmaxf(mx, v);
@@ -139,7 +142,7 @@ __device__ __forceinline__ void em_window(const float* __restrict__ values, int 
     __syncthreads();
     mn = 1e20f;
     mx = -1e20f;
-    for (int q = 0; q < kEmThreads / 32; q++) {
+    for (int q = 0; q < NT / 32; q++) {
         mn = fminf(mn, shmin[q]);
         mx = fmaxf(mx, shmax[q]);
     }
@@ -150,7 +153,7 @@ __device__ __forceinline__ void em_window(const float* __restrict__ values, int 
     // initial assignment, zero values excluded (noiselevel.cpp:398-423)
     EmRed r{0.0, 0.0, 0, 0};
     int flag = 0;
-    for (int i = fs + tid; i <= ls; i += kEmThreads) {
+    for (int i = fs + tid; i <= ls; i += NT) {
         float v = values[i];
         signed char a;
         if (v == 0.0f) {
@@ -166,7 +169,7 @@ __device__ __forceinline__ void em_window(const float* __restrict__ values, int 
         }
         asg[i] = a;
     }
-    block_reduce(r, flag, sh, shflag);
+    block_reduce<NT>(r, flag, sh, shflag);
     if (r.n1 > 0) mean1 = __double2float_rn(r.s1 / (double)r.n1);
     if (r.n2 > 0) mean2 = __double2float_rn(r.s2 / (double)r.n2);
     if (r.n1 == 0 && r.n2 == 0) {
@@ -182,7 +185,7 @@ __device__ __forceinline__ void em_window(const float* __restrict__ values, int 
     auto variances = [&](float m1, float m2, float& v1, float& v2) {
         EmRed q{0.0, 0.0, 0, 0};
         int f = 0;
-        for (int i = fs + tid; i <= ls; i += kEmThreads) {
+        for (int i = fs + tid; i <= ls; i += NT) {
             float v = values[i];
             signed char a = asg[i];
             if (a == 0) {
@@ -193,7 +196,7 @@ __device__ __forceinline__ void em_window(const float* __restrict__ values, int 
                 q.s2 += (double)__fmul_rn(d, d);
             }
         }
-        block_reduce(q, f, sh, shflag);
+        block_reduce<NT>(q, f, sh, shflag);
         v1 = __double2float_rn(q.s1 / (double)(n1 > 1 ? n1 : 1));
         v2 = __double2float_rn(q.s2 / (double)(n2 > 1 ? n2 : 1));
     };
@@ -209,7 +212,7 @@ __device__ __forceinline__ void em_window(const float* __restrict__ values, int 
         iters++;
         EmRed q{0.0, 0.0, 0, 0};
         int f = 0;
-        for (int i = fs + tid; i <= ls; i += kEmThreads) {
+        for (int i = fs + tid; i <= ls; i += NT) {
             float v = values[i];
             if (v == 0.0f) continue;
             float p1 = cluster_prob(v, mean1, var1);
@@ -231,7 +234,7 @@ __device__ __forceinline__ void em_window(const float* __restrict__ values, int 
                 q.n1++;
             }
         }
-        block_reduce(q, f, sh, shflag);
+        block_reduce<NT>(q, f, sh, shflag);
         change = f;
         n1 = q.n1;
         n2 = q.n2;
@@ -251,15 +254,16 @@ __device__ __forceinline__ void em_window(const float* __restrict__ values, int 
     }
 }
 
-__global__ void __launch_bounds__(kEmThreads) noise_em_kernel(const float* __restrict__ values,
-                                                             const int2* __restrict__ windows,
-                                                             const long long* __restrict__ scratch_off,
-                                                             signed char* __restrict__ assign_scratch,
-                                                             float* __restrict__ out_mean,
-                                                             float* __restrict__ out_sd) {
+template <int NT>
+__global__ void __launch_bounds__(NT) noise_em_kernel(const float* __restrict__ values,
+                                                      const int2* __restrict__ windows,
+                                                      const long long* __restrict__ scratch_off,
+                                                      signed char* __restrict__ assign_scratch,
+                                                      float* __restrict__ out_mean,
+                                                      float* __restrict__ out_sd) {
     const int w = blockIdx.x;
     const int fs = windows[w].x, ls = windows[w].y;
-    em_window(values, fs, ls, assign_scratch + scratch_off[w] - fs, w, out_mean, out_sd);
+    em_window<NT>(values, fs, ls, assign_scratch + scratch_off[w] - fs, w, out_mean, out_sd);
 }
 
 // ---- allocation-free EM: scratch in file-scope device arrays ----
@@ -287,8 +291,8 @@ __global__ void __launch_bounds__(kEmThreads) noise_em_noalloc_kernel(
     float* __restrict__ out_sd) {
     const int w = blockIdx.x;
     const NoAllocWindow win = windows[w];
-    em_window(values, win.first, win.last, assign_scratch + win.offset - win.first, w, out_mean,
-              out_sd);
+    em_window<kEmThreads>(values, win.first, win.last, assign_scratch + win.offset - win.first, w,
+                          out_mean, out_sd);
 }
 
 // Device addresses of the two arrays, looked up once per device with that
@@ -412,10 +416,16 @@ cudaError_t launch_noise_patchstd(const float* stack, long long pitch_y, long lo
 
 cudaError_t launch_noise_em(const float* values, const int2* windows, int n_windows,
                             const long long* scratch_off, signed char* scratch, float* out_mean,
-                            float* out_sd, cudaStream_t st) {
+                            float* out_sd, cudaStream_t st, long long mean_window) {
     if (n_windows <= 0) return cudaSuccess;
-    noise_em_kernel<<<n_windows, kEmThreads, 0, st>>>(values, windows, scratch_off, scratch,
-                                                      out_mean, out_sd);
+    // long windows (few of them, e.g. a global estimate or a short stack) get
+    // 1024 threads each so one CTA per window still keeps an SM busy
+    if (mean_window >= kEmWideWindow)
+        noise_em_kernel<1024><<<n_windows, 1024, 0, st>>>(values, windows, scratch_off, scratch,
+                                                          out_mean, out_sd);
+    else
+        noise_em_kernel<kEmThreads><<<n_windows, kEmThreads, 0, st>>>(values, windows, scratch_off,
+                                                                      scratch, out_mean, out_sd);
     return cudaGetLastError();
 }
 

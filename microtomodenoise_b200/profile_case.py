@@ -4,6 +4,9 @@
         two iterations of a 512x512x64 grain pack, patch r2 search r5, FP16
         form: iteration 1 with the shipped proposal (k = 112 per 8^3 tile, the
         one-tile-per-CTA kernel), iteration 2 full search (the 32-wide kernel).
+    python -m microtomodenoise_b200.profile_case learned
+        the whole learned + FP16 job (noise estimates, 4 iterations, k = 144
+        per 32x8x8 block) on a 512x512x128 grain pack, for a launch list.
 """
 from __future__ import annotations
 
@@ -33,5 +36,25 @@ def fast_case():
     net.close()
 
 
+def learned_case():
+    import torch
+    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, synth
+    from microtomodenoise_b200.proposal import ProposalNet, default_weights
+    vol = synth.grain_pack_volume((128, 512, 512), seed=0)
+    raw = torch.from_numpy(vol).cuda()
+    out = torch.empty_like(raw)
+    net = ProposalNet.load(default_weights((2, 2, 2), (5, 5, 5)))
+    g = IterativeNLM_GPU()
+    g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=(2, 2, 2),
+                                                    radius_searchspace=(5, 5, 5), precision="f16",
+                                                    noise_mode="z-adaptive", n_samples=100000))
+    g.attach_proposal(net, 144, 0.0, tiles_x=4)
+    g.denoise(raw.data_ptr(), on_device=True, out=out.data_ptr())
+    torch.cuda.synchronize()
+    print("ok", g.describe(), g.proposal_stats())
+    g.free_device()
+    net.close()
+
+
 if __name__ == "__main__":
-    {"fast": fast_case}[sys.argv[1] if len(sys.argv) > 1 else "fast"]()
+    {"fast": fast_case, "learned": learned_case}[sys.argv[1] if len(sys.argv) > 1 else "fast"]()
