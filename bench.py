@@ -61,7 +61,9 @@ METRIC = "voxel-iter/s 512^3 p2 s5 (plain FP32, whole job incl. noise estimates)
 SHAPE = (512, 512, 512)
 PR, SR, ITERS = (2, 2, 2), (5, 5, 5), 4
 S_OFFSETS, P_TAPS = 514, 33
-FLOP_PER_VOXEL_ITER = S_OFFSETS * (2 * P_TAPS + 20)   # algorithmic, see DESIGN.md
+# algorithmic FLOP per voxel-iteration: per offset 2 per weighted tap, 2 for
+# the squared difference, 18 for multiplier, Pade weight, cutoff and sums
+FLOP_PER_VOXEL_ITER = S_OFFSETS * (2 * P_TAPS + 20)
 BYTES_PER_VOXEL_ITER_F32 = 12                          # read raw + prev, write result
 
 
