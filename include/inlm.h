@@ -359,6 +359,21 @@ int inlm_geometry(const inlm_params* p, int nz, int* search_xyz, int* n_search, 
 int inlm_noise_draw_samples(const int shape[3], uint64_t n_samples, int patchsize,
                             int circular_mask_diameter, unsigned int seed, int64_t* out);
 
+/* ---------------- one stack on several GPUs of this process ----------------
+ * The n_gpus mode of IterativeNLM_GPU::Run_GaussianNoise_GPUBlocks
+ * (iternlm_gpu.cu:1732-2115): the inlm_denoise schedule on a host-resident
+ * stack split in z over n_parts sub-volumes, part i on device device_ids[i]
+ * (ids may repeat). Every part owns a run of 8-slice units and keeps halos of
+ * its neighbours' slices, copied device to device after every iteration;
+ * noise estimates gather every part's patch stds and run one EM. The result
+ * equals inlm_denoise's bit for bit in every precision form (no proposal).
+ * Noise modes: global, z-adaptive, manual. sigma0_out / sigma1_out (nullable,
+ * nz floats) as inlm_denoise reports them. Every slab must be at least one
+ * halo deep (8 slices for z padding up to 8). */
+int inlm_denoise_multi(const int shape[3], const inlm_params* p, const float* raw_host,
+                       float* out_host, int n_parts, const int* device_ids, float* sigma0_out,
+                       float* sigma1_out);
+
 /* ---------------- resume ---------------- */
 
 /* Installs a finished iteration's result read back from disk instead of

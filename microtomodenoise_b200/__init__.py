@@ -26,7 +26,7 @@ from . import _lib
 from ._lib import InlmError, InlmParams, NOISE_MODES, PRECISIONS
 
 __all__ = ["DenoiseParameters", "IterativeNLM_GPU", "NoiseLevel", "Batch", "denoise",
-           "stream_denoise", "InlmError"]
+           "denoise_multi", "stream_denoise", "InlmError"]
 
 
 @dataclass
@@ -416,6 +416,24 @@ def stream_denoise(raw: np.ndarray, params: DenoiseParameters, slab_depth: int =
     _lib.check(rc, "stream_denoise")
     keys = ("ms", "h2d_bytes", "d2h_bytes", "slabs", "halo", "slab_depth")
     return out, s0, s1, dict(zip(keys, st.tolist()))
+
+
+def denoise_multi(raw: np.ndarray, params: DenoiseParameters, device_ids, out: Optional[np.ndarray] = None):
+    """The denoise schedule on a host-resident stack split in z over the GPUs
+    device_ids (inlm_denoise_multi; ids may repeat). Returns (result, sigma0,
+    sigma1), equal to denoise()'s."""
+    raw = _f32c(raw)
+    if out is None:
+        out = np.empty(raw.shape, np.float32)
+    nz = raw.shape[0]
+    s0 = np.zeros(nz, np.float32)
+    s1 = np.zeros(nz, np.float32)
+    ids = np.ascontiguousarray(device_ids, np.int32)
+    cp = params.to_c()
+    rc = _lib.load().inlm_denoise_multi(_shape_c(raw.shape), C.byref(cp), raw.ctypes.data, out.ctypes.data,
+                                        len(ids), ids.ctypes.data, s0.ctypes.data, s1.ctypes.data)
+    _lib.check(rc, "denoise_multi")
+    return out, s0, s1
 
 
 def denoise(raw: np.ndarray, params: Optional[DenoiseParameters] = None):

@@ -45,6 +45,7 @@ LIB_SOURCES = [
     "api_stream.cu",
     "color_kernels.cu",
     "api_color.cu",
+    "api_multi.cu",
     "geometry.cpp",
     "sampling.cpp",
     "tiff_io.cpp",
