@@ -373,6 +373,8 @@ int inlm_noise_draw_samples(const int shape[3], uint64_t n_samples, int patchsiz
 int inlm_denoise_multi(const int shape[3], const inlm_params* p, const float* raw_host,
                        float* out_host, int n_parts, const int* device_ids, float* sigma0_out,
                        float* sigma1_out);
+/* Number of CUDA devices this process sees (0 without a driver or device). */
+int inlm_device_count(int* n);
 
 /* ---------------- resume ---------------- */
 

@@ -43,7 +43,7 @@ EXPORTS = (
     "inlm_get_result_slices", "inlm_set_result_slices", "inlm_noise_patchstd_slab",
     "inlm_noise_estimate_from_patchstd", "inlm_rgb_denoise", "inlm_tiff_read_rgb",
     "inlm_tiff_write_rgb", "inlm_attach_proposal_grouped", "inlm_proposal_select_grouped",
-    "inlm_stream_denoise_grouped", "inlm_denoise_multi",
+    "inlm_stream_denoise_grouped", "inlm_denoise_multi", "inlm_device_count",
 )
 
 
@@ -157,6 +157,7 @@ def load(path: str = "") -> C.CDLL:
     L.inlm_stream_denoise.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp,
                                       C.c_int, C.c_float, vp, vp, vp]
     L.inlm_set_result.argtypes = [vp, C.c_int, vp, vp]
+    L.inlm_device_count.argtypes = [C.POINTER(C.c_int)]
     L.inlm_denoise_multi.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp, vp, vp]
     L.inlm_stream_denoise_grouped.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp,
                                               C.c_int, C.c_float, C.c_int, vp, vp, vp]

@@ -245,3 +245,13 @@ extern "C" int inlm_denoise_multi(const int shape[3], const inlm_params* p, cons
     if (sigma1_out) std::copy(s1.begin(), s1.end(), sigma1_out);
     return INLM_OK;
 }
+
+extern "C" int inlm_device_count(int* n) {
+    if (!n) return fail(INLM_ERR_ARG, "null argument");
+    *n = 0;
+    if (cudaGetDeviceCount(n) != cudaSuccess) {
+        cudaGetLastError();
+        *n = 0;
+    }
+    return INLM_OK;
+}

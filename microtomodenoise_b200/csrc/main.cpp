@@ -11,7 +11,8 @@
 // image (and <outdir>/denoise_iterations/<image>_iterNN.tif without
 // --cleanup). Not built: the CPU filter (-gpus 0).
 // Additions: -precision f32|f16, -seed N (noise sample draw), -slab N
-// (z-slab depth when the stack does not fit on the device).
+// (z-slab depth when the stack does not fit on the device), -gpulist a,b,...
+// (the devices of the multi-GPU split; -gpus N takes N devices from -gpu0).
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -138,6 +139,7 @@ int main(int argc, char* argv[]) {
     string inpath = "", outpath = "";
     bool verbose = false;
     int slab_depth = 64;
+    std::vector<int> gpulist;
     protocol::DenoiseParameters params;
     string rootpath;
 
@@ -208,6 +210,18 @@ int main(int argc, char* argv[]) {
         else if (a == "-precision") params.gpu.precision = next();
         else if (a == "-seed") params.noiselevel.seed = (unsigned int)strtoul(next(), nullptr, 10);
         else if (a == "-slab") slab_depth = atoi(next());
+        else if (a == "-gpulist") {
+            // explicit devices of the multi-GPU split, e.g. 0,1,2,3 (may repeat)
+            gpulist.clear();
+            const string v = next();
+            size_t pos = 0;
+            while (pos <= v.size()) {
+                const size_t c = v.find(',', pos);
+                gpulist.push_back(atoi(v.substr(pos, c == string::npos ? string::npos : c - pos).c_str()));
+                if (c == string::npos) break;
+                pos = c + 1;
+            }
+        }
         else if (a == "-h" || a == "-help" || a == "--help") {
             cout << "iterNLM (B200): iterative 3D nonlocal means for tomographic stacks.\n"
                     "usage: iterNLM -i <slice directory | stack.tif> [-o <outdir>] [-iter N] "
@@ -252,6 +266,7 @@ int main(int argc, char* argv[]) {
         cout << "Error! This build filters on the GPU only (-gpus 0 asks for the CPU filter)" << endl;
         return -1;
     }
+    if (gpulist.size() == 1) params.gpu.deviceID = gpulist[0];
     if (shape[2] == 1) {
         params.radius_patchspace[2] = 0;
         params.radius_searchspace[2] = 0;
@@ -310,7 +325,34 @@ int main(int argc, char* argv[]) {
     float *sigma0 = nullptr, *sigma1 = nullptr;
     float* output = (float*)malloc(nstack * sizeof(float));
 
-    if (max_parallelslices == 0) {
+    // several GPUs (-gpus N, the reference's default is 2): the stack split in
+    // z over them, whole job, final iteration saved (as the streamed branch)
+    int n_devices = 0;
+    if (inlm_device_count(&n_devices) != INLM_OK) n_devices = 0;
+    std::vector<int> ids = gpulist;
+    if (ids.empty())
+        for (int i = 0; i < std::min(params.gpu.n_gpus, n_devices); i++)
+            ids.push_back((params.gpu.deviceID + i) % std::max(n_devices, 1));
+    const int n_use = (int)ids.size();
+    const bool multi = n_use > 1 && max_parallelslices > 0 && !params.io.resume &&
+                       params.noiselevel.mode != "semimanual" && shape[2] >= 16 * n_use;
+
+    if (multi) {
+        gpu.free_device();
+        cout << "Processing " << shape[2] << " slices on " << n_use << " GPUs" << endl;
+        inlm_params q = protocol::to_inlm(params);
+        sigma0 = (float*)malloc(shape[2] * sizeof(float));
+        sigma1 = (float*)malloc(shape[2] * sizeof(float));
+        if (protocol::report(inlm_denoise_multi(shape, &q, instack, output, n_use, ids.data(), sigma0, sigma1),
+                             "denoise_multi"))
+            return -2;
+        if (!params.io.cleanup || verbose) {
+            hdcom.SaveNoisefile(sigma0, shape[2], outpath, "noise_vs_slice00");
+            if (params.maxiterations > 1) hdcom.SaveNoisefile(sigma1, shape[2], outpath, "noise_vs_slice01");
+        }
+        params.io.active_outpath = iterdir(params.maxiterations);
+        if (save(output, params.io.active_outpath)) return -1;
+    } else if (max_parallelslices == 0) {
         // the stack exceeds device memory: z-slab streaming of the whole job
         cout << "Data exceed GPU capacity. Streaming slabs of " << slab_depth << " slices" << endl;
         inlm_params q = protocol::to_inlm(params);

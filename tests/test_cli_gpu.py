@@ -140,3 +140,20 @@ def test_cli_fp16_form(gpu, stack):
     want = g.get_result()
     g.free_device()
     assert np.array_equal(got, want)
+
+
+def test_cli_multi_gpu_split(gpu, tmp_path):
+    """-gpulist 0,0: the stack split over two parts (the multi-GPU path on one
+    device; it engages from 16 slices per part); the final iteration equals
+    the single-GPU run."""
+    vol = synth.spheres_volume((40, 32, 36), n_spheres=8, rmin=3, rmax=8, seed=2)
+    tmp = tmp_path
+    tiffio.save_stack(vol, str(tmp / "in"), "slice")
+    args = ["-i", tmp / "in", "-iter", 2, "-search", 3, "-patch", 1, "-noise", "global",
+            "-nsamples", 20000, "-seed", 5]
+    _cli(*args, "-o", tmp / "one", "-gpus", 1)
+    log = _cli(*args, "-o", tmp / "two", "-gpulist", "0,0")
+    assert "on 2 GPUs" in log
+    one = tiffio.read_stack(str(tmp / "one" / "denoise-iteration02"))
+    two = tiffio.read_stack(str(tmp / "two" / "denoise-iteration02"))
+    assert np.array_equal(one, two)
