@@ -12,6 +12,7 @@
 // launches) is captured once in a CUDA graph and replayed.
 #include <array>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -451,8 +452,13 @@ extern "C" int inlm_batch_create(int n, const int* shapes, const inlm_params* pa
             int occ = 0;
             if (batch_kernel_setup(shape, b->d[v]->tcfg.smem_bytes, &occ) != cudaSuccess || occ < 1)
                 return bail(fail(INLM_ERR_CUDA, "occupancy query failed"));
+            // a group's volumes share the patch weights (the kernel reads them
+            // from its first volume's parameters: constant-bank operands)
+            const inlm_denoiser* dv = b->d[v];
             auto it = std::find_if(b->groups.begin(), b->groups.end(), [&](const inlm_batch::Group& g) {
-                return g.shape == shape && g.occ == occ;
+                const inlm_denoiser* d0 = b->d[g.vols[0]];
+                return g.shape == shape && g.occ == occ && d0->geo.taps.size() == dv->geo.taps.size() &&
+                       std::memcmp(d0->targs.w, dv->targs.w, dv->geo.taps.size() * sizeof(float)) == 0;
             });
             if (it == b->groups.end()) {
                 b->groups.push_back(inlm_batch::Group{});

@@ -147,9 +147,13 @@ __device__ __forceinline__ void accumulate_rows_n(const float* __restrict__ D0, 
 constexpr int kOffGroup = 2;
 
 template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED = false>
+// aw supplies the patch weights: a kernel parameter at a fixed offset, so
+// every tap's weight is a constant-bank operand (the batch kernel passes its
+// group's first volume, whose weights every volume of the group shares; read
+// through a runtime volume index they would cost a load per tap).
 __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const TileArgs& a, int bx,
                                               int by, int bz, unsigned char* smem,
-                                              uint32_t parity) {
+                                              uint32_t parity, const TileArgs& aw) {
     using G = TileGeom<RX, RY, RZ, TZ>;
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
     float* prevb = reinterpret_cast<float*>(smem + 128);
@@ -333,7 +337,7 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
         f32x2 d[NO][NP];
         {
             const int ro = rowoff + RZ * G::DPLANE + RY * G::DP;
-            const float w0 = a.w[0];
+            const float w0 = aw.w[0];
 #pragma unroll
             for (int o = 0; o < NO; o++) {
                 float win[16];
@@ -342,7 +346,7 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
                 for (int p = 0; p < NP; p++) d[o][p] = mul_pair(win[RX + 2 * p], win[RX + 2 * p + 1], w0);
             }
         }
-        accumulate_rows_n<RX, RY, RZ, TZ, NO, 0, FUSED>(D0, DSZ, rowoff, d, a);
+        accumulate_rows_n<RX, RY, RZ, TZ, NO, 0, FUSED>(D0, DSZ, rowoff, d, aw);
 #pragma unroll
         for (int o = 0; o < NO; o++)
             if (s + o < a.S) accumulate(d[o], dl[o].y);
@@ -386,7 +390,7 @@ __global__ void __launch_bounds__(32 * TZ, 1)
     }
     __syncthreads();
     tile_f32_body<RX, RY, RZ, TZ, RAW_SMEM, FUSED>(&tm_prev, a, blockIdx.x, blockIdx.y, blockIdx.z, smem,
-                                                  0);
+                                                  0, a);
 }
 
 // Persistent batch kernel: CTAs take (volume, tile) items from a counter
@@ -401,7 +405,7 @@ __device__ __forceinline__ bool batch_item(const BatchParams& bp, int v, int loc
     const int rest = local / a.tiles_x;
     const int by = rest % a.tiles_y;
     const int bz = rest / a.tiles_y;
-    return tile_f32_body<RX, RY, RZ, 8, RAW_SMEM>(&bp.maps[v], a, bx, by, bz, smem, parity);
+    return tile_f32_body<RX, RY, RZ, 8, RAW_SMEM>(&bp.maps[v], a, bx, by, bz, smem, parity, bp.args[0]);
 }
 
 static_assert(sizeof(BatchParams) <= 32764, "batch parameter block exceeds the kernel parameter limit");

@@ -91,3 +91,21 @@ def test_autotune_keeps_results(gpu, port):
     want = port.denoise_f32(raw, FilterParams(search_radius=(3, 3, 3), patch_radius=(2, 2, 2)),
                             sig[None])
     assert np.array_equal(got, want)
+
+
+def test_batch_groups_by_patch_weights(gpu):
+    """Volumes of one patch shape whose weights differ (the distance-weight
+    table with z anisotropy; the CPU table ignores anisotropy) run in separate
+    launch groups: a group's kernel reads the weights of its first volume."""
+    cs = [((16, 40, 48), DenoiseParameters(radius_patchspace=(2, 2, 2), radius_searchspace=(3, 3, 3),
+                                           noise_mode="manual", sigma=(0.05, 0.04), z_anisotropy=za,
+                                           weight_table="distweight"))
+          for za in (1.0, 2.0, 1.0, 0.5)]
+    raws = [synth.small_case(s, seed=90 + i) for i, (s, _) in enumerate(cs)]
+    b = Batch([s for s, _ in cs], [p for _, p in cs])
+    desc = b.describe()
+    assert desc.count("persistent nlm_batch_f32<p222") == 3, desc
+    outs = b.run(raws)
+    for i, ((s, p), raw, got) in enumerate(zip(cs, raws, outs)):
+        assert np.array_equal(got, single(raw, p)), f"volume {i} z_anisotropy {p.z_anisotropy}"
+    b.close()
