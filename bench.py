@@ -398,10 +398,107 @@ def cpu_reference_rate(vol, target_s=15.0, threads=None):
     return rate, info
 
 
+PUBLISHED = {"job_s": 8.5, "hardware": "Tesla V100 (sm_70)", "iterations": 4,
+             "shape_xyz": [256, 256, 256], "patch_radius": 1, "search_radius": 10, "nslices": 11,
+             "source": "iterNLM_v0.3 README benchmark figure caption (4 iterations, 256^3)"}
+
+
+def reference_gpu_rates(vol):
+    """The reference's own GPU class (Denoiser/iternlm_gpu.cu compiled
+    unmodified for sm_100a, oracle/_ref/libiternlm_gpu_ref.so) on this GPU,
+    driven as the reference driver drives its whole-stack path: iteration 2's
+    Run_GaussianNoise (reflective padding, the patch kernel and, as shipped,
+    apply_filter_generic after it; the call synchronises) by host wall time.
+    Two cases: a 512x512x128 slab (z 192..319) of the headline volume at p2
+    s5, and the published configuration (256^3 grain pack, p1, s10, 11
+    slices: 3102 offsets). Sigma fixed at 0.045."""
+    from microtomodenoise_b200 import synth
+    from oracle.oracle import ReferenceGPU, reference_gpu_available
+    if not reference_gpu_available():
+        return {"unavailable": "oracle/_ref/libiternlm_gpu_ref.so not built (needs the reference tree)"}
+    ref = ReferenceGPU()
+    out = {"kernel": "IterativeNLM_GPU::Run_GaussianNoise as shipped (iternlm_gpu.cu:1651-1728): "
+                     "pad_reflective + apply_filter_patchNNN + apply_filter_generic, sm_100a build"}
+    nz = vol.shape[0]
+    z0 = max(0, nz // 2 - 64)
+    cases = [("headline_slab", np.ascontiguousarray(vol[z0:z0 + 128]), PR[0], SR[0],
+              f"512x512x128 slab (z {z0}..{z0 + 127}) of the 512^3 grain pack, p2 s5 (514 offsets)"),
+             ("published_config", synth.grain_pack_volume((256, 256, 256), seed=0), 1, 10,
+              "256^3 grain pack, p1 s10, 11 slices (3102 offsets)")]
+    for name, sub, pr, sr, desc in cases:
+        sig = np.full((2, sub.shape[0]), 0.045, np.float32)
+        try:
+            _, ms = ref.denoise(sub, pr, sr, sig, want_result=False)
+        except Exception as e:
+            out[name] = {"error": str(e)[:200]}
+            continue
+        out[name] = {"workload": desc, "iteration_ms": float(ms[1]), "first_iteration_ms": float(ms[0]),
+                     "value": float(sub.size / (ms[1] / 1e3)), "unit": "voxel-iter/s"}
+    return out
+
+
+def run_published_config(local, stream):
+    """This build's exact FP32 whole job on the configuration of the
+    reference's only published GPU figure: 256^3, patch r1, search r10, 11
+    slices (3102 offsets), 4 iterations, z-adaptive noise (the reference
+    defaults), on a seeded 256^3 grain pack; device-timed and end to end from
+    pinned host buffers. The published 8.5 s is the reference program's wall
+    time on a V100."""
+    import torch
+    import ctypes as C
+    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, _lib, synth
+    vol = synth.grain_pack_volume((256, 256, 256), seed=0)
+    dp = DenoiseParameters(radius_patchspace=(1, 1, 1), radius_searchspace=(10, 10, 10), nslices=11,
+                           maxiterations=4, alpha=0.5, noise_mode="z-adaptive", zwindow=100,
+                           n_samples=100000, noise_seed=0, deviceID=local)
+    g = IterativeNLM_GPU()
+    g.configure_device(vol.shape, dp)
+    g.set_stream(stream.cuda_stream)
+    raw_dev = torch.from_numpy(vol).cuda()
+    out_dev = torch.empty_like(raw_dev)
+    host_raw = torch.from_numpy(vol).pin_memory()
+    host_out = torch.empty(vol.shape, dtype=torch.float32).pin_memory()
+    s0 = np.zeros(256, np.float32)
+    s1 = np.zeros(256, np.float32)
+    L = _lib.load()
+    for _ in range(2):
+        g.denoise(raw_dev.data_ptr(), on_device=True, out=out_dev.data_ptr())
+    g.filter_kernel_ms()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(2):
+        g.denoise(raw_dev.data_ptr(), on_device=True, out=out_dev.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    job_ms = e0.elapsed_time(e1) / 2
+    kms, _ = g.filter_kernel_ms()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(2):
+        _lib.check(L.inlm_denoise(g._h, host_raw.data_ptr(), host_out.data_ptr(), 0, s0.ctypes.data,
+                                  s1.ctypes.data), "denoise")
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1) / 2
+    desc = g.describe()
+    g.free_device()
+    vox_iters = float(vol.size) * 4
+    return {"workload": "256^3 grain pack, patch r1 (7 taps), search r10 with 11 slices (3102 offsets), "
+                        "4 iterations, alpha 0.5, z-adaptive noise (window 100, 1e5 samples)",
+            "kernel": desc, "job_ms": job_ms, "e2e_job_ms": e2e_ms, "filter_ms_per_iteration": kms,
+            "value": vox_iters / (e2e_ms / 1e3), "unit": "voxel-iter/s",
+            "published_reference": dict(PUBLISHED, value=vox_iters / PUBLISHED["job_s"]),
+            "speedup_vs_published_e2e": PUBLISHED["job_s"] * 1e3 / e2e_ms}
+
+
 def run_reference_arm(args, rank):
     if rank != 0:
         return
     vol = make_volume()
+    if args.reference_gpu_only:
+        print(json.dumps({"impl": "reference", "reference_gpu": reference_gpu_rates(vol)}), flush=True)
+        return
     threads = os.cpu_count()
     rates = []
     for i in range(args.warmup + args.steps):
@@ -410,13 +507,18 @@ def run_reference_arm(args, rank):
             rates.append(rate)
     value = float(np.mean(rates))
     info["value"] = value
+    try:  # the reference's own GPU class on this GPU, beside the CPU timing
+        ref_gpu = reference_gpu_rates(vol)
+    except Exception as e:
+        ref_gpu = {"error": str(e)[:200]}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "voxel-iter/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded grain pack)",
             "config": workload_config(), "cpu_baseline": info,
             "e2e": {"value": value, "unit": "voxel-iter/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "reference_gpu": ref_gpu}
     print(json.dumps(line), flush=True)
 
 
@@ -572,6 +674,9 @@ def main():
     ap.add_argument("--form-steps", type=int, default=2)
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-published", action="store_true")
+    ap.add_argument("--reference-gpu-only", action="store_true",
+                    help="--impl reference: only the reference GPU class timings")
     ap.add_argument("--workload", default="grain512",
                     choices=["grain512", "learned1024", "stream2048", "rgb4k"],
                     help="grain512: the headline bench line; the others: one-step "
@@ -724,6 +829,11 @@ def main():
             line["forms"] = run_forms(vol, clean, sig_iters, value, args, local, stream)
         except Exception as e:
             line["forms"] = {"error": str(e)[:300]}
+    if rank == 0 and world == 1 and not args.no_published:
+        try:
+            line["published_config"] = run_published_config(local, stream)
+        except Exception as e:
+            line["published_config"] = {"error": str(e)[:300]}
     if rank == 0 and world == 1 and not args.no_batch:
         try:
             line["batch"] = run_batch(args, local)

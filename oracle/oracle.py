@@ -7,6 +7,11 @@
   from its unmodified sources (oracle/_ref/libiternlm_ref.so, built by
   ``make -C oracle ref`` where the reference tree exists). Used to pin the port
   and as the timed CPU baseline.
+* ``ReferenceGPU``: the reference's own GPU class (Denoiser/iternlm_gpu.cu)
+  compiled unmodified for sm_100a (oracle/_ref/libiternlm_gpu_ref.so, built by
+  ``make -C oracle ref_gpu``): the reference GPU kernel timed beside the
+  product. Its expf weights and its generic-kernel fall-through make it differ
+  from the CPU reference, so it is a timing baseline, not a checker.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module. The product (microtomodenoise_b200) never does.
@@ -22,6 +27,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "libinlm_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libiternlm_ref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libiternlm_gpu_ref.so")
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -333,6 +339,38 @@ class _RefRgbParams(C.Structure):
 
 def reference_available() -> bool:
     return os.path.exists(REF_SO)
+
+
+def reference_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_SO)
+
+
+class ReferenceGPU:
+    """The reference's own GPU class, whole-stack path (iternlm_gpu.cu:1651-1728)
+    on device 0, driven as the reference driver drives it."""
+
+    def __init__(self, path: str = REF_GPU_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref_gpu`")
+        L = self.lib = C.CDLL(path)
+        L.ref_gpu_run.restype = C.c_int
+        L.ref_gpu_run.argtypes = [C.c_int * 3, C.c_int, C.c_int, C.c_int, C.c_float, _f32p, _f32p,
+                                  C.c_int, C.c_void_p, _f64p]
+
+    def denoise(self, raw: np.ndarray, patch_radius: int, search_radius: int, sigmas: np.ndarray,
+                nslices: int = 11, beta: float = 1.0, want_result: bool = True):
+        """Runs len(sigmas) iterations; returns (result or None, ms per
+        Run_GaussianNoise call). Raises if the stack does not fit in one pass."""
+        raw = np.ascontiguousarray(raw, np.float32)
+        sig = np.ascontiguousarray(np.atleast_2d(sigmas), np.float32)
+        iters = sig.shape[0]
+        out = np.empty_like(raw) if want_result else None
+        ms = np.zeros(iters, np.float64)
+        rc = self.lib.ref_gpu_run(_shape3(raw), patch_radius, search_radius, nslices, beta, raw.ravel(),
+                                  sig.ravel(), iters, out.ctypes.data if want_result else None, ms)
+        if rc != 0:
+            raise RuntimeError(f"reference GPU run failed: {rc}")
+        return out, ms
 
 
 class Reference:
