@@ -451,6 +451,7 @@ static void denoiser_free(inlm_denoiser* d) {
     cudaFree(d->d_mult);
     cudaFree(d->d_err);
     cudaFree(d->d_search_delta);
+    cudaFree(d->d_group_zb);
     cudaFree(d->d_search_off);
     cudaFree(d->d_patch_off);
     cudaFree(d->d_weights);
@@ -495,6 +496,28 @@ static int raw_plane_pitch(int rpx, int rby) {
 // Tiled FP32 configuration for one candidate (CTA depth tz, raw staged in
 // shared memory or read from global): tables, kernel arguments, TMA map.
 // *ok = false when the candidate does not apply or does not fit.
+// Raw-slab schedule: for each group of kOffGroup consecutive offsets, the z
+// offset from which the TZ + 1 staged raw planes start. The search list must
+// run z-major (the reference order does: iternlm_prepare.cpp:102-150), so a
+// group spans at most two z offsets; the slab moves only when a group needs a
+// plane past it. Returns false if the list is not z-major or the slab would
+// not be smaller than the whole box.
+static bool raw_slab_table(const Geometry& g, int szc, int tz, std::vector<int>* out) {
+    const int S = (int)g.search.size();
+    if (S == 0 || tz + 1 >= tz + 2 * szc) return false;
+    for (int s = 1; s < S; s++)
+        if (g.search[s].z < g.search[s - 1].z) return false;
+    out->clear();
+    int zb = g.search[0].z;
+    for (int s = 0; s < S; s += kOffGroup) {
+        const int lo = g.search[s].z, hi = g.search[std::min(s + kOffGroup, S) - 1].z;
+        if (hi - lo > 1) return false;
+        if (lo < zb || hi > zb + 1) zb = lo;
+        out->push_back(zb);
+    }
+    return true;
+}
+
 int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     const Geometry& g = d->geo;
     const int* pr = g.patch_radius;
@@ -541,7 +564,24 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
     TileConfig tc{pr[0], pr[1], pr[2], tz, raw_smem, 0, fused};
     size_t sm = tile_smem_bytes(tc, a);
+    a.raw_slab = 0;
+    a.group_zb = nullptr;
+    std::vector<int> zb;
+    if (raw_smem && tz == 8 && (sm == 0 || sm > (size_t)smem_max) && raw_slab_table(g, a.szc, tz, &zb)) {
+        // the whole raw box does not fit: stage TZ + 1 planes per z offset pair
+        a.rbz = tz + 1;
+        a.raw_slab = 1;
+        tc.raw_slab = true;
+        sm = tile_smem_bytes(tc, a);
+    }
     if (sm == 0 || sm > (size_t)smem_max) return INLM_OK;
+    if (a.raw_slab) {
+        cudaFree(d->d_group_zb);
+        d->d_group_zb = nullptr;
+        CUDA_TRY(dalloc(&d->d_group_zb, zb.size()));
+        CUDA_TRY(cudaMemcpy(d->d_group_zb, zb.data(), zb.size() * sizeof(int), cudaMemcpyHostToDevice));
+        a.group_zb = d->d_group_zb;
+    }
     tc.smem_bytes = sm;
     a.tiles_x = (d->shape[0] + kTX - 1) / kTX;
     a.tiles_y = (d->shape[1] + kTY - 1) / kTY;
@@ -1173,7 +1213,7 @@ extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
         snprintf(buf, len,
                  "nlm_tile_f32%s<%d,%d,%d> tz=%d raw_%s smem=%zu S=%zu P=%zu weights=%s pad=%d,%d,%d",
                  d->tcfg.fused ? "_fused" : "", d->tcfg.rx, d->tcfg.ry, d->tcfg.rz, d->tcfg.tz,
-                 d->tcfg.raw_smem ? "smem" : "global",
+                 d->tcfg.raw_smem ? (d->targs.raw_slab ? "slab" : "smem") : "global",
                  d->tcfg.smem_bytes, g.search.size(), g.taps.size(),
                  g.specialised && d->p.weight_table == INLM_WEIGHTS_CPU ? "cpu-table" : "distweight",
                  g.pad[0], g.pad[1], g.pad[2]);

@@ -144,6 +144,7 @@ struct inlm_denoiser {
     float* d_mult = nullptr;
     int* d_err = nullptr;
     int2* d_search_delta = nullptr;
+    int* d_group_zb = nullptr;  // raw-slab form: first z offset of the slab per offset group
     long long* d_search_off = nullptr;
     long long* d_patch_off = nullptr;
     float* d_weights = nullptr;

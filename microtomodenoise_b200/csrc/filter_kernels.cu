@@ -175,12 +175,8 @@ __device__ __forceinline__ void accumulate_rows_n(const float* __restrict__ D0, 
     }
 }
 
-// Offsets per barrier step of the exact kernel (D buffers in shared memory).
-// Two measured 3.4% faster than one (eight independent chains per thread);
-// three gave 0.3% more for 21 KB more shared memory at patch radius 2.
-constexpr int kOffGroup = 2;
 
-template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED = false>
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED = false, bool SLAB = false>
 // aw supplies the patch weights: a kernel parameter at a fixed offset, so
 // every tap's weight is a constant-bank operand (the batch kernel passes its
 // group's first volume, whose weights every volume of the group shares; read
@@ -189,6 +185,7 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
                                               int by, int bz, unsigned char* smem,
                                               uint32_t parity, const TileArgs& aw) {
     using G = TileGeom<RX, RY, RZ, TZ>;
+    static_assert(!SLAB || RAW_SMEM, "the raw slab is a shared-memory staging");
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
     float* prevb = reinterpret_cast<float*>(smem + 128);
     const int pplane = a.pbx * a.pby;
@@ -214,12 +211,12 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
         // prev box starts at the tile origin in padded coordinates (x aligned to 32)
         tma_load_3d(prevb, tm_prev, X0, Y0, Z0, bar);
     }
-    if (RAW_SMEM) {
-        // raw over tile + search halo, coalesced rows re-pitched while the
-        // TMA load is in flight; positions past the volume read the zeroed
-        // slack planes behind it and are never used
+    // raw over tile + search halo, planes [zoff, zoff + rbz) of the raw box,
+    // coalesced rows re-pitched; positions past the volume read the zeroed
+    // slack planes behind it and are never used
+    auto stage_raw = [&](int zoff) {
         const int rb_n = a.rbx * a.rby * a.rbz;
-        const float* rsrc = a.raw_pad + (long long)(Z0 + RZ) * a.gpitch_z +
+        const float* rsrc = a.raw_pad + (long long)(Z0 + RZ + zoff) * a.gpitch_z +
                             (long long)(Y0 + RY) * a.gpitch_y + X0;
         for (int i = tid; i < rb_n; i += G::NT) {
             int xx = i % a.rbx;
@@ -229,6 +226,16 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
             rawb[zz * a.rplane + yy * rpx + xx] =
                 __ldg(rsrc + (long long)zz * a.gpitch_z + (long long)yy * a.gpitch_y + xx);
         }
+    };
+    // Slab form (the whole raw box does not fit beside the prev box): the
+    // offsets run z-major, so a group of offsets reads at most two z offsets;
+    // shared memory holds the TZ + 1 planes from z offset slab_zb on and is
+    // restaged when a group needs later planes.
+    int slab_zb = 0;
+    if (RAW_SMEM) {
+        // staged while the prev box's TMA load is in flight
+        if (SLAB) slab_zb = __ldg(&a.group_zb[0]);
+        stage_raw(SLAB ? a.szc + slab_zb : 0);
     }
 
     // Each thread owns NQ fixed column pairs of the D volume (rows have an
@@ -271,16 +278,13 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
     const f32x2 m2 = splat2(m);
     const int rowoff = k * G::DPLANE + j * G::DP + x0;
 
-    int rbase;
-    long long gbase;
-    if (RAW_SMEM) {
-        rbase = (a.szc + k) * a.rplane + (a.syr + j) * rpx + (RX + a.sxr + x0);
-        gbase = 0;
-    } else {
-        rbase = 0;
-        gbase = (long long)(Z0 + k + a.pz) * a.gpitch_z + (long long)(Y0 + j + a.py) * a.gpitch_y +
-                (X0 + x0 + a.px);
-    }
+    // raw positions: rbase + delta in raw-box coordinates (shared memory; in
+    // the slab form shifted by the slab's first plane), gbase + delta in the
+    // padded volume (global)
+    const int rbase_box = RAW_SMEM ? (a.szc + k) * a.rplane + (a.syr + j) * rpx + (RX + a.sxr + x0) : 0;
+    int rbase = rbase_box - (SLAB ? (a.szc + slab_zb) * a.rplane : 0);
+    const long long gbase = (long long)(Z0 + k + a.pz) * a.gpitch_z +
+                            (long long)(Y0 + j + a.py) * a.gpitch_y + (X0 + x0 + a.px);
 
     constexpr int NP = kVoxPerThread / 2;
     f32x2 acc[NP], wsum[NP];
@@ -366,6 +370,17 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
 #pragma unroll
     for (int o = 0; o < NO; o++) dl[o] = __ldg(&a.search_delta[min(o, a.S - 1)]);
     for (int s = 0; s < a.S; s += NO) {
+        if (SLAB) {
+            // every thread reads the same entry: a uniform branch; the
+            // previous group's raw reads ended at its closing barrier, and
+            // the barrier after phase A publishes the new planes
+            const int zb = __ldg(&a.group_zb[s / NO]);
+            if (zb != slab_zb) {
+                slab_zb = zb;
+                stage_raw(a.szc + zb);
+                rbase = rbase_box - (a.szc + zb) * a.rplane;
+            }
+        }
         int2 dln[NO];
 #pragma unroll
         for (int o = 0; o < NO; o++) dln[o] = __ldg(&a.search_delta[min(s + NO + o, a.S - 1)]);
@@ -401,7 +416,7 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
         for (int r = 0; r < kVoxPerThread; r++) {
             int x = X0 + x0 + r;
             if (x < a.nx) {
-                float raw0 = RAW_SMEM ? rawb[rbase + r] : __ldg(&a.raw_pad[gbase + r]);
+                float raw0 = (RAW_SMEM && !SLAB) ? rawb[rbase + r] : __ldg(&a.raw_pad[gbase + r]);
                 const float2 acp = unpack2(acc[r / 2]), wsp = unpack2(wsum[r / 2]);
                 float ac = (r & 1) ? acp.y : acp.x;
                 float ws = (r & 1) ? wsp.y : wsp.x;
@@ -420,7 +435,7 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
     return true;
 }
 
-template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED>
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED, bool SLAB>
 __global__ void __launch_bounds__(32 * TZ, 1)
     nlm_tile_f32_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -430,8 +445,8 @@ __global__ void __launch_bounds__(32 * TZ, 1)
         fence_mbar_init();
     }
     __syncthreads();
-    tile_f32_body<RX, RY, RZ, TZ, RAW_SMEM, FUSED>(&tm_prev, a, blockIdx.x, blockIdx.y, blockIdx.z, smem,
-                                                  0, a);
+    tile_f32_body<RX, RY, RZ, TZ, RAW_SMEM, FUSED, SLAB>(&tm_prev, a, blockIdx.x, blockIdx.y, blockIdx.z,
+                                                        smem, 0, a);
 }
 
 // Persistent batch kernel: CTAs take (volume, tile) items from a counter
@@ -575,11 +590,11 @@ static size_t smem_bytes_for(const TileArgs& a) {
     return 128 + 4 * (pb + rb + kOffGroup * d);
 }
 
-template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED = false>
+template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED = false, bool SLAB = false>
 static cudaError_t launch_inst(const CUtensorMap* tmp, const CUtensorMap* tmr, const TileArgs& a,
                                int tiles_z, size_t smem, cudaStream_t st) {
     (void)tmr;
-    auto kern = nlm_tile_f32_kernel<RX, RY, RZ, TZ, RAW_SMEM, FUSED>;
+    auto kern = nlm_tile_f32_kernel<RX, RY, RZ, TZ, RAW_SMEM, FUSED, SLAB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
@@ -588,7 +603,7 @@ static cudaError_t launch_inst(const CUtensorMap* tmp, const CUtensorMap* tmr, c
 }
 
 int batch_kind(const TileConfig& c) {
-    if (c.tz != 8) return -1;
+    if (c.tz != 8 || c.raw_slab) return -1;  // the slab form runs as its own launch
     if (c.rx == 1 && c.ry == 1 && c.rz == 1) return c.raw_smem ? kBatchP111Smem : kBatchP111Glob;
     if (c.rx == 2 && c.ry == 2 && c.rz == 2) return c.raw_smem ? kBatchP222Smem : kBatchP222Glob;
     if (c.rx == 3 && c.ry == 3 && c.rz == 3) return c.raw_smem ? kBatchP333Smem : kBatchP333Glob;
@@ -658,6 +673,12 @@ cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,
                                cudaStream_t st) {
 #define X(A, B, C)                                                                             \
     if (c.rx == A && c.ry == B && c.rz == C) {                                                 \
+        if (c.raw_slab && c.tz == 8 && c.raw_smem)                                             \
+            return c.fused ? launch_inst<A, B, C, 8, true, true, true>(tm_prev, tm_raw, a, tiles_z,  \
+                                                                      c.smem_bytes, st)        \
+                           : launch_inst<A, B, C, 8, true, false, true>(tm_prev, tm_raw, a, tiles_z, \
+                                                                       c.smem_bytes, st);      \
+        if (c.raw_slab) return cudaErrorInvalidConfiguration;                                  \
         if (c.fused && c.tz == 8 && c.raw_smem)                                                \
             return launch_inst<A, B, C, 8, true, true>(tm_prev, tm_raw, a, tiles_z, c.smem_bytes, st); \
         if (c.fused && c.tz == 8 && !c.raw_smem)                                               \

@@ -24,6 +24,9 @@ def cases():
                                         noise_mode="global", noise_seed=4)),
         ((12, 64, 64), DenoiseParameters(radius_patchspace=(1, 1, 1), radius_searchspace=(5, 5, 5),
                                          noise_mode="global", maxiterations=2, noise_seed=5)),
+        # raw staged as a slab (search radius 10): its own launch inside the graph
+        ((14, 36, 40), DenoiseParameters(radius_patchspace=(1, 1, 1), radius_searchspace=(10, 10, 10),
+                                         noise_mode="global", noise_seed=6)),
     ]
 
 

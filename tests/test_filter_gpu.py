@@ -73,6 +73,24 @@ def test_filter_bit_exact_vs_oracle_odd_sizes(gpu, port, shape, pr, sr):
     assert np.array_equal(got, want), desc
 
 
+@pytest.mark.parametrize("shape,pr,sr", [((20, 40, 48), (1, 1, 1), (10, 10, 10)),
+                                         ((18, 33, 45), (2, 2, 2), (7, 7, 7)),
+                                         ((16, 24, 40), (1, 1, 2), (9, 9, 9)),
+                                         ((9, 30, 37), (1, 1, 1), (10, 10, 10))])
+def test_raw_slab_bit_exact(gpu, port, shape, pr, sr):
+    """Search radii whose whole raw box does not fit beside the prev box stage
+    raw as a slab of TZ + 1 planes per pair of z offsets, restaged as the
+    z-major offsets move on: bit-identical to the reference like every form
+    (nz = 9: a volume shallower than the slab's reach)."""
+    raw = synth.small_case(shape, seed=sum(shape) + 3)
+    sig = np.stack([np.full(shape[0], 0.06, np.float32),
+                    np.linspace(0.03, 0.08, shape[0], dtype=np.float32)])
+    got, desc = run_gpu(raw, pr, sr, sig)
+    assert "raw_slab" in desc, desc
+    want = port.denoise_f32(raw, FilterParams(search_radius=sr, patch_radius=pr), sig, all_iters=True)
+    assert np.array_equal(got, want), desc
+
+
 def test_distweight_table_and_generic_kernel(gpu, port):
     raw = synth.small_case((12, 16, 20), seed=4)
     sig = np.full((2, 12), 0.06, np.float32)
@@ -179,7 +197,8 @@ def test_512_cube_p2s5_sampled_voxels(gpu, port):
 @pytest.mark.parametrize("pr,sr,shape", [((1, 1, 1), (3, 3, 3), (24, 40, 56)),
                                          ((2, 2, 2), (3, 3, 3), (20, 33, 47)),
                                          ((3, 3, 3), (2, 2, 2), (16, 40, 40)),
-                                         ((2, 2, 1), (4, 4, 4), (24, 48, 48))])
+                                         ((2, 2, 1), (4, 4, 4), (24, 48, 48)),
+                                         ((2, 2, 2), (7, 7, 7), (18, 40, 44))])  # raw slab
 def test_fused_form_tolerance(gpu, port, pr, sr, shape):
     """precision="f32_fma": the tiled kernel with fused multiply-adds, a
     Horner Pade and a fast division. Tolerance, written here: relative error
