@@ -214,7 +214,7 @@ struct inlm_batch {
     // persistent launch groups: volumes of one patch shape whose shared
     // memory allows the same number of CTAs per SM
     struct Group {
-        int shape = 0;  // batch kind: patch radius kind / 2 + 1, raw placement kind % 2
+        int shape = 0;  // batch kind (BatchKind: patch radius and raw placement)
         int occ = 1;    // CTAs per SM
         size_t smem = 0;
         int ctas = 0;
@@ -439,7 +439,7 @@ extern "C" int inlm_batch_create(int n, const int* shapes, const inlm_params* pa
     nb = (int)b->order.size();
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    for (int shape = 0; shape < 6; shape++) {
+    for (int shape = 0; shape < kBatchKinds; shape++) {
         size_t smax = 0;
         for (int v : b->order)
             if (b->kind[v] == shape) smax = std::max(smax, b->d[v]->tcfg.smem_bytes);
@@ -563,19 +563,21 @@ extern "C" int inlm_batch_run(inlm_batch* b, const float* const* raws, float* co
 
 extern "C" int inlm_batch_describe(inlm_batch* b, char* buf, size_t len) {
     if (!b || !buf || !len) return fail(INLM_ERR_ARG, "null argument");
-    static const char* kinds[] = {"p111/raw_smem", "p111/raw_global", "p222/raw_smem",
-                                  "p222/raw_global", "p333/raw_smem", "p333/raw_global"};
+    static const char* kinds[kBatchKinds] = {"p111/raw_smem", "p111/raw_global", "p222/raw_smem",
+                                             "p222/raw_global", "p333/raw_smem", "p333/raw_global",
+                                             "p111/raw_slab",  "p222/raw_slab",   "p333/raw_slab"};
     std::string s;
     char line[256];
     std::snprintf(line, sizeof line, "graph of %zu nodes; %d volumes\n", b->graph_nodes, b->n);
     s += line;
     for (const auto& g : b->groups) {
-        const int r = g.shape / 2 + 1;
+        const bool slab = g.shape >= kBatchP111Slab;
+        const int r = slab ? g.shape - kBatchP111Slab + 1 : g.shape / 2 + 1;
         std::snprintf(line, sizeof line,
                       "persistent nlm_batch_f32<p%d%d%d, raw_%s>: %d volumes, %d CTAs x 256 threads "
                       "(%d per SM), %zu B shared\n",
-                      r, r, r, g.shape % 2 ? "global" : "smem", (int)g.vols.size(), g.ctas, g.occ,
-                      g.smem);
+                      r, r, r, slab ? "slab" : g.shape % 2 ? "global" : "smem", (int)g.vols.size(), g.ctas,
+                      g.occ, g.smem);
         s += line;
     }
     for (int v = 0; v < b->n; v++) {

@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(32 * TZ, 1)
 // until the batch is done; each volume runs the body of its patch shape and
 // tile configuration (kind). Items are numbered volume by volume in the order
 // the host gives (heaviest tiles first), tiles x-fastest within a volume.
-template <int RX, int RY, int RZ, bool RAW_SMEM>
+template <int RX, int RY, int RZ, bool RAW_SMEM, bool SLAB>
 __device__ __forceinline__ bool batch_item(const BatchParams& bp, int v, int local,
                                            unsigned char* smem, uint32_t parity) {
     const TileArgs& a = bp.args[v];
@@ -461,7 +461,8 @@ __device__ __forceinline__ bool batch_item(const BatchParams& bp, int v, int loc
     const int rest = local / a.tiles_x;
     const int by = rest % a.tiles_y;
     const int bz = rest / a.tiles_y;
-    return tile_f32_body<RX, RY, RZ, 8, RAW_SMEM>(&bp.maps[v], a, bx, by, bz, smem, parity, bp.args[0]);
+    return tile_f32_body<RX, RY, RZ, 8, RAW_SMEM, false, SLAB>(&bp.maps[v], a, bx, by, bz, smem, parity,
+                                                              bp.args[0]);
 }
 
 static_assert(sizeof(BatchParams) <= 32764, "batch parameter block exceeds the kernel parameter limit");
@@ -470,7 +471,7 @@ static_assert(sizeof(BatchParams) <= 32764, "batch parameter block exceeds the k
 // bodies would carry the largest one's registers, shared memory and code for
 // every tile); volumes of any size and search radius. Radius 1 keeps to 128
 // registers so two CTAs fit an SM, as its per-volume kernel does.
-template <int R, bool RAW_SMEM>
+template <int R, bool RAW_SMEM, bool SLAB = false>
 __global__ void __launch_bounds__(256, R == 1 ? 2 : 1)
     nlm_batch_f32_kernel(const __grid_constant__ BatchParams bp) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -490,7 +491,7 @@ __global__ void __launch_bounds__(256, R == 1 ? 2 : 1)
         int v = 0;
         while (v + 1 < bp.n && item >= bp.item_begin[v + 1]) v++;
         const int local = item - bp.item_begin[v];
-        const bool ok = batch_item<R, R, R, RAW_SMEM>(bp, v, local, smem, parity);
+        const bool ok = batch_item<R, R, R, RAW_SMEM, SLAB>(bp, v, local, smem, parity);
         if (!ok) break;  // uniform over the CTA; the error flag is set
         parity ^= 1u;
     }
@@ -603,19 +604,22 @@ static cudaError_t launch_inst(const CUtensorMap* tmp, const CUtensorMap* tmr, c
 }
 
 int batch_kind(const TileConfig& c) {
-    if (c.tz != 8 || c.raw_slab) return -1;  // the slab form runs as its own launch
-    if (c.rx == 1 && c.ry == 1 && c.rz == 1) return c.raw_smem ? kBatchP111Smem : kBatchP111Glob;
-    if (c.rx == 2 && c.ry == 2 && c.rz == 2) return c.raw_smem ? kBatchP222Smem : kBatchP222Glob;
-    if (c.rx == 3 && c.ry == 3 && c.rz == 3) return c.raw_smem ? kBatchP333Smem : kBatchP333Glob;
+    if (c.tz != 8) return -1;
+    if (c.rx == 1 && c.ry == 1 && c.rz == 1)
+        return c.raw_slab ? kBatchP111Slab : c.raw_smem ? kBatchP111Smem : kBatchP111Glob;
+    if (c.rx == 2 && c.ry == 2 && c.rz == 2)
+        return c.raw_slab ? kBatchP222Slab : c.raw_smem ? kBatchP222Smem : kBatchP222Glob;
+    if (c.rx == 3 && c.ry == 3 && c.rz == 3)
+        return c.raw_slab ? kBatchP333Slab : c.raw_smem ? kBatchP333Smem : kBatchP333Glob;
     return -1;
 }
 
-template <int R, bool RAW>
+template <int R, bool RAW, bool SLAB = false>
 static cudaError_t batch_setup_r(size_t smem, int* ctas_per_sm) {
-    cudaError_t e = cudaFuncSetAttribute(nlm_batch_f32_kernel<R, RAW>,
+    cudaError_t e = cudaFuncSetAttribute(nlm_batch_f32_kernel<R, RAW, SLAB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, nlm_batch_f32_kernel<R, RAW>,
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, nlm_batch_f32_kernel<R, RAW, SLAB>,
                                                          256, smem);
 }
 
@@ -627,6 +631,9 @@ cudaError_t batch_kernel_setup(int kind, size_t smem, int* ctas_per_sm) {
         case kBatchP222Glob: return batch_setup_r<2, false>(smem, ctas_per_sm);
         case kBatchP333Smem: return batch_setup_r<3, true>(smem, ctas_per_sm);
         case kBatchP333Glob: return batch_setup_r<3, false>(smem, ctas_per_sm);
+        case kBatchP111Slab: return batch_setup_r<1, true, true>(smem, ctas_per_sm);
+        case kBatchP222Slab: return batch_setup_r<2, true, true>(smem, ctas_per_sm);
+        case kBatchP333Slab: return batch_setup_r<3, true, true>(smem, ctas_per_sm);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -640,6 +647,9 @@ cudaError_t launch_batch_kernel(int kind, const BatchParams& bp, int ctas, size_
         case kBatchP222Glob: nlm_batch_f32_kernel<2, false><<<ctas, 256, smem, st>>>(bp); break;
         case kBatchP333Smem: nlm_batch_f32_kernel<3, true><<<ctas, 256, smem, st>>>(bp); break;
         case kBatchP333Glob: nlm_batch_f32_kernel<3, false><<<ctas, 256, smem, st>>>(bp); break;
+        case kBatchP111Slab: nlm_batch_f32_kernel<1, true, true><<<ctas, 256, smem, st>>>(bp); break;
+        case kBatchP222Slab: nlm_batch_f32_kernel<2, true, true><<<ctas, 256, smem, st>>>(bp); break;
+        case kBatchP333Slab: nlm_batch_f32_kernel<3, true, true><<<ctas, 256, smem, st>>>(bp); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

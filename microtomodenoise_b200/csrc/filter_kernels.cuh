@@ -88,6 +88,10 @@ enum BatchKind : int {
     kBatchP222Glob = 3,
     kBatchP333Smem = 4,
     kBatchP333Glob = 5,
+    kBatchP111Slab = 6,  // raw staged as a z-offset slab
+    kBatchP222Slab = 7,
+    kBatchP333Slab = 8,
+    kBatchKinds = 9,
 };
 struct BatchParams {
     CUtensorMap maps[kBatchMax];     // prev-box maps (64-byte aligned, first)

@@ -7,6 +7,10 @@
     python -m microtomodenoise_b200.profile_case learned
         the whole learned + FP16 job (noise estimates, 4 iterations, k = 144
         per 32x8x8 block) on a 512x512x128 grain pack, for a launch list.
+    python -m microtomodenoise_b200.profile_case slab
+        two exact FP32 iterations of a 256^3 grain pack at the reference's
+        default geometry (patch r1, search r10, 11 slices: 3102 offsets), the
+        tile kernel with raw staged as a z-offset slab.
 """
 from __future__ import annotations
 
@@ -56,5 +60,22 @@ def learned_case():
     net.close()
 
 
+def slab_case():
+    import torch
+    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, synth
+    vol = synth.grain_pack_volume((256, 256, 256), seed=0)
+    raw = torch.from_numpy(vol).cuda()
+    g = IterativeNLM_GPU()
+    g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=(1, 1, 1),
+                                                    radius_searchspace=(10, 10, 10), nslices=11))
+    g.set_sigma(np.full(256, 0.045, np.float32))
+    g.Run_GaussianNoise_device(1, raw.data_ptr())
+    g.Run_GaussianNoise_device(2)
+    torch.cuda.synchronize()
+    ms, n = g.filter_kernel_ms()
+    print("ok", g.describe(), f"{ms:.1f} ms per launch ({n})")
+    g.free_device()
+
+
 if __name__ == "__main__":
-    {"fast": fast_case, "learned": learned_case}[sys.argv[1] if len(sys.argv) > 1 else "fast"]()
+    {"fast": fast_case, "learned": learned_case, "slab": slab_case}[sys.argv[1] if len(sys.argv) > 1 else "fast"]()

@@ -24,7 +24,7 @@ def cases():
                                         noise_mode="global", noise_seed=4)),
         ((12, 64, 64), DenoiseParameters(radius_patchspace=(1, 1, 1), radius_searchspace=(5, 5, 5),
                                          noise_mode="global", maxiterations=2, noise_seed=5)),
-        # raw staged as a slab (search radius 10): its own launch inside the graph
+        # raw staged as a slab (search radius 10): the persistent slab body
         ((14, 36, 40), DenoiseParameters(radius_patchspace=(1, 1, 1), radius_searchspace=(10, 10, 10),
                                          noise_mode="global", noise_seed=6)),
     ]
@@ -45,6 +45,7 @@ def test_batch_equals_single_volume_runs(gpu):
     desc = b.describe()
     print(desc)
     assert "persistent nlm_batch_f32<" in desc and "own launch" in desc
+    assert "persistent nlm_batch_f32<p111, raw_slab>" in desc
     outs = b.run(raws)
     assert b.last_ms > 0
     for i, ((s, p), raw, got) in enumerate(zip(cs, raws, outs)):
