@@ -114,3 +114,13 @@ def test_f64_oracle_close_to_f32(port, golden_filter):
     f64 = port.denoise_f64(raw, p, sig)
     rel = np.abs(f32 - f64) / np.maximum(np.abs(f64), 1e-6)
     assert np.median(rel) < 1e-6
+
+
+def test_reference_gpu_build_loads_and_exports():
+    """The reference GPU class build (oracle/Makefile ref_gpu, where the
+    reference tree exists) loads without a GPU and exports its driver entry."""
+    from oracle.oracle import REF_GPU_SO, reference_gpu_available
+    if not reference_gpu_available():
+        pytest.skip("reference GPU build absent")
+    lib = ctypes.CDLL(REF_GPU_SO)
+    assert hasattr(lib, "ref_gpu_run")
