@@ -105,3 +105,17 @@ def test_missing_library_fails_loudly(tmp_path):
             _lib.load(str(tmp_path / "nope.so"))
         finally:
             _lib._lib = _lib._lib_saved
+
+
+@pytest.mark.parametrize("pr,sr,nsl", [((1, 1, 1), (10, 10, 10), 11), ((2, 2, 2), (7, 7, 7), 11),
+                                       ((1, 1, 2), (9, 9, 9), 21), ((3, 3, 3), (7, 7, 7), 15),
+                                       ((2, 2, 1), (4, 6, 3), 5)])
+def test_search_list_runs_z_major(lib, pr, sr, nsl):
+    """The raw-slab staging of the tile kernel relies on the search offsets
+    running z-major (the reference order, iternlm_prepare.cpp:102-150): a pair
+    of consecutive offsets then spans at most two z offsets."""
+    s, _, _, _ = _geometry(lib, DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, nslices=nsl))
+    z = s[:, 2]
+    assert np.all(np.diff(z) >= 0)
+    pairs = [z[i:i + 2] for i in range(0, len(z), 2)]
+    assert max(int(p.max() - p.min()) for p in pairs) <= 1
