@@ -197,8 +197,8 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
     const int RB = RAW_SMEM ? a.rplane * a.rbz : 0;
     float* D = rawb + round_up32(RB);
     constexpr int DSZ = round_up32(G::DPLANE * G::DD);
-    // D is double-buffered: phase A of offset s+1 writes one buffer while
-    // phase B of offset s reads the other, one barrier per offset.
+    // kOffGroup D buffers: phase A writes one per offset of the group, a
+    // barrier, phase B reads them all, a barrier.
     float* const D0 = D;
 
     const int tid = threadIdx.x;
