@@ -11,8 +11,10 @@
 // FMA) build bit for bit.
 //
 // Tiled kernel: a CTA stages the padded previous iterate over its tile plus
-// search+patch halo into shared memory with one 3D TMA load and, when it fits,
-// raw over the tile plus search halo with coalesced loads (odd row pitch).
+// search+patch halo into shared memory with one 3D TMA load and raw over the
+// tile plus search halo with coalesced loads (odd row pitch): the whole raw
+// box when it fits, else a slab of TZ + 1 planes that follows the z-major
+// offsets, else none (raw read from global memory as aligned float4s).
 // Offsets go in groups of two: it writes the squared-difference volumes
 // D_s = (prev(.+s) - prev(.))^2 of both over the tile plus patch halo to
 // shared memory, then each thread applies the patch stencil to both for 8
