@@ -334,8 +334,14 @@ int main(int argc, char* argv[]) {
         for (int i = 0; i < std::min(params.gpu.n_gpus, n_devices); i++)
             ids.push_back((params.gpu.deviceID + i) % std::max(n_devices, 1));
     const int n_use = (int)ids.size();
+    // the split's thinnest slab (8-slice units split evenly; the last part may
+    // lose up to 7 slices to the stack's end) must cover the z halo
+    const int zpad = std::min(params.nslices / 2, params.radius_searchspace[2]) + params.radius_patchspace[2];
+    const int halo = (std::max(zpad, 1) + 7) / 8 * 8;
+    const int units = (shape[2] + 7) / 8;
+    const bool slabs_deep = n_use > 1 && 8 * (units / n_use) - 7 >= halo;
     const bool multi = n_use > 1 && max_parallelslices > 0 && !params.io.resume &&
-                       params.noiselevel.mode != "semimanual" && shape[2] >= 16 * n_use;
+                       params.noiselevel.mode != "semimanual" && shape[2] >= 16 * n_use && slabs_deep;
 
     if (multi) {
         gpu.free_device();
