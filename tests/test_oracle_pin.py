@@ -98,6 +98,25 @@ def test_port_filter_matches_reference_build(port, reference, pr):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("pr", [(1, 1, 1), (2, 2, 2)])
+def test_port_filter_matches_reference_build_with_nan_input(port, reference, pr):
+    """NaN voxels (e.g. masked regions) propagate through the restatement as
+    through the reference: a NaN distance fails the Pade cutoff test and
+    weighs 0, a NaN raw value poisons every sum it enters. Same positions,
+    same finite values."""
+    rng = np.random.default_rng(11 + sum(pr))
+    raw = rng.random((9, 13, 17), dtype=np.float32)
+    raw[4, 6, 8] = np.nan
+    raw[0, 0, 3] = np.nan
+    p = FilterParams(search_radius=(2, 2, 2), patch_radius=pr)
+    sig = np.full((2, 9), 0.3, np.float32)
+    got = port.denoise_f32(raw, p, sig, all_iters=True)
+    want, _ = reference.denoise(raw, p, sig, n_threads=2, all_iters=True)
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    assert np.isnan(want).any() and (~np.isnan(want)).any()
+    assert np.array_equal(got[~np.isnan(got)], want[~np.isnan(want)])
+
+
 def test_port_em_matches_reference_build(port, reference):
     rng = np.random.default_rng(3)
     v = np.concatenate([rng.normal(0.05, 0.005, 3000), rng.normal(0.2, 0.03, 1000)]).astype(np.float32)
