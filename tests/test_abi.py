@@ -119,3 +119,22 @@ def test_search_list_runs_z_major(lib, pr, sr, nsl):
     assert np.all(np.diff(z) >= 0)
     pairs = [z[i:i + 2] for i in range(0, len(z), 2)]
     assert max(int(p.max() - p.min()) for p in pairs) <= 1
+
+
+def test_multi_gpu_entry_points_without_a_gpu(lib):
+    """inlm_denoise_multi checks its arguments before it touches a device;
+    inlm_device_count reports 0 devices here without failing."""
+    n = C.c_int(-1)
+    assert lib.inlm_device_count(C.byref(n)) == 0 and n.value >= 0
+    p = _lib.InlmParams()
+    lib.inlm_default_params(C.byref(p))
+    shape = (C.c_int * 3)(16, 16, 32)
+    buf = np.zeros(16 * 16 * 32, np.float32)
+    ids = (C.c_int * 2)(0, 0)
+    assert lib.inlm_denoise_multi(shape, C.byref(p), None, buf.ctypes.data, 2, ids, None, None) == -1
+    assert lib.inlm_denoise_multi(shape, C.byref(p), buf.ctypes.data, buf.ctypes.data, 0, ids,
+                                  None, None) == -1
+    assert "n_parts" in lib.inlm_last_error().decode()
+    if n.value == 0:  # valid arguments, no device: INLM_ERR_NODEVICE
+        assert lib.inlm_denoise_multi(shape, C.byref(p), buf.ctypes.data, buf.ctypes.data, 2, ids,
+                                      None, None) == -3
