@@ -91,6 +91,23 @@ def test_raw_slab_bit_exact(gpu, port, shape, pr, sr):
     assert np.array_equal(got, want), desc
 
 
+@pytest.mark.parametrize("pr,sr", [((1, 1, 1), (2, 2, 2)), ((2, 2, 2), (3, 3, 3))])
+def test_nan_input_propagates_as_the_oracle(gpu, port, pr, sr):
+    """NaN voxels: a NaN distance fails the Pade cutoff and weighs 0, a NaN
+    raw value poisons the sums it enters; the NaN positions and every finite
+    value equal the oracle's (pinned to the reference build on the same
+    case)."""
+    rng = np.random.default_rng(11 + sum(pr))
+    raw = rng.random((12, 21, 37), dtype=np.float32)
+    raw[5, 10, 18] = np.nan
+    raw[0, 0, 3] = np.nan
+    sig = np.full((2, 12), 0.3, np.float32)
+    got, desc = run_gpu(raw, pr, sr, sig)
+    want = port.denoise_f32(raw, FilterParams(search_radius=sr, patch_radius=pr), sig, all_iters=True)
+    assert np.array_equal(np.isnan(got), np.isnan(want)), desc
+    assert np.array_equal(got[~np.isnan(got)], want[~np.isnan(want)]), desc
+
+
 def test_distweight_table_and_generic_kernel(gpu, port):
     raw = synth.small_case((12, 16, 20), seed=4)
     sig = np.full((2, 12), 0.06, np.float32)
