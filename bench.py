@@ -21,19 +21,17 @@ weak scaling, no data-path collective); time = max over ranks.
 
 ``forms`` (rank 0, one GPU): the same whole job in the fused FP32 form
 (fused multiply-adds, within 1e-4 relative of the reference except at
-weights that cross the Pade cutoff), the FP16-storage form and
-in the learned-proposal + FP16 form (k = 144 of 514 offsets per 32x8x8 block,
-the four 8^3 tiles' predictions summed, run by the full-width kernel, without
-fallback: the fastest setting measured within 0.1 dB of the FP64 oracle's
-PSNR against the clean phantom; k = 104 per 8^3 tile with the one-tile
-kernel; and k = 256 per tile with fallback to full
-search below 0.95 predicted kept mass, which fires on every tile of this
-volume), each with
-its speed-up over the plain FP32 job, the proposal's fallback fraction and
-evaluated-offset fraction, and its accuracy: max-abs error and PSNR against
-the FP64 full-search oracle on two sub-blocks (a corner and a central 40^3
-block, computed on crops with a 28-voxel margin, the reach of 4 iterations),
-plus PSNR against the clean phantom next to the FP64 oracle's own.
+weights that cross the Pade cutoff), the FP16-storage form, and the
+learned-proposal + FP16 form: one list of LEARNED_K offsets per 32x8x8 block
+(the four 8^3 tiles' predictions summed, run by the full-width kernel), with
+full search for every block whose predicted kept weight mass is below
+LEARNED_MIN_MASS; beside it the same lists without fallback and k = 256 per
+8^3 tile with the 0.95 threshold, which falls back on every tile of this
+volume. Each form reports its speed-up over the plain FP32 job, the
+proposal's fallback and evaluated-offset fractions, and its accuracy (see
+run_forms): PSNR against the clean phantom over the whole volume beside the
+plain FP32 result's, and max-abs error and PSNR against the FP64
+full-search oracle on 64 seeded 16^3 sub-blocks.
 
 ``batch`` (rank 0, one GPU): 24 seeded volumes, sizes uniform from 64^3 to
 384x384x256, spheres on a background with blurred noise of sigma uniform in
@@ -65,6 +63,10 @@ S_OFFSETS, P_TAPS = 514, 33
 # the squared difference, 18 for multiplier, Pade weight, cutoff and sums
 FLOP_PER_VOXEL_ITER = S_OFFSETS * (2 * P_TAPS + 20)
 BYTES_PER_VOXEL_ITER_F32 = 12                          # read raw + prev, write result
+# learned + FP16 form of the headline line: one offset list per 32x8x8 block
+# of k offsets, full search for blocks whose predicted kept mass is below
+# LEARNED_MIN_MASS
+LEARNED_K, LEARNED_MIN_MASS = 144, 0.0
 
 
 def log(*a):
@@ -143,16 +145,32 @@ def measured_peaks():
         return {}
 
 
-def profile_traffic():
-    """DRAM bytes per filter launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "nlm_tile_f32_p2s5_512.md")
+# DRAM traffic of one 512^3 launch of the headline filter kernel
+# (nlm_tile_f32_kernel<2,2,2,8,raw smem>): dram__bytes_read.sum +
+# dram__bytes_write.sum of one 512x512x128 launch captured by ncu
+# (profiles/nlm_tile_f32_p2s5_512.md gives the command), times 4: the traffic
+# is the tiles' halo boxes plus the result, so it grows with the tile count.
+FILTER_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, one 512x512x128 launch, x4"
+FILTER_TRAFFIC_BYTES_PER_LAUNCH = 4 * 459.8e6
+
+
+def fp32_arithmetic_peak(device: int):
+    """FP32 CUDA-core peak in TFLOP/s: SMs x 128 FP32 lanes x 2 flop per FFMA
+    x the maximum SM clock (nvidia-smi clocks.max.sm, else the driver-measured
+    peaks file's sm_max_mhz)."""
+    import torch
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = None
     try:
-        for ln in open(path):
-            if ln.startswith("traffic_bytes_per_launch:"):
-                return float(ln.split(":", 1)[1].strip())
+        out = subprocess.run(["nvidia-smi", "-i", str(device), "--query-gpu=clocks.max.sm",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                             timeout=20).stdout.strip()
+        mhz = float(out.splitlines()[0])
     except Exception:
-        pass
-    return None
+        mhz = measured_peaks().get("sm_max_mhz")
+    if not mhz:
+        return None, "no SM clock available"
+    return sms * 128 * 2 * mhz * 1e6 / 1e12, f"{sms} SMs x 128 FP32 lanes x 2 flop x {mhz:.0f} MHz (clocks.max.sm)"
 
 
 def make_volume(seed=0, return_clean=False):
@@ -168,18 +186,11 @@ def psnr(a, b, peak=1.0):
     return float("inf") if mse == 0 else 10 * np.log10(peak * peak / mse)
 
 
-def sub_blocks(shape, inner=40, margin=28):
-    """(crop slices, interior slices within the crop) of a corner block (the
-    volume's own faces need no margin) and a central block."""
-    out = []
-    c0 = tuple(slice(0, min(n, inner + margin)) for n in shape)
-    i0 = tuple(slice(0, min(n, inner)) for n in shape)
-    out.append((c0, i0))
-    lo = [max(0, n // 2 - inner // 2 - margin) for n in shape]
-    c1 = tuple(slice(l, min(n, n // 2 + inner // 2 + margin)) for l, n in zip(lo, shape))
-    i1 = tuple(slice(n // 2 - inner // 2 - l, n // 2 + inner // 2 - l) for l, n in zip(lo, shape))
-    out.append((c1, i1))
-    return out
+def sub_block_corners(shape, n=64, size=16, seed=0):
+    """n seeded lower corners (z, y, x) of size^3 blocks anywhere in the volume
+    (faces, edges and corners included)."""
+    rng = np.random.default_rng(seed)
+    return [tuple(int(rng.integers(0, dim - size + 1)) for dim in shape) for _ in range(n)]
 
 
 def batch_workload(seed=0, n=24, lo=(64, 64, 64), hi=(384, 384, 256)):
@@ -263,25 +274,39 @@ def run_batch(args, local, small=False):
 
 
 def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
-    """FP16 and learned + FP16 forms: whole-job throughput and accuracy."""
-    import ctypes as C
+    """Precision and learned forms: whole-job throughput and accuracy.
+
+    Throughput: each form's whole job (its own noise estimates) timed like the
+    headline. Accuracy: every form re-run with the FP32 job's sigma schedule
+    held fixed, then
+      * over the whole volume: PSNR against the clean phantom, and its
+        difference to the plain FP32 result's (bit-exact to the reference's
+        CPU filter, within ~1e-6 of FP64);
+      * on 64 seeded 16^3 sub-blocks: max-abs error and PSNR against the FP64
+        full-search oracle, and PSNR against the clean phantom next to the
+        FP64 oracle's own on the same blocks."""
     import torch
-    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, _lib
+    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU
     from microtomodenoise_b200.proposal import ProposalNet, default_weights
     from oracle.oracle import FilterParams, Port
 
     net = ProposalNet.load(default_weights(PR, SR), device=local)
     forms = [("f32", "f32", None), ("f32_fused", "f32_fma", None), ("fp16", "f16", None),
-             ("learned_fp16", "f16", (144, 0.0, 4)), ("learned_fp16_pertile_k104", "f16", (104, 0.0, 1)),
-             ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
+             ("learned_fp16", "f16", (LEARNED_K, LEARNED_MIN_MASS, 4)),
+             ("learned_fp16_no_fallback", "f16", (LEARNED_K, 0.0, 4)),
+             ("learned_fp16_k256_mass095", "f16", (256, 0.95, 1))]
     for item in filter(None, args.learned_extra.split(",")):
-        k, t = (int(v) for v in item.split("@"))
-        forms.append((f"learned_fp16_k{k}_t{t}", "f16", (k, 0.0, t)))
+        k, t, m = (item.split("@") + ["0"])[:3]
+        forms.append((f"learned_fp16_k{k}_t{t}_m{m}", "f16", (int(k), float(m), int(t))))
     raw_dev = torch.from_numpy(vol).cuda()
     out_dev = torch.empty_like(raw_dev)
     vox = float(np.prod(vol.shape))
-    res = {}
-    crops = {}
+    corners = sub_block_corners(vol.shape)
+    bs = 16
+    crop = lambda a: [a[z:z + bs, y:y + bs, x:x + bs] for z, y, x in corners]
+    cat = lambda xs: np.concatenate([x.ravel() for x in xs])
+    clean_blocks = cat(crop(clean))
+    res, blocks, whole = {}, {}, {}
     for name, prec, prop in forms:
         dp = DenoiseParameters(radius_patchspace=PR, radius_searchspace=SR, maxiterations=ITERS,
                                alpha=0.5, noise_mode="z-adaptive", zwindow=100, n_samples=100000,
@@ -290,11 +315,10 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
         g.configure_device(vol.shape, dp)
         g.set_stream(stream.cuda_stream)
         if prop:
-            g.attach_proposal(net, prop[0], prop[1], tiles_x=prop[2] if len(prop) > 2 else 1)
+            g.attach_proposal(net, prop[0], prop[1], tiles_x=prop[2])
         r = {"kernel": g.describe()}
         if name != "f32":
-            for _ in range(1):
-                g.denoise(raw_dev.data_ptr(), on_device=True, out=out_dev.data_ptr())
+            g.denoise(raw_dev.data_ptr(), on_device=True, out=out_dev.data_ptr())
             g.filter_kernel_ms()
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
@@ -306,15 +330,14 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / args.form_steps
             kms, kn = g.filter_kernel_ms()
-            r["kernel"] = g.describe()  # after the runs: the proposal selects the per-tile kernel
+            r["kernel"] = g.describe()  # after the runs: the proposal selects the plan kernel
             r.update({"value": vox * ITERS / (ms / 1e3), "unit": "voxel-iter/s",
                       "ms_per_step": ms, "steps": args.form_steps, "warmup": 1,
                       "speedup_vs_f32": vox * ITERS / (ms / 1e3) / value_f32,
                       "filter_kernel_avg_ms": kms})
             if prop:
                 st = g.proposal_stats()
-                r.update({"k": prop[0], "min_mass": prop[1],
-                          "tiles_per_plan": prop[2] if len(prop) > 2 else 1,
+                r.update({"k": prop[0], "min_mass": prop[1], "tiles_per_plan": prop[2],
                           "fallback_fraction": st["fallback_tiles"] / max(st["tiles"], 1),
                           "fraction_evaluated": st["fraction_evaluated"]})
         # accuracy run: the FP32 job's sigma schedule, fixed, for every form
@@ -324,35 +347,34 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
         g.get_result_device(out_dev.data_ptr())
         torch.cuda.synchronize()
         out = out_dev.cpu().numpy()
-        crops[name] = [out[c][i] for c, i in sub_blocks(vol.shape)]
+        whole[name] = psnr(out, clean)
+        blocks[name] = cat(crop(out))
         res[name] = r
         g.free_device()
+        del out
         log(f"form {name}: {r}")
     net.close()
-    # FP64 full-search oracle on the crops
     port = Port()
-    fp = FilterParams(search_radius=SR, patch_radius=PR)
-    ref, cl = [], []
     t = time.time()
-    for c, i in sub_blocks(vol.shape):
-        crop = np.ascontiguousarray(vol[c])
-        sig = np.ascontiguousarray(sig_iters[:, c[0]])
-        ref.append(port.denoise_f64(crop, fp, sig)[i])
-        cl.append(clean[c][i])
+    ref = port.denoise_f64_blocks(vol, FilterParams(search_radius=SR, patch_radius=PR), sig_iters,
+                                  corners, (bs, bs, bs))
     log(f"FP64 oracle on {len(ref)} sub-blocks: {time.time() - t:.1f}s")
-    cat = lambda xs: np.concatenate([x.ravel() for x in xs])
-    r64, c64 = cat(ref), cat(cl)
-    p64 = psnr(r64, c64)
+    r64 = cat(ref)
+    p64 = psnr(r64, clean_blocks)
     for name in res:
-        got = cat(crops[name])
+        got = blocks[name]
         res[name]["accuracy"] = {
+            "psnr_vs_clean_db": whole[name],
+            "delta_vs_f32_db": whole[name] - whole["f32"],
             "max_abs_vs_fp64": float(np.abs(got - r64).max()),
             "psnr_vs_fp64_db": psnr(got, r64),
-            "psnr_vs_clean_db": psnr(got, c64),
-            "fp64_psnr_vs_clean_db": p64,
-            "delta_vs_fp64_oracle_db": psnr(got, c64) - p64,
-            "sub_blocks": "corner and central 40^3 blocks, FP64 oracle on crops with a 28-voxel "
-                          "margin, sigma schedule of the FP32 job held fixed"}
+            "blocks_psnr_vs_clean_db": psnr(got, clean_blocks),
+            "blocks_fp64_psnr_vs_clean_db": p64,
+            "blocks_delta_vs_fp64_oracle_db": psnr(got, clean_blocks) - p64,
+            "how": "psnr_vs_clean / delta_vs_f32: whole volume against the clean phantom, minus the "
+                   "plain FP32 result's; *_fp64 and blocks_*: 64 seeded 16^3 sub-blocks against the "
+                   "FP64 full-search oracle (oracle/denoise_f64_blocks); sigma schedule of the FP32 "
+                   "job held fixed"}
     return res
 
 
@@ -663,6 +685,66 @@ def run_rgb_workload(args):
     print(json.dumps(res), flush=True)
 
 
+def run_profile_case(args):
+    """Small cases of the filter kernels for ncu captures (one GPU, a few GB):
+
+    f32:     two exact FP32 iterations (sigma 0.14) of a grain pack of --shape
+             (default 128x512x512) at patch r2 search r5: the headline kernel.
+    fast:    two iterations of a 64x512x512 grain pack, patch r2 search r5,
+             FP16 form: iteration 1 with the shipped proposal (k = 112 per 8^3
+             tile, one tile per CTA), iteration 2 full search (32-wide kernel).
+    learned: the whole learned + FP16 job (noise estimates, 4 iterations,
+             one list per 32x8x8 block) on a 128x512x512 grain pack.
+    slab:    two exact FP32 iterations of a 256^3 grain pack at the
+             reference's default geometry (patch r1, search r10, 11 slices:
+             3102 offsets), the tile kernel with raw staged as a z slab."""
+    import torch
+    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, synth
+    from microtomodenoise_b200.proposal import ProposalNet, default_weights
+    case = args.case
+    net = None
+    if case in ("f32", "slab"):
+        shape = SHAPE if case == "f32" else (256, 256, 256)
+        pr, sr = ((2, 2, 2), (5, 5, 5)) if case == "f32" else ((1, 1, 1), (10, 10, 10))
+        vol = synth.grain_pack_volume(shape, seed=0)
+        g = IterativeNLM_GPU()
+        g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr,
+                                                        nslices=11))
+        g.set_sigma(np.full(shape[0], 0.14 if case == "f32" else 0.045, np.float32))
+        raw = torch.from_numpy(vol).cuda()
+        g.Run_GaussianNoise_device(1, raw.data_ptr())
+        g.Run_GaussianNoise_device(2)
+    elif case == "fast":
+        vol = synth.grain_pack_volume((64, 512, 512), seed=0)
+        raw = torch.from_numpy(vol).cuda()
+        net = ProposalNet.load(default_weights((2, 2, 2), (5, 5, 5)))
+        g = IterativeNLM_GPU()
+        g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=(2, 2, 2),
+                                                        radius_searchspace=(5, 5, 5), precision="f16"))
+        g.set_sigma(np.full(64, 0.14, np.float32))
+        g.attach_proposal(net, 112, 0.0)
+        g.Run_GaussianNoise_device(1, raw.data_ptr())
+        g.attach_proposal(None)
+        g.Run_GaussianNoise_device(2)
+    else:
+        vol = synth.grain_pack_volume((128, 512, 512), seed=0)
+        raw = torch.from_numpy(vol).cuda()
+        out = torch.empty_like(raw)
+        net = ProposalNet.load(default_weights((2, 2, 2), (5, 5, 5)))
+        g = IterativeNLM_GPU()
+        g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=(2, 2, 2),
+                                                        radius_searchspace=(5, 5, 5), precision="f16",
+                                                        noise_mode="z-adaptive", n_samples=100000))
+        g.attach_proposal(net, LEARNED_K, LEARNED_MIN_MASS, tiles_x=4)
+        g.denoise(raw.data_ptr(), on_device=True, out=out.data_ptr())
+    torch.cuda.synchronize()
+    ms, n = g.filter_kernel_ms()
+    log(f"profile case {case}: {g.describe()}; {ms:.2f} ms per filter launch ({n})")
+    g.free_device()
+    if net is not None:
+        net.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -678,12 +760,16 @@ def main():
     ap.add_argument("--reference-gpu-only", action="store_true",
                     help="--impl reference: only the reference GPU class timings")
     ap.add_argument("--workload", default="grain512",
-                    choices=["grain512", "learned1024", "stream2048", "rgb4k"],
-                    help="grain512: the headline bench line; the others: one-step "
-                         "measurements of the large workloads (see run_large_workload)")
+                    choices=["grain512", "learned1024", "stream2048", "rgb4k", "profile"],
+                    help="grain512: the headline bench line; learned1024, stream2048, rgb4k: "
+                         "one-step measurements of the large workloads (run_large_workload, "
+                         "run_rgb_workload); profile: a small case for ncu (--case)")
+    ap.add_argument("--case", default="f32", choices=["f32", "fast", "learned", "slab"],
+                    help="--workload profile: which small case (see run_profile_case)")
     ap.add_argument("--stream-depth", type=int, default=128)
     ap.add_argument("--learned-extra", default="",
-                    help="extra learned + FP16 forms in the headline run, k@tiles_per_plan[,...]")
+                    help="extra learned + FP16 forms in the headline run, "
+                         "k@tiles_per_plan[@min_mass][,...]")
     ap.add_argument("--k-list", default="",
                     help="learned1024: comma-separated k values to sweep (no fallback)")
     ap.add_argument("--shape", default="512,512,512",
@@ -706,6 +792,8 @@ def main():
             torch.cuda.set_device(local)
             if args.workload == "rgb4k":
                 run_rgb_workload(args)
+            elif args.workload == "profile":
+                run_profile_case(args)
             else:
                 run_large_workload(args)
         return
@@ -722,9 +810,7 @@ def main():
     import ctypes as C
 
     L = _lib.load()
-    peak = C.c_double(0)
-    _lib.check(L.inlm_probe_fp32_peak(local, C.byref(peak)), "probe")
-    fp32_peak = peak.value
+    fp32_peak, peak_source = fp32_arithmetic_peak(local)
 
     vol, clean = make_volume(seed=0, return_clean=True)
     dp = DenoiseParameters(radius_patchspace=PR, radius_searchspace=SR, maxiterations=ITERS,
@@ -801,7 +887,7 @@ def main():
     value = world * vox * ITERS * args.steps / (ms / 1e3)
     value_e2e = world * vox * ITERS * args.e2e_steps / (ms_e2e / 1e3)
     achieved = FLOP_PER_VOXEL_ITER * vox / (filt_ms * 1e-3) / 1e12
-    traffic = profile_traffic()
+    traffic = FILTER_TRAFFIC_BYTES_PER_LAUNCH * vox / (512.0 ** 3)
     line = {
         "metric": METRIC, "value": value, "unit": "voxel-iter/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -812,10 +898,10 @@ def main():
                 "ms_per_step": ms_e2e / args.e2e_steps},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak if fp32_peak else None,
-                     "traffic": traffic,
+                     "traffic": traffic, "traffic_source": FILTER_TRAFFIC_SOURCE,
                      "kernel": g.describe(), "kernel_avg_ms": filt_ms, "kernel_launches": filt_n,
                      "flop_per_voxel_iter": FLOP_PER_VOXEL_ITER,
-                     "peak_source": "measured in this run: all-SM FFMA loop (2 flop/FFMA)",
+                     "peak_source": "FP32 arithmetic peak: " + peak_source,
                      "hbm": {"achieved_gbs": BYTES_PER_VOXEL_ITER_F32 * vox / (filt_ms * 1e-3) / 1e9,
                              "peak_gbs": measured_peaks().get("hbm_gbs"),
                              "bytes_per_voxel_iter": BYTES_PER_VOXEL_ITER_F32}},

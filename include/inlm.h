@@ -161,11 +161,6 @@ int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const int* count, c
 /* Number of kernels this handle has launched since creation. */
 int inlm_kernel_launches(inlm_denoiser* d, uint64_t* count);
 
-/* Measures the FP32 FMA throughput of the device in TFLOP/s (2 flops per
- * FFMA) with an all-SM loop of independent FMA chains timed by CUDA events;
- * the roofline denominator of the FP32-bound filter. */
-int inlm_probe_fp32_peak(int device_id, double* tflops);
-
 /* ---------------- noise level (NoiseLevel) ---------------- */
 
 /* shape as above; n_samples random 2D patches of patchsize^2 voxels. The
@@ -201,10 +196,17 @@ int inlm_noise_patchstd(inlm_noise* n, float* out, uint64_t max_n);
  * applications whose device memory is owned by their own pool.
  *
  * values_dev: n_values per-sample patch stds (device); windows_host: 2 values
- * per window (first, last sample index, inclusive; last < first = empty),
- * host memory; mean_dev / sd_dev: n_windows outputs (device), the lower
- * cluster's mean and std per window, as inlm_noise_estimate computes them.
- * Runs on the calling thread's current device, on `stream` (NULL = default).
+ * per window (first, last sample index, inclusive; last < first = empty,
+ * whose outputs are 0), host memory, read before the call returns;
+ * mean_dev / sd_dev: n_windows outputs (device), the lower cluster's mean and
+ * std per window, as inlm_noise_estimate computes them.
+ * Runs on the calling thread's current device, on `stream`. The call only
+ * enqueues kernels (the window table travels in their launch parameters): it
+ * copies nothing from host memory and does not wait, so the outputs are
+ * ready once `stream` reaches them. NULL is the legacy default stream, which
+ * synchronises with every blocking stream of the context; while another
+ * thread captures a stream, pass a stream created with
+ * cudaStreamNonBlocking.
  * Limits: n_windows <= 16384 and the window lengths summing to at most
  * 16777216 samples; larger requests return INLM_ERR_ARG.
  * The first call on a device looks up the arrays' device addresses; make

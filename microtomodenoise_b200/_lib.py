@@ -31,7 +31,7 @@ EXPORTS = (
     "inlm_get_result_device", "inlm_denoise", "inlm_set_stream", "inlm_filter_kernel_ms",
     "inlm_describe", "inlm_noise_create", "inlm_noise_destroy", "inlm_noise_estimate",
     "inlm_noise_samples", "inlm_noise_patchstd", "inlm_geometry", "inlm_noise_draw_samples",
-    "inlm_kernel_launches", "inlm_probe_fp32_peak", "inlm_noise_em_noalloc",
+    "inlm_kernel_launches", "inlm_noise_em_noalloc",
     "inlm_tile_grid", "inlm_set_offset_plan",
     "inlm_proposal_create", "inlm_proposal_destroy", "inlm_proposal_n_params",
     "inlm_proposal_set_params", "inlm_proposal_get_params", "inlm_proposal_logits",
@@ -128,7 +128,6 @@ def load(path: str = "") -> C.CDLL:
                                 C.POINTER(C.c_int), vp]
     L.inlm_noise_draw_samples.argtypes = [C.c_int * 3, C.c_uint64, C.c_int, C.c_int, C.c_uint, vp]
     L.inlm_kernel_launches.argtypes = [vp, C.POINTER(C.c_uint64)]
-    L.inlm_probe_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.inlm_tile_grid.argtypes = [vp, C.c_int * 3, C.c_int * 3]
     L.inlm_set_offset_plan.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int]
     L.inlm_noise_em_noalloc.argtypes = [vp, vp, C.c_int64, vp, C.c_int, vp, vp]

@@ -36,7 +36,6 @@ NVCC_FLAGS = ARCH + [
 LIB_SOURCES = [
     "filter_kernels.cu",
     "filter_fast.cu",
-    "probe.cu",
     "noise_kernels.cu",
     "api.cu",
     "proposal.cu",

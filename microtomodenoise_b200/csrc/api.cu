@@ -18,7 +18,6 @@
 #include "api_internal.hpp"
 #include "noise_kernels.cuh"
 #include "sampling.hpp"
-#include "probe.cuh"
 
 using namespace inlm;
 
@@ -1266,16 +1265,6 @@ extern "C" int inlm_noise_draw_samples(const int shape[3], uint64_t n_samples, i
 extern "C" int inlm_kernel_launches(inlm_denoiser* d, uint64_t* count) {
     if (!d || !count) return fail(INLM_ERR_ARG, "null argument");
     *count = d->launches;
-    return INLM_OK;
-}
-
-extern "C" int inlm_probe_fp32_peak(int device_id, double* tflops) {
-    if (!tflops) return fail(INLM_ERR_ARG, "null argument");
-    CUDA_TRY(cudaSetDevice(device_id));
-    double best = 0.0;
-    int rc = probe_fp32_fma(device_id, &best);
-    if (rc) return fail(INLM_ERR_CUDA, "fp32 probe failed");
-    *tflops = best;
     return INLM_OK;
 }
 

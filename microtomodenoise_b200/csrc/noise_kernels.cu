@@ -275,15 +275,29 @@ __global__ void __launch_bounds__(NT) noise_em_kernel(const float* __restrict__ 
 // leaves the last call's contents behind; calls whose work overlaps on the
 // GPU (different streams, or different host threads) race on them.
 // Nothing needs clearing between calls: the EM writes every assignment of a
-// window (its initial pass) before it reads any, and the host rewrites the
-// window table for every call.
+// window (its initial pass) before it reads any, and every call rewrites the
+// window-table entries it uses.
+// The window table reaches the device inside kernel launch parameters (a
+// small copy kernel per 1024 windows), so a call enqueues kernels only: no
+// host-to-device copy from pageable memory and no wait on the host.
 struct NoAllocWindow {
-    int first, last;     // inclusive sample range
+    int first, last;     // inclusive sample range (last < first: empty)
     long long offset;    // byte offset of the window's assignments in the scratch
 };
 
 static __device__ __align__(256) signed char g_noalloc_assign[kNoAllocAssignBytes];
 static __device__ __align__(256) NoAllocWindow g_noalloc_windows[kNoAllocMaxWindows];
+
+constexpr int kNoAllocChunk = 1024;  // windows per launch-parameter block (16 KiB)
+struct NoAllocTableChunk {
+    int base, count;
+    NoAllocWindow win[kNoAllocChunk];
+};
+
+__global__ void __launch_bounds__(256) noalloc_table_kernel(const __grid_constant__ NoAllocTableChunk c,
+                                                            NoAllocWindow* __restrict__ table) {
+    for (int i = threadIdx.x; i < c.count; i += blockDim.x) table[c.base + i] = c.win[i];
+}
 
 __global__ void __launch_bounds__(kEmThreads) noise_em_noalloc_kernel(
     const float* __restrict__ values, const NoAllocWindow* __restrict__ windows,
@@ -333,23 +347,28 @@ cudaError_t launch_noise_em_noalloc(int device, const float* values, const long 
     NoAllocPtrs ptrs;
     cudaError_t e = noalloc_setup(device, &ptrs);
     if (e != cudaSuccess) return e;
-    NoAllocWindow table[256];
+    // the chunk is copied into the launch parameters when the kernel is enqueued
+    static thread_local NoAllocTableChunk chunk;
     long long offset = 0;
-    // the window table goes up in chunks through a small host buffer
-    for (int base = 0; base < n_windows; base += 256) {
-        int cnt = n_windows - base < 256 ? n_windows - base : 256;
+    for (int base = 0; base < n_windows; base += kNoAllocChunk) {
+        const int cnt = n_windows - base < kNoAllocChunk ? n_windows - base : kNoAllocChunk;
+        chunk.base = base;
+        chunk.count = cnt;
         for (int i = 0; i < cnt; i++) {
-            long long f = windows_host[2 * (base + i)], l = windows_host[2 * (base + i) + 1];
-            table[i].first = (int)f;
-            table[i].last = (int)l;
-            table[i].offset = offset;
-            offset += (l >= f) ? (l - f + 1) : 0;
+            const long long f = windows_host[2 * (base + i)], l = windows_host[2 * (base + i) + 1];
+            NoAllocWindow& w = chunk.win[i];
+            if (l < f) {  // empty: stored as 0..-1 whatever the caller's values
+                w.first = 0;
+                w.last = -1;
+            } else {
+                w.first = (int)f;
+                w.last = (int)l;
+            }
+            w.offset = offset;
+            offset += (long long)w.last - w.first + 1;
         }
-        // synchronous for pageable host memory, so table can be reused
-        e = cudaMemcpyAsync(ptrs.windows + base, table, cnt * sizeof(NoAllocWindow),
-                            cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) return e;
-        e = cudaStreamSynchronize(st);
+        noalloc_table_kernel<<<1, 256, 0, st>>>(chunk, ptrs.windows);
+        e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     noise_em_noalloc_kernel<<<n_windows, kEmThreads, 0, st>>>(values, ptrs.windows, ptrs.assign,

@@ -95,6 +95,7 @@ class Port:
                                       _f32p, C.c_void_p]
         L.ora_denoise_f64.argtypes = [_f32p, C.c_int * 3, C.POINTER(_CParams), _f32p, C.c_int,
                                       _f64p]
+        L.ora_filter_f64.argtypes = [_f64p, _f64p, C.c_int * 3, C.POINTER(_CParams), _f64p, _f64p]
         L.ora_filter_f32_voxels.argtypes = [_f32p, _f32p, C.c_int * 3, C.POINTER(_CParams), _f32p,
                                             C.c_int64, _i64p, _f32p]
         L.ora_denoise_f64_plan.argtypes = [_f32p, C.c_int * 3, C.POINTER(_CParams), _f32p, C.c_int,
@@ -227,6 +228,65 @@ class Port:
         out = np.empty(raw.shape, np.float64)
         self.lib.ora_denoise_f64(raw.ravel(), _shape3(raw), C.byref(_cparams(p)), sig.ravel(),
                                  sig.shape[0], out.ravel())
+        return out
+
+    def denoise_f64_blocks(self, raw: np.ndarray, p: FilterParams, sigmas: np.ndarray,
+                           corners, size) -> list:
+        """The FP64 full-search result of the last iteration on sub-blocks of
+        a volume, without filtering the whole volume: iteration k runs on the
+        block grown by (n_iter - k) x the filter's reach (its padding) per
+        side, clipped to the volume, from iteration k-1 on that box grown by
+        one reach; positions outside the volume take the reference's
+        reflective rule (-i below 0, 2n-i-2 above n-1). corners: (z, y, x)
+        lower corners; size: (dz, dy, dx). Returns one float64 array per
+        block. Same arithmetic as ora_denoise_f64 (ora_filter_f64 on crops)."""
+        raw = np.ascontiguousarray(raw, np.float32)
+        sig = np.ascontiguousarray(np.atleast_2d(sigmas), np.float32)
+        n_iter = sig.shape[0]
+        pad = self.padding(p)[::-1]  # (z, y, x)
+        shp = raw.shape
+        cp = _cparams(p)
+        beta = float(np.float32(p.beta))
+        s64 = sig.astype(np.float64)
+        mults = [-1.0 / (s64[k] * s64[k] * beta) for k in range(n_iter)]  # as ora_denoise_f64
+
+        def mirror(i, n):
+            i = np.asarray(i)
+            for _ in range(64):
+                i = np.where(i < 0, -i, i)
+                i = np.where(i > n - 1, 2 * n - i - 2, i)
+            return i
+
+        out = []
+        for c in corners:
+            boxes = []  # iteration k's box (lo, hi) per axis, k = 1..n_iter
+            for k in range(1, n_iter + 1):
+                g = n_iter - k
+                boxes.append([(max(0, c[a] - g * pad[a]), min(shp[a], c[a] + size[a] + g * pad[a]))
+                              for a in range(3)])
+            prev = None  # iterate k-1 on boxes[k-2]
+            for k in range(n_iter):
+                box = boxes[k]
+                idx = [mirror(np.arange(lo - pad[a], hi + pad[a]), shp[a]) for a, (lo, hi) in enumerate(box)]
+                raw_pad = raw[np.ix_(*idx)].astype(np.float64)
+                if k == 0:
+                    prev_pad = raw_pad
+                else:
+                    pb = boxes[k - 1]
+                    rel = [ix - pb[a][0] for a, ix in enumerate(idx)]
+                    for a in range(3):
+                        assert rel[a].min() >= 0 and rel[a].max() < pb[a][1] - pb[a][0], "box too small"
+                    prev_pad = prev[np.ix_(*rel)]
+                inner = [hi - lo for lo, hi in box]
+                res = np.empty(inner, np.float64)
+                m = np.ascontiguousarray(mults[k][box[0][0]:box[0][1]])
+                self.lib.ora_filter_f64(np.ascontiguousarray(raw_pad).ravel(),
+                                        np.ascontiguousarray(prev_pad).ravel(),
+                                        (C.c_int * 3)(inner[2], inner[1], inner[0]), C.byref(cp), m,
+                                        res.ravel())
+                prev = res
+            lo = [c[a] - boxes[-1][a][0] for a in range(3)]
+            out.append(prev[lo[0]:lo[0] + size[0], lo[1]:lo[1] + size[1], lo[2]:lo[2] + size[2]].copy())
         return out
 
     # ---- colour path ----

@@ -143,3 +143,20 @@ def test_reference_gpu_build_loads_and_exports():
         pytest.skip("reference GPU build absent")
     lib = ctypes.CDLL(REF_GPU_SO)
     assert hasattr(lib, "ref_gpu_run")
+
+
+def test_fp64_blocks_equal_the_whole_volume_fp64(port):
+    """The FP64 sub-block oracle (iterations on shrinking boxes) gives the
+    whole-volume FP64 result on every block, edges and corners included."""
+    from microtomodenoise_b200 import synth
+    vol = synth.small_case((20, 34, 40), seed=11)
+    p = FilterParams(search_radius=(3, 3, 2), patch_radius=(2, 2, 1))
+    rng = np.random.default_rng(0)
+    sig = rng.uniform(0.03, 0.08, (3, 20)).astype(np.float32)
+    want = port.denoise_f64(vol, p, sig)
+    size = (6, 7, 8)
+    corners = [(0, 0, 0), (14, 27, 32), (7, 13, 16), (0, 27, 5)]
+    got = port.denoise_f64_blocks(vol, p, sig, corners, size)
+    for c, g in zip(corners, got):
+        w = want[c[0]:c[0] + size[0], c[1]:c[1] + size[1], c[2]:c[2] + size[2]]
+        assert np.array_equal(g, w), f"block at {c}"

@@ -84,3 +84,70 @@ def test_noalloc_em_rejects_oversized_requests(gpu):
     rc = lib.inlm_noise_em_noalloc(None, values.data_ptr(), n, bad.ctypes.data, 1,
                                    out.data_ptr(), out.data_ptr())
     assert rc == -1
+
+
+def test_noalloc_em_empty_windows_store_no_range(gpu):
+    """An empty window (last < first) yields zeros whatever its indices are,
+    and does not shift the scratch of the windows after it: first = 2^32,
+    last = 5 would read as 0..5 if the indices were truncated to 32 bits."""
+    torch = pytest.importorskip("torch")
+    lib = _lib.load()
+    vol = synth.small_case((16, 40, 48), seed=7)
+    nl = NoiseLevel(6000, 15, vol.shape, seed=2)
+    nl.get_noiselevel(vol, DenoiseParameters(noise_mode="global"))
+    ps = nl.patchstd()
+    nl.close()
+    n = len(ps)
+    want, want_mean = _noalloc_sigma(lib, torch, ps, [[0, n - 1]], 1.0)
+    windows = [[1 << 32, 5], [0, n - 1], [7, 6]]
+    got, mean = _noalloc_sigma(lib, torch, ps, windows, 1.0)
+    assert mean[0] == 0.0 and mean[2] == 0.0
+    assert abs(got[1] / want[0] - 1) <= REL_TOL
+
+
+def test_noalloc_em_beside_a_global_mode_capture(gpu):
+    """The call enqueues kernels only, so it may run on a non-blocking stream
+    while another thread captures a CUDA graph in global capture mode (where
+    cudaMalloc, or a copy from pageable host memory, would invalidate the
+    capture). Both the call and the capture must succeed."""
+    import threading
+    torch = pytest.importorskip("torch")
+    lib = _lib.load()
+    vol = synth.small_case((16, 40, 48), seed=9)
+    nl = NoiseLevel(6000, 15, vol.shape, seed=4)
+    nl.get_noiselevel(vol, DenoiseParameters(noise_mode="global"))
+    ps = nl.patchstd()
+    nl.close()
+    n = len(ps)
+    want, _ = _noalloc_sigma(lib, torch, ps, [[0, n - 1]], 1.0)  # first call, before any capture
+    values = torch.from_numpy(np.ascontiguousarray(ps, np.float32)).cuda()
+    mean = torch.full((1,), -1.0, dtype=torch.float32, device="cuda")
+    sd = torch.full((1,), -1.0, dtype=torch.float32, device="cuda")
+    win = np.array([0, n - 1], np.int64)
+    side = torch.cuda.Stream()  # torch creates its streams with cudaStreamNonBlocking
+    x = torch.zeros(16, device="cuda")
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    capturing, called = threading.Event(), threading.Event()
+    rc_box = []
+
+    def caller():
+        capturing.wait(30)
+        rc_box.append(lib.inlm_noise_em_noalloc(C.c_void_p(side.cuda_stream), values.data_ptr(), n,
+                                                win.ctypes.data, 1, mean.data_ptr(), sd.data_ptr()))
+        called.set()
+
+    t = threading.Thread(target=caller)
+    t.start()
+    with torch.cuda.graph(graph, capture_error_mode="global"):
+        capturing.set()
+        assert called.wait(30), "the call did not return while the capture was open"
+        x.add_(1.0)
+    t.join(30)
+    assert rc_box == [0], lib.inlm_last_error()
+    side.synchronize()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert float(x.sum()) == 16.0
+    got = (mean.cpu().numpy() + sd.cpu().numpy()).astype(np.float32)
+    assert abs(got[0] / want[0] - 1) <= REL_TOL
