@@ -158,6 +158,22 @@ int inlm_tile_grid(inlm_denoiser* d, int tile_shape[3], int tiles[3]);
 int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const int* count, const int* offsets,
                          int n_offsets, int on_device);
 
+/* Test hooks for the failure paths (no counterpart in the reference, whose
+ * allocation failures surface as CUDA error strings, iternlm_gpu.cu:1608-1618).
+ * inlm_debug_fail_allocation(n): the device allocation that follows n further
+ * successful ones fails, once, as cudaMalloc fails when memory runs out (the
+ * calling entry point then returns INLM_ERR_NOMEM and releases what it had
+ * allocated); n < 0 disarms. inlm_debug_live_allocations: the number of device
+ * allocations of this library not yet released (a leak check). */
+int inlm_debug_fail_allocation(int64_t n);
+int inlm_debug_live_allocations(int64_t* n);
+/* Runs, on the handle's stream, a one-CTA kernel whose bounded mbarrier wait
+ * (the wait of every TMA-staged filter kernel, ~1 s budget there) is never
+ * satisfied, with a budget of `cycles` (0..2e9): the wait gives up, the kernel
+ * records the timeout in the handle's error word and returns, and this call
+ * returns INLM_ERR_TIMEOUT as a filter call would. The handle stays usable. */
+int inlm_debug_wait_expiry(inlm_denoiser* d, int64_t cycles);
+
 /* Number of kernels this handle has launched since creation. */
 int inlm_kernel_launches(inlm_denoiser* d, uint64_t* count);
 
@@ -377,6 +393,38 @@ int inlm_denoise_multi(const int shape[3], const inlm_params* p, const float* ra
                        float* sigma1_out);
 /* Number of CUDA devices this process sees (0 without a driver or device). */
 int inlm_device_count(int* n);
+/* Free and total memory of a device in bytes (cudaMemGetInfo; the reference
+ * sizes its blocks from it, iternlm_gpu.cu:1537-1566). */
+int inlm_device_memory(int device, size_t* free_bytes, size_t* total_bytes);
+
+/* ---------------- one iteration at a time over host-resident volumes ----------------
+ * replaces the host-RAM overload of IterativeNLM_GPU::Run_GaussianNoise_GPUBlocks
+ * (iternlm_gpu.h:31, iternlm_gpu.cu:1729-1886), which the reference driver
+ * calls once per iteration when the stack is larger than one GPU holds or
+ * runs on several GPUs (main.cpp:379, 472). With one device the volume is
+ * walked in z-slabs of slab_depth slices (rounded up to 8) as
+ * inlm_stream_denoise does; with several, the stack is split over them as
+ * inlm_denoise_multi does. The caller schedules sigma and the iterations (and
+ * estimates the noise), as with the single-volume handle. Results equal
+ * inlm_run_iteration's bit for bit in every precision form (no proposal).
+ * Unlike the reference, which overwrites its previous-iterate buffer slab by
+ * slab while later slabs still read it, a call reads prev_host and writes a
+ * distinct out_host. */
+typedef struct inlm_blocks inlm_blocks;
+/* device_ids: n_devices ids (may repeat; NULL with one device: p->device_id). */
+int inlm_blocks_create(const int shape[3], const inlm_params* p, int n_devices,
+                       const int* device_ids, int slab_depth, inlm_blocks** out);
+int inlm_blocks_destroy(inlm_blocks* b);
+/* Slices per slab (one device) or the deepest part (several). */
+int inlm_blocks_slab_depth(const inlm_blocks* b, int* depth);
+/* sigma of the following iterations, nz floats (host). */
+int inlm_blocks_set_sigma(inlm_blocks* b, const float* sigma_host);
+/* Iteration iter (>= 1) from raw_host and, for iter > 1, the previous iterate
+ * prev_host, into out_host (nx*ny*nz floats each, host; out_host != prev_host).
+ * The buffers are page-locked for the duration of the call where they are not
+ * already. Returns once out_host holds the result. */
+int inlm_blocks_run_iteration(inlm_blocks* b, int iter, const float* raw_host,
+                              const float* prev_host, float* out_host);
 
 /* ---------------- resume ---------------- */
 

@@ -44,6 +44,9 @@ EXPORTS = (
     "inlm_noise_estimate_from_patchstd", "inlm_rgb_denoise", "inlm_tiff_read_rgb",
     "inlm_tiff_write_rgb", "inlm_attach_proposal_grouped", "inlm_proposal_select_grouped",
     "inlm_stream_denoise_grouped", "inlm_denoise_multi", "inlm_device_count",
+    "inlm_blocks_create", "inlm_blocks_destroy", "inlm_blocks_slab_depth", "inlm_blocks_set_sigma",
+    "inlm_blocks_run_iteration", "inlm_device_memory", "inlm_debug_fail_allocation",
+    "inlm_debug_live_allocations", "inlm_debug_wait_expiry",
 )
 
 
@@ -157,6 +160,15 @@ def load(path: str = "") -> C.CDLL:
                                       C.c_int, C.c_float, vp, vp, vp]
     L.inlm_set_result.argtypes = [vp, C.c_int, vp, vp]
     L.inlm_device_count.argtypes = [C.POINTER(C.c_int)]
+    L.inlm_debug_fail_allocation.argtypes = [C.c_int64]
+    L.inlm_debug_live_allocations.argtypes = [C.POINTER(C.c_int64)]
+    L.inlm_debug_wait_expiry.argtypes = [vp, C.c_int64]
+    L.inlm_device_memory.argtypes = [C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+    L.inlm_blocks_create.argtypes = [C.c_int * 3, C.POINTER(InlmParams), C.c_int, vp, C.c_int, C.POINTER(vp)]
+    L.inlm_blocks_destroy.argtypes = [vp]
+    L.inlm_blocks_slab_depth.argtypes = [vp, C.POINTER(C.c_int)]
+    L.inlm_blocks_set_sigma.argtypes = [vp, vp]
+    L.inlm_blocks_run_iteration.argtypes = [vp, C.c_int, vp, vp, vp]
     L.inlm_denoise_multi.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp, vp, vp]
     L.inlm_stream_denoise_grouped.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp,
                                               C.c_int, C.c_float, C.c_int, vp, vp, vp]

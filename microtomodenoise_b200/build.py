@@ -45,6 +45,7 @@ LIB_SOURCES = [
     "color_kernels.cu",
     "api_color.cu",
     "api_multi.cu",
+    "api_blocks.cu",
     "geometry.cpp",
     "sampling.cpp",
     "tiff_io.cpp",

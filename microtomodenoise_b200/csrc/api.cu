@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -17,6 +18,7 @@
 
 #include "api_internal.hpp"
 #include "noise_kernels.cuh"
+#include "common.cuh"
 #include "sampling.hpp"
 
 using namespace inlm;
@@ -36,6 +38,54 @@ int inlm::fail(int code, const char* fmt, ...) {
 }
 
 extern "C" const char* inlm_last_error(void) { return g_last_error.c_str(); }
+
+// ---------------- device allocations ----------------
+
+// Live device allocations of the library, and the allocation-failure
+// injection of the tests: with g_fail_after = n >= 0 the allocation after n
+// further successful ones fails (once) as cudaMalloc does when memory runs out.
+static std::atomic<long long> g_live_allocations{0};
+static std::atomic<long long> g_fail_after{-1};
+
+cudaError_t inlm::device_malloc(void** p, size_t bytes) {
+    *p = nullptr;
+    long long n = g_fail_after.load();
+    while (n >= 0) {
+        if (g_fail_after.compare_exchange_weak(n, n - 1)) {
+            if (n == 0) return cudaErrorMemoryAllocation;  // now -1: disarmed
+            break;
+        }
+    }
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) g_live_allocations++;
+    return e;
+}
+
+cudaError_t inlm::device_free(void* p) {
+    if (!p) return cudaSuccess;
+    g_live_allocations--;
+    return cudaFree(p);
+}
+
+extern "C" int inlm_debug_fail_allocation(int64_t after) {
+    g_fail_after.store(after < 0 ? -1 : after);
+    return INLM_OK;
+}
+
+extern "C" int inlm_debug_wait_expiry(inlm_denoiser* d, int64_t cycles) {
+    if (!d) return fail(INLM_ERR_ARG, "null handle");
+    if (cycles < 0 || cycles > kWaitCycles) return fail(INLM_ERR_ARG, "cycles outside 0..%lld", kWaitCycles);
+    CUDA_TRY(cudaSetDevice(d->device));
+    CUDA_TRY(launch_selftest_wait(d->d_err, (long long)cycles, d->stream));
+    d->launches++;
+    return check_device_error(d);
+}
+
+extern "C" int inlm_debug_live_allocations(int64_t* n) {
+    if (!n) return fail(INLM_ERR_ARG, "null argument");
+    *n = g_live_allocations.load();
+    return INLM_OK;
+}
 
 extern "C" void inlm_default_params(inlm_params* p) {
     // protocol::DenoiseParameters defaults, denoise_parameters.h:11-73
@@ -106,15 +156,15 @@ static int encode_map_3d(CUtensorMap* tm, const void* base, int ex, int ey, int 
 void inlm::noise_free(inlm_noise* n) {
     if (!n) return;
     cudaSetDevice(n->device);
-    cudaFree(n->d_samples);
-    cudaFree(n->d_patchstd);
-    cudaFree(n->d_stack);
-    cudaFree(n->d_windows);
-    cudaFree(n->d_scratch_off);
-    cudaFree(n->d_assign);
-    cudaFree(n->d_mean);
-    cudaFree(n->d_sd);
-    cudaFree(n->d_sigma);
+    device_free(n->d_samples);
+    device_free(n->d_patchstd);
+    device_free(n->d_stack);
+    device_free(n->d_windows);
+    device_free(n->d_scratch_off);
+    device_free(n->d_assign);
+    device_free(n->d_mean);
+    device_free(n->d_sd);
+    device_free(n->d_sigma);
     if (n->own_stream && n->stream) cudaStreamDestroy(n->stream);
 }
 
@@ -195,7 +245,7 @@ int inlm::noise_prepare(inlm_noise* n, const inlm_params* p, int* nwin, bool* fi
                 total += std::max(0, en[z] - st[z] + 1);
             }
             if ((size_t)total > n->assign_cap) {
-                cudaFree(n->d_assign);
+                device_free(n->d_assign);
                 n->d_assign = nullptr;
                 n->assign_cap = 0;
                 CUDA_TRY(dalloc(&n->d_assign, (size_t)total));
@@ -215,7 +265,7 @@ int inlm::noise_prepare(inlm_noise* n, const inlm_params* p, int* nwin, bool* fi
             int2 w = make_int2(0, (int)ns - 1);
             long long off = 0;
             if ((size_t)ns > n->assign_cap) {
-                cudaFree(n->d_assign);
+                device_free(n->d_assign);
                 n->d_assign = nullptr;
                 n->assign_cap = 0;
                 CUDA_TRY(dalloc(&n->d_assign, (size_t)ns));
@@ -244,9 +294,12 @@ int inlm::noise_em_finish(inlm_noise* n, const inlm_params* p, int nwin) {
     return INLM_OK;
 }
 
+// d_stack NULL: the stack is in host memory (h_stack) and larger than the
+// device holds; its samples' patch stds are taken slab by slab through the
+// staging buffer n->d_stack (n->stack_slices slices).
 static int noise_estimate_device(inlm_noise* n, inlm_params* p, const float* d_stack,
                                  long long pitch_y, long long pitch_z, std::vector<float>* host_sigma,
-                                 bool* sigma_on_host) {
+                                 bool* sigma_on_host, const float* h_stack = nullptr) {
     const int nz = n->shape[2];
     *sigma_on_host = false;
     const int mode = p->noise_mode;
@@ -265,9 +318,27 @@ static int noise_estimate_device(inlm_noise* n, inlm_params* p, const float* d_s
     int rc = noise_prepare(n, p, &nwin, &first);
     if (rc) return rc;
     const long long ns = (long long)n->samples.size();
-    CUDA_TRY(launch_noise_patchstd(d_stack, pitch_y, pitch_z, n->shape[0],
-                                   (long long)n->shape[0] * n->shape[1], n->d_samples, ns,
-                                   n->patchsize, n->d_patchstd, n->stream));
+    const long long plane = (long long)n->shape[0] * n->shape[1];
+    if (d_stack) {
+        CUDA_TRY(launch_noise_patchstd(d_stack, pitch_y, pitch_z, n->shape[0], plane, n->d_samples, ns,
+                                       n->patchsize, n->d_patchstd, n->stream));
+    } else {
+        // patches lie within one slice, so each slab gives its own samples' stds
+        const int S = std::max(1, n->stack_slices);
+        for (int z0 = 0; z0 < nz; z0 += S) {
+            const int z1 = std::min(nz, z0 + S);
+            const long long i0 = std::lower_bound(n->samples.begin(), n->samples.end(), z0 * plane) -
+                                 n->samples.begin();
+            const long long i1 = std::lower_bound(n->samples.begin(), n->samples.end(), z1 * plane) -
+                                 n->samples.begin();
+            if (i1 == i0) continue;
+            CUDA_TRY(cudaMemcpyAsync(n->d_stack, h_stack + z0 * plane, (size_t)(z1 - z0) * plane * 4,
+                                     cudaMemcpyHostToDevice, n->stream));
+            CUDA_TRY(launch_noise_patchstd(n->d_stack, n->shape[0], plane, n->shape[0], plane,
+                                           n->d_samples + i0, i1 - i0, n->patchsize, n->d_patchstd + i0,
+                                           n->stream, z0));
+        }
+    }
     if (mode == INLM_NOISE_SEMIMANUAL) {
         // noiselevel.cpp:62-79
         std::vector<float> ps(ns);
@@ -303,14 +374,29 @@ extern "C" int inlm_noise_estimate(inlm_noise* n, inlm_params* p, const float* s
     const long long nvox = (long long)n->shape[0] * n->shape[1] * n->shape[2];
     const float* d_stack = stack;
     if (!on_device) {
-        if (!n->d_stack) CUDA_TRY(dalloc(&n->d_stack, nvox));
-        CUDA_TRY(cudaMemcpyAsync(n->d_stack, stack, nvox * 4, cudaMemcpyHostToDevice, n->stream));
-        d_stack = n->d_stack;
+        const long long plane = (long long)n->shape[0] * n->shape[1];
+        if (!n->d_stack) {
+            // the whole stack where it fits, else a staging slab of <= 256 MiB
+            if (dalloc(&n->d_stack, nvox) == cudaSuccess) {
+                n->stack_slices = n->shape[2];
+            } else {
+                cudaGetLastError();
+                n->d_stack = nullptr;
+                n->stack_slices = (int)std::max<long long>(1, std::min<long long>(n->shape[2], (256ll << 20) / (plane * 4)));
+                CUDA_TRY(dalloc(&n->d_stack, n->stack_slices * plane));
+            }
+        }
+        if (n->stack_slices == n->shape[2]) {
+            CUDA_TRY(cudaMemcpyAsync(n->d_stack, stack, nvox * 4, cudaMemcpyHostToDevice, n->stream));
+            d_stack = n->d_stack;
+        } else {
+            d_stack = nullptr;  // slab by slab from the host
+        }
     }
     std::vector<float> hs;
     bool on_host = false;
     int rc = noise_estimate_device(n, p, d_stack, n->shape[0], (long long)n->shape[0] * n->shape[1],
-                                   &hs, &on_host);
+                                   &hs, &on_host, on_device ? nullptr : stack);
     if (rc != INLM_OK) return rc;
     if (on_host) {
         std::memcpy(sigma_out, hs.data(), n->shape[2] * 4);
@@ -356,7 +442,13 @@ extern "C" int inlm_noise_patchstd_slab(inlm_noise* n, const inlm_params* p, con
     const long long plane = (long long)n->shape[0] * n->shape[1];
     const float* d_slab = slab;
     if (!on_device) {
-        if (!n->d_stack) CUDA_TRY(dalloc(&n->d_stack, plane * nz));
+        if (!n->d_stack || n->stack_slices < n_slices) {
+            CUDA_TRY(cudaStreamSynchronize(n->stream));
+            device_free(n->d_stack);
+            n->d_stack = nullptr;
+            CUDA_TRY(dalloc(&n->d_stack, plane * nz));
+            n->stack_slices = nz;
+        }
         CUDA_TRY(cudaMemcpyAsync(n->d_stack, slab, plane * n_slices * 4, cudaMemcpyHostToDevice, n->stream));
         d_slab = n->d_stack;
     }
@@ -442,23 +534,23 @@ static void denoiser_free(inlm_denoiser* d) {
         cudaEventDestroy(t.a);
         cudaEventDestroy(t.b);
     }
-    cudaFree(d->d_raw_pad);
-    cudaFree(d->d_prev_pad);
-    cudaFree(d->d_next);
-    cudaFree(d->d_sigma);
-    cudaFree(d->d_sigma0);
-    cudaFree(d->d_mult);
-    cudaFree(d->d_err);
-    cudaFree(d->d_search_delta);
-    cudaFree(d->d_group_zb);
-    cudaFree(d->d_search_off);
-    cudaFree(d->d_patch_off);
-    cudaFree(d->d_weights);
-    cudaFree(d->d_raw_h);
-    cudaFree(d->d_prev_h);
-    cudaFree(d->d_plan_start);
-    cudaFree(d->d_plan_off);
-    cudaFree(d->d_search_delta8);
+    device_free(d->d_raw_pad);
+    device_free(d->d_prev_pad);
+    device_free(d->d_next);
+    device_free(d->d_sigma);
+    device_free(d->d_sigma0);
+    device_free(d->d_mult);
+    device_free(d->d_err);
+    device_free(d->d_search_delta);
+    device_free(d->d_group_zb);
+    device_free(d->d_search_off);
+    device_free(d->d_patch_off);
+    device_free(d->d_weights);
+    device_free(d->d_raw_h);
+    device_free(d->d_prev_h);
+    device_free(d->d_plan_start);
+    device_free(d->d_plan_off);
+    device_free(d->d_search_delta8);
     proposal_release(d);
     d->aux.release();
     if (d->noise) {
@@ -575,7 +667,7 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     }
     if (sm == 0 || sm > (size_t)smem_max) return INLM_OK;
     if (a.raw_slab) {
-        cudaFree(d->d_group_zb);
+        device_free(d->d_group_zb);
         d->d_group_zb = nullptr;
         CUDA_TRY(dalloc(&d->d_group_zb, zb.size()));
         CUDA_TRY(cudaMemcpy(d->d_group_zb, zb.data(), zb.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -783,8 +875,8 @@ extern "C" int inlm_denoiser_create(const int shape[3], const inlm_params* p, in
         dalloc(&d->d_err, 1) != cudaSuccess || cudaMemset(d->d_err, 0, 4) != cudaSuccess)
         return bail(fail(INLM_ERR_NOMEM, "device allocation failed"));
     if (f16) {
-        if (cudaMalloc(&d->d_raw_h, npad * 2) != cudaSuccess ||
-            cudaMalloc(&d->d_prev_h, npad * 2) != cudaSuccess)
+        if (device_malloc(&d->d_raw_h, npad * 2) != cudaSuccess ||
+            device_malloc(&d->d_prev_h, npad * 2) != cudaSuccess)
             return bail(fail(INLM_ERR_NOMEM, "device allocation of %.2f GB failed",
                              (2.0 * npad * 2 + nvox * 4) / 1e9));
         if (cudaMemset(d->d_raw_h, 0, npad * 2) != cudaSuccess ||
@@ -1348,7 +1440,7 @@ extern "C" int inlm_set_offset_plan(inlm_denoiser* d, const int* start, const in
     }
     if (!d->d_plan_start) CUDA_TRY(dalloc(&d->d_plan_start, 2 * (size_t)n));
     if (d->plan_cap < std::max(n_offsets, 1)) {
-        cudaFree(d->d_plan_off);
+        device_free(d->d_plan_off);
         d->d_plan_off = nullptr;
         d->plan_cap = 0;
         CUDA_TRY(dalloc(&d->d_plan_off, (size_t)std::max(n_offsets, 1)));

@@ -242,9 +242,9 @@ static void batch_free(inlm_batch* b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     for (inlm_denoiser* d : b->d)
         if (d) inlm_denoiser_destroy(d);
-    for (float* p : b->in) cudaFree(p);
-    for (float* p : b->sigma_manual) cudaFree(p);
-    cudaFree(b->d_counters);
+    for (float* p : b->in) device_free(p);
+    for (float* p : b->sigma_manual) device_free(p);
+    device_free(b->d_counters);
     for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
     for (cudaEvent_t e : b->join) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);

@@ -33,17 +33,17 @@ struct RgbJob {
     std::vector<float> host;       // one channel-triple staging area
     ~RgbJob() {
         for (auto& b : ch)
-            for (float* p : b) cudaFree(p);
-        cudaFree(d_samples);
-        cudaFree(d_ps);
-        cudaFree(d_win);
-        cudaFree(d_off);
-        cudaFree(d_assign);
-        cudaFree(d_mean);
-        cudaFree(d_sd);
-        cudaFree(d_search);
-        cudaFree(d_taps);
-        cudaFree(d_w);
+            for (float* p : b) device_free(p);
+        device_free(d_samples);
+        device_free(d_ps);
+        device_free(d_win);
+        device_free(d_off);
+        device_free(d_assign);
+        device_free(d_mean);
+        device_free(d_sd);
+        device_free(d_search);
+        device_free(d_taps);
+        device_free(d_w);
         if (st) cudaStreamDestroy(st);
     }
 };

@@ -25,11 +25,18 @@ namespace inlm {
 // Records the calling thread's error text (inlm_last_error) and returns code.
 int fail(int code, const char* fmt, ...);
 
+// Every device allocation and release of the library goes through these two:
+// they keep the live-allocation count and carry the allocation-failure
+// injection of the tests (inlm_debug_fail_allocation). device_free(NULL) is a
+// no-op.
+cudaError_t device_malloc(void** p, size_t bytes);
+cudaError_t device_free(void* p);
+
 template <typename T>
 static inline cudaError_t dalloc(T** p, size_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
-    return cudaMalloc((void**)p, n * sizeof(T));
+    return device_malloc((void**)p, n * sizeof(T));
 }
 
 // Grow-only device buffer.
@@ -38,15 +45,15 @@ struct DevBuf {
     size_t bytes = 0;
     cudaError_t ensure(size_t n) {
         if (n <= bytes && p) return cudaSuccess;
-        cudaFree(p);
+        device_free(p);
         p = nullptr;
         bytes = 0;
-        cudaError_t e = cudaMalloc(&p, n ? n : 1);
+        cudaError_t e = device_malloc(&p, n ? n : 1);
         if (e == cudaSuccess) bytes = n;
         return e;
     }
     void release() {
-        cudaFree(p);
+        device_free(p);
         p = nullptr;
         bytes = 0;
     }
@@ -85,6 +92,7 @@ struct inlm_noise {
     long long* d_samples = nullptr;
     float* d_patchstd = nullptr;
     float* d_stack = nullptr;  // staging for host stacks
+    int stack_slices = 0;      // slices d_stack holds: nz, or a slab when the stack does not fit
     int zwindow_cached = -1;
     int2* d_windows = nullptr;
     long long* d_scratch_off = nullptr;
@@ -205,4 +213,25 @@ int noise_em_finish(inlm_noise* n, const inlm_params* p, int nwin);
 // filter's plan at its per-CTA lists (api_proposal.cu).
 int proposal_enqueue(inlm_denoiser* d);
 void proposal_release(inlm_denoiser* d);
+
+// Per-iteration engines over host-resident volumes (inlm_blocks_*): z-slab
+// streaming on one device (api_stream.cu) or the stack split over several
+// devices (api_multi.cu).
+struct BlocksBackend {
+    virtual ~BlocksBackend() {}
+    virtual int set_sigma(const float* sigma_host) = 0;
+    virtual int iteration(int iter, const float* raw_host, const float* prev_host, float* out_host) = 0;
+    virtual int slab_depth() const = 0;
+};
+int make_stream_blocks(const int shape[3], const inlm_params* p, int slab_depth, BlocksBackend** out);
+int make_multi_blocks(const int shape[3], const inlm_params* p, int n_parts, const int* device_ids,
+                      BlocksBackend** out);
 }  // namespace inlm
+
+struct inlm_blocks {
+    inlm::BlocksBackend* be = nullptr;
+    int shape[3] = {0, 0, 0};
+    int last_iter = 0;
+    bool sigma_set = false;
+    ~inlm_blocks() { delete be; }
+};

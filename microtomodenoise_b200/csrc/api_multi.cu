@@ -14,6 +14,7 @@
 // bit for bit in every precision form. Devices may repeat in the list (two
 // sub-volumes on one GPU), which is how a one-GPU machine runs this path.
 #include <algorithm>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -35,7 +36,7 @@ struct Part {
         if (noise) inlm_noise_destroy(noise);
         if (d_stage) {
             cudaSetDevice(device);
-            cudaFree(d_stage);
+            device_free(d_stage);
         }
     }
 };
@@ -253,5 +254,107 @@ extern "C" int inlm_device_count(int* n) {
         cudaGetLastError();
         *n = 0;
     }
+    return INLM_OK;
+}
+
+// ---------------- per-iteration engine over several devices ----------------
+//
+// The same split, one iteration per call with the caller's sigma and buffers
+// (the n_gpus blocks of IterativeNLM_GPU::Run_GaussianNoise_GPUBlocks,
+// Denoiser/iternlm_gpu.cu:1729-1886): iteration 1 takes each part's slices of
+// raw; a later iteration installs each part's sub-volume of the previous
+// iterate from host memory (its halos included, so no device-to-device
+// exchange is needed) and filters it; every part's owned slices go to the
+// output.
+namespace {
+
+struct MultiBlocks final : BlocksBackend {
+    std::vector<Part> parts;
+    long long plane = 0;
+    int depth = 0;
+    int slab_depth() const override { return depth; }
+    int set_sigma(const float* sigma) override {
+        return each_part(parts, [&](size_t i) -> int { return inlm_set_sigma(parts[i].d, sigma + parts[i].a); });
+    }
+    int iteration(int it, const float* raw, const float* prev, float* out) override {
+        return each_part(parts, [&](size_t i) -> int {
+            Part& q = parts[i];
+            const long long off = (long long)q.a * plane;
+            int r;
+            if (it == 1) {
+                r = inlm_run_iteration(q.d, 1, raw + off);
+            } else {
+                // the whole sub-volume, halos included, from the caller's previous
+                // iterate (raw is padded once, with the first installed result)
+                r = q.d->last_iter < 1 ? inlm_set_result(q.d, 1, prev + off, raw + off)
+                                       : inlm_set_result(q.d, it - 1, prev + off, nullptr);
+                if (!r) r = inlm_run_iteration(q.d, it, nullptr);
+            }
+            if (r) return r;
+            return inlm_get_result_slices(q.d, q.z0 - q.a, q.z1 - q.z0, out + (long long)q.z0 * plane, 0);
+        });
+    }
+};
+
+}  // namespace
+
+int inlm::make_multi_blocks(const int shape[3], const inlm_params* p, int n_parts, const int* device_ids,
+                            BlocksBackend** out) {
+    if (n_parts < 1 || !device_ids) return fail(INLM_ERR_ARG, "n_parts must be >= 1");
+    const int nz = shape[2];
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(INLM_ERR_NODEVICE, "no CUDA device");
+    }
+    for (int i = 0; i < n_parts; i++)
+        if (device_ids[i] < 0 || device_ids[i] >= ndev)
+            return fail(INLM_ERR_ARG, "device %d of %d", device_ids[i], ndev);
+    const int units = (nz + 7) / 8;
+    if (units < n_parts) return fail(INLM_ERR_ARG, "%d slices give fewer than %d slabs of 8", nz, n_parts);
+    const int pz = std::min(p->nslices / 2, p->search_radius[2]) + p->patch_radius[2];
+    const int halo = (std::max(pz, 1) + 7) / 8 * 8;
+    auto* b = new MultiBlocks();
+    std::unique_ptr<MultiBlocks> guard(b);
+    b->plane = (long long)shape[0] * shape[1];
+    b->parts.resize(n_parts);
+    int u = 0;
+    for (int i = 0; i < n_parts; i++) {
+        const int n = units / n_parts + (i < units % n_parts ? 1 : 0);
+        Part& q = b->parts[i];
+        q.device = device_ids[i];
+        q.z0 = std::min(nz, 8 * u);
+        q.z1 = std::min(nz, 8 * (u + n));
+        u += n;
+        q.a = std::max(0, q.z0 - halo);
+        q.b = std::min(nz, q.z1 + halo);
+        b->depth = std::max(b->depth, q.z1 - q.z0);
+        if (n_parts > 1 && q.z1 - q.z0 < halo)
+            return fail(INLM_ERR_ARG, "slab %d..%d is shallower than the halo of %d slices", q.z0, q.z1 - 1, halo);
+    }
+    const inlm_params q0 = *p;
+    int rc = each_part(b->parts, [&](size_t i) -> int {
+        Part& q = b->parts[i];
+        inlm_params qi = q0;
+        qi.device_id = q.device;
+        qi.n_samples = 0;  // the caller estimates the noise
+        const int sh[3] = {shape[0], shape[1], q.b - q.a};
+        return inlm_denoiser_create(sh, &qi, &q.d);
+    });
+    if (rc) return rc;
+    *out = guard.release();
+    return INLM_OK;
+}
+
+extern "C" int inlm_device_memory(int device, size_t* free_bytes, size_t* total_bytes) {
+    if (!free_bytes || !total_bytes) return fail(INLM_ERR_ARG, "null argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(INLM_ERR_NODEVICE, "no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return fail(INLM_ERR_ARG, "device %d of %d", device, ndev);
+    CUDA_TRY(cudaSetDevice(device));
+    CUDA_TRY(cudaMemGetInfo(free_bytes, total_bytes));
     return INLM_OK;
 }

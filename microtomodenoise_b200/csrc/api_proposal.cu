@@ -22,12 +22,12 @@ static void proposal_free(inlm_proposal* p) {
     if (!p) return;
     cudaSetDevice(p->device);
     if (p->stream) cudaStreamSynchronize(p->stream);
-    cudaFree(p->d_w);
-    cudaFree(p->d_m);
-    cudaFree(p->d_v);
-    cudaFree(p->d_g);
-    cudaFree(p->d_wb);
-    cudaFree(p->d_loss);
+    device_free(p->d_w);
+    device_free(p->d_m);
+    device_free(p->d_v);
+    device_free(p->d_g);
+    device_free(p->d_wb);
+    device_free(p->d_loss);
     for (DevBuf* b : {&p->pad, &p->a1, &p->a2, &p->a3, &p->a4, &p->glog, &p->d1, &p->d2, &p->d3,
                       &p->d4, &p->counters})
         b->release();

@@ -18,6 +18,7 @@
 //     EM once over all samples.
 // Results equal the in-memory schedule (inlm_denoise) bit for bit.
 #include <map>
+#include <memory>
 
 #include "api_internal.hpp"
 #include "noise_kernels.cuh"
@@ -49,11 +50,11 @@ struct StreamJob {
         for (auto& kv : pairs)
             for (int j = 0; j < 2; j++) {
                 if (kv.second.d[j]) inlm_denoiser_destroy(kv.second.d[j]);
-                cudaFree(kv.second.stage[j]);
+                device_free(kv.second.stage[j]);
             }
         if (noise) inlm_noise_destroy(noise);
-        cudaFree(d_sig0);
-        cudaFree(d_sig);
+        device_free(d_sig0);
+        device_free(d_sig);
         if (tmp_host) cudaFreeHost(tmp_host);
         if (reg_raw) cudaHostUnregister(const_cast<float*>(raw_host));
         if (reg_out) cudaHostUnregister(out_host);
@@ -91,6 +92,82 @@ int get_pair(StreamJob& J, const inlm_params& p, int depth, inlm_proposal* net, 
         }
     }
     *out = &sp;
+    return INLM_OK;
+}
+
+// One iteration over every slab: slab [z0, z1) is filtered as the sub-volume
+// [z0 - halo, z1 + halo) on one of the two denoisers of its depth (they
+// alternate, so one slab's copies overlap the other's kernels); raw from
+// raw_host, the previous iterate from prev_host (iteration > 1), the slab's
+// result to next_host. With patchstd, each slab's result also gives the
+// patch stds of the samples in its own slices. J.d_sig holds the sigma of
+// this iteration; every slab's stream waits for the event `ready` first.
+int stream_pass(StreamJob& J, const inlm_params& p, int it, const std::vector<int>& z0s, int sd,
+                int halo, inlm_proposal* net, int k, float min_mass, const float* raw_host,
+                const float* prev_host, float* next_host, bool patchstd, cudaEvent_t ready,
+                double* h2d, double* d2h) {
+    const int nz = J.shape[2];
+    int s = 0;
+    for (int z0 : z0s) {
+        const int z1 = std::min(nz, z0 + sd);
+        const int a = std::max(0, z0 - halo), b = std::min(nz, z1 + halo);
+        SlabPair* sp;
+        int rc = get_pair(J, p, b - a, net, k, min_mass, &sp);
+        if (rc) return rc;
+        const int j = s++ & 1;
+        inlm_denoiser* d = sp->d[j];
+        cudaStream_t st = d->stream;
+        const size_t sub = (size_t)(b - a) * J.plane * 4;
+        // the sub-volume's sigma slice and multiplier
+        CUDA_TRY(cudaStreamWaitEvent(st, ready, 0));
+        CUDA_TRY(cudaMemcpyAsync(d->d_sigma, J.d_sig + a, (b - a) * 4, cudaMemcpyDeviceToDevice, st));
+        rc = upload_sigma_device(d);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(sp->stage[j], raw_host + a * J.plane, sub, cudaMemcpyHostToDevice, st));
+        *h2d += sub;
+        if (it > 1) {
+            CUDA_TRY(cudaMemcpyAsync(d->d_next, prev_host + a * J.plane, sub, cudaMemcpyHostToDevice, st));
+            *h2d += sub;
+        }
+        if (d->use_fast) {
+            rc = pad_into_half(d, sp->stage[j], d->d_raw_h);
+            if (rc) return rc;
+            if (it == 1) {
+                CUDA_TRY(cudaMemcpyAsync(d->d_prev_h, d->d_raw_h, d->pitch_z * d->nzp * 2,
+                                         cudaMemcpyDeviceToDevice, st));
+            } else {
+                rc = pad_into_half(d, d->d_next, d->d_prev_h);
+                if (rc) return rc;
+            }
+            if (d->prop.net) {
+                rc = proposal_enqueue(d);
+                if (rc) return rc;
+            }
+        } else {
+            rc = pad_into(d, sp->stage[j], d->d_raw_pad);
+            if (rc) return rc;
+            if (it == 1) {
+                CUDA_TRY(cudaMemcpyAsync(d->d_prev_pad, d->d_raw_pad, d->pitch_z * d->nzp * 4,
+                                         cudaMemcpyDeviceToDevice, st));
+            } else {
+                rc = pad_into(d, d->d_next, d->d_prev_pad);
+                if (rc) return rc;
+            }
+        }
+        rc = launch_filter(d);
+        if (rc) return rc;
+        d->last_iter = it;
+        CUDA_TRY(cudaMemcpyAsync(next_host + z0 * J.plane, d->d_next + (z0 - a) * J.plane,
+                                 (z1 - z0) * J.plane * 4, cudaMemcpyDeviceToHost, st));
+        *d2h += (z1 - z0) * J.plane * 4.0;
+        if (patchstd) {
+            long long i0, i1;
+            sample_range(J.noise->samples, J.plane, z0, z1, &i0, &i1);
+            CUDA_TRY(launch_noise_patchstd(d->d_next, J.shape[0], J.plane, J.shape[0], J.plane,
+                                           J.noise->d_samples + i0, i1 - i0, J.noise->patchsize,
+                                           J.noise->d_patchstd + i0, st, a));
+        }
+    }
     return INLM_OK;
 }
 
@@ -219,65 +296,10 @@ extern "C" int inlm_stream_denoise_grouped(const int shape[3], const inlm_params
         // the last iteration writes the caller's buffer
         float* next_host = ((maxit - it) % 2 == 0) ? out_host : J.tmp_host;
         const bool estimate = (it == 1 && maxit > 1) || (it > 1 && p->continuous_estimate && maxit > it + 1);
-        int s = 0;
-        for (int z0 : z0s) {
-            const int z1 = std::min(nz, z0 + sd);
-            const int a = std::max(0, z0 - halo), b = std::min(nz, z1 + halo);
-            SlabPair* sp;
-            int rc = get_pair(J, *p, b - a, net, k, min_mass, &sp);
-            if (rc) return rc;
-            const int j = s++ & 1;
-            inlm_denoiser* d = sp->d[j];
-            cudaStream_t st = d->stream;
-            const size_t sub = (size_t)(b - a) * J.plane * 4;
-            // the sub-volume's sigma slice and multiplier
-            CUDA_TRY(cudaStreamWaitEvent(st, t0, 0));
-            CUDA_TRY(cudaMemcpyAsync(d->d_sigma, J.d_sig + a, (b - a) * 4, cudaMemcpyDeviceToDevice, st));
-            rc = upload_sigma_device(d);
-            if (rc) return rc;
-            CUDA_TRY(cudaMemcpyAsync(sp->stage[j], raw_host + a * J.plane, sub, cudaMemcpyHostToDevice, st));
-            h2d += sub;
-            if (it > 1) {
-                CUDA_TRY(cudaMemcpyAsync(d->d_next, prev_host + a * J.plane, sub, cudaMemcpyHostToDevice, st));
-                h2d += sub;
-            }
-            if (d->use_fast) {
-                rc = pad_into_half(d, sp->stage[j], d->d_raw_h);
-                if (rc) return rc;
-                if (it == 1) {
-                    CUDA_TRY(cudaMemcpyAsync(d->d_prev_h, d->d_raw_h, d->pitch_z * d->nzp * 2,
-                                             cudaMemcpyDeviceToDevice, st));
-                } else {
-                    rc = pad_into_half(d, d->d_next, d->d_prev_h);
-                    if (rc) return rc;
-                }
-                if (d->prop.net) {
-                    rc = proposal_enqueue(d);
-                    if (rc) return rc;
-                }
-            } else {
-                rc = pad_into(d, sp->stage[j], d->d_raw_pad);
-                if (rc) return rc;
-                if (it == 1) {
-                    CUDA_TRY(cudaMemcpyAsync(d->d_prev_pad, d->d_raw_pad, d->pitch_z * d->nzp * 4,
-                                             cudaMemcpyDeviceToDevice, st));
-                } else {
-                    rc = pad_into(d, d->d_next, d->d_prev_pad);
-                    if (rc) return rc;
-                }
-            }
-            rc = launch_filter(d);
-            if (rc) return rc;
-            d->last_iter = it;
-            CUDA_TRY(cudaMemcpyAsync(next_host + z0 * J.plane, d->d_next + (z0 - a) * J.plane,
-                                     (z1 - z0) * J.plane * 4, cudaMemcpyDeviceToHost, st));
-            d2h += (z1 - z0) * J.plane * 4.0;
-            if (estimate && !manual) {
-                rc = slab_patchstd(d->d_next, a, z0, z1, st);
-                if (rc) return rc;
-            }
-        }
-        int rc = sync_all();
+        int rc = stream_pass(J, *p, it, z0s, sd, halo, net, k, min_mass, raw_host, prev_host, next_host,
+                             estimate && !manual, t0, &h2d, &d2h);
+        if (rc) return rc;
+        rc = sync_all();
         if (rc) return rc;
         for (auto& kv : J.pairs)
             for (int j = 0; j < 2; j++) {
@@ -317,5 +339,104 @@ extern "C" int inlm_stream_denoise_grouped(const int shape[3], const inlm_params
         stats[4] = halo;
         stats[5] = sd;
     }
+    return INLM_OK;
+}
+
+// ---------------- per-iteration engine on one device ----------------
+//
+// The same slab walk, one iteration per call, with the caller's sigma and the
+// caller's buffers: what the host-RAM overload of
+// IterativeNLM_GPU::Run_GaussianNoise_GPUBlocks (Denoiser/iternlm_gpu.cu:
+// 1729-1886) does for each block of slices. The caller's volumes are
+// page-locked for the duration of a call.
+namespace {
+
+struct HostPin {
+    std::vector<void*> regs;
+    void pin(const void* ptr, size_t bytes) {
+        for (void* r : regs)
+            if (r == ptr) return;
+        if (cudaHostRegister(const_cast<void*>(ptr), bytes, cudaHostRegisterPortable) == cudaSuccess)
+            regs.push_back(const_cast<void*>(ptr));
+        else
+            cudaGetLastError();  // already page-locked, or not registrable: copies still work
+    }
+    ~HostPin() {
+        for (void* r : regs) cudaHostUnregister(r);
+    }
+};
+
+struct StreamBlocks final : BlocksBackend {
+    StreamJob J;
+    inlm_params p;
+    std::vector<int> z0s;
+    int sd = 0, halo = 0;
+    cudaEvent_t ready = nullptr;
+
+    ~StreamBlocks() override {
+        cudaSetDevice(p.device_id);
+        for (auto& kv : J.pairs)
+            for (int j = 0; j < 2; j++)
+                if (kv.second.d[j]) cudaStreamSynchronize(kv.second.d[j]->stream);
+        if (ready) cudaEventDestroy(ready);
+    }
+    int slab_depth() const override { return sd; }
+    int set_sigma(const float* sigma) override {
+        CUDA_TRY(cudaSetDevice(p.device_id));
+        CUDA_TRY(cudaMemcpyAsync(J.d_sig, sigma, J.shape[2] * 4, cudaMemcpyHostToDevice, J.main));
+        CUDA_TRY(cudaEventRecord(ready, J.main));
+        CUDA_TRY(cudaStreamSynchronize(J.main));
+        return INLM_OK;
+    }
+    int iteration(int it, const float* raw, const float* prev, float* out) override {
+        CUDA_TRY(cudaSetDevice(p.device_id));
+        const size_t bytes = (size_t)J.plane * J.shape[2] * 4;
+        HostPin pin;
+        pin.pin(raw, bytes);
+        if (it > 1) pin.pin(prev, bytes);
+        pin.pin(out, bytes);
+        double h2d = 0, d2h = 0;
+        int rc = stream_pass(J, p, it, z0s, sd, halo, nullptr, 0, 0.f, raw, prev, out, false, ready, &h2d,
+                             &d2h);
+        // every slab's copies finish before the buffers are unpinned
+        for (auto& kv : J.pairs)
+            for (int j = 0; j < 2; j++) {
+                cudaError_t e = cudaStreamSynchronize(kv.second.d[j]->stream);
+                if (rc == INLM_OK && e != cudaSuccess) rc = fail(INLM_ERR_CUDA, "%s", cudaGetErrorString(e));
+                if (rc == INLM_OK) rc = check_device_error(kv.second.d[j]);
+            }
+        return rc;
+    }
+};
+
+}  // namespace
+
+int inlm::make_stream_blocks(const int shape[3], const inlm_params* p, int slab_depth, BlocksBackend** out) {
+    if (slab_depth < 1) return fail(INLM_ERR_ARG, "slab depth must be >= 1");
+    CUDA_TRY(cudaSetDevice(p->device_id));
+    auto* b = new StreamBlocks();
+    std::unique_ptr<StreamBlocks> guard(b);
+    b->p = *p;
+    for (int i = 0; i < 3; i++) b->J.shape[i] = shape[i];
+    b->J.plane = (long long)shape[0] * shape[1];
+    const int nz = shape[2];
+    const int pz = std::min(p->nslices / 2, p->search_radius[2]) + p->patch_radius[2];
+    b->halo = round_up8(std::max(pz, 1));
+    b->sd = round_up8(slab_depth);
+    for (int z = 0; z < nz; z += b->sd) b->z0s.push_back(z);
+    CUDA_TRY(cudaStreamCreateWithFlags(&b->J.main, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&b->ready, cudaEventDisableTiming));
+    CUDA_TRY(dalloc(&b->J.d_sig0, nz));
+    CUDA_TRY(dalloc(&b->J.d_sig, nz));
+    // the denoisers of every sub-volume depth, created now so that a device
+    // too small for them fails here rather than in the first iteration
+    for (int z0 : b->z0s) {
+        const int z1 = std::min(nz, z0 + b->sd);
+        SlabPair* sp;
+        int rc = get_pair(b->J, *p, std::min(nz, z1 + b->halo) - std::max(0, z0 - b->halo), nullptr, 0, 0.f,
+                          &sp);
+        if (rc) return rc;
+    }
+    *out = guard.release();
     return INLM_OK;
 }

@@ -1,0 +1,4 @@
+// The reference header Denoiser/iternlm_gpu.h, provided by this library's C++ shim (iternlm.hpp)
+// so that a driver written against the reference compiles unchanged.
+#pragma once
+#include "iternlm.hpp"

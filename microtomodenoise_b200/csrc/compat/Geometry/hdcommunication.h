@@ -1,0 +1,4 @@
+// The reference header Geometry/hdcommunication.h, provided by this library's C++ shim (iternlm.hpp)
+// so that a driver written against the reference compiles unchanged.
+#pragma once
+#include "iternlm.hpp"

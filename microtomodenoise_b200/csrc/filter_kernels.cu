@@ -762,5 +762,28 @@ cudaError_t launch_sigma_blend(const float* sigma0, float* sigma1, float alpha, 
     return cudaGetLastError();
 }
 
+// ---- failure-path self-test of the bounded wait ----
+// One CTA arms an mbarrier for 1024 bytes that no copy delivers and waits on
+// it with mbar_wait_bounded, the wait every TMA-staged kernel uses, under a
+// budget of `cycles`: the wait gives up, the CTA agrees on it as the filter
+// kernels do and records DEV_TMA_TIMEOUT, and the kernel returns. No copy is
+// in flight, so nothing is left pending when the CTA exits.
+__global__ void __launch_bounds__(32) selftest_wait_kernel(int* err, long long cycles) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 1024u);
+    const bool arrived = mbar_wait_bounded(&bar, 0, cycles);
+    if (!__syncthreads_and(arrived) && threadIdx.x == 0) set_error(err, DEV_TMA_TIMEOUT);
+}
+
+cudaError_t launch_selftest_wait(int* err, long long cycles, cudaStream_t st) {
+    selftest_wait_kernel<<<1, 32, 0, st>>>(err, cycles);
+    return cudaGetLastError();
+}
+
 }  // namespace inlm
 

@@ -113,4 +113,8 @@ cudaError_t launch_batch_kernel(int kind, const BatchParams& bp, int ctas, size_
 // the order the kernel accumulates them; used to check host/device agreement.
 int tile_kernel_tap_order(int rx, int ry, int rz, int* xyz, int max_taps);
 
+// Failure-path self-test: a bounded mbarrier wait that nothing satisfies,
+// with a budget of `cycles`; records DEV_TMA_TIMEOUT in *err.
+cudaError_t launch_selftest_wait(int* err, long long cycles, cudaStream_t st);
+
 }  // namespace inlm

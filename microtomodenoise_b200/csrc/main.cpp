@@ -11,8 +11,9 @@
 // image (and <outdir>/denoise_iterations/<image>_iterNN.tif without
 // --cleanup). Not built: the CPU filter (-gpus 0).
 // Additions: -precision f32|f16, -seed N (noise sample draw), -slab N
-// (z-slab depth when the stack does not fit on the device), -gpulist a,b,...
-// (the devices of the multi-GPU split; -gpus N takes N devices from -gpu0).
+// (stream the stack through one device in z-slabs of N slices; without it
+// slabs are used only when the stack does not fit), -gpulist a,b,... (the
+// devices of the multi-GPU split; -gpus N takes N devices from -gpu0).
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -33,112 +34,10 @@ using std::cout;
 using std::endl;
 using std::string;
 
-namespace {
-
-// true when every slice file first..last of the iteration directory exists
-// and all have one size (the --resume test, iternlm_gpu.cu:1665-1684)
-bool iteration_on_disk(const string& dir, int first, int last) {
-    long long size = -1;
-    for (int i = first; i <= last; i++) {
-        struct stat st;
-        const string f = dir + "/denoised" + hdcom::zfill_int2string(i, 4) + ".tif";
-        if (stat(f.c_str(), &st) != 0) return false;
-        if (size < 0) size = (long long)st.st_size;
-        else if ((long long)st.st_size != size) return false;
-    }
-    return true;
-}
-
-float* read_iteration(const string& dir, int first, int last, int shape[3]) {
-    const size_t nslice = (size_t)shape[0] * shape[1];
-    float* out = (float*)malloc(nslice * shape[2] * sizeof(float));
-    for (int i = first; i <= last; i++) {
-        const string f = dir + "/denoised" + hdcom::zfill_int2string(i, 4) + ".tif";
-        if (inlm_tiff_read(f.c_str(), -1, -1, out + (size_t)(i - first) * nslice, nslice) != INLM_OK) {
-            protocol::report(INLM_ERR_IO, "resume");
-            free(out);
-            return nullptr;
-        }
-    }
-    return out;
-}
-
-struct ColorSave {
-    string dir, name;
-    int nx, ny;
-    int status;
-};
-
-// saves one iteration of the colour job (color_denoising.h:73-84)
-void save_color_iteration(int iter, const float* r, const float* g, const float* b, void* user) {
-    ColorSave* s = static_cast<ColorSave*>(user);
-    const int rc = inlm_tiff_write_rgb(s->dir.c_str(), (s->name + "_iter" + hdcom::zfill_int2string(iter, 2)).c_str(),
-                                       r, g, b, s->nx, s->ny);
-    if (rc != INLM_OK) s->status = protocol::report(rc, "saving iteration");
-}
-
-// The colour driver (color_denoise::run_colorimage_denoising,
-// Color/color_denoising.h:19-150): every RGB image of the input, 2D, on the GPU.
-int run_color(const string& inpath, const string& outpath, protocol::DenoiseParameters& params) {
-    std::vector<string> files;
-    const bool single = inpath.size() >= 3 && (inpath.substr(inpath.size() - 3) == "tif" ||
-                                               (inpath.size() >= 4 && inpath.substr(inpath.size() - 4) == "tiff"));
-    if (single) {
-        files.push_back(inpath);
-    } else {
-        std::error_code ec;
-        for (const auto& e : std::filesystem::directory_iterator(inpath, ec)) {
-            const string f = e.path().string();
-            if ((f.size() > 4 && f.substr(f.size() - 4) == ".tif") || (f.size() > 5 && f.substr(f.size() - 5) == ".tiff"))
-                files.push_back(f);
-        }
-        std::sort(files.begin(), files.end());
-    }
-    // the colour driver's fixed settings (color_denoising.h:25-28)
-    params.radius_patchspace[2] = 0;
-    params.radius_searchspace[2] = 0;
-    params.nslices = 1;
-    params.noiselevel.n_samples = 2048;
-    const inlm_params q = protocol::to_inlm(params);
-    const inlm_color_params cp = {params.color.stabilize_variance ? 1 : 0, params.color.independent_channels ? 1 : 0,
-                                  params.color.average_channelsigma ? 1 : 0};
-    for (const string& file : files) {
-        cout << "--------------------------------------" << endl;
-        const size_t slash = file.rfind('/');
-        string name = file.substr(slash == string::npos ? 0 : slash + 1);
-        name = name.substr(0, name.rfind('.'));
-        cout << "image: " << name << endl;
-        int shape[2];
-        if (protocol::report(inlm_tiff_read_rgb(file.c_str(), shape, nullptr, nullptr, nullptr, 0), "reading image"))
-            return -1;
-        const size_t n = (size_t)shape[0] * shape[1];
-        std::vector<float> in(3 * n), out(3 * n);
-        if (protocol::report(inlm_tiff_read_rgb(file.c_str(), shape, in.data(), in.data() + n, in.data() + 2 * n, n),
-                             "reading image"))
-            return -1;
-        ColorSave save{outpath + "/denoise_iterations/", name, shape[0], shape[1], INLM_OK};
-        float s_first[3], s_last[3];
-        const int rc = inlm_rgb_denoise(shape[0], shape[1], &q, &cp, in.data(), in.data() + n, in.data() + 2 * n,
-                                        out.data(), out.data() + n, out.data() + 2 * n,
-                                        params.io.cleanup ? nullptr : save_color_iteration, &save, s_first, s_last);
-        if (protocol::report(rc, "rgb_denoise") || save.status) return -2;
-        cout << "initial noise level: " << s_first[0] << ", " << s_first[1] << ", " << s_first[2] << endl;
-        cout << "final noise level: " << s_last[0] << ", " << s_last[1] << ", " << s_last[2] << endl;
-        if (protocol::report(inlm_tiff_write_rgb(outpath.c_str(), (name + "_denoised").c_str(), out.data(),
-                                                 out.data() + n, out.data() + 2 * n, shape[0], shape[1]),
-                             "saving image"))
-            return -1;
-    }
-    cout << "--------------------------------------" << endl;
-    return 0;
-}
-
-}  // namespace
-
 int main(int argc, char* argv[]) {
     string inpath = "", outpath = "";
     bool verbose = false;
-    int slab_depth = 64;
+    int slab_depth = 0;  // -slab N: stream z-slabs of N slices even when the stack fits
     std::vector<int> gpulist;
     protocol::DenoiseParameters params;
     string rootpath;
@@ -256,7 +155,8 @@ int main(int argc, char* argv[]) {
     }
     if (params.io.rgb) {
         cout << "Switching to RGB-Denoiser!" << endl;
-        return run_color(inpath, outpath, params);
+        std::vector<string> files{inpath};
+        return color_denoise::run_colorimage_denoising(files, outpath, &params);
     }
     if (is_rgb) {
         cout << "Error! RGB input: run with --color" << endl;
@@ -314,67 +214,45 @@ int main(int argc, char* argv[]) {
         return outpath + "/denoise-iteration" + hdcom::zfill_int2string(iter, 2) + "/";
     };
 
-    denoise::IterativeNLM_GPU gpu;
-    const int max_parallelslices = gpu.configure_device(shape, &params);
-    if (max_parallelslices == -2) return -2;
-    if (max_parallelslices == -1) {
-        cout << "Error! No CUDA device found (this build has no CPU filter)" << endl;
-        return -1;
-    }
-
-    float *sigma0 = nullptr, *sigma1 = nullptr;
-    float* output = (float*)malloc(nstack * sizeof(float));
-
-    // several GPUs (-gpus N, the reference's default is 2): the stack split in
-    // z over them, whole job, final iteration saved (as the streamed branch)
+    // devices: -gpulist, else -gpus N from -gpu0 (the reference's n_gpus
+    // mode, default 2), clipped to the devices present
     int n_devices = 0;
     if (inlm_device_count(&n_devices) != INLM_OK) n_devices = 0;
     std::vector<int> ids = gpulist;
     if (ids.empty())
-        for (int i = 0; i < std::min(params.gpu.n_gpus, n_devices); i++)
-            ids.push_back((params.gpu.deviceID + i) % std::max(n_devices, 1));
-    const int n_use = (int)ids.size();
-    // the split's thinnest slab (8-slice units split evenly; the last part may
-    // lose up to 7 slices to the stack's end) must cover the z halo
+        for (int i = 0; i < std::min(params.gpu.n_gpus, n_devices - params.gpu.deviceID); i++)
+            ids.push_back(params.gpu.deviceID + i);
+    if (ids.empty() && n_devices > 0) ids.push_back(params.gpu.deviceID % n_devices);
+    // a split needs every part at least one z halo deep (8-slice units split
+    // evenly; the last part may lose up to 7 slices to the stack's end)
     const int zpad = std::min(params.nslices / 2, params.radius_searchspace[2]) + params.radius_patchspace[2];
     const int halo = (std::max(zpad, 1) + 7) / 8 * 8;
     const int units = (shape[2] + 7) / 8;
-    const bool slabs_deep = n_use > 1 && 8 * (units / n_use) - 7 >= halo;
-    const bool multi = n_use > 1 && max_parallelslices > 0 && !params.io.resume &&
-                       params.noiselevel.mode != "semimanual" && shape[2] >= 16 * n_use && slabs_deep;
+    if (ids.size() > 1 && !(8 * (units / (int)ids.size()) - 7 >= halo && shape[2] >= 16 * (int)ids.size()))
+        ids.resize(1);
 
-    if (multi) {
+    denoise::IterativeNLM_GPU gpu;
+    int n_parallelslices = n_devices > 0 ? gpu.configure_devices(shape, &params, ids) : -1;
+    if (n_parallelslices == -2) return -2;
+    if (n_parallelslices == -1) {
+        cout << "Error! No CUDA device found (this build has no CPU filter)" << endl;
+        return -1;
+    }
+    // -slab N below the stack depth: z-slab streaming on one device
+    if (ids.size() == 1 && slab_depth > 0 && slab_depth < shape[2]) {
         gpu.free_device();
-        cout << "Processing " << shape[2] << " slices on " << n_use << " GPUs" << endl;
-        inlm_params q = protocol::to_inlm(params);
-        sigma0 = (float*)malloc(shape[2] * sizeof(float));
-        sigma1 = (float*)malloc(shape[2] * sizeof(float));
-        if (protocol::report(inlm_denoise_multi(shape, &q, instack, output, n_use, ids.data(), sigma0, sigma1),
-                             "denoise_multi"))
-            return -2;
-        if (!params.io.cleanup || verbose) {
-            hdcom.SaveNoisefile(sigma0, shape[2], outpath, "noise_vs_slice00");
-            if (params.maxiterations > 1) hdcom.SaveNoisefile(sigma1, shape[2], outpath, "noise_vs_slice01");
-        }
-        params.io.active_outpath = iterdir(params.maxiterations);
-        if (save(output, params.io.active_outpath)) return -1;
-    } else if (max_parallelslices == 0) {
-        // the stack exceeds device memory: z-slab streaming of the whole job
-        cout << "Data exceed GPU capacity. Streaming slabs of " << slab_depth << " slices" << endl;
-        inlm_params q = protocol::to_inlm(params);
-        sigma0 = (float*)malloc(shape[2] * sizeof(float));
-        sigma1 = (float*)malloc(shape[2] * sizeof(float));
-        if (protocol::report(inlm_stream_denoise(shape, &q, instack, output, slab_depth, nullptr, 0, 0.f,
-                                                 sigma0, sigma1, nullptr),
-                             "stream_denoise"))
-            return -2;
-        if (!params.io.cleanup || verbose) {
-            hdcom.SaveNoisefile(sigma0, shape[2], outpath, "noise_vs_slice00");
-            if (params.maxiterations > 1) hdcom.SaveNoisefile(sigma1, shape[2], outpath, "noise_vs_slice01");
-        }
-        params.io.active_outpath = iterdir(params.maxiterations);
-        if (save(output, params.io.active_outpath)) return -1;
-    } else {
+        n_parallelslices = gpu.configure_devices(shape, &params, ids, slab_depth);
+        if (n_parallelslices < 0) return -2;
+    }
+    const bool blocks = n_parallelslices < shape[2];
+    if (blocks) {
+        if (ids.size() > 1) cout << "Processing " << shape[2] << " slices on " << ids.size() << " GPUs" << endl;
+        else cout << "Streaming z-slabs of " << n_parallelslices << " slices through the GPU" << endl;
+    }
+
+    float *sigma0 = nullptr, *sigma1 = nullptr;
+    float* output = (float*)malloc(nstack * sizeof(float));
+    {
         noise::NoiseLevel noise(params.noiselevel.n_samples, params.noiselevel.patchsize, shape);
         auto estimate = [&](float* stack, float*& sigma, int index, const char* what) {
             bool available = false;
@@ -396,19 +274,29 @@ int main(int argc, char* argv[]) {
         auto run = [&](int iter) {
             params.io.active_outpath = iterdir(iter);
             const auto t0 = std::chrono::high_resolution_clock::now();
-            if (params.io.resume && iteration_on_disk(params.io.active_outpath, params.io.firstslice, params.io.lastslice)) {
-                float* r = read_iteration(params.io.active_outpath, params.io.firstslice, params.io.lastslice, shape);
-                if (!r) return false;
-                gpu.set_result(iter, r, instack);
-                std::memcpy(output, r, nstack * sizeof(float));
-                free(r);
-                cout << "iteration " << iter << " read in from disk" << endl;
-                return gpu.status == INLM_OK;
+            if (blocks) {
+                // host-RAM blocks (main.cpp:377-384, 471-478): the result lands
+                // in output; --resume reads a finished iteration back
+                gpu.Run_GaussianNoise_GPUBlocks(iter, instack, output, shape, &params);
+                if (gpu.status) return false;
+                if (gpu.resumed) return true;
+            } else {
+                if (params.io.resume &&
+                    hdcom::iteration_on_disk(params.io.active_outpath, params.io.firstslice, params.io.lastslice)) {
+                    float* r = hdcom::read_iteration(params.io.active_outpath, params.io.firstslice,
+                                                     params.io.lastslice, shape);
+                    if (!r) return false;
+                    gpu.set_result(iter, r, instack);
+                    std::memcpy(output, r, nstack * sizeof(float));
+                    free(r);
+                    cout << "iteration " << iter << " read in from disk" << endl;
+                    return gpu.status == INLM_OK;
+                }
+                gpu.Run_GaussianNoise(iter, instack, shape, &params);
+                if (gpu.status) return false;
+                gpu.get_result(output, shape);
+                if (gpu.status) return false;
             }
-            gpu.Run_GaussianNoise(iter, instack, shape, &params);
-            if (gpu.status) return false;
-            gpu.get_result(output, shape);
-            if (gpu.status) return false;
             const std::chrono::duration<double> dt = std::chrono::high_resolution_clock::now() - t0;
             cout << "iteration " << iter << " took " << dt.count() << " s                          " << endl;
             if (iter == 1 || !params.io.cleanup || iter == params.maxiterations)

@@ -138,3 +138,38 @@ def test_multi_gpu_entry_points_without_a_gpu(lib):
     if n.value == 0:  # valid arguments, no device: INLM_ERR_NODEVICE
         assert lib.inlm_denoise_multi(shape, C.byref(p), buf.ctypes.data, buf.ctypes.data, 2, ids,
                                       None, None) == -3
+
+
+def test_blocks_entry_points_check_arguments(lib):
+    """The per-iteration host-RAM engine rejects bad arguments before it
+    touches a device."""
+    p = _lib.InlmParams()
+    lib.inlm_default_params(C.byref(p))
+    h = C.c_void_p(None)
+    shape = (C.c_int * 3)(16, 16, 16)
+    assert lib.inlm_blocks_create(shape, C.byref(p), 0, None, 8, C.byref(h)) == -1
+    assert "n_devices" in lib.inlm_last_error().decode()
+    assert lib.inlm_blocks_create(shape, None, 1, None, 8, C.byref(h)) == -1
+    assert lib.inlm_blocks_run_iteration(None, 1, None, None, None) == -1
+    assert lib.inlm_blocks_set_sigma(None, None) == -1
+
+
+REF_MAIN = os.path.join(os.environ.get("INLM_REFERENCE_DIR", "/root/reference/iterNLM_v0.3"), "main.cpp")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_MAIN), reason="reference sources not present")
+def test_reference_driver_compiles_against_the_shim(tmp_path):
+    """The reference's unmodified main.cpp compiles against this library's C++
+    shim: csrc/compat provides its header names (denoise_parameters.h,
+    Geometry/, Noise/, Denoiser/, Color/). It is compiled from a copy because
+    a quoted include searches the source file's own directory first."""
+    import shutil
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    csrc = os.path.join(root, "microtomodenoise_b200", "csrc")
+    src = tmp_path / "main.cpp"
+    shutil.copy(REF_MAIN, src)
+    r = subprocess.run(["g++", "-fsyntax-only", "-std=c++17", "-fopenmp", "-I" + os.path.join(csrc, "compat"),
+                        "-I" + csrc, "-I" + os.path.join(root, "include"), str(src)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-3000:]

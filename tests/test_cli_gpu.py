@@ -142,18 +142,77 @@ def test_cli_fp16_form(gpu, stack):
     assert np.array_equal(got, want)
 
 
-def test_cli_multi_gpu_split(gpu, tmp_path):
-    """-gpulist 0,0: the stack split over two parts (the multi-GPU path on one
-    device; it engages from 16 slices per part); the final iteration equals
-    the single-GPU run."""
+def _iterations(out, n):
+    return [tiffio.read_stack(str(out / f"denoise-iteration{k:02d}")) for k in range(1, n + 1)]
+
+
+def _noise_files(out):
+    return {n: (out / n).read_text() for n in sorted(os.listdir(out)) if n.startswith("noise_vs_slice")}
+
+
+@pytest.mark.parametrize("split", [["-gpulist", "0,0"], ["-slab", 16]], ids=["two_parts", "z_slabs"])
+def test_cli_blocks_save_every_iteration(gpu, tmp_path, split):
+    """The stack split over two parts (-gpulist 0,0: the multi-GPU path on one
+    device) or streamed through one device in z-slabs of 16 slices (-slab 16)
+    runs the host-RAM blocks per iteration (Run_GaussianNoise_GPUBlocks,
+    main.cpp:377-384, 471-478): every iteration folder and every noise file,
+    --continuous included, equals the single-GPU run's."""
     vol = synth.spheres_volume((40, 32, 36), n_spheres=8, rmin=3, rmax=8, seed=2)
     tmp = tmp_path
     tiffio.save_stack(vol, str(tmp / "in"), "slice")
-    args = ["-i", tmp / "in", "-iter", 2, "-search", 3, "-patch", 1, "-noise", "global",
-            "-nsamples", 20000, "-seed", 5]
+    args = ["-i", tmp / "in", "-iter", 4, "-search", 3, "-patch", 1, "-noise", "z-adaptive",
+            "-nsamples", 20000, "-seed", 5, "--continuous"]
     _cli(*args, "-o", tmp / "one", "-gpus", 1)
-    log = _cli(*args, "-o", tmp / "two", "-gpulist", "0,0")
-    assert "on 2 GPUs" in log
-    one = tiffio.read_stack(str(tmp / "one" / "denoise-iteration02"))
-    two = tiffio.read_stack(str(tmp / "two" / "denoise-iteration02"))
-    assert np.array_equal(one, two)
+    log = _cli(*args, "-o", tmp / "two", *split)
+    assert ("on 2 GPUs" in log) if split[0] == "-gpulist" else ("Streaming z-slabs of 16" in log)
+    for k, (a, b) in enumerate(zip(_iterations(tmp / "one", 4), _iterations(tmp / "two", 4))):
+        assert np.array_equal(a, b), f"iteration {k + 1}"
+    assert _noise_files(tmp / "one") == _noise_files(tmp / "two")
+    assert len(_noise_files(tmp / "one")) == 3  # sigma0, sigma1 and the --continuous estimate before iteration 4
+
+
+@pytest.mark.parametrize("split", [["-slab", 16], ["-gpulist", "0,0"]], ids=["z_slabs", "two_parts"])
+def test_cli_blocks_match_oracle_and_resume(gpu, port, tmp_path, split):
+    """Host-RAM blocks at patch radius 3, search radius 7: z-slabs of 16
+    slices through one device, or two parts (slices 0-23 and 24-39, halos of
+    8): every iteration bit-exact against the oracle (manual sigma); a
+    --resume run continues from the saved iterations."""
+    vol = synth.spheres_volume((40, 30, 34), n_spheres=8, rmin=3, rmax=8, seed=12)
+    tiffio.save_stack(vol, str(tmp_path / "in"), "slice")
+    args = ["-i", tmp_path / "in", "-o", tmp_path / "out", "-iter", 3, "-search", 7, "-patch", 3,
+            "-noise", "manual", "-sigma0", 0.05, "-sigma1", 0.03, *split]
+    _cli(*args)
+    got = _iterations(tmp_path / "out", 3)
+    p = FilterParams(search_radius=(7, 7, 7), patch_radius=(3, 3, 3))
+    s0 = np.full(40, 0.05, np.float32)
+    blend = (np.float32(0.5) * s0 + np.float32(0.5) * np.full(40, 0.03, np.float32)).astype(np.float32)
+    want = port.denoise_f32(vol, p, np.stack([s0, blend, blend]), all_iters=True)
+    for k in range(3):
+        assert np.array_equal(got[k], want[k]), f"iteration {k + 1}"
+    shutil.rmtree(tmp_path / "out" / "denoise-iteration03")
+    log = _cli(*args, "--resume")
+    assert "iteration 2 read in from disk" in log
+    assert np.array_equal(_iterations(tmp_path / "out", 3)[2], want[2])
+
+
+REFDRIVER = os.path.join(ROOT, "oracle", "_ref", "iterNLM_refdriver")
+
+
+@pytest.mark.skipif(not os.path.exists(REFDRIVER), reason="reference driver not built (needs the reference tree)")
+def test_reference_driver_runs_on_this_library(gpu, port, stack):
+    """The reference's own main.cpp, unmodified, compiled against this
+    library's C++ shim (oracle/Makefile refdriver): its whole-stack GPU flow
+    (configure_device, set_sigma, Run_GaussianNoise, get_result, the TIFF
+    saves) runs on this build, bit-exact against the oracle."""
+    vol, tmp = stack
+    out = tmp / "out"
+    r = subprocess.run([REFDRIVER, "-i", str(tmp / "in"), "-o", str(out), "-iter", "2", "-search", "3",
+                        "-patch", "1", "-noise", "manual", "-sigma0", "0.05", "-sigma1", "0.03"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    p = FilterParams(search_radius=(3, 3, 3), patch_radius=(1, 1, 1))
+    s0 = np.full(12, 0.05, np.float32)
+    blend = (np.float32(0.5) * s0 + np.float32(0.5) * np.full(12, 0.03, np.float32)).astype(np.float32)
+    want = port.denoise_f32(vol, p, np.stack([s0, blend]), all_iters=True)
+    got = _iterations(out, 2)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
