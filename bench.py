@@ -151,7 +151,7 @@ def measured_peaks():
 # (profiles/nlm_tile_f32_p2s5_512.md gives the command), times 4: the traffic
 # is the tiles' halo boxes plus the result, so it grows with the tile count.
 FILTER_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, one 512x512x128 launch, x4"
-FILTER_TRAFFIC_BYTES_PER_LAUNCH = 4 * 459.8e6
+FILTER_TRAFFIC_BYTES_PER_LAUNCH = 4 * (336.96e6 + 123.74e6)
 
 
 def fp32_arithmetic_peak(device: int):
@@ -296,8 +296,12 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
              ("learned_fp16_no_fallback", "f16", (LEARNED_K, 0.0, 4)),
              ("learned_fp16_k256_mass095", "f16", (256, 0.95, 1))]
     for item in filter(None, args.learned_extra.split(",")):
-        k, t, m = (item.split("@") + ["0"])[:3]
-        forms.append((f"learned_fp16_k{k}_t{t}_m{m}", "f16", (int(k), float(m), int(t))))
+        f = item.split("@")
+        k, t = f[0], f[1] if len(f) > 1 else "1"
+        m = f[2] if len(f) > 2 else "0"
+        prec = f[3] if len(f) > 3 else "f16"
+        rel = float(m[1:]) if m.startswith("r") else 0.0
+        forms.append((f"learned_{prec}_k{k}_t{t}_m{m}", prec, (int(k), 0.0 if rel else float(m), int(t), rel)))
     raw_dev = torch.from_numpy(vol).cuda()
     out_dev = torch.empty_like(raw_dev)
     vox = float(np.prod(vol.shape))
@@ -315,7 +319,7 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
         g.configure_device(vol.shape, dp)
         g.set_stream(stream.cuda_stream)
         if prop:
-            g.attach_proposal(net, prop[0], prop[1], tiles_x=prop[2])
+            g.attach_proposal(net, prop[0], prop[1], tiles_x=prop[2], rel_mass=prop[3] if len(prop) > 3 else 0.0)
         r = {"kernel": g.describe()}
         if name != "f32":
             g.denoise(raw_dev.data_ptr(), on_device=True, out=out_dev.data_ptr())
@@ -338,6 +342,7 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
             if prop:
                 st = g.proposal_stats()
                 r.update({"k": prop[0], "min_mass": prop[1], "tiles_per_plan": prop[2],
+                          "rel_mass": prop[3] if len(prop) > 3 else 0.0,
                           "fallback_fraction": st["fallback_tiles"] / max(st["tiles"], 1),
                           "fraction_evaluated": st["fraction_evaluated"]})
         # accuracy run: the FP32 job's sigma schedule, fixed, for every form
@@ -544,22 +549,48 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def psnr_chunked(a, b, peak=1.0, chunk=32):
+    """PSNR over a volume without float64 copies of the whole of it."""
+    se, n = 0.0, 0
+    for z in range(0, a.shape[0], chunk):
+        d = a[z:z + chunk].astype(np.float64) - b[z:z + chunk]
+        se += float(np.sum(d * d))
+        n += d.size
+    return float("inf") if se == 0 else 10 * np.log10(peak * peak / (se / n))
+
+
+def parse_learned(spec):
+    """k@tiles_per_plan[@min_mass] with min_mass rX: relative threshold X."""
+    f = spec.split("@")
+    k, t = int(f[0]), int(f[1]) if len(f) > 1 else 1
+    m = f[2] if len(f) > 2 else "0"
+    rel = float(m[1:]) if m.startswith("r") else 0.0
+    return k, t, (0.0 if rel else float(m)), rel
+
+
 def run_large_workload(args):
     """One-step measurements of the two large workloads (rank 0, one GPU):
 
     learned1024: float32 1024x1024x512 grain pack (noise 0.05 blurred 1, no
       rings), patch r3 search r7 (1326 offsets), 4 iterations, global noise:
-      the whole job in plain FP32, FP16 full search, and learned + FP16 with
-      k = 896 per 32x8x8 block (no fallback) and k = 256 per 8^3 tile with
-      fallback below 0.95 predicted kept mass.
-    stream2048: a 2048x2048xZ slab stack (Z = --stream-depth) of the grain pack
-      with noise sigma drifting 0.02 -> 0.08 along z (blur 1) and rings of
-      amplitude 0.03, z-adaptive noise, patch r3 search r7, 4 iterations, held
-      in host memory and streamed in z-slabs of 64 slices (inlm_stream_denoise):
-      plain FP32 and learned + FP16 (k = 896 per 32x8x8 block, no fallback).
-    PSNR against the clean phantom over the whole volume for every form."""
+      the whole job in plain FP32, FP16 full search, and learned + FP16 forms
+      (--k-list k@tiles[@min_mass], default 896@4 and 256@1@0.95), PSNR
+      against the clean phantom over the whole volume for every form.
+    stream2048: a 2048x2048xZ grain pack (Z = --stream-depth, 1024 for the
+      17 GB configuration) with noise sigma drifting 0.02 -> 0.08 along z
+      (blur 1) and rings of amplitude 0.03, z-adaptive noise, patch r3 search
+      r7, 4 iterations, held in host memory and streamed through the GPU in
+      z-slabs of --slab slices: the plain FP32 whole job and the learned +
+      FP16 whole job (--stream-learned k@tiles[@min_mass]), each with its own
+      noise estimates, PSNR against the clean phantom over the whole volume;
+      then the learned form again with the plain job's sigma schedule held
+      fixed (inlm_blocks_*, one iteration at a time), and the FP64
+      full-search result on 64 seeded 128^3 sub-blocks with the same
+      schedule (inlm_denoise_f64_blocks): max-abs error and PSNR of both forms
+      against it, and PSNR against the clean phantom on those blocks."""
     import torch
-    from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, stream_denoise, synth
+    from microtomodenoise_b200 import (Blocks, DenoiseParameters, IterativeNLM_GPU, denoise_f64_blocks,
+                                       stream_denoise, synth)
     from microtomodenoise_b200.proposal import ProposalNet, default_weights
     pr, sr = (3, 3, 3), (7, 7, 7)
     net = ProposalNet.load(default_weights(pr, sr))
@@ -571,33 +602,36 @@ def run_large_workload(args):
                                              seed=0, return_clean=True)
     else:
         shape = (args.stream_depth, 2048, 2048)
+        try:
+            import psutil
+            need = 7 * 4 * float(np.prod(shape))
+            have = float(psutil.virtual_memory().total)
+            if have < need:
+                print(json.dumps({"workload": args.workload, "skipped":
+                                  f"host memory {have / 1e9:.0f} GB < {need / 1e9:.0f} GB needed"}), flush=True)
+                return
+        except ImportError:
+            pass
         vol, clean = synth.grain_pack_volume(shape, noise_blur=1.0, ring_amp=0.03,
                                              sigma_drift=(0.02, 0.08), seed=0, return_clean=True)
     log(f"generated {shape} in {time.time() - t:.1f}s")
+    res["generate_s"] = time.time() - t
     vox = float(np.prod(shape)) * ITERS
     res["config"] = {"shape_xyz": [shape[2], shape[1], shape[0]], "patch_radius": 3,
                      "search_radius": 7, "offsets": 1326, "iterations": ITERS}
-    forms = [("f32", "f32", None), ("fp16", "f16", None), ("learned_fp16_k896_t4", "f16", (896, 0.0, 4)),
-             ("learned_fp16_k256_mass095", "f16", (256, 0.95))]
-    if args.k_list:
-        # a sweep of k (no fallback; k@t: one list per t 8^3 tiles along x)
-        # beside plain FP32 and FP16 full search
+    if args.workload == "learned1024":
         forms = [("f32", "f32", None), ("fp16", "f16", None)]
-        for item in args.k_list.split(","):
-            k, _, t = item.partition("@")
-            forms.append((f"learned_fp16_k{k}" + (f"_t{t}" if t else ""), "f16", (int(k), 0.0, int(t or 1))))
-    if args.workload == "stream2048":
-        forms = [("f32", "f32", None), ("learned_fp16_k896_t4", "f16", (896, 0.0, 4))]
-    ref_psnr = None
-    for name, prec, prop in forms:
-        dp = DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, maxiterations=ITERS,
-                               alpha=0.5, noise_seed=0, precision=prec,
-                               noise_mode="global" if args.workload == "learned1024" else "z-adaptive")
-        if args.workload == "learned1024":
+        for item in (args.k_list or "896@4,256@1@0.95").split(","):
+            k, tx, mm, rel = parse_learned(item)
+            forms.append((f"learned_fp16_{item}", "f16", (k, mm, tx, rel)))
+        ref_psnr = None
+        for name, prec, prop in forms:
+            dp = DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, maxiterations=ITERS,
+                                   alpha=0.5, noise_seed=0, precision=prec, noise_mode="global")
             g = IterativeNLM_GPU()
             g.configure_device(shape, dp)
             if prop:
-                g.attach_proposal(net, prop[0], prop[1], tiles_x=prop[2] if len(prop) > 2 else 1)
+                g.attach_proposal(net, prop[0], prop[1], tiles_x=prop[2], rel_mass=prop[3])
             raw = torch.from_numpy(vol).cuda()
             out = torch.empty_like(raw)
             torch.cuda.synchronize()
@@ -611,28 +645,75 @@ def run_large_workload(args):
             r = {"ms_per_job": ms, "value": vox / (ms / 1e3), "unit": "voxel-iter/s", "kernel": g.describe()}
             if prop:
                 st = g.proposal_stats()
-                r.update({"k": prop[0], "min_mass": prop[1],
+                r.update({"k": prop[0], "min_mass": prop[1], "tiles_per_plan": prop[2], "rel_mass": prop[3],
                           "fallback_fraction": st["fallback_tiles"] / max(st["tiles"], 1),
                           "fraction_evaluated": st["fraction_evaluated"]})
             o = out.cpu().numpy()
             g.free_device()
             del raw, out
-        else:
-            o, _, _, st = stream_denoise(vol, dp, slab_depth=64, net=net if prop else None,
-                                         k=prop[0] if prop else 0, min_mass=prop[1] if prop else 0.0,
-                                         tiles_x=prop[2] if prop and len(prop) > 2 else 1)
-            ms = st["ms"]
-            r = {"ms_per_job": ms, "value": vox / (ms / 1e3), "unit": "voxel-iter/s",
-                 "h2d_bytes": st["h2d_bytes"], "d2h_bytes": st["d2h_bytes"], "slabs": st["slabs"],
-                 "halo": st["halo"]}
-            if prop:
-                r.update({"k": prop[0], "min_mass": prop[1]})
-        r["psnr_vs_clean_db"] = psnr(o, clean)
-        if name == "f32":
-            ref_psnr = r["psnr_vs_clean_db"]
-        r["delta_vs_f32_db"] = r["psnr_vs_clean_db"] - ref_psnr
-        res["forms"][name] = r
-        log(f"{name}: {r}")
+            r["psnr_vs_clean_db"] = psnr(o, clean)
+            if name == "f32":
+                ref_psnr = r["psnr_vs_clean_db"]
+            r["delta_vs_f32_db"] = r["psnr_vs_clean_db"] - ref_psnr
+            res["forms"][name] = r
+            log(f"{name}: {r}")
+    else:
+        k, tx, mm, rel = parse_learned(args.stream_learned)
+        dp32 = DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, maxiterations=ITERS, alpha=0.5,
+                                 noise_seed=0, precision="f32", noise_mode="z-adaptive")
+        dp16 = DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, maxiterations=ITERS, alpha=0.5,
+                                 noise_seed=0, precision="f16", noise_mode="z-adaptive")
+        out32, s0, s1, st = stream_denoise(vol, dp32, slab_depth=args.slab)
+        r32 = {"ms_per_job": st["ms"], "value": vox / (st["ms"] / 1e3), "unit": "voxel-iter/s",
+               "h2d_bytes": st["h2d_bytes"], "d2h_bytes": st["d2h_bytes"], "slabs": st["slabs"],
+               "halo": st["halo"], "psnr_vs_clean_db": psnr_chunked(out32, clean)}
+        log(f"f32: {r32}")
+        outl, _, _, st = stream_denoise(vol, dp16, slab_depth=args.slab, net=net, k=k, min_mass=mm,
+                                        tiles_x=tx, rel_mass=rel)
+        rl = {"ms_per_job": st["ms"], "value": vox / (st["ms"] / 1e3), "unit": "voxel-iter/s",
+              "k": k, "tiles_per_plan": tx, "min_mass": mm, "rel_mass": rel, "slabs": st["slabs"],
+              "halo": st["halo"], "psnr_vs_clean_db": psnr_chunked(outl, clean)}
+        rl["delta_vs_f32_db"] = rl["psnr_vs_clean_db"] - r32["psnr_vs_clean_db"]
+        rl["speedup_vs_f32"] = r32["ms_per_job"] / rl["ms_per_job"]
+        log(f"learned: {rl}")
+        # accuracy with the FP32 job's sigma schedule held fixed
+        sched = np.stack([s0] + [(np.float32(0.5) * s0 + np.float32(0.5) * s1).astype(np.float32)] * (ITERS - 1))
+        t = time.time()
+        b = Blocks(shape, dp16, slab_depth=args.slab)
+        b.attach_proposal(net, k, mm, tiles_x=tx, rel_mass=rel)
+        other = np.empty_like(vol)
+        bufs, prev = [outl, other], None
+        for it in range(ITERS):
+            b.set_sigma(sched[it])
+            o = bufs[it % 2]
+            b.run_iteration(it + 1, vol, prev, o)
+            prev = o
+        b.close()
+        fixed = prev
+        rl["fixed_schedule_s"] = time.time() - t
+        t = time.time()
+        bs = 128
+        corners = sub_block_corners(shape, n=64, size=bs, seed=0)
+        ref = denoise_f64_blocks(vol, DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr), sched,
+                                 corners, (bs, bs, bs))
+        fp64_s = time.time() - t
+        crop = lambda a: np.concatenate([a[z:z + bs, y:y + bs, x:x + bs].ravel() for z, y, x in corners])
+        r64, c64 = np.concatenate([x.ravel() for x in ref]), crop(clean)
+        p64 = psnr(r64, c64)
+        for r, o in ((r32, out32), (rl, fixed)):
+            got = crop(o)
+            d = np.abs(got - r64)
+            per_block = [psnr(g_, w_) for g_, w_ in zip(np.split(got, len(corners)), np.split(r64, len(corners)))]
+            r["accuracy"] = {"max_abs_vs_fp64": float(d.max()), "psnr_vs_fp64_db": psnr(got, r64),
+                             "psnr_vs_fp64_db_per_block_min": float(np.min(per_block)),
+                             "psnr_vs_fp64_db_per_block_median": float(np.median(per_block)),
+                             "blocks_psnr_vs_clean_db": psnr(got, c64), "blocks_fp64_psnr_vs_clean_db": p64,
+                             "blocks_delta_vs_fp64_oracle_db": psnr(got, c64) - p64}
+        res["fp64"] = {"blocks": len(corners), "size": bs, "seconds": fp64_s,
+                       "how": "inlm_denoise_f64_blocks (GPU, FP64 full search, bit-exact to the oracle's FP64 "
+                              "restatement) with the plain job's sigma schedule"}
+        res["forms"] = {"f32": r32, "learned_fp16": rl}
+        log(f"accuracy: f32 {r32['accuracy']}, learned {rl['accuracy']}")
     f32 = res["forms"]["f32"]["ms_per_job"]
     for v in res["forms"].values():
         v["speedup_vs_f32"] = f32 / v["ms_per_job"]
@@ -766,12 +847,16 @@ def main():
                          "run_rgb_workload); profile: a small case for ncu (--case)")
     ap.add_argument("--case", default="f32", choices=["f32", "fast", "learned", "slab"],
                     help="--workload profile: which small case (see run_profile_case)")
-    ap.add_argument("--stream-depth", type=int, default=128)
+    ap.add_argument("--stream-depth", type=int, default=1024)
+    ap.add_argument("--slab", type=int, default=64, help="stream2048: z-slab depth")
+    ap.add_argument("--stream-learned", default="896@4@r0.9",
+                    help="stream2048: the learned + FP16 form, k@tiles_per_plan[@min_mass|@rX]")
     ap.add_argument("--learned-extra", default="",
                     help="extra learned + FP16 forms in the headline run, "
-                         "k@tiles_per_plan[@min_mass][,...]")
+                         "k@tiles_per_plan[@min_mass[@precision]][,...]; min_mass rX: relative "
+                         "threshold X x the mean predicted kept mass; precision f16 or f16_df32")
     ap.add_argument("--k-list", default="",
-                    help="learned1024: comma-separated k values to sweep (no fallback)")
+                    help="learned1024: learned + FP16 forms, k@tiles_per_plan[@min_mass|@rX][,...]")
     ap.add_argument("--shape", default="512,512,512",
                     help="nz,ny,nx of the volume (smaller shapes only for profiling runs)")
     args = ap.parse_args()

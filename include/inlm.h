@@ -275,6 +275,12 @@ int inlm_proposal_train(inlm_proposal* p, int n_examples, const float* const* vo
 int inlm_proposal_select(inlm_proposal* p, const float* vol_dev, const float* scale_dev,
                          const int shape[3], int k, float min_mass, uint32_t* bitmap_dev,
                          float* pred_mass_dev, int* n_fallback);
+/* Inference layers 2-4 (3^3 convs, 16 -> 16 channels) on the tensor cores
+ * (on = 1, the default: tcgen05 implicit GEMMs with TF32 operands, the BF16
+ * weights exact in TF32, FP32 accumulation in tensor memory) or on the CUDA
+ * cores (on = 0: FP32 activations; the reference of the tensor-core path).
+ * Training (inlm_proposal_train) always runs the CUDA-core forward. */
+int inlm_proposal_set_tensor_cores(inlm_proposal* p, int on);
 /* Attaches a proposal to an FP16-form denoiser (p == NULL detaches): every
  * later iteration runs the network on its previous iterate and evaluates the
  * selected offsets per 8^3 tile. */
@@ -286,6 +292,16 @@ int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, float min_ma
  * per offset; the predicted kept mass is the mean over the four tiles). */
 int inlm_attach_proposal_grouped(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass,
                                  int tiles_x);
+/* The same with a fallback threshold relative to the volume: a list whose
+ * predicted kept mass is below rel_mass x the mean predicted kept mass of
+ * all lists of the iteration (0 < rel_mass <= 1; 0: off) evaluates every
+ * offset, as does one below min_mass. The mean adapts the threshold to k, S,
+ * sigma and the data, so the fallback picks the lists whose kept mass is poor
+ * for this volume, where an absolute threshold that a flat weight
+ * distribution never reaches falls back everywhere. The mean is summed in a
+ * fixed order: the same lists fall back on every run. */
+int inlm_attach_proposal_ex(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass, float rel_mass,
+                            int tiles_x);
 /* inlm_proposal_select for groups of tiles_x 8^3 tiles along x: bitmap and
  * pred_mass hold one entry per group, groups ordered z, y, x. */
 int inlm_proposal_select_grouped(inlm_proposal* p, const float* vol_dev, const float* scale_dev,
@@ -362,6 +378,30 @@ int inlm_stream_denoise_grouped(const int shape[3], const inlm_params* p, const 
                                 float* out_host, int slab_depth, inlm_proposal* net, int k,
                                 float min_mass, int tiles_x, float* sigma0_out, float* sigma1_out,
                                 double* stats);
+/* The same with the relative fallback of inlm_attach_proposal_ex; its mean is
+ * taken over each sub-volume's lists (so results with rel_mass > 0 depend on
+ * the slab depth; with rel_mass = 0 they equal the in-memory schedule's). */
+int inlm_stream_denoise_ex(const int shape[3], const inlm_params* p, const float* raw_host,
+                           float* out_host, int slab_depth, inlm_proposal* net, int k, float min_mass,
+                           float rel_mass, int tiles_x, float* sigma0_out, float* sigma1_out,
+                           double* stats);
+
+/* ---------------- FP64 full-search reference on sub-blocks ----------------
+ * No counterpart in the reference, whose filter computes in FP32. The
+ * full-search result of the last of n_iter iterations in FP64 (every product,
+ * sum and quotient a separately rounded double, iterates kept in double,
+ * m = -1/(sigma*sigma*beta) in double; the reference's algorithm,
+ * iternlm_cpu.cpp:795-834, and its reflective padding) on n_blocks blocks of
+ * size[3] voxels (x, y, z) with lower corners corners[3*b..] (x, y, z), without
+ * filtering the whole volume: iteration k runs on the block grown by
+ * (n_iter - k) x the padding per side. raw: the unpadded FP32 volume, host
+ * (on_device = 0) or device memory; sigmas: n_iter x nz (host); out_host:
+ * n_blocks blocks of size[2] x size[1] x size[0] doubles, x fastest. The
+ * precision reference of the FP16 and learned forms at volume sizes a CPU
+ * cannot finish; it equals the oracle's FP64 restatement bit for bit. */
+int inlm_denoise_f64_blocks(const int shape[3], const inlm_params* p, const float* raw, int on_device,
+                            const float* sigmas, int n_iter, const int* corners, int n_blocks,
+                            const int size[3], double* out_host);
 
 /* ---------------- host-only helpers (no device needed) ---------------- */
 
@@ -415,6 +455,11 @@ typedef struct inlm_blocks inlm_blocks;
 int inlm_blocks_create(const int shape[3], const inlm_params* p, int n_devices,
                        const int* device_ids, int slab_depth, inlm_blocks** out);
 int inlm_blocks_destroy(inlm_blocks* b);
+/* One device only, before the first iteration: the FP16 form evaluates the
+ * offsets a learned proposal selects (as inlm_attach_proposal_ex; the slabs'
+ * halos grow to >= 16 slices, the network's receptive field). */
+int inlm_blocks_attach_proposal(inlm_blocks* b, inlm_proposal* net, int k, float min_mass,
+                                float rel_mass, int tiles_x);
 /* Slices per slab (one device) or the deepest part (several). */
 int inlm_blocks_slab_depth(const inlm_blocks* b, int* depth);
 /* sigma of the following iterations, nz floats (host). */

@@ -26,7 +26,7 @@ from . import _lib
 from ._lib import InlmError, InlmParams, NOISE_MODES, PRECISIONS
 
 __all__ = ["DenoiseParameters", "IterativeNLM_GPU", "NoiseLevel", "Batch", "denoise",
-           "denoise_multi", "stream_denoise", "InlmError"]
+           "denoise_multi", "denoise_f64_blocks", "stream_denoise", "Blocks", "InlmError"]
 
 
 @dataclass
@@ -231,16 +231,17 @@ class IterativeNLM_GPU:
         _lib.check(_lib.load().inlm_tile_grid(self._h, ts, tc), "tile_grid")
         return tuple(ts), tuple(tc)
 
-    def attach_proposal(self, net, k: int = 256, min_mass: float = 0.95, tiles_x: int = 1) -> None:
+    def attach_proposal(self, net, k: int = 256, min_mass: float = 0.95, tiles_x: int = 1,
+                        rel_mass: float = 0.0) -> None:
         """Evaluates only each 8^3 tile's top-k offsets predicted by `net` (a
         proposal.ProposalNet), or every offset where the predicted kept mass
-        is below min_mass. tiles_x = 4 ranks one list per 4 tiles along x
-        (32 x 8 x 8 blocks, the full-width kernel). net=None returns to full
-        search. FP16 form only."""
+        is below min_mass, or below rel_mass x its mean over the volume.
+        tiles_x = 4 ranks one list per 4 tiles along x (32 x 8 x 8 blocks, the
+        full-width kernel). net=None returns to full search. FP16 form only."""
         self._need()
         h = net._h if net is not None else None
-        _lib.check(_lib.load().inlm_attach_proposal_grouped(self._h, h, int(k), float(min_mass),
-                                                            int(tiles_x)), "attach_proposal")
+        _lib.check(_lib.load().inlm_attach_proposal_ex(self._h, h, int(k), float(min_mass), float(rel_mass),
+                                                       int(tiles_x)), "attach_proposal")
         self._proposal = net  # keep the network alive while attached
 
     def proposal_stats(self) -> dict:
@@ -395,10 +396,11 @@ class Batch:
 
 def stream_denoise(raw: np.ndarray, params: DenoiseParameters, slab_depth: int = 64,
                    net=None, k: int = 256, min_mass: float = 0.95, out: Optional[np.ndarray] = None,
-                   tiles_x: int = 1):
+                   tiles_x: int = 1, rel_mass: float = 0.0):
     """The denoise schedule for a host-resident volume, filtered in z-slabs
-    (inlm_stream_denoise_grouped; tiles_x as IterativeNLM_GPU.attach_proposal).
-    Returns (result, sigma0, sigma1, stats) with stats =
+    (inlm_stream_denoise_ex; tiles_x and rel_mass as
+    IterativeNLM_GPU.attach_proposal, the relative threshold's mean taken per
+    sub-volume). Returns (result, sigma0, sigma1, stats) with stats =
     {ms, h2d_bytes, d2h_bytes, slabs, halo, slab_depth}."""
     raw = _f32c(raw)
     if out is None:
@@ -408,14 +410,55 @@ def stream_denoise(raw: np.ndarray, params: DenoiseParameters, slab_depth: int =
     s1 = np.zeros(nz, np.float32)
     st = np.zeros(6, np.float64)
     cp = params.to_c()
-    rc = _lib.load().inlm_stream_denoise_grouped(_shape_c(raw.shape), C.byref(cp), raw.ctypes.data,
-                                                 out.ctypes.data, int(slab_depth),
-                                                 net._h if net is not None else None, int(k),
-                                                 float(min_mass), int(tiles_x), s0.ctypes.data,
-                                                 s1.ctypes.data, st.ctypes.data)
+    rc = _lib.load().inlm_stream_denoise_ex(_shape_c(raw.shape), C.byref(cp), raw.ctypes.data,
+                                            out.ctypes.data, int(slab_depth),
+                                            net._h if net is not None else None, int(k),
+                                            float(min_mass), float(rel_mass), int(tiles_x), s0.ctypes.data,
+                                            s1.ctypes.data, st.ctypes.data)
     _lib.check(rc, "stream_denoise")
     keys = ("ms", "h2d_bytes", "d2h_bytes", "slabs", "halo", "slab_depth")
     return out, s0, s1, dict(zip(keys, st.tolist()))
+
+
+class Blocks:
+    """One iteration at a time over host-resident volumes (inlm_blocks_*, the
+    host-RAM Run_GaussianNoise_GPUBlocks): z-slabs of slab_depth slices on one
+    device, or the stack split over several device_ids. The caller sets sigma
+    before iterations and estimates the noise itself."""
+
+    def __init__(self, shape_zyx, params: DenoiseParameters, device_ids=(0,), slab_depth: int = 64):
+        self.shape = tuple(int(v) for v in shape_zyx)
+        ids = np.ascontiguousarray(device_ids, np.int32)
+        cp = params.to_c()
+        self._h = C.c_void_p(None)
+        _lib.check(_lib.load().inlm_blocks_create(_shape_c(self.shape), C.byref(cp), len(ids), ids.ctypes.data,
+                                                  int(slab_depth), C.byref(self._h)), "blocks_create")
+        self._net = None
+
+    def attach_proposal(self, net, k: int, min_mass: float = 0.0, tiles_x: int = 4, rel_mass: float = 0.0):
+        _lib.check(_lib.load().inlm_blocks_attach_proposal(self._h, net._h, int(k), float(min_mass),
+                                                           float(rel_mass), int(tiles_x)), "blocks_attach_proposal")
+        self._net = net
+
+    def set_sigma(self, sigma) -> None:
+        s = _f32c(sigma)
+        _lib.check(_lib.load().inlm_blocks_set_sigma(self._h, s.ctypes.data), "blocks_set_sigma")
+
+    def run_iteration(self, it: int, raw: np.ndarray, prev: Optional[np.ndarray], out: np.ndarray) -> None:
+        _lib.check(_lib.load().inlm_blocks_run_iteration(self._h, int(it), raw.ctypes.data,
+                                                         prev.ctypes.data if prev is not None else None,
+                                                         out.ctypes.data), "blocks_run_iteration")
+
+    def close(self) -> None:
+        if self._h:
+            _lib.load().inlm_blocks_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def denoise_multi(raw: np.ndarray, params: DenoiseParameters, device_ids, out: Optional[np.ndarray] = None):
@@ -434,6 +477,29 @@ def denoise_multi(raw: np.ndarray, params: DenoiseParameters, device_ids, out: O
                                         len(ids), ids.ctypes.data, s0.ctypes.data, s1.ctypes.data)
     _lib.check(rc, "denoise_multi")
     return out, s0, s1
+
+
+def denoise_f64_blocks(raw, params: DenoiseParameters, sigmas: np.ndarray, corners, size,
+                       shape=None) -> list:
+    """FP64 full-search result of the last of len(sigmas) iterations on
+    size = (dz, dy, dx) blocks at the (z, y, x) corners of a volume, on the GPU
+    (inlm_denoise_f64_blocks): the precision reference of the FP16 and learned
+    forms. raw: a host array, or a device pointer with shape=(nz, ny, nx).
+    sigmas: (n_iter, nz). Returns one float64 (dz, dy, dx) array per block."""
+    on_device = not isinstance(raw, np.ndarray)
+    if not on_device:
+        raw = _f32c(raw)
+        shape = raw.shape
+    sig = np.ascontiguousarray(np.atleast_2d(sigmas), np.float32)
+    cxyz = np.ascontiguousarray([[c[2], c[1], c[0]] for c in corners], np.int32)
+    sz = (C.c_int * 3)(int(size[2]), int(size[1]), int(size[0]))
+    out = np.empty((len(corners),) + tuple(size), np.float64)
+    cp = params.to_c()
+    rc = _lib.load().inlm_denoise_f64_blocks(_shape_c(shape), C.byref(cp), raw if on_device else raw.ctypes.data,
+                                             int(on_device), sig.ctypes.data, sig.shape[0], cxyz.ctypes.data,
+                                             len(corners), sz, out.ctypes.data)
+    _lib.check(rc, "denoise_f64_blocks")
+    return list(out)
 
 
 def denoise(raw: np.ndarray, params: Optional[DenoiseParameters] = None):

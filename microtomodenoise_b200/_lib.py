@@ -35,6 +35,7 @@ EXPORTS = (
     "inlm_tile_grid", "inlm_set_offset_plan",
     "inlm_proposal_create", "inlm_proposal_destroy", "inlm_proposal_n_params",
     "inlm_proposal_set_params", "inlm_proposal_get_params", "inlm_proposal_logits",
+    "inlm_proposal_set_tensor_cores",
     "inlm_proposal_train", "inlm_proposal_select", "inlm_attach_proposal", "inlm_proposal_stats",
     "inlm_weight_map", "inlm_net_input",
     "inlm_autotune", "inlm_batch_create", "inlm_batch_destroy", "inlm_batch_run",
@@ -42,11 +43,11 @@ EXPORTS = (
     "inlm_tiff_shape", "inlm_tiff_read", "inlm_tiff_write_sequence",
     "inlm_get_result_slices", "inlm_set_result_slices", "inlm_noise_patchstd_slab",
     "inlm_noise_estimate_from_patchstd", "inlm_rgb_denoise", "inlm_tiff_read_rgb",
-    "inlm_tiff_write_rgb", "inlm_attach_proposal_grouped", "inlm_proposal_select_grouped",
+    "inlm_tiff_write_rgb", "inlm_attach_proposal_grouped", "inlm_attach_proposal_ex", "inlm_proposal_select_grouped",
     "inlm_stream_denoise_grouped", "inlm_denoise_multi", "inlm_device_count",
     "inlm_blocks_create", "inlm_blocks_destroy", "inlm_blocks_slab_depth", "inlm_blocks_set_sigma",
-    "inlm_blocks_run_iteration", "inlm_device_memory", "inlm_debug_fail_allocation",
-    "inlm_debug_live_allocations", "inlm_debug_wait_expiry",
+    "inlm_blocks_run_iteration", "inlm_blocks_attach_proposal", "inlm_stream_denoise_ex", "inlm_device_memory", "inlm_debug_fail_allocation",
+    "inlm_debug_live_allocations", "inlm_debug_wait_expiry", "inlm_denoise_f64_blocks",
 )
 
 
@@ -140,12 +141,14 @@ def load(path: str = "") -> C.CDLL:
     L.inlm_proposal_set_params.argtypes = [vp, vp, C.c_int64]
     L.inlm_proposal_get_params.argtypes = [vp, vp, C.c_int64]
     L.inlm_proposal_logits.argtypes = [vp, vp, vp, C.c_int * 3, vp]
+    L.inlm_proposal_set_tensor_cores.argtypes = [vp, C.c_int]
     L.inlm_proposal_train.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_float,
                                       C.POINTER(C.c_double), vp]
     L.inlm_proposal_select.argtypes = [vp, vp, vp, C.c_int * 3, C.c_int, C.c_float, vp, vp,
                                        C.POINTER(C.c_int)]
     L.inlm_attach_proposal.argtypes = [vp, vp, C.c_int, C.c_float]
     L.inlm_attach_proposal_grouped.argtypes = [vp, vp, C.c_int, C.c_float, C.c_int]
+    L.inlm_attach_proposal_ex.argtypes = [vp, vp, C.c_int, C.c_float, C.c_float, C.c_int]
     L.inlm_proposal_select_grouped.argtypes = [vp, vp, vp, C.c_int * 3, C.c_int, C.c_int, C.c_float,
                                                vp, vp, C.POINTER(C.c_int)]
     L.inlm_proposal_stats.argtypes = [vp, C.c_int64 * 5]
@@ -163,11 +166,16 @@ def load(path: str = "") -> C.CDLL:
     L.inlm_debug_fail_allocation.argtypes = [C.c_int64]
     L.inlm_debug_live_allocations.argtypes = [C.POINTER(C.c_int64)]
     L.inlm_debug_wait_expiry.argtypes = [vp, C.c_int64]
+    L.inlm_denoise_f64_blocks.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, C.c_int, vp, C.c_int, vp,
+                                          C.c_int, C.c_int * 3, vp]
     L.inlm_device_memory.argtypes = [C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     L.inlm_blocks_create.argtypes = [C.c_int * 3, C.POINTER(InlmParams), C.c_int, vp, C.c_int, C.POINTER(vp)]
     L.inlm_blocks_destroy.argtypes = [vp]
     L.inlm_blocks_slab_depth.argtypes = [vp, C.POINTER(C.c_int)]
     L.inlm_blocks_set_sigma.argtypes = [vp, vp]
+    L.inlm_blocks_attach_proposal.argtypes = [vp, vp, C.c_int, C.c_float, C.c_float, C.c_int]
+    L.inlm_stream_denoise_ex.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp, C.c_int,
+                                         C.c_float, C.c_float, C.c_int, vp, vp, vp]
     L.inlm_blocks_run_iteration.argtypes = [vp, C.c_int, vp, vp, vp]
     L.inlm_denoise_multi.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp, vp, vp]
     L.inlm_stream_denoise_grouped.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp,

@@ -39,6 +39,7 @@ LIB_SOURCES = [
     "noise_kernels.cu",
     "api.cu",
     "proposal.cu",
+    "proposal_tc.cu",
     "api_proposal.cu",
     "api_batch.cu",
     "api_stream.cu",
@@ -46,6 +47,7 @@ LIB_SOURCES = [
     "api_color.cu",
     "api_multi.cu",
     "api_blocks.cu",
+    "filter_f64.cu",
     "geometry.cpp",
     "sampling.cpp",
     "tiff_io.cpp",

@@ -46,6 +46,15 @@ extern "C" int inlm_blocks_slab_depth(const inlm_blocks* b, int* depth) {
     return INLM_OK;
 }
 
+extern "C" int inlm_blocks_attach_proposal(inlm_blocks* b, inlm_proposal* net, int k, float min_mass,
+                                           float rel_mass, int tiles_x) {
+    if (!b || !net) return fail(INLM_ERR_ARG, "null argument");
+    if (k < 1) return fail(INLM_ERR_ARG, "k must be >= 1");
+    if (!(rel_mass >= 0.f && rel_mass <= 1.f)) return fail(INLM_ERR_ARG, "rel_mass must be in 0..1");
+    if (b->last_iter > 0) return fail(INLM_ERR_STATE, "attach the proposal before the first iteration");
+    return b->be->attach_proposal(net, k, min_mass, rel_mass, tiles_x);
+}
+
 extern "C" int inlm_blocks_set_sigma(inlm_blocks* b, const float* sigma_host) {
     if (!b || !sigma_host) return fail(INLM_ERR_ARG, "null argument");
     int rc = b->be->set_sigma(sigma_host);

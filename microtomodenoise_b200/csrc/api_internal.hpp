@@ -118,6 +118,8 @@ struct inlm_proposal {
     float* d_g = nullptr;
     __nv_bfloat16* d_wb = nullptr;
     double* d_loss = nullptr;
+    int* d_err = nullptr;  // device error word of the tensor-core layers' bounded waits
+    bool tc = true;        // inference layers 2-4 on the tensor cores (training: CUDA cores)
     long long step = 0;
     inlm::DevBuf pad, a1, a2, a3, a4, glog, d1, d2, d3, d4, counters;
 };
@@ -127,12 +129,13 @@ struct ProposalRun {
     inlm_proposal* net = nullptr;
     int k = 0;
     float min_mass = 0.95f;
+    float rel_mass = 0.f;  // > 0: fallback below rel_mass x the mean predicted kept mass
     int nwords = 0;
     long long n_tiles = 0;
     inlm::Dim3i t8{0, 0, 0};
     int group = 1;         // 8^3 tiles per plan along x: 1, or 4 (the 32 x 8 x 8 CTA)
     long long n_plan = 0;  // plan lists (tiles / groups)
-    inlm::DevBuf a1, a2, a3, a4, bitmap, pmass, counters, scale, plan_start, plan_off;
+    inlm::DevBuf a1, a2, a3, a4, bitmap, pmass, counters, scale, plan_start, plan_off, mass_sum;
 };
 
 struct inlm_denoiser {
@@ -222,6 +225,9 @@ struct BlocksBackend {
     virtual int set_sigma(const float* sigma_host) = 0;
     virtual int iteration(int iter, const float* raw_host, const float* prev_host, float* out_host) = 0;
     virtual int slab_depth() const = 0;
+    virtual int attach_proposal(inlm_proposal*, int, float, float, int) {
+        return fail(INLM_ERR_UNSUPPORTED, "the proposal runs on the one-device blocks only");
+    }
 };
 int make_stream_blocks(const int shape[3], const inlm_params* p, int slab_depth, BlocksBackend** out);
 int make_multi_blocks(const int shape[3], const inlm_params* p, int n_parts, const int* device_ids,

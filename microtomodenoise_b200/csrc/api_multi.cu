@@ -286,8 +286,9 @@ struct MultiBlocks final : BlocksBackend {
             } else {
                 // the whole sub-volume, halos included, from the caller's previous
                 // iterate (raw is padded once, with the first installed result)
-                r = q.d->last_iter < 1 ? inlm_set_result(q.d, 1, prev + off, raw + off)
-                                       : inlm_set_result(q.d, it - 1, prev + off, nullptr);
+                // (installing iteration 1 pads raw with it, so it takes raw)
+                r = (q.d->last_iter < 1 || it - 1 == 1) ? inlm_set_result(q.d, 1, prev + off, raw + off)
+                                                        : inlm_set_result(q.d, it - 1, prev + off, nullptr);
                 if (!r) r = inlm_run_iteration(q.d, it, nullptr);
             }
             if (r) return r;

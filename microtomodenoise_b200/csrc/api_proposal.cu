@@ -28,6 +28,7 @@ static void proposal_free(inlm_proposal* p) {
     device_free(p->d_g);
     device_free(p->d_wb);
     device_free(p->d_loss);
+    device_free(p->d_err);
     for (DevBuf* b : {&p->pad, &p->a1, &p->a2, &p->a3, &p->a4, &p->glog, &p->d1, &p->d2, &p->d3,
                       &p->d4, &p->counters})
         b->release();
@@ -51,6 +52,7 @@ extern "C" int inlm_proposal_create(int n_offsets, int device_id, inlm_proposal*
         dalloc(&p->d_w, n) != cudaSuccess || dalloc(&p->d_m, n) != cudaSuccess ||
         dalloc(&p->d_v, n) != cudaSuccess || dalloc(&p->d_g, n) != cudaSuccess ||
         dalloc(&p->d_wb, n) != cudaSuccess || dalloc(&p->d_loss, 1) != cudaSuccess ||
+        dalloc(&p->d_err, 1) != cudaSuccess || cudaMemset(p->d_err, 0, 4) != cudaSuccess ||
         cudaMemset(p->d_w, 0, n * 4) != cudaSuccess || cudaMemset(p->d_m, 0, n * 4) != cudaSuccess ||
         cudaMemset(p->d_v, 0, n * 4) != cudaSuccess || cudaMemset(p->d_wb, 0, n * 2) != cudaSuccess) {
         proposal_free(p);
@@ -95,6 +97,24 @@ extern "C" int inlm_proposal_get_params(inlm_proposal* p, float* params, int64_t
     return INLM_OK;
 }
 
+// The tensor-core layers' bounded waits report through p->d_err.
+static int proposal_check_error(inlm_proposal* p) {
+    int h = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h, p->d_err, 4, cudaMemcpyDeviceToHost, p->stream));
+    CUDA_TRY(cudaStreamSynchronize(p->stream));
+    if (h != 0) {
+        cudaMemsetAsync(p->d_err, 0, 4, p->stream);
+        return fail(INLM_ERR_TIMEOUT, "device wait gave up (code %d)", h);
+    }
+    return INLM_OK;
+}
+
+extern "C" int inlm_proposal_set_tensor_cores(inlm_proposal* p, int on) {
+    if (!p) return fail(INLM_ERR_ARG, "null handle");
+    p->tc = on != 0;
+    return INLM_OK;
+}
+
 static int check_shape(const int shape[3]) {
     if (!shape) return fail(INLM_ERR_ARG, "null shape");
     for (int i = 0; i < 3; i++)
@@ -134,13 +154,12 @@ extern "C" int inlm_proposal_logits(inlm_proposal* p, const float* vol, const fl
     rc = example_input(p, vol, scale, shape, &in);
     if (rc) return rc;
     CUDA_TRY(prop_levels_alloc(&p->a1, &p->a2, &p->a3, &p->a4, shape[0], shape[1], shape[2]));
-    CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, prop_acts(p), p->stream));
+    CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, prop_acts(p), p->stream, NetTc{p->tc, p->d_err}));
     Dim3i lv[4];
     net_levels(shape[0], shape[1], shape[2], lv);
     CUDA_TRY(net_logits(p->L, p->d_wb, p->d_w, p->a4.as<float>(), lv[3].x * lv[3].y * lv[3].z, logits,
                         p->stream));
-    CUDA_TRY(cudaStreamSynchronize(p->stream));
-    return INLM_OK;
+    return proposal_check_error(p);
 }
 
 extern "C" int inlm_proposal_train(inlm_proposal* p, int n_examples, const float* const* vols,
@@ -212,7 +231,7 @@ extern "C" int inlm_proposal_select(inlm_proposal* p, const float* vol, const fl
     CUDA_TRY(prop_levels_alloc(&p->a1, &p->a2, &p->a3, &p->a4, shape[0], shape[1], shape[2]));
     CUDA_TRY(p->counters.ensure(16));
     CUDA_TRY(cudaMemsetAsync(p->counters.p, 0, 16, p->stream));
-    CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, prop_acts(p), p->stream));
+    CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, prop_acts(p), p->stream, NetTc{p->tc, p->d_err}));
     Dim3i lv[4];
     net_levels(shape[0], shape[1], shape[2], lv);
     const int nt = lv[3].x * lv[3].y * lv[3].z;
@@ -223,7 +242,7 @@ extern "C" int inlm_proposal_select(inlm_proposal* p, const float* vol, const fl
     CUDA_TRY(cudaMemcpyAsync(cnt, p->counters.p, 16, cudaMemcpyDeviceToHost, p->stream));
     CUDA_TRY(cudaStreamSynchronize(p->stream));
     if (n_fallback) *n_fallback = cnt[0];
-    return INLM_OK;
+    return proposal_check_error(p);
 }
 
 extern "C" int inlm_proposal_select_grouped(inlm_proposal* p, const float* vol, const float* scale,
@@ -241,7 +260,7 @@ extern "C" int inlm_proposal_select_grouped(inlm_proposal* p, const float* vol, 
     CUDA_TRY(prop_levels_alloc(&p->a1, &p->a2, &p->a3, &p->a4, shape[0], shape[1], shape[2]));
     CUDA_TRY(p->counters.ensure(16));
     CUDA_TRY(cudaMemsetAsync(p->counters.p, 0, 16, p->stream));
-    CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, prop_acts(p), p->stream));
+    CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, prop_acts(p), p->stream, NetTc{p->tc, p->d_err}));
     Dim3i lv[4];
     net_levels(shape[0], shape[1], shape[2], lv);
     CUDA_TRY(net_select_group(p->L, p->d_wb, p->d_w, p->a4.as<float>(), lv[3], tiles_x, k, min_mass, bitmap,
@@ -250,7 +269,7 @@ extern "C" int inlm_proposal_select_grouped(inlm_proposal* p, const float* vol, 
     CUDA_TRY(cudaMemcpyAsync(cnt, p->counters.p, 16, cudaMemcpyDeviceToHost, p->stream));
     CUDA_TRY(cudaStreamSynchronize(p->stream));
     if (n_fallback) *n_fallback = cnt[0];
-    return INLM_OK;
+    return proposal_check_error(p);
 }
 
 // ---------------- denoiser side ----------------
@@ -258,7 +277,7 @@ extern "C" int inlm_proposal_select_grouped(inlm_proposal* p, const float* vol, 
 void inlm::proposal_release(inlm_denoiser* d) {
     ProposalRun& r = d->prop;
     for (DevBuf* b : {&r.a1, &r.a2, &r.a3, &r.a4, &r.bitmap, &r.pmass, &r.counters, &r.scale,
-                      &r.plan_start, &r.plan_off})
+                      &r.plan_start, &r.plan_off, &r.mass_sum})
         b->release();
     r.net = nullptr;
 }
@@ -269,6 +288,11 @@ extern "C" int inlm_attach_proposal(inlm_denoiser* d, inlm_proposal* p, int k, f
 
 extern "C" int inlm_attach_proposal_grouped(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass,
                                             int tiles_x) {
+    return inlm_attach_proposal_ex(d, p, k, min_mass, 0.f, tiles_x);
+}
+
+extern "C" int inlm_attach_proposal_ex(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass,
+                                       float rel_mass, int tiles_x) {
     if (!d) return fail(INLM_ERR_ARG, "null handle");
     CUDA_TRY(cudaSetDevice(d->device));
     CUDA_TRY(cudaStreamSynchronize(d->stream));
@@ -295,9 +319,11 @@ extern "C" int inlm_attach_proposal_grouped(inlm_denoiser* d, inlm_proposal* p, 
         return fail(INLM_ERR_ARG, "proposal trained for %d offsets, the denoiser searches %d", p->L.S,
                     d->fargs.S);
     if (k < 1) return fail(INLM_ERR_ARG, "k must be >= 1");
+    if (!(rel_mass >= 0.f && rel_mass <= 1.f)) return fail(INLM_ERR_ARG, "rel_mass must be in 0..1");
     ProposalRun& r = d->prop;
     r.k = k;
     r.min_mass = min_mass;
+    r.rel_mass = rel_mass;
     r.nwords = (p->L.S + 31) / 32;
     Dim3i lv[4];
     net_levels(d->shape[0], d->shape[1], d->shape[2], lv);
@@ -315,6 +341,7 @@ extern "C" int inlm_attach_proposal_grouped(inlm_denoiser* d, inlm_proposal* p, 
     CUDA_TRY(r.scale.ensure((size_t)d->shape[2] * 4));
     CUDA_TRY(r.plan_start.ensure((size_t)2 * n * 4));
     CUDA_TRY(r.plan_off.ensure((size_t)n * p->L.S * 4));
+    CUDA_TRY(r.mass_sum.ensure(8));
     if ((long long)n * p->L.S >= (1ll << 31))
         return fail(INLM_ERR_ARG, "volume too large for one plan table; stream it in z-slabs");
     std::vector<int> st(n);
@@ -343,7 +370,7 @@ int inlm::proposal_enqueue(inlm_denoiser* d) {
     in.nz = d->shape[2];
     in.scale = r.scale.as<float>();
     NetActs act{r.a1.as<float>(), r.a2.as<float>(), r.a3.as<float>(), r.a4.as<float>()};
-    CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, act, d->stream));
+    CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, act, d->stream, NetTc{p->tc, d->d_err}));
     CUDA_TRY(cudaMemsetAsync(r.counters.p, 0, 16, d->stream));
     if (r.group == 1)
         CUDA_TRY(net_select(p->L, p->d_wb, p->d_w, act.a4, (int)r.n_tiles, r.k, r.min_mass,
@@ -355,8 +382,9 @@ int inlm::proposal_enqueue(inlm_denoiser* d) {
                                   r.counters.as<int>(), d->stream));
     int* ps = r.plan_start.as<int>();
     CUDA_TRY(net_plan_tiles(r.bitmap.as<unsigned>(), r.nwords, r.n_plan, p->L.S,
-                            r.plan_off.as<int>(), ps + r.n_plan, r.counters.as<int>(), d->stream));
-    d->launches += 7;  // scale, 4 layers, select, plan
+                            r.plan_off.as<int>(), ps + r.n_plan, r.counters.as<int>(), d->stream,
+                            r.pmass.as<float>(), r.mass_sum.as<double>(), r.rel_mass));
+    d->launches += r.rel_mass > 0.f ? 8 : 7;  // scale, 4 layers, select, (mass sum,) plan
     if (r.group == 1) {
         d->fargs8.plan_start = ps;
         d->fargs8.plan_count = ps + r.n_plan;

@@ -45,6 +45,7 @@ struct StreamJob {
     float* out_host = nullptr;
     cudaStream_t main = nullptr;
     int tiles_x = 1;  // proposal lists per 8^3 tile (1) or per 32 x 8 x 8 block (4)
+    float rel_mass = 0.f;  // relative fallback (the mean over each sub-volume's lists)
 
     ~StreamJob() {
         for (auto& kv : pairs)
@@ -87,7 +88,7 @@ int get_pair(StreamJob& J, const inlm_params& p, int depth, inlm_proposal* net, 
         if (rc) return rc;
         CUDA_TRY(dalloc(&sp.stage[j], (size_t)J.plane * depth));
         if (net) {
-            rc = inlm_attach_proposal_grouped(sp.d[j], net, k, min_mass, J.tiles_x);
+            rc = inlm_attach_proposal_ex(sp.d[j], net, k, min_mass, J.rel_mass, J.tiles_x);
             if (rc) return rc;
         }
     }
@@ -185,7 +186,16 @@ extern "C" int inlm_stream_denoise_grouped(const int shape[3], const inlm_params
                                            const float* raw_host, float* out_host, int slab_depth,
                                            inlm_proposal* net, int k, float min_mass, int tiles_x,
                                            float* sigma0_out, float* sigma1_out, double* stats) {
+    return inlm_stream_denoise_ex(shape, p, raw_host, out_host, slab_depth, net, k, min_mass, 0.f, tiles_x,
+                                  sigma0_out, sigma1_out, stats);
+}
+
+extern "C" int inlm_stream_denoise_ex(const int shape[3], const inlm_params* p, const float* raw_host,
+                                      float* out_host, int slab_depth, inlm_proposal* net, int k,
+                                      float min_mass, float rel_mass, int tiles_x, float* sigma0_out,
+                                      float* sigma1_out, double* stats) {
     if (!shape || !p || !raw_host || !out_host) return fail(INLM_ERR_ARG, "null argument");
+    if (!(rel_mass >= 0.f && rel_mass <= 1.f)) return fail(INLM_ERR_ARG, "rel_mass must be in 0..1");
     if (tiles_x != 1 && tiles_x != 4) return fail(INLM_ERR_ARG, "tiles_x must be 1 or 4");
     if (slab_depth < 1) return fail(INLM_ERR_ARG, "slab depth must be >= 1");
     if (p->noise_mode != INLM_NOISE_GLOBAL && p->noise_mode != INLM_NOISE_ZADAPTIVE &&
@@ -198,6 +208,7 @@ extern "C" int inlm_stream_denoise_grouped(const int shape[3], const inlm_params
     CUDA_TRY(cudaSetDevice(p->device_id));
     StreamJob J;
     J.tiles_x = tiles_x;
+    J.rel_mass = rel_mass;
     for (int i = 0; i < 3; i++) J.shape[i] = shape[i];
     J.plane = (long long)shape[0] * shape[1];
     J.raw_host = raw_host;
@@ -372,6 +383,9 @@ struct StreamBlocks final : BlocksBackend {
     std::vector<int> z0s;
     int sd = 0, halo = 0;
     cudaEvent_t ready = nullptr;
+    inlm_proposal* net = nullptr;
+    int k = 0;
+    float min_mass = 0.f;
 
     ~StreamBlocks() override {
         cudaSetDevice(p.device_id);
@@ -381,6 +395,34 @@ struct StreamBlocks final : BlocksBackend {
         if (ready) cudaEventDestroy(ready);
     }
     int slab_depth() const override { return sd; }
+    int attach_proposal(inlm_proposal* n, int kk, float mm, float rel, int tiles_x) override {
+        if (net) return fail(INLM_ERR_STATE, "a proposal is attached already");
+        if (p.precision == INLM_PRECISION_F32 || p.precision == INLM_PRECISION_F32_FMA)
+            return fail(INLM_ERR_UNSUPPORTED, "the proposal drives the FP16 form");
+        if (tiles_x != 1 && tiles_x != 4) return fail(INLM_ERR_ARG, "tiles_x must be 1 or 4");
+        // the sub-volume denoisers are rebuilt with the proposal attached;
+        // halos of >= 16 slices cover its receptive field
+        for (auto& kv : J.pairs)
+            for (int j = 0; j < 2; j++) {
+                if (kv.second.d[j]) inlm_denoiser_destroy(kv.second.d[j]);
+                device_free(kv.second.stage[j]);
+            }
+        J.pairs.clear();
+        net = n;
+        k = kk;
+        min_mass = mm;
+        J.tiles_x = tiles_x;
+        J.rel_mass = rel;
+        halo = std::max(halo, 16);
+        const int nz = J.shape[2];
+        for (int z0 : z0s) {
+            const int z1 = std::min(nz, z0 + sd);
+            SlabPair* sp;
+            int rc = get_pair(J, p, std::min(nz, z1 + halo) - std::max(0, z0 - halo), net, k, min_mass, &sp);
+            if (rc) return rc;
+        }
+        return INLM_OK;
+    }
     int set_sigma(const float* sigma) override {
         CUDA_TRY(cudaSetDevice(p.device_id));
         CUDA_TRY(cudaMemcpyAsync(J.d_sig, sigma, J.shape[2] * 4, cudaMemcpyHostToDevice, J.main));
@@ -396,7 +438,7 @@ struct StreamBlocks final : BlocksBackend {
         if (it > 1) pin.pin(prev, bytes);
         pin.pin(out, bytes);
         double h2d = 0, d2h = 0;
-        int rc = stream_pass(J, p, it, z0s, sd, halo, nullptr, 0, 0.f, raw, prev, out, false, ready, &h2d,
+        int rc = stream_pass(J, p, it, z0s, sd, halo, net, k, min_mass, raw, prev, out, false, ready, &h2d,
                              &d2h);
         // every slab's copies finish before the buffers are unpinned
         for (auto& kv : J.pairs)

@@ -690,16 +690,47 @@ __global__ void __launch_bounds__(32 * kSelWarps)
     }
 }
 
-// Per 8^3 tile (one warp): the kept offsets in ascending order, compacted
-// from the tile's bitmap into plan_off[tile * S ...]; plan_count[tile].
+// Sum of the n predicted kept masses in a fixed order (one CTA: strided
+// per-thread sums, then a tree), so the mean, and the relative fallback
+// threshold taken from it, are the same on every run.
+__global__ void __launch_bounds__(1024) net_mass_sum_kernel(const float* __restrict__ mass, long long n,
+                                                            double* __restrict__ out) {
+    __shared__ double red[1024];
+    double s = 0.0;
+    for (long long i = threadIdx.x; i < n; i += 1024) s += (double)mass[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 512; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = red[0];
+}
+
+// Per plan list (one warp): the kept offsets in ascending order, compacted
+// from the list's bitmap into plan_off[t * S ...]; plan_count[t]. With
+// rel > 0 a list whose predicted kept mass is below rel x the mean over all
+// lists (mass_sum / n_tiles) takes every offset instead (counters[0] counts
+// it).
 __global__ void net_plan_tiles_kernel(const unsigned* __restrict__ bitmap, int nwords,
                                       long long n_tiles, int S, int* __restrict__ plan_off,
-                                      int* __restrict__ plan_count, int* counters) {
+                                      int* __restrict__ plan_count, int* counters,
+                                      const float* __restrict__ pred_mass, const double* __restrict__ mass_sum,
+                                      float rel) {
     const int lane = threadIdx.x & 31;
     const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     if (t >= n_tiles) return;
     const unsigned* row = bitmap + t * nwords;
     int* out = plan_off + t * (long long)S;
+    if (rel > 0.f && pred_mass[t] < (float)((double)rel * (mass_sum[0] / (double)n_tiles))) {
+        for (int k = lane; k < S; k += 32) out[k] = k;
+        if (lane == 0) {
+            plan_count[t] = S;
+            atomicAdd(&counters[0], 1);
+            atomicAdd(&counters[1], S);
+        }
+        return;
+    }
     int n = 0;
     for (int w0 = 0; w0 < nwords; w0 += 32) {
         const int wd = w0 + lane;
@@ -769,7 +800,7 @@ __global__ void __launch_bounds__(256) normalise_rows_kernel(float* map, int S) 
     } while (0)
 
 cudaError_t net_forward(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const NetIn& in,
-                        const NetActs& act, cudaStream_t st) {
+                        const NetActs& act, cudaStream_t st, const NetTc& tc) {
     Dim3i lv[4];
     net_levels(in.nx, in.ny, in.nz, lv);
     if (in.half)
@@ -779,6 +810,13 @@ cudaError_t net_forward(const NetLayout& L, const __nv_bfloat16* wb, const float
         net_l1_fwd_kernel<float><<<grid_for(nvox(lv[1]), 256), 256, 0, st>>>(in, lv[1], wb + L.w1,
                                                                              wf + L.b1, act.a1);
     INLM_LAUNCH_CHECK();
+    if (tc.on) {
+        cudaError_t e = net_conv_fwd_tc(act.a1, lv[1], act.a2, lv[2], 2, wb + L.w2, wf + L.b2, tc.err, st);
+        if (e != cudaSuccess) return e;
+        e = net_conv_fwd_tc(act.a2, lv[2], act.a3, lv[3], 2, wb + L.w3, wf + L.b3, tc.err, st);
+        if (e != cudaSuccess) return e;
+        return net_conv_fwd_tc(act.a3, lv[3], act.a4, lv[3], 1, wb + L.w4, wf + L.b4, tc.err, st);
+    }
     net_conv_fwd_kernel<2><<<grid_for(nvox(lv[2]), 128), 128, 0, st>>>(act.a1, lv[1], act.a2, lv[2],
                                                                        wb + L.w2, wf + L.b2);
     INLM_LAUNCH_CHECK();
@@ -916,11 +954,17 @@ cudaError_t net_select_group(const NetLayout& L, const __nv_bfloat16* wb, const 
 }
 
 cudaError_t net_plan_tiles(const unsigned* bitmap, int nwords, long long n_tiles, int S,
-                           int* plan_off, int* plan_count, int* counters, cudaStream_t st) {
+                           int* plan_off, int* plan_count, int* counters, cudaStream_t st,
+                           const float* pred_mass, double* mass_sum, float rel) {
     if (n_tiles <= 0) return cudaSuccess;
+    if (rel > 0.f) {
+        net_mass_sum_kernel<<<1, 1024, 0, st>>>(pred_mass, n_tiles, mass_sum);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     const long long blocks = (n_tiles * 32 + 127) / 128;
     net_plan_tiles_kernel<<<(unsigned)blocks, 128, 0, st>>>(bitmap, nwords, n_tiles, S, plan_off,
-                                                            plan_count, counters);
+                                                            plan_count, counters, pred_mass, mass_sum, rel);
     return cudaGetLastError();
 }
 

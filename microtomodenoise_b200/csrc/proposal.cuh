@@ -42,8 +42,18 @@ struct NetActs {
     float* a4;  // level 3 x 16 (tile features)
 };
 
+// Tensor-core switch of the forward pass: layers 2-4 as tcgen05 implicit
+// GEMMs (proposal_tc.cu) instead of the CUDA-core kernels; err (nullable)
+// receives DEV_TMA_TIMEOUT if a bounded wait of those kernels runs out.
+struct NetTc {
+    bool on = false;
+    int* err = nullptr;
+};
 cudaError_t net_forward(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const NetIn& in,
-                        const NetActs& act, cudaStream_t st);
+                        const NetActs& act, cudaStream_t st, const NetTc& tc = NetTc());
+// One 3^3 conv layer (16 -> 16, stride 1 or 2, bias, ReLU) on the tensor cores.
+cudaError_t net_conv_fwd_tc(const float* in, Dim3i li, float* out, Dim3i lo, int stride,
+                            const __nv_bfloat16* W, const float* b, int* err, cudaStream_t st);
 cudaError_t net_logits(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const float* a4,
                        int n_tiles, float* logits, cudaStream_t st);
 
@@ -80,8 +90,11 @@ cudaError_t net_select(const NetLayout& L, const __nv_bfloat16* wb, const float*
 cudaError_t net_select_group(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const float* a4,
                              Dim3i t8, int G, int K, float min_mass, unsigned* bitmap, int nwords,
                              float* pred_mass, int* counters, cudaStream_t st);
+// rel > 0: lists whose pred_mass is below rel x its mean take every offset
+// (mass_sum: one double of device scratch).
 cudaError_t net_plan_tiles(const unsigned* bitmap, int nwords, long long n_tiles, int S,
-                           int* plan_off, int* plan_count, int* counters, cudaStream_t st);
+                           int* plan_off, int* plan_count, int* counters, cudaStream_t st,
+                           const float* pred_mass = nullptr, double* mass_sum = nullptr, float rel = 0.f);
 
 // Per-slice input scale from the filter multiplier m = -1/(sigma^2 beta).
 cudaError_t net_scale_from_mult(const float* mult, int nz, float* scale, cudaStream_t st);

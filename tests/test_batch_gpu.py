@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from microtomodenoise_b200 import Batch, DenoiseParameters, IterativeNLM_GPU, synth
+from oracle.oracle import FilterParams
 
 pytestmark = pytest.mark.gpu
 
@@ -113,3 +114,54 @@ def test_batch_groups_by_patch_weights(gpu):
     for i, ((s, p), raw, got) in enumerate(zip(cs, raws, outs)):
         assert np.array_equal(got, single(raw, p)), f"volume {i} z_anisotropy {p.z_anisotropy}"
     b.close()
+
+
+def test_batch_at_config3_sizes_against_the_oracle(gpu, port):
+    """The batch at the batched workload's largest sizes, pinned to the oracle
+    directly rather than through the single-volume path: a 384x384x256 volume
+    at patch radius 3, search radius 7 (the costliest shape of the mix), a
+    256x200x160 one at patch radius 2, search radius 5 and a 64^3 one at patch
+    radius 1, search radius 3 in one batch with manual sigma. Iteration 1 (one
+    batched iteration) and iteration 2 (a two-iteration batch) are compared
+    at 1500 seeded voxels per volume, faces and edges included, with the
+    oracle's FP32 filter (bit-exact to the reference's CPU filter) evaluated
+    at those voxels on the reflectively padded raw volume and previous
+    iterate."""
+    shapes = [(256, 384, 384), (160, 200, 256), (64, 64, 64)]
+    radii = [((3, 3, 3), (7, 7, 7)), ((2, 2, 2), (5, 5, 5)), ((1, 1, 1), (3, 3, 3))]
+    raws = [synth.spheres_volume(s, n_spheres=40, rmin=4, rmax=20, noise_std=0.05, seed=300 + i)
+            for i, s in enumerate(shapes)]
+    sig = (0.06, 0.045)
+
+    def params(pr, sr, iters):
+        return DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, noise_mode="manual",
+                                 sigma=sig, maxiterations=iters)
+
+    b1 = Batch(shapes, [params(pr, sr, 1) for pr, sr in radii])
+    it1 = b1.run(raws)
+    b1.close()
+    b2 = Batch(shapes, [params(pr, sr, 2) for pr, sr in radii])
+    it2 = b2.run(raws)
+    b2.close()
+    rng = np.random.default_rng(7)
+    for (pr, sr), raw, o1, o2 in zip(radii, raws, it1, it2):
+        nz, ny, nx = raw.shape
+        p = FilterParams(search_radius=sr, patch_radius=pr)
+        pad = port.padding(p)
+        # seeded voxels: uniform, plus the volume's corners and face centres
+        vox = list(rng.integers(0, raw.size, 1500 - 14))
+        for z in (0, nz - 1):
+            for y in (0, ny - 1):
+                for x in (0, nx - 1):
+                    vox.append((z * ny + y) * nx + x)
+        for z, y, x in ((0, ny // 2, nx // 2), (nz - 1, ny // 2, nx // 2), (nz // 2, 0, nx // 2),
+                        (nz // 2, ny - 1, nx // 2), (nz // 2, ny // 2, 0), (nz // 2, ny // 2, nx - 1)):
+            vox.append((z * ny + y) * nx + x)
+        vox = np.asarray(vox, np.int64)
+        raw_pad = port.pad_reflective(raw, pad)
+        s0 = np.full(nz, sig[0], np.float32)
+        s1 = (np.float32(0.5) * s0 + np.float32(0.5) * np.full(nz, sig[1], np.float32)).astype(np.float32)
+        want1 = port.filter_voxels(raw_pad, raw_pad, raw.shape, p, s0, vox)
+        assert np.array_equal(o1.ravel()[vox], want1), f"iteration 1, shape {raw.shape}"
+        want2 = port.filter_voxels(raw_pad, port.pad_reflective(o1, pad), raw.shape, p, s1, vox)
+        assert np.array_equal(o2.ravel()[vox], want2), f"iteration 2, shape {raw.shape}"

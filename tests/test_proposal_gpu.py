@@ -66,9 +66,12 @@ def block_close(got, want, S, tol):
 
 
 def test_logits_vs_oracle(gpu):
+    """CUDA-core forward: FP32 activations, within 1e-4 of the logits' range
+    of the FP64 restatement."""
     P = prop_mod()
     S = 40
     net = P.ProposalNet(S)
+    net.set_tensor_cores(False)
     params = rand_params(S, 1)
     net.set_params(params)
     ex, (vol, scale, _) = example((13, 22, 35), 3, S)
@@ -76,6 +79,38 @@ def test_logits_vs_oracle(gpu):
     want = po.forward(params, vol, scale, S)
     assert got.shape == want.shape
     assert np.abs(got - want).max() <= 1e-4 * np.abs(want).max() + 1e-5
+    net.close()
+
+
+@pytest.mark.parametrize("shape", [(13, 22, 35), (40, 72, 90)])
+def test_tensor_core_logits_vs_oracle(gpu, shape):
+    """Layers 2-4 on the tensor cores (tcgen05 kind::tf32, accumulators in
+    tensor memory): the activations enter the products rounded to TF32, so
+    the logits stay within 3e-3 of their range of the FP64 restatement (the
+    CUDA-core path: 1e-4), and the top-k sets agree on all but a few tiles
+    where two offsets are within that rounding of each other. A volume whose
+    level-2 activations span many 128-voxel tiles exercises the persistent
+    tile loop and the partial last tile."""
+    P = prop_mod()
+    S = 40
+    net = P.ProposalNet(S)
+    params = rand_params(S, 1)
+    net.set_params(params)
+    ex, (vol, scale, _) = example(shape, 3, S)
+    want = po.forward(params, vol, scale, S)
+    got = net.logits(ex.vol, ex.scale).cpu().numpy()
+    net.set_tensor_cores(False)
+    ref = net.logits(ex.vol, ex.scale).cpu().numpy()
+    rng_ = np.abs(want).max()
+    err = np.abs(got - want).max() / rng_
+    print(f"tensor-core logits: max error {err:.2e} of the range (CUDA cores: "
+          f"{np.abs(ref - want).max() / rng_:.2e})")
+    assert err <= 3e-3
+    k = 10
+    top_tc = np.argsort(-got, axis=1, kind="stable")[:, :k]
+    top_ref = np.argsort(-ref, axis=1, kind="stable")[:, :k]
+    same = np.mean([set(a) == set(b) for a, b in zip(top_tc, top_ref)])
+    assert same >= 0.9, same
     net.close()
 
 

@@ -81,3 +81,42 @@ def test_stream_grouped_proposal(gpu, port):
     got, _, _, st = stream_denoise(raw, p, slab_depth=16, net=net, k=40, min_mass=0.0, tiles_x=4)
     assert np.array_equal(got, want)
     net.close()
+
+
+def test_blocks_with_grouped_proposal_equal_in_memory(gpu, port):
+    """The per-iteration engine (inlm_blocks_*) with a learned proposal and
+    one list per 32x8x8 block: every iteration equals the in-memory FP16
+    learned form's, given the same sigma; with the relative fallback on, a
+    whole volume in one slab gives the in-memory result too (one mean over
+    the same lists)."""
+    from microtomodenoise_b200 import Blocks
+    from microtomodenoise_b200.proposal import ProposalNet
+    from oracle.oracle import FilterParams
+    from test_proposal_gpu import rand_params
+    raw = synth.small_case((48, 40, 72), seed=13)
+    p = DenoiseParameters(radius_patchspace=(1, 1, 1), radius_searchspace=(3, 3, 3), precision="f16")
+    S = len(port.search_offsets(FilterParams(search_radius=(3, 3, 3), patch_radius=(1, 1, 1))))
+    net = ProposalNet(S)
+    net.set_params(rand_params(S, 14))
+    sig = [np.full(48, 0.06, np.float32), np.full(48, 0.05, np.float32), np.full(48, 0.05, np.float32)]
+    for slab, rel in ((16, 0.0), (48, 0.9)):
+        g = IterativeNLM_GPU()
+        g.configure_device(raw.shape, p)
+        g.attach_proposal(net, 40, 0.0, tiles_x=4, rel_mass=rel)
+        want = []
+        for it, s in enumerate(sig):
+            g.set_sigma(s)
+            g.Run_GaussianNoise(it + 1, raw if it == 0 else None)
+            want.append(g.get_result())
+        g.free_device()
+        b = Blocks(raw.shape, p, slab_depth=slab)
+        b.attach_proposal(net, 40, 0.0, tiles_x=4, rel_mass=rel)
+        prev = None
+        for it, s in enumerate(sig):
+            b.set_sigma(s)
+            out = np.empty_like(raw)
+            b.run_iteration(it + 1, raw, prev, out)
+            assert np.array_equal(out, want[it]), f"slab {slab}, iteration {it + 1}"
+            prev = out
+        b.close()
+    net.close()
