@@ -16,8 +16,13 @@ exceed L2 (126 MB) between steps.
     python bench.py [--gpus N --steps K --warmup W]
     python bench.py --impl reference     # the reference CPU filter on host cores
 
-Multi-GPU (torchrun): each rank denoises its own volume (independent jobs,
-weak scaling, no data-path collective); time = max over ranks.
+Multi-GPU (torchrun, N ranks): one 512x512x(512N) volume split in z, each
+rank owning 512 slices (weak scaling) and filtering them with 8 slices of
+each neighbour (sharded.ZSlabJob): the neighbours' halo slices are swapped
+over NCCL after every iteration and the noise estimates all-reduce the
+per-sample patch stds, as the reference's n_gpus blocks split a stack
+(Denoiser/iternlm_gpu.cu:1729-1886); time = max over ranks. ``--split`` runs
+that path on one GPU (one rank).
 
 ``forms`` (rank 0, one GPU): the same whole job in the fused FP32 form
 (fused multiply-adds, within 1e-4 relative of the reference except at
@@ -766,6 +771,49 @@ def run_rgb_workload(args):
     print(json.dumps(res), flush=True)
 
 
+def run_train_workload(args):
+    """Training speed of the proposal network for patch radius 3 / search
+    radius 7 (1326 offsets, the shipped p3 s7 net's shape): Adam steps on
+    batches of 4 examples of 128^3 (the shipped training's batch), the
+    network input a seeded grain pack and the targets random per-tile
+    distributions (a step's cost does not depend on their values), with
+    layers 2-4 on the CUDA cores and then on the tensor cores (forward and
+    input gradients; weight gradients on the CUDA cores in both)."""
+    import torch
+    from microtomodenoise_b200 import synth
+    from microtomodenoise_b200.proposal import Example, ProposalNet, tiles8
+    S = 1326
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(0)
+    exs = []
+    for i in range(4):
+        v = synth.grain_pack_volume((128, 128, 128), noise_std=0.05, noise_blur=1.0, ring_amp=0.0, seed=100 + i)
+        nt = int(np.prod(tiles8(v.shape)))
+        t = rng.random((nt, S)).astype(np.float32) ** 4
+        t /= t.sum(axis=1, keepdims=True)
+        exs.append(Example(torch.from_numpy(v).to(dev), torch.full((128,), 7.0, device=dev),
+                           torch.from_numpy(t).to(dev)))
+    res = {"workload": "proposal training, S = 1326 (p3 s7), batches of 4 examples of 128^3"}
+    for name, tc in (("cuda_cores", False), ("tensor_cores", True)):
+        net = ProposalNet(S)
+        net.init(seed=0)
+        net.set_tensor_cores(True, training=tc)
+        for _ in range(3):
+            net.train_step(exs, 1e-3)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        n = max(args.steps, 10)
+        for _ in range(n):
+            net.train_step(exs, 1e-3)
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t
+        res[name] = {"steps": n, "ms_per_step": secs / n * 1e3, "steps_per_s": n / secs}
+        net.close()
+        log(f"{name}: {res[name]}")
+    res["speedup"] = res["tensor_cores"]["steps_per_s"] / res["cuda_cores"]["steps_per_s"]
+    print(json.dumps(res), flush=True)
+
+
 def run_profile_case(args):
     """Small cases of the filter kernels for ncu captures (one GPU, a few GB):
 
@@ -826,6 +874,72 @@ def run_profile_case(args):
         net.close()
 
 
+def run_split(args, rank, world, local):
+    """The z-slab split of one 512x512x(512 N) volume over N ranks (see the
+    module docstring): value = device-resident job (raw and result in HBM),
+    e2e = the same with the rank's raw slices from host memory and its result
+    slices back to it."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from microtomodenoise_b200 import DenoiseParameters
+    from microtomodenoise_b200.sharded import ZSlabJob
+    if not dist.is_initialized():
+        kw = {"device_id": torch.device("cuda", local)} if args.backend == "nccl" else {}
+        dist.init_process_group(args.backend, timeout=datetime.timedelta(seconds=300), **kw)
+    vol = make_volume(seed=0)  # this rank's 512 slices (every rank holds one copy of the pack)
+    full = (SHAPE[0] * world,) + SHAPE[1:]
+    dp = DenoiseParameters(radius_patchspace=PR, radius_searchspace=SR, maxiterations=ITERS, alpha=0.5,
+                           noise_mode="z-adaptive", zwindow=100, n_samples=100000, noise_seed=0,
+                           deviceID=local)
+    job = ZSlabJob(full, dp)
+    stream = job.be.stream
+    sync_dev = "cuda" if args.backend == "nccl" else "cpu"
+
+    def barrier():
+        dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, n):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=sync_dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t[0])
+
+    job.load(vol)
+    for _ in range(args.warmup):
+        job.run_loaded()
+    with ClockSampler(local) as clk:
+        ms = timed(job.run_loaded, args.steps)
+    ms_e2e = timed(lambda: (job.run(vol)), args.e2e_steps)
+    job.close()
+    vox = float(np.prod(full))
+    line = {
+        "metric": METRIC, "value": vox * ITERS * args.steps / (ms / 1e3), "unit": "voxel-iter/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded grain pack, 512^3 per rank)",
+        "config": dict(workload_config(), split=f"one {SHAPE[2]}x{SHAPE[1]}x{full[0]} volume split in z over "
+                                                f"{world} ranks ({args.backend}), {job.halo}-slice halos swapped "
+                                                "after every iteration, patch stds all-reduced",
+                       parallelism=f"z-slab split x{world}"),
+        "e2e": {"value": vox * ITERS * args.e2e_steps / (ms_e2e / 1e3), "unit": "voxel-iter/s",
+                "h2d_bytes_per_step": int(vol.nbytes), "d2h_bytes_per_step": int(vol.nbytes),
+                "ms_per_step": ms_e2e / args.e2e_steps, "per": "rank (own slices in, own slices out)"},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -841,7 +955,7 @@ def main():
     ap.add_argument("--reference-gpu-only", action="store_true",
                     help="--impl reference: only the reference GPU class timings")
     ap.add_argument("--workload", default="grain512",
-                    choices=["grain512", "learned1024", "stream2048", "rgb4k", "profile"],
+                    choices=["grain512", "learned1024", "stream2048", "rgb4k", "profile", "train"],
                     help="grain512: the headline bench line; learned1024, stream2048, rgb4k: "
                          "one-step measurements of the large workloads (run_large_workload, "
                          "run_rgb_workload); profile: a small case for ncu (--case)")
@@ -857,6 +971,10 @@ def main():
                          "threshold X x the mean predicted kept mass; precision f16 or f16_df32")
     ap.add_argument("--k-list", default="",
                     help="learned1024: learned + FP16 forms, k@tiles_per_plan[@min_mass|@rX][,...]")
+    ap.add_argument("--split", action="store_true",
+                    help="time the z-slab split path (sharded.ZSlabJob) even on one GPU")
+    ap.add_argument("--backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process group of the split path (gloo: exchange through host memory)")
     ap.add_argument("--shape", default="512,512,512",
                     help="nz,ny,nx of the volume (smaller shapes only for profiling runs)")
     args = ap.parse_args()
@@ -879,6 +997,8 @@ def main():
                 run_rgb_workload(args)
             elif args.workload == "profile":
                 run_profile_case(args)
+            elif args.workload == "train":
+                run_train_workload(args)
             else:
                 run_large_workload(args)
         return
@@ -886,10 +1006,14 @@ def main():
     import torch
     import torch.distributed as dist
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    if world > 1 or args.split:
+        if world == 1 and not dist.is_initialized():
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29533")
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
+        run_split(args, rank, world, local)
+        return
 
     from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, _lib
     import ctypes as C

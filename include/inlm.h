@@ -275,12 +275,14 @@ int inlm_proposal_train(inlm_proposal* p, int n_examples, const float* const* vo
 int inlm_proposal_select(inlm_proposal* p, const float* vol_dev, const float* scale_dev,
                          const int shape[3], int k, float min_mass, uint32_t* bitmap_dev,
                          float* pred_mass_dev, int* n_fallback);
-/* Inference layers 2-4 (3^3 convs, 16 -> 16 channels) on the tensor cores
- * (on = 1, the default: tcgen05 implicit GEMMs with TF32 operands, the BF16
- * weights exact in TF32, FP32 accumulation in tensor memory) or on the CUDA
- * cores (on = 0: FP32 activations; the reference of the tensor-core path).
- * Training (inlm_proposal_train) always runs the CUDA-core forward. */
-int inlm_proposal_set_tensor_cores(inlm_proposal* p, int on);
+/* Layers 2-4 (3^3 convs, 16 -> 16 channels) on the tensor cores: tcgen05
+ * implicit GEMMs with TF32 operands (the BF16 weights exact in TF32) and FP32
+ * accumulation in tensor memory; else on the CUDA cores with FP32
+ * activations (the reference of the tensor-core path). mode bit 0: inference
+ * (set by default); bit 1: training, the forward pass and the input
+ * gradients of inlm_proposal_train (clear by default; its weight gradients
+ * always run on the CUDA cores). */
+int inlm_proposal_set_tensor_cores(inlm_proposal* p, int mode);
 /* Attaches a proposal to an FP16-form denoiser (p == NULL detaches): every
  * later iteration runs the network on its previous iterate and evaluates the
  * selected offsets per 8^3 tile. */

@@ -119,7 +119,8 @@ struct inlm_proposal {
     __nv_bfloat16* d_wb = nullptr;
     double* d_loss = nullptr;
     int* d_err = nullptr;  // device error word of the tensor-core layers' bounded waits
-    bool tc = true;        // inference layers 2-4 on the tensor cores (training: CUDA cores)
+    bool tc = true;         // inference layers 2-4 on the tensor cores
+    bool train_tc = false;  // training forward and input gradients of layers 2-4 on the tensor cores
     long long step = 0;
     inlm::DevBuf pad, a1, a2, a3, a4, glog, d1, d2, d3, d4, counters;
 };

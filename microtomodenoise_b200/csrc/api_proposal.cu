@@ -109,9 +109,11 @@ static int proposal_check_error(inlm_proposal* p) {
     return INLM_OK;
 }
 
-extern "C" int inlm_proposal_set_tensor_cores(inlm_proposal* p, int on) {
+extern "C" int inlm_proposal_set_tensor_cores(inlm_proposal* p, int mode) {
     if (!p) return fail(INLM_ERR_ARG, "null handle");
-    p->tc = on != 0;
+    if (mode < 0 || mode > 3) return fail(INLM_ERR_ARG, "mode must be 0..3");
+    p->tc = (mode & 1) != 0;
+    p->train_tc = (mode & 2) != 0;
     return INLM_OK;
 }
 
@@ -194,11 +196,12 @@ extern "C" int inlm_proposal_train(inlm_proposal* p, int n_examples, const float
         net_levels(sh[0], sh[1], sh[2], lv);
         const long long nt = (long long)lv[3].x * lv[3].y * lv[3].z;
         CUDA_TRY(p->glog.ensure((size_t)nt * p->L.S * 4));
-        CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, prop_acts(p), p->stream));
+        const NetTc ttc{p->train_tc, p->d_err};
+        CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, prop_acts(p), p->stream, ttc));
         NetGradScratch gs{p->glog.as<float>(), p->d1.as<float>(), p->d2.as<float>(),
                           p->d3.as<float>(), p->d4.as<float>()};
         CUDA_TRY(net_backward(p->L, p->d_wb, p->d_w, in, prop_acts(p), targets[e], inv_n, gs, p->d_g,
-                              p->d_loss, p->stream));
+                              p->d_loss, p->stream, ttc));
     }
     if (grad_host) {
         CUDA_TRY(cudaMemcpyAsync(grad_host, p->d_g, np * 4, cudaMemcpyDeviceToHost, p->stream));
@@ -214,7 +217,7 @@ extern "C" int inlm_proposal_train(inlm_proposal* p, int n_examples, const float
     CUDA_TRY(cudaMemcpyAsync(&loss, p->d_loss, 8, cudaMemcpyDeviceToHost, p->stream));
     CUDA_TRY(cudaStreamSynchronize(p->stream));
     if (loss_out) *loss_out = loss;
-    return INLM_OK;
+    return proposal_check_error(p);
 }
 
 extern "C" int inlm_proposal_select(inlm_proposal* p, const float* vol, const float* scale,

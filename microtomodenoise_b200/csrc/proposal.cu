@@ -842,7 +842,8 @@ static int per_block_for(long long n, int target_blocks) {
 
 cudaError_t net_backward(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const NetIn& in,
                          const NetActs& act, const float* target, float inv_n,
-                         const NetGradScratch& s, float* grad, double* loss, cudaStream_t st) {
+                         const NetGradScratch& s, float* grad, double* loss, cudaStream_t st,
+                         const NetTc& tc) {
     Dim3i lv[4];
     net_levels(in.nx, in.ny, in.nz, lv);
     const int n_tiles = (int)nvox(lv[3]);
@@ -869,9 +870,14 @@ cudaError_t net_backward(const NetLayout& L, const __nv_bfloat16* wb, const floa
         net_conv_wgrad_kernel<1><<<(int)((nvox(lv[3]) + pb - 1) / pb), 256, 0, st>>>(
             act.a3, lv[3], s.d4, lv[3], pb, grad + L.w4, grad + L.b4);
         INLM_LAUNCH_CHECK();
-        net_conv_dgrad_kernel<1><<<grid_for(nvox(lv[3]), 128), 128, 0, st>>>(s.d4, lv[3], wb + L.w4,
-                                                                             act.a3, lv[3], s.d3);
-        INLM_LAUNCH_CHECK();
+        if (tc.on) {
+            cudaError_t e = net_conv_dgrad_tc(s.d4, lv[3], wb + L.w4, act.a3, lv[3], s.d3, 1, tc.err, st);
+            if (e != cudaSuccess) return e;
+        } else {
+            net_conv_dgrad_kernel<1><<<grid_for(nvox(lv[3]), 128), 128, 0, st>>>(s.d4, lv[3], wb + L.w4,
+                                                                                 act.a3, lv[3], s.d3);
+            INLM_LAUNCH_CHECK();
+        }
     }
     // L3 (stride 2, level 2 -> level 3)
     {
@@ -879,9 +885,14 @@ cudaError_t net_backward(const NetLayout& L, const __nv_bfloat16* wb, const floa
         net_conv_wgrad_kernel<2><<<(int)((nvox(lv[3]) + pb - 1) / pb), 256, 0, st>>>(
             act.a2, lv[2], s.d3, lv[3], pb, grad + L.w3, grad + L.b3);
         INLM_LAUNCH_CHECK();
-        net_conv_dgrad_kernel<2><<<grid_for(nvox(lv[2]), 128), 128, 0, st>>>(s.d3, lv[3], wb + L.w3,
-                                                                             act.a2, lv[2], s.d2);
-        INLM_LAUNCH_CHECK();
+        if (tc.on) {
+            cudaError_t e = net_conv_dgrad_tc(s.d3, lv[3], wb + L.w3, act.a2, lv[2], s.d2, 2, tc.err, st);
+            if (e != cudaSuccess) return e;
+        } else {
+            net_conv_dgrad_kernel<2><<<grid_for(nvox(lv[2]), 128), 128, 0, st>>>(s.d3, lv[3], wb + L.w3,
+                                                                                 act.a2, lv[2], s.d2);
+            INLM_LAUNCH_CHECK();
+        }
     }
     // L2 (stride 2, level 1 -> level 2)
     {
@@ -889,9 +900,14 @@ cudaError_t net_backward(const NetLayout& L, const __nv_bfloat16* wb, const floa
         net_conv_wgrad_kernel<2><<<(int)((nvox(lv[2]) + pb - 1) / pb), 256, 0, st>>>(
             act.a1, lv[1], s.d2, lv[2], pb, grad + L.w2, grad + L.b2);
         INLM_LAUNCH_CHECK();
-        net_conv_dgrad_kernel<2><<<grid_for(nvox(lv[1]), 128), 128, 0, st>>>(s.d2, lv[2], wb + L.w2,
-                                                                             act.a1, lv[1], s.d1);
-        INLM_LAUNCH_CHECK();
+        if (tc.on) {
+            cudaError_t e = net_conv_dgrad_tc(s.d2, lv[2], wb + L.w2, act.a1, lv[1], s.d1, 2, tc.err, st);
+            if (e != cudaSuccess) return e;
+        } else {
+            net_conv_dgrad_kernel<2><<<grid_for(nvox(lv[1]), 128), 128, 0, st>>>(s.d2, lv[2], wb + L.w2,
+                                                                                 act.a1, lv[1], s.d1);
+            INLM_LAUNCH_CHECK();
+        }
     }
     // L1
     {

@@ -69,7 +69,12 @@ struct NetGradScratch {
 };
 cudaError_t net_backward(const NetLayout& L, const __nv_bfloat16* wb, const float* wf, const NetIn& in,
                          const NetActs& act, const float* target, float inv_n,
-                         const NetGradScratch& s, float* grad, double* loss, cudaStream_t st);
+                         const NetGradScratch& s, float* grad, double* loss, cudaStream_t st,
+                         const NetTc& tc = NetTc());
+// Input gradient of one 3^3 conv layer on the tensor cores: din = [ain > 0] *
+// the transposed conv of G (level lo) with W, over level li.
+cudaError_t net_conv_dgrad_tc(const float* G, Dim3i lo, const __nv_bfloat16* W, const float* ain, Dim3i li,
+                              float* din, int stride, int* err, cudaStream_t st);
 
 cudaError_t net_adam(float* w, float* m, float* v, const float* g, __nv_bfloat16* wb, long long n,
                      float lr, float beta1, float beta2, float eps, float bc1, float bc2,

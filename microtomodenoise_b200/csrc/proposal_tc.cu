@@ -83,10 +83,16 @@ __device__ __forceinline__ void tc_load16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-template <int STRIDE>
+// DGRAD = false: the forward conv, out[o] over the output level lo from in
+// at level li. DGRAD = true: its input gradient, out[i] over the input level
+// li from the output gradient in = G at level lo: out[i][ci] = [act[i][ci] >
+// 0] * sum over taps t with STRIDE*o + d_t = i of sum_co G[o][co] W[t][ci][co]
+// (B row ci, K index (t, co)); no bias.
+template <int STRIDE, bool DGRAD>
 __global__ void __launch_bounds__(kTcM, 1)
     net_conv_tc_kernel(const float* __restrict__ in, Dim3i li, float* __restrict__ out, Dim3i lo,
-                       const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias, int* err) {
+                       const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias,
+                       const float* __restrict__ act, int* err) {
     extern __shared__ __align__(1024) unsigned char smem[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);           // 2 mbarriers
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + 64);
@@ -106,16 +112,18 @@ __global__ void __launch_bounds__(kTcM, 1)
         mbar_init(&bars[1], 1);
         fence_mbar_init();
     }
-    // B: W[t][ci][co] as row co, K index t*16 + ci, widened to FP32 (exact)
+    // B: W[t][ci][co] as row co, K index t*16 + ci (forward) or row ci, K
+    // index t*16 + co (input gradient), widened to FP32 (exact)
     for (int i = tid; i < 27 * kNetC * kNetC; i += kTcM) {
         const int t = i / (kNetC * kNetC), ci = (i / kNetC) % kNetC, co = i % kNetC;
-        const int kc = t * 4 + ci / 4;
-        float* dst = reinterpret_cast<float*>(Bs + ((co >> 3) * kBChunks + kc) * kCore + (co & 7) * 16);
-        dst[ci & 3] = __bfloat162float(W[i]);
+        const int row = DGRAD ? ci : co, kk = DGRAD ? co : ci;
+        const int kc = t * 4 + kk / 4;
+        float* dst = reinterpret_cast<float*>(Bs + ((row >> 3) * kBChunks + kc) * kCore + (row & 7) * 16);
+        dst[kk & 3] = __bfloat162float(W[i]);
     }
     float bs[kNetC];
 #pragma unroll
-    for (int c = 0; c < kNetC; c++) bs[c] = bias[c];
+    for (int c = 0; c < kNetC; c++) bs[c] = DGRAD ? 0.f : bias[c];
     fence_proxy_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -126,17 +134,20 @@ __global__ void __launch_bounds__(kTcM, 1)
 
     uint32_t phase[2] = {0u, 0u};
     bool ok = true;
-    const long long n = (long long)lo.x * lo.y * lo.z;
+    // rows of the GEMM: output voxels (forward) or input voxels (gradient)
+    const Dim3i lr = DGRAD ? li : lo;  // the level of the rows
+    const Dim3i lg = DGRAD ? lo : li;  // the level gathered from
+    const long long n = (long long)lr.x * lr.y * lr.z;
     const long long tiles = (n + kTcM - 1) / kTcM;
     for (long long tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const long long o = tile * kTcM + tid;
         int ox = 0, oy = 0, oz = 0;
         const bool live = o < n;
         if (live) {
-            ox = (int)(o % lo.x);
-            const long long r = o / lo.x;
-            oy = (int)(r % lo.y);
-            oz = (int)(r / lo.y);
+            ox = (int)(o % lr.x);
+            const long long r = o / lr.x;
+            oy = (int)(r % lr.y);
+            oz = (int)(r / lr.y);
         }
         // stage s gathers taps 9s .. 9s + 8 into buffer s % 2
         for (int s = 0; s < 3 && ok; s++) {
@@ -153,11 +164,25 @@ __global__ void __launch_bounds__(kTcM, 1)
             for (int lt = 0; lt < kTapsPerStage; lt++) {
                 const int t = s * kTapsPerStage + lt;
                 const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-                const int ix = STRIDE * ox + dx, iy = STRIDE * oy + dy, iz = STRIDE * oz + dz;
+                int ix, iy, iz;
+                bool inside;
+                if (!DGRAD) {
+                    ix = STRIDE * ox + dx;
+                    iy = STRIDE * oy + dy;
+                    iz = STRIDE * oz + dz;
+                    inside = true;
+                } else {
+                    // the output voxel whose tap t reads this input voxel
+                    const int qx = ox - dx, qy = oy - dy, qz = oz - dz;
+                    inside = (STRIDE == 1) || (((qx | qy | qz) & 1) == 0);
+                    ix = qx / STRIDE;
+                    iy = qy / STRIDE;
+                    iz = qz / STRIDE;
+                }
                 float4 v[4];
-                if (live && ix >= 0 && ix < li.x && iy >= 0 && iy < li.y && iz >= 0 && iz < li.z) {
+                if (live && inside && ix >= 0 && ix < lg.x && iy >= 0 && iy < lg.y && iz >= 0 && iz < lg.z) {
                     const float4* src = reinterpret_cast<const float4*>(
-                        in + (((long long)iz * li.y + iy) * li.x + ix) * kNetC);
+                        in + (((long long)iz * lg.y + iy) * lg.x + ix) * kNetC);
 #pragma unroll
                     for (int q = 0; q < 4; q++) v[q] = __ldg(src + q);
                 } else {
@@ -203,11 +228,22 @@ __global__ void __launch_bounds__(kTcM, 1)
         tc_load16(tmem + ((uint32_t)(warp * 32) << 16), acc);
         if (live) {
             float4* dst = reinterpret_cast<float4*>(out + o * kNetC);
+            if (!DGRAD) {
 #pragma unroll
-            for (int q = 0; q < 4; q++)
-                dst[q] = make_float4(fmaxf(acc[4 * q] + bs[4 * q], 0.f), fmaxf(acc[4 * q + 1] + bs[4 * q + 1], 0.f),
-                                     fmaxf(acc[4 * q + 2] + bs[4 * q + 2], 0.f),
-                                     fmaxf(acc[4 * q + 3] + bs[4 * q + 3], 0.f));
+                for (int q = 0; q < 4; q++)
+                    dst[q] = make_float4(fmaxf(acc[4 * q] + bs[4 * q], 0.f), fmaxf(acc[4 * q + 1] + bs[4 * q + 1], 0.f),
+                                         fmaxf(acc[4 * q + 2] + bs[4 * q + 2], 0.f),
+                                         fmaxf(acc[4 * q + 3] + bs[4 * q + 3], 0.f));
+            } else {
+                // the ReLU of the layer that produced this input
+                const float4* am = reinterpret_cast<const float4*>(act + o * kNetC);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float4 a = __ldg(am + q);
+                    dst[q] = make_float4(a.x > 0.f ? acc[4 * q] : 0.f, a.y > 0.f ? acc[4 * q + 1] : 0.f,
+                                         a.z > 0.f ? acc[4 * q + 2] : 0.f, a.w > 0.f ? acc[4 * q + 3] : 0.f);
+                }
+            }
         }
         // the next tile's first product overwrites the accumulator
         tc_fence_before();
@@ -231,26 +267,34 @@ __global__ void __launch_bounds__(kTcM, 1)
 
 }  // namespace
 
-cudaError_t net_conv_fwd_tc(const float* in, Dim3i li, float* out, Dim3i lo, int stride,
-                            const __nv_bfloat16* W, const float* b, int* err, cudaStream_t st) {
-    const long long n = (long long)lo.x * lo.y * lo.z;
+template <int STRIDE, bool DGRAD>
+static cudaError_t launch_tc(const float* in, Dim3i li, float* out, Dim3i lo, const __nv_bfloat16* W,
+                             const float* b, const float* act, int* err, cudaStream_t st) {
+    const Dim3i lr = DGRAD ? li : lo;
+    const long long n = (long long)lr.x * lr.y * lr.z;
     if (n <= 0) return cudaSuccess;
     const long long tiles = (n + kTcM - 1) / kTcM;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = (int)std::min<long long>(tiles, sms);
-    cudaError_t e;
-    if (stride == 2) {
-        e = cudaFuncSetAttribute(net_conv_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
-        if (e != cudaSuccess) return e;
-        net_conv_tc_kernel<2><<<grid, kTcM, kTcSmem, st>>>(in, li, out, lo, W, b, err);
-    } else {
-        e = cudaFuncSetAttribute(net_conv_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
-        if (e != cudaSuccess) return e;
-        net_conv_tc_kernel<1><<<grid, kTcM, kTcSmem, st>>>(in, li, out, lo, W, b, err);
-    }
+    cudaError_t e = cudaFuncSetAttribute(net_conv_tc_kernel<STRIDE, DGRAD>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    if (e != cudaSuccess) return e;
+    net_conv_tc_kernel<STRIDE, DGRAD><<<grid, kTcM, kTcSmem, st>>>(in, li, out, lo, W, b, act, err);
     return cudaGetLastError();
+}
+
+cudaError_t net_conv_fwd_tc(const float* in, Dim3i li, float* out, Dim3i lo, int stride,
+                            const __nv_bfloat16* W, const float* b, int* err, cudaStream_t st) {
+    return stride == 2 ? launch_tc<2, false>(in, li, out, lo, W, b, nullptr, err, st)
+                       : launch_tc<1, false>(in, li, out, lo, W, b, nullptr, err, st);
+}
+
+cudaError_t net_conv_dgrad_tc(const float* G, Dim3i lo, const __nv_bfloat16* W, const float* ain, Dim3i li,
+                              float* din, int stride, int* err, cudaStream_t st) {
+    return stride == 2 ? launch_tc<2, true>(G, li, din, lo, W, nullptr, ain, err, st)
+                       : launch_tc<1, true>(G, li, din, lo, W, nullptr, ain, err, st);
 }
 
 }  // namespace inlm

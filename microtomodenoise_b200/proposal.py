@@ -112,12 +112,14 @@ class ProposalNet:
                    "proposal_get_params")
         return p
 
-    def set_tensor_cores(self, on: bool) -> None:
-        """Inference runs layers 2-4 on the tensor cores (tcgen05, TF32
-        operands, FP32 accumulation; the default) or on the CUDA cores (FP32
-        activations, the reference of the tensor-core path). Training always
-        uses the CUDA-core forward."""
-        _lib.check(_lib.load().inlm_proposal_set_tensor_cores(self._h, int(bool(on))), "proposal_set_tensor_cores")
+    def set_tensor_cores(self, on: bool, training: bool = False) -> None:
+        """Layers 2-4 on the tensor cores (tcgen05, TF32 operands, FP32
+        accumulation) or on the CUDA cores (FP32 activations, the reference of
+        the tensor-core path): `on` for inference (the default), `training`
+        for the forward pass and input gradients of train_step / gradients
+        (off by default; weight gradients always run on the CUDA cores)."""
+        mode = (1 if on else 0) | (2 if training else 0)
+        _lib.check(_lib.load().inlm_proposal_set_tensor_cores(self._h, mode), "proposal_set_tensor_cores")
 
     def save(self, path: str, **meta) -> None:
         np.savez(path, params=self.get_params(), S=self.S, **meta)

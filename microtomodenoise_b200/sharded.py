@@ -271,7 +271,13 @@ class ZSlabJob:
         Returns (this rank's result slices, sigma0, sigma1) as host arrays,
         sigma1 being the estimate on iteration 1's result before the alpha
         blend (zeros for a single iteration), as inlm_denoise reports it."""
-        p = self.params
+        self.load(raw_own)
+        s0, s1 = self.run_loaded()
+        return self.be.result_own(), s0, s1
+
+    def load(self, raw_own: np.ndarray) -> None:
+        """Puts this rank's raw slices, and its neighbours' raw halo slices,
+        on its GPU (the first exchange of the job)."""
         raw_own = np.ascontiguousarray(raw_own, np.float32)
         assert raw_own.shape == (self.z1 - self.z0,) + self.full[1:], raw_own.shape
         h = min(self.halo, self.z1 - self.z0)
@@ -280,6 +286,11 @@ class ZSlabJob:
         r_lo, r_hi = self.ex.swap(lo, hi, shp, shp)
         self.be.set_raw(raw_own, r_lo, r_hi)
 
+    def run_loaded(self):
+        """The whole schedule on the raw volume load() put on the GPU; the
+        result stays there (result_own() copies it out). Returns (sigma0,
+        sigma1)."""
+        p = self.params
         s0 = self._estimate("raw")
         self.be.set_sigma(s0)
         self.be.iterate(1)
@@ -295,7 +306,7 @@ class ZSlabJob:
             if p.continuous_estimate and p.maxiterations > it + 1:
                 self.be.set_sigma(self._blend(s0, self._estimate("result")))
         # sigma1 as inlm_denoise reports it: the pre-blend estimate on iteration 1's result
-        return self.be.result_own(), s0, s1
+        return s0, s1
 
     def _blend(self, s0, s1):
         a = np.float32(self.params.alpha)

@@ -131,6 +131,27 @@ def test_gradients_vs_oracle(gpu):
     net.close()
 
 
+def test_tensor_core_training_gradients_vs_oracle(gpu):
+    """Training with layers 2-4 on the tensor cores (forward and input
+    gradients; weight gradients on the CUDA cores): the loss within 1e-3 and
+    every parameter block's gradient within 2e-2 of its largest entry of the
+    FP64 restatement (TF32 rounds the activations and the back-propagated
+    gradients to 10 mantissa bits; the CUDA-core path meets 2e-4)."""
+    P = prop_mod()
+    S = 24
+    net = P.ProposalNet(S)
+    net.set_tensor_cores(True, training=True)
+    params = rand_params(S, 2)
+    net.set_params(params)
+    e1, o1 = example((13, 22, 35), 5, S)
+    e2, o2 = example((24, 40, 48), 6, S)
+    loss, g = net.gradients([e1, e2])
+    want_loss, want_g = po.loss_and_grad(params, [o1, o2], S)
+    assert abs(loss - want_loss) <= 1e-3 * abs(want_loss)
+    block_close(g, want_g, S, 2e-2)
+    net.close()
+
+
 def test_adam_step_and_bf16_weights(gpu):
     P = prop_mod()
     S = 16
