@@ -30,13 +30,15 @@ weights that cross the Pade cutoff), the FP16-storage form, and the
 learned-proposal + FP16 form: one list of LEARNED_K offsets per 32x8x8 block
 (the four 8^3 tiles' predictions summed, run by the full-width kernel), with
 full search for every block whose predicted kept weight mass is below
-LEARNED_MIN_MASS; beside it the same lists without fallback and k = 256 per
-8^3 tile with the 0.95 threshold, which falls back on every tile of this
-volume. Each form reports its speed-up over the plain FP32 job, the
-proposal's fallback and evaluated-offset fractions, and its accuracy (see
-run_forms): PSNR against the clean phantom over the whole volume beside the
-plain FP32 result's, and max-abs error and PSNR against the FP64
-full-search oracle on 64 seeded 16^3 sub-blocks.
+LEARNED_REL x the mean over the volume's blocks; beside it the same lists at
+k = 176 without fallback and at k = 160 with fallback below 0.85 x the mean
+(the 4x points), and k = 256 per 8^3 tile with the absolute 0.95 threshold,
+which falls back on every tile of this volume. Each form reports its
+speed-up over the plain FP32 job, the proposal's fallback and
+evaluated-offset fractions, and its accuracy (see run_forms): PSNR against
+the clean phantom over the whole volume beside the plain FP32 result's, and
+max-abs error and PSNR against the FP64 full-search oracle on 64 seeded 16^3
+sub-blocks.
 
 ``batch`` (rank 0, one GPU): 24 seeded volumes, sizes uniform from 64^3 to
 384x384x256, spheres on a background with blurred noise of sigma uniform in
@@ -69,9 +71,11 @@ S_OFFSETS, P_TAPS = 514, 33
 FLOP_PER_VOXEL_ITER = S_OFFSETS * (2 * P_TAPS + 20)
 BYTES_PER_VOXEL_ITER_F32 = 12                          # read raw + prev, write result
 # learned + FP16 form of the headline line: one offset list per 32x8x8 block
-# of k offsets, full search for blocks whose predicted kept mass is below
-# LEARNED_MIN_MASS
-LEARNED_K, LEARNED_MIN_MASS = 144, 0.0
+# of LEARNED_K offsets, full search for the blocks whose predicted kept mass
+# is below LEARNED_REL x the mean over the volume's blocks (the fastest
+# setting measured within 0.1 dB of the plain and FP64 results with the
+# fallback on)
+LEARNED_K, LEARNED_MIN_MASS, LEARNED_REL = 208, 0.0, 0.9
 
 
 def log(*a):
@@ -297,9 +301,10 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
 
     net = ProposalNet.load(default_weights(PR, SR), device=local)
     forms = [("f32", "f32", None), ("f32_fused", "f32_fma", None), ("fp16", "f16", None),
-             ("learned_fp16", "f16", (LEARNED_K, LEARNED_MIN_MASS, 4)),
-             ("learned_fp16_no_fallback", "f16", (LEARNED_K, 0.0, 4)),
-             ("learned_fp16_k256_mass095", "f16", (256, 0.95, 1))]
+             ("learned_fp16", "f16", (LEARNED_K, LEARNED_MIN_MASS, 4, LEARNED_REL)),
+             ("learned_fp16_k176", "f16", (176, 0.0, 4, 0.0)),
+             ("learned_fp16_k160_r085", "f16", (160, 0.0, 4, 0.85)),
+             ("learned_fp16_k256_mass095", "f16", (256, 0.95, 1, 0.0))]
     for item in filter(None, args.learned_extra.split(",")):
         f = item.split("@")
         k, t = f[0], f[1] if len(f) > 1 else "1"
@@ -864,7 +869,7 @@ def run_profile_case(args):
         g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=(2, 2, 2),
                                                         radius_searchspace=(5, 5, 5), precision="f16",
                                                         noise_mode="z-adaptive", n_samples=100000))
-        g.attach_proposal(net, LEARNED_K, LEARNED_MIN_MASS, tiles_x=4)
+        g.attach_proposal(net, LEARNED_K, LEARNED_MIN_MASS, tiles_x=4, rel_mass=LEARNED_REL)
         g.denoise(raw.data_ptr(), on_device=True, out=out.data_ptr())
     torch.cuda.synchronize()
     ms, n = g.filter_kernel_ms()

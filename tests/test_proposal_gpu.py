@@ -156,6 +156,7 @@ def test_adam_step_and_bf16_weights(gpu):
     P = prop_mod()
     S = 16
     net = P.ProposalNet(S)
+    net.set_tensor_cores(False)  # the 1e-4 check below is the CUDA-core path's
     params = rand_params(S, 3)
     net.set_params(params)
     ex, o = example((12, 16, 20), 8, S)
