@@ -561,9 +561,9 @@ static void denoiser_free(inlm_denoiser* d) {
 }
 
 // Plane pitch (floats) of the raw box: the smallest padding of rpx * rby for
-// which the phase-B raw reads of a warp (8 rows j, 4 planes, one column) fall
-// in distinct banks.
-static int raw_plane_pitch(int rpx, int rby) {
+// which the phase-B raw reads of a warp (8 rows j, 4 planes pstride apart,
+// one column) fall in distinct banks.
+static int raw_plane_pitch(int rpx, int rby, int pstride = 1) {
     const int base = rpx * rby;
     for (int pad = 0; pad < 32; pad++) {
         const int pl = base + pad;
@@ -571,7 +571,7 @@ static int raw_plane_pitch(int rpx, int rby) {
         for (int col = 0; col < 8 && ok; col++) {
             unsigned used = 0;
             for (int l = 0; l < 32; l++) {
-                const unsigned bank = (unsigned)((l >> 3) * pl + (l & 7) * rpx + col) % 32u;
+                const unsigned bank = (unsigned)((l >> 3) * pstride * pl + (l & 7) * rpx + col) % 32u;
                 if (used & (1u << bank)) {
                     ok = false;
                     break;
@@ -624,7 +624,8 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
         if (order[3 * t] != g.taps[t].x || order[3 * t + 1] != g.taps[t].y ||
             order[3 * t + 2] != g.taps[t].z)
             return INLM_OK;
-    if (!((tz == 8) || (tz == 4 && !raw_smem))) return INLM_OK;
+    // tz 16: the two-planes-per-thread kernel (raw staged in shared memory)
+    if (!((tz == 8) || (tz == 4 && !raw_smem) || (tz == 16 && raw_smem))) return INLM_OK;
     const bool fused = d->p.precision == INLM_PRECISION_F32_FMA;
     if (fused && tz != 8) return INLM_OK;  // the fused form is instantiated at CTA depth 8
 
@@ -650,7 +651,7 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     a.rbz = tz + 2 * a.szc;
     if (a.pbx > 256 || a.pby > 256 || a.pbz > 256) return INLM_OK;
     if ((long long)a.pbx * a.pby * a.pbz >= 65536) return INLM_OK;  // 16-bit index table
-    a.rplane = raw_plane_pitch(a.rbx + 1, a.rby);
+    a.rplane = raw_plane_pitch(a.rbx + 1, a.rby, tz == 16 ? 2 : 1);
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
     TileConfig tc{pr[0], pr[1], pr[2], tz, raw_smem, 0, fused};
@@ -658,7 +659,8 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     a.raw_slab = 0;
     a.group_zb = nullptr;
     std::vector<int> zb;
-    if (raw_smem && tz == 8 && (sm == 0 || sm > (size_t)smem_max) && raw_slab_table(g, a.szc, tz, &zb)) {
+    if (raw_smem && (tz == 8 || tz == 16) && (sm == 0 || sm > (size_t)smem_max) &&
+        raw_slab_table(g, a.szc, tz, &zb)) {
         // the whole raw box does not fit: stage TZ + 1 planes per z offset pair
         a.rbz = tz + 1;
         a.raw_slab = 1;
@@ -710,7 +712,7 @@ static int choose_tile_config(inlm_denoiser* d) {
     const struct {
         int tz;
         bool raw;
-    } cands[] = {{8, true}, {8, false}, {4, false}};
+    } cands[] = {{16, true}, {8, true}, {8, false}, {4, false}};
     for (auto c : cands) {
         bool ok = false;
         int rc = tile_config_try(d, c.tz, c.raw, &ok);
@@ -756,7 +758,11 @@ static int build_fast_config(inlm_denoiser* d, int tx, FastConfig* cfg, FastArgs
     a.pby = kTY + 2 * a.py;
     a.rbx = (pr[0] + tx + 2 * a.sxr + 3) / 4 * 4;
     a.rby = kTY + 2 * a.syr;
-    for (int t = 0; t < nt; t++) a.w[t] = g.weights[t];
+    for (int t = 0; t < nt; t++) {
+        a.w[t] = g.weights[t];
+        const __half h = __float2half_rn(g.weights[t]);
+        a.wh[t] = __halves2half2(h, h);
+    }
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
     const bool dh = d->p.precision == INLM_PRECISION_F16;
@@ -854,11 +860,11 @@ extern "C" int inlm_denoiser_create(const int shape[3], const inlm_params* p, in
     d->nzp = shape[2] + 2 * g.pad[2];
     d->pitch_y = (d->nxp + 31) / 32 * 32;
     d->pitch_z = d->pitch_y * d->nyp;
-    // Tiles that stick out of the volume (z up to TZ-1 planes, y up to TY-1
-    // rows, x up to 31 columns past the end) read raw from global memory at
-    // positions they never store; kSlackPlanes zeroed planes after the padded
-    // volume keep every such read inside the allocation.
-    const long long kSlackPlanes = 9;
+    // Tiles that stick out of the volume (z up to TZ-1 planes with TZ <= 16,
+    // y up to TY-1 rows, x up to 31 columns past the end) read raw from global
+    // memory at positions they never store; kSlackPlanes zeroed planes after
+    // the padded volume keep every such read inside the allocation.
+    const long long kSlackPlanes = 17;
     const long long npad = d->pitch_z * (d->nzp + kSlackPlanes);
     const long long nvox = (long long)shape[0] * shape[1] * shape[2];
     int rc = INLM_OK;

@@ -104,7 +104,7 @@ int tune_class(const inlm_params& p0, bool batch, TuneResult* out) {
         int tz;
         bool raw;
     };
-    const Cand cands[] = {{8, true}, {8, false}, {4, false}};
+    const Cand cands[] = {{16, true}, {8, true}, {8, false}, {4, false}};
     double best = 1e30;
     TuneResult res;
     bool any = false;

@@ -8,8 +8,12 @@
 //   * squared differences D = (prev(.+s) - prev(.))^2 are formed in FP32 and
 //     kept in shared memory as FP16 (D_HALF) or FP32, scaled by the tile's
 //     1/sigma^2 so FP16 holds them in its normal range;
-//   * patch distances, Pade weights, weighted sums and weight sums accumulate
-//     in FP32 with fused multiply-adds;
+//   * patch distances: with FP16 D planes, half2 fused multiply-adds on pairs
+//     of voxels straight from the FP16 rows (two taps per instruction, no
+//     conversions; the weight-mass passes keep FP32 sums); with FP32 D planes,
+//     FP32 fused multiply-adds;
+//   * Pade weights, weighted sums and weight sums accumulate in FP32 with
+//     fused multiply-adds;
 //   * the final per-voxel normalisation (acc + wmax*raw)/(wsum + wmax) is FP64.
 // Offsets: every search offset, or a per-CTA list of offset indices. With
 // TX = 8 a CTA is one 8^3 tile, so a list is the learned proposal's top-K for
@@ -102,6 +106,83 @@ __device__ __forceinline__ void fast_rows(const unsigned char* __restrict__ Db, 
             for (int r = 0; r < VPT; r++) dist[r] = fmaf(win[XOFF + RX + r + xp], w, dist[r]);
         }
         fast_rows<RX, RY, RZ, TZ, TX, D_HALF, VPT, XOFF, RI + 1>(Db, rowoff, dist, a);
+    }
+}
+
+// Patch distances in half2 pairs (voxels 2p, 2p+1): the FP16 D row is read as
+// half2 registers; pairs that start on an odd column are assembled from two
+// neighbours; taps are HFMA2 with the tap weight in both halves.
+template <int RX, int RY, int RZ, int TZ, int TX, int VPT, int XOFF, int RI>
+__device__ __forceinline__ void fast_rows_h2(const unsigned char* __restrict__ Db, int rowoff,
+                                             __half2 (&dist)[VPT / 2], const FastArgs& a) {
+    using G = TileGeom<RX, RY, RZ, TZ, TX>;
+    using F = FastGeom<RX, RY, RZ, TZ, TX, true>;
+    if constexpr (RI < G::rows.n) {
+        constexpr int zp = G::rows.zp[RI];
+        constexpr int yp = G::rows.yp[RI];
+        constexpr int e = G::rows.e[RI];
+        constexpr int first = RowFirst<RX, RY, RZ, RI>::value;
+        constexpr int LO = XOFF + RX - e, HI = XOFF + RX + VPT - 1 + e;
+        static_assert(HI < 16, "row window");
+        const uint4* rowp = reinterpret_cast<const uint4*>(
+            Db + (size_t)(rowoff + (zp + RZ) * F::DPLANE + (yp + RY) * F::DP) * 2);
+        __half2 hw[8];
+#pragma unroll
+        for (int c = LO / 8; c <= HI / 8; c++) {
+            const uint4 v = rowp[c];
+            hw[4 * c + 0] = *reinterpret_cast<const __half2*>(&v.x);
+            hw[4 * c + 1] = *reinterpret_cast<const __half2*>(&v.y);
+            hw[4 * c + 2] = *reinterpret_cast<const __half2*>(&v.z);
+            hw[4 * c + 3] = *reinterpret_cast<const __half2*>(&v.w);
+        }
+#pragma unroll
+        for (int xp = -e; xp <= e; xp++) {
+            if (zp == 0 && yp == 0 && xp == 0) continue;
+            const int t = first + (xp + e) - ((zp == 0 && yp == 0 && xp > 0) ? 1 : 0);
+            const __half2 w = a.wh[t];
+#pragma unroll
+            for (int p = 0; p < VPT / 2; p++) {
+                const int i = XOFF + RX + 2 * p + xp;
+                const __half2 v = (i & 1) == 0 ? hw[i / 2]
+                                               : __halves2half2(__high2half(hw[i / 2]),
+                                                                __low2half(hw[i / 2 + 1]));
+                dist[p] = __hfma2(v, w, dist[p]);
+            }
+        }
+        fast_rows_h2<RX, RY, RZ, TZ, TX, VPT, XOFF, RI + 1>(Db, rowoff, dist, a);
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ, int TX, int VPT, int XOFF>
+__device__ __forceinline__ void tile_distances_h2(const unsigned char* __restrict__ Dr, int rowoff,
+                                                  float (&dist)[VPT], const FastArgs& a) {
+    using F = FastGeom<RX, RY, RZ, TZ, TX, true>;
+    constexpr int LO = XOFF + RX, HI = XOFF + RX + VPT - 1;
+    const uint4* rowp = reinterpret_cast<const uint4*>(Dr + (size_t)(rowoff + RZ * F::DPLANE + RY * F::DP) * 2);
+    __half2 hw[8];
+#pragma unroll
+    for (int c = LO / 8; c <= (HI + 1) / 8 && c < 2; c++) {
+        const uint4 v = rowp[c];
+        hw[4 * c + 0] = *reinterpret_cast<const __half2*>(&v.x);
+        hw[4 * c + 1] = *reinterpret_cast<const __half2*>(&v.y);
+        hw[4 * c + 2] = *reinterpret_cast<const __half2*>(&v.z);
+        hw[4 * c + 3] = *reinterpret_cast<const __half2*>(&v.w);
+    }
+    __half2 dh[VPT / 2];
+    const __half2 w0 = a.wh[0];
+#pragma unroll
+    for (int p = 0; p < VPT / 2; p++) {
+        const int i = LO + 2 * p;
+        const __half2 v = (i & 1) == 0 ? hw[i / 2]
+                                       : __halves2half2(__high2half(hw[i / 2]), __low2half(hw[i / 2 + 1]));
+        dh[p] = __hmul2(v, w0);
+    }
+    fast_rows_h2<RX, RY, RZ, TZ, TX, VPT, XOFF, 0>(Dr, rowoff, dh, a);
+#pragma unroll
+    for (int p = 0; p < VPT / 2; p++) {
+        const float2 f = __half22float2(dh[p]);
+        dist[2 * p] = f.x;
+        dist[2 * p + 1] = f.y;
     }
 }
 
@@ -317,6 +398,13 @@ __global__ void __launch_bounds__(TX * TZ * 8 / FastThreads<TX>::VPT, TX == 32 ?
                         tile_distances<RX, RY, RZ, TZ, TX, D_HALF, VPT, VPT>(Dr, rowoff, dist, a);
                     else
                         tile_distances<RX, RY, RZ, TZ, TX, D_HALF, VPT, 0>(Dr, rowoff, dist, a);
+                } else if constexpr (D_HALF && !MASS) {
+                    // the weight-sum pass of the mass maps keeps FP32 sums, like
+                    // the MASS pass it normalises (a uniform branch)
+                    if (a.aux)
+                        tile_distances<RX, RY, RZ, TZ, TX, D_HALF, VPT, 0>(Dr, rowoff, dist, a);
+                    else
+                        tile_distances_h2<RX, RY, RZ, TZ, TX, VPT, 0>(Dr, rowoff, dist, a);
                 } else {
                     tile_distances<RX, RY, RZ, TZ, TX, D_HALF, VPT, 0>(Dr, rowoff, dist, a);
                 }

@@ -31,6 +31,7 @@ struct FastArgs {
     float* map;                             // MASS: per-8^3-tile weight mass [tile][S]
     int t8x, t8y;                           // 8^3 tile grid (x, y)
     float w[kMaxTaps];
+    __half2 wh[kMaxTaps];                   // the same weights in FP16, both halves
 };
 
 struct FastConfig {

@@ -437,6 +437,297 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
     return true;
 }
 
+// ---- two z-planes per thread: CTA of 32 x 8 x 16 voxels ----
+//
+// The per-voxel arithmetic of tile_f32_body, with a thread owning 8 x voxels
+// on two adjacent planes k and k + 1. Patch row (zp, yp) of plane k + 1 is D
+// row (zp + 1, yp) counted from plane k, so one D row serves plane k's patch
+// row (dz, yp) and plane k + 1's patch row (dz - 1, yp): each row window is
+// loaded once for both planes (patch radius 2: 18 windows per offset for 16
+// voxels instead of 26). Walking the rows in (dz, yp) order keeps each plane's
+// patch rows in reference order, so every sum is formed in the same order as
+// before. One offset per barrier step: a second D buffer does not fit beside
+// the 16-deep prev box.
+
+struct RowPairs {
+    int n;
+    int dz[64], yp[64];
+    int r0[64], r1[64];  // patch row of plane k / of plane k + 1 read from this D row, or -1
+};
+
+constexpr RowPairs make_row_pairs(int rx, int ry, int rz) {
+    const PatchRows rows = make_patch_rows(rx, ry, rz);
+    RowPairs u{};
+    for (int dz = -rz; dz <= rz + 1; dz++)
+        for (int yp = -ry; yp <= ry; yp++) {
+            int r0 = -1, r1 = -1;
+            for (int i = 0; i < rows.n; i++) {
+                if (rows.zp[i] == dz && rows.yp[i] == yp) r0 = i;
+                if (rows.zp[i] == dz - 1 && rows.yp[i] == yp) r1 = i;
+            }
+            if (r0 < 0 && r1 < 0) continue;
+            u.dz[u.n] = dz;
+            u.yp[u.n] = yp;
+            u.r0[u.n] = r0;
+            u.r1[u.n] = r1;
+            u.n++;
+        }
+    return u;
+}
+
+template <int RX, int RY, int RZ>
+struct RowPairsOf {
+    static constexpr RowPairs v = make_row_pairs(RX, RY, RZ);
+};
+
+// The taps of patch row RI (reference order) on a loaded row window.
+template <int RX, int RY, int RZ, int RI>
+__device__ __forceinline__ void row_taps(const float (&win)[16], f32x2 (&d)[kVoxPerThread / 2],
+                                         const TileArgs& a) {
+    using G = TileGeom<RX, RY, RZ, 16>;
+    constexpr int zp = G::rows.zp[RI];
+    constexpr int yp = G::rows.yp[RI];
+    constexpr int e = G::rows.e[RI];
+    constexpr int first = RowFirst<RX, RY, RZ, RI>::value;
+#pragma unroll
+    for (int xp = -e; xp <= e; xp++) {
+        if (zp == 0 && yp == 0 && xp == 0) continue;
+        const int t = first + (xp + e) - ((zp == 0 && yp == 0 && xp > 0) ? 1 : 0);
+        const float w = a.w[t];
+#pragma unroll
+        for (int p = 0; p < kVoxPerThread / 2; p++) {
+            const int i = RX + 2 * p + xp;
+            d[p] = add2(d[p], mul_pair(win[i], win[i + 1], w));
+        }
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ, int UI>
+__device__ __forceinline__ void accumulate_row_pairs(const float* __restrict__ D, int rowoff,
+                                                     f32x2 (&d0)[kVoxPerThread / 2],
+                                                     f32x2 (&d1)[kVoxPerThread / 2],
+                                                     const TileArgs& a) {
+    using G = TileGeom<RX, RY, RZ, TZ>;
+    using U = RowPairsOf<RX, RY, RZ>;
+    if constexpr (UI < U::v.n) {
+        constexpr int r0 = U::v.r0[UI];
+        constexpr int r1 = U::v.r1[UI];
+        constexpr int e0 = r0 >= 0 ? G::rows.e[r0 >= 0 ? r0 : 0] : 0;
+        constexpr int e1 = r1 >= 0 ? G::rows.e[r1 >= 0 ? r1 : 0] : 0;
+        constexpr int em = e0 > e1 ? e0 : e1;
+        constexpr int lo = (RX - em) / 4;
+        constexpr int hi = (RX + kVoxPerThread - 1 + em) / 4;
+        const int ro = rowoff + (U::v.dz[UI] + RZ) * G::DPLANE + (U::v.yp[UI] + RY) * G::DP;
+        float win[16];
+        load_window<lo, hi>(D + ro, win);
+        if constexpr (r0 >= 0) row_taps<RX, RY, RZ, (r0 >= 0 ? r0 : 0)>(win, d0, a);
+        if constexpr (r1 >= 0) row_taps<RX, RY, RZ, (r1 >= 0 ? r1 : 0)>(win, d1, a);
+        accumulate_row_pairs<RX, RY, RZ, TZ, UI + 1>(D, rowoff, d0, d1, a);
+    }
+}
+
+// Raw staged in shared memory: the whole box (SLAB = false) or TZ + 1 planes
+// following the z-major offsets (SLAB = true), as in tile_f32_body.
+template <int RX, int RY, int RZ, bool SLAB>
+__device__ __forceinline__ void tile_f32_z2_body(const CUtensorMap* tm_prev, const TileArgs& a,
+                                                 unsigned char* smem) {
+    constexpr int TZ = 16;
+    constexpr int NT = 256;
+    using G = TileGeom<RX, RY, RZ, TZ>;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+    float* prevb = reinterpret_cast<float*>(smem + 128);
+    const int pplane = a.pbx * a.pby;
+    const int PB = pplane * a.pbz;
+    float* rawb = prevb + round_up32(PB);
+    const int rpx = a.rbx + 1;
+    float* D = rawb + round_up32(a.rplane * a.rbz);
+
+    const int tid = threadIdx.x;
+    const int X0 = blockIdx.x * kTX;
+    const int Y0 = blockIdx.y * kTY;
+    const int Z0 = blockIdx.z * TZ;
+
+    if (tid == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)PB * 4u);
+        tma_load_3d(prevb, tm_prev, X0, Y0, Z0, bar);
+    }
+    auto stage_raw = [&](int zoff) {
+        const int rb_n = a.rbx * a.rby * a.rbz;
+        const float* rsrc = a.raw_pad + (long long)(Z0 + RZ + zoff) * a.gpitch_z +
+                            (long long)(Y0 + RY) * a.gpitch_y + X0;
+        for (int i = tid; i < rb_n; i += NT) {
+            int xx = i % a.rbx;
+            int rest = i / a.rbx;
+            int yy = rest % a.rby;
+            int zz = rest / a.rby;
+            rawb[zz * a.rplane + yy * rpx + xx] =
+                __ldg(rsrc + (long long)zz * a.gpitch_z + (long long)yy * a.gpitch_y + xx);
+        }
+    };
+    int slab_zb = 0;
+    if (SLAB) slab_zb = __ldg(&a.group_zb[0]);
+    stage_raw(SLAB ? a.szc + slab_zb : 0);
+
+    constexpr int NPAIR = G::ND / 2;
+    constexpr int NQ = (NPAIR + NT - 1) / NT;
+    int qpi[NQ], qdi[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        int e = min(tid + q * NT, NPAIR - 1);  // the tail repeats the last pair
+        int f = 2 * e;
+        int c = f % G::DW;
+        int rest = f / G::DW;
+        int r = rest % G::DH;
+        int p = rest / G::DH;
+        qpi[q] = (p - RZ + a.pz) * pplane + (r - RY + a.py) * a.pbx + (c - RX + a.px);
+        qdi[q] = p * G::DPLANE + r * G::DP + c;
+    }
+
+    const bool arrived = mbar_wait_bounded(bar, 0);
+    if (!__syncthreads_and(arrived)) {
+        if (tid == 0) set_error(a.err, DEV_TMA_TIMEOUT);
+        return;
+    }
+    f32x2 qog[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) qog[q] = pack2(prevb[qpi[q]], prevb[qpi[q] + 1]);
+
+    // lane map: warp w covers x sub-block w % 4 and planes 8*(w/4)..+7; lane =
+    // (row j, plane pair), planes k and k + 1
+    const int warp = tid >> 5, lane = tid & 31;
+    const int k = 8 * (warp >> 2) + 2 * (lane >> 3);
+    const int j = lane & 7;
+    const int x0 = (warp & 3) * kVoxPerThread;
+    const f32x2 m0 = splat2(a.mult[min(Z0 + k, a.nz - 1)]);
+    const f32x2 m1 = splat2(a.mult[min(Z0 + k + 1, a.nz - 1)]);
+    const int rowoff = k * G::DPLANE + j * G::DP + x0;
+    const int rbase_box = (a.szc + k) * a.rplane + (a.syr + j) * rpx + (RX + a.sxr + x0);
+    int rbase = rbase_box - (SLAB ? (a.szc + slab_zb) * a.rplane : 0);
+
+    constexpr int NP = kVoxPerThread / 2;
+    f32x2 acc0[NP], wsum0[NP], acc1[NP], wsum1[NP];
+    float wmax0[kVoxPerThread], wmax1[kVoxPerThread];
+#pragma unroll
+    for (int p = 0; p < NP; p++) acc0[p] = wsum0[p] = acc1[p] = wsum1[p] = 0ull;
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) wmax0[r] = wmax1[r] = 0.0f;
+
+    const f32x2 c12 = splat2(12.f), c120 = splat2(120.f);
+
+    auto phase_a = [&](int dlx) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            f32x2 sh = pack2(prevb[qpi[q] + dlx], prevb[qpi[q] + dlx + 1]);
+            f32x2 v = sub2(sh, qog[q]);
+            *reinterpret_cast<f32x2*>(D + qdi[q]) = mul2_to_mul(v, v);  // stored, not added
+        }
+    };
+
+    // weight and accumulation of one offset for one plane's 8 voxels (the
+    // exact Pade form of tile_f32_body)
+    auto accumulate = [&](const f32x2 (&dist)[NP], const f32x2 m2, int rb, f32x2 (&acc)[NP],
+                          f32x2 (&wsum)[NP], float (&wmax)[kVoxPerThread]) {
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            const float2 rsv = make_float2(rawb[rb + 2 * p], rawb[rb + 2 * p + 1]);
+            const f32x2 x = mul2_to_mul(dist[p], m2);
+            const float2 xs = unpack2(x);
+            const float2 x12 = unpack2(mul2_to_mul(c12, x));
+            const float2 xx = unpack2(mul2_to_mul(x, x));
+            const f32x2 ta = mul_pair(xs, make_float2(60.f, 60.f));
+            const f32x2 tb = mul_pair(x12, xs);
+            const f32x2 tc = mul_pair(xx, xs);
+            const float2 num = unpack2(add2(add2(add2(c120, ta), tb), tc));
+            const float2 den = unpack2(sub2(add2(sub2(c120, ta), tb), tc));
+            const float q0 = __fdiv_rn(num.x, den.x), q1 = __fdiv_rn(num.y, den.y);
+            const float w0 = (xs.x > -3.56648f) ? q0 : 0.0f;
+            const float w1 = (xs.y > -3.56648f) ? q1 : 0.0f;
+            acc[p] = add2(acc[p], mul_pair(make_float2(w0, w1), rsv));
+            wsum[p] = add2(wsum[p], pack2(w0, w1));
+            wmax[2 * p] = fmaxf(wmax[2 * p], w0);
+            wmax[2 * p + 1] = fmaxf(wmax[2 * p + 1], w1);
+        }
+    };
+
+    int2 dl = __ldg(&a.search_delta[0]);
+    for (int s = 0; s < a.S; s++) {
+        if (SLAB) {
+            // uniform branch; the previous offset's raw reads ended at its
+            // closing barrier and the barrier after phase A publishes the planes
+            const int zb = __ldg(&a.group_zb[s / kOffGroup]);
+            if (zb != slab_zb) {
+                slab_zb = zb;
+                stage_raw(a.szc + zb);
+                rbase = rbase_box - (a.szc + zb) * a.rplane;
+            }
+        }
+        const int2 dln = __ldg(&a.search_delta[min(s + 1, a.S - 1)]);
+        phase_a(dl.x);
+        __syncthreads();
+        f32x2 d0[NP], d1[NP];
+        {
+            const float w0 = a.w[0];
+            float win[16];
+            load_window<RX / 4, (RX + kVoxPerThread - 1) / 4>(D + rowoff + RZ * G::DPLANE + RY * G::DP, win);
+#pragma unroll
+            for (int p = 0; p < NP; p++) d0[p] = mul_pair(win[RX + 2 * p], win[RX + 2 * p + 1], w0);
+            load_window<RX / 4, (RX + kVoxPerThread - 1) / 4>(
+                D + rowoff + (RZ + 1) * G::DPLANE + RY * G::DP, win);
+#pragma unroll
+            for (int p = 0; p < NP; p++) d1[p] = mul_pair(win[RX + 2 * p], win[RX + 2 * p + 1], w0);
+        }
+        accumulate_row_pairs<RX, RY, RZ, TZ, 0>(D, rowoff, d0, d1, a);
+        accumulate(d0, m0, rbase + dl.y, acc0, wsum0, wmax0);
+        accumulate(d1, m1, rbase + a.rplane + dl.y, acc1, wsum1, wmax1);
+        __syncthreads();
+        dl = dln;
+    }
+
+    const int y = Y0 + j;
+#pragma unroll
+    for (int pl = 0; pl < 2; pl++) {
+        const int z = Z0 + k + pl;
+        if (z >= a.nz || y >= a.ny) continue;
+        float* orow = a.out + ((long long)z * a.ny + y) * a.nx;
+        const long long gb = (long long)(z + a.pz) * a.gpitch_z + (long long)(y + a.py) * a.gpitch_y +
+                             (X0 + x0 + a.px);
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) {
+            const int x = X0 + x0 + r;
+            if (x < a.nx) {
+                const float raw0 = SLAB ? __ldg(&a.raw_pad[gb + r]) : rawb[rbase + pl * a.rplane + r];
+                const float2 acp = unpack2(pl ? acc1[r / 2] : acc0[r / 2]);
+                const float2 wsp = unpack2(pl ? wsum1[r / 2] : wsum0[r / 2]);
+                const float wm = pl ? wmax1[r] : wmax0[r];
+                float ac = (r & 1) ? acp.y : acp.x;
+                float ws = (r & 1) ? wsp.y : wsp.x;
+                float res;
+                if (wm > 0.0f) {
+                    ac = __fadd_rn(ac, __fmul_rn(wm, raw0));
+                    ws = __fadd_rn(ws, wm);
+                    res = __fdiv_rn(ac, ws);
+                } else {
+                    res = raw0;
+                }
+                orow[x] = res;
+            }
+        }
+    }
+}
+
+template <int RX, int RY, int RZ, bool SLAB>
+__global__ void __launch_bounds__(256, 1)
+    nlm_tile_f32_z2_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (threadIdx.x == 0) {
+        prefetch_tmap(&tm_prev);
+        mbar_init(reinterpret_cast<uint64_t*>(smem), 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    tile_f32_z2_body<RX, RY, RZ, SLAB>(&tm_prev, a, smem);
+}
+
 template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED, bool SLAB>
 __global__ void __launch_bounds__(32 * TZ, 1)
     nlm_tile_f32_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
@@ -590,7 +881,19 @@ static size_t smem_bytes_for(const TileArgs& a) {
     size_t pb = round_up32(a.pbx * a.pby * a.pbz);
     size_t rb = RAW_SMEM ? round_up32(a.rplane * a.rbz) : 0;
     size_t d = round_up32(G::DPLANE * G::DD);
-    return 128 + 4 * (pb + rb + kOffGroup * d);
+    // the 16-deep kernel keeps one D buffer (one offset per barrier step)
+    return 128 + 4 * (pb + rb + (TZ == 16 ? 1 : kOffGroup) * d);
+}
+
+template <int RX, int RY, int RZ, bool SLAB>
+static cudaError_t launch_z2(const CUtensorMap* tmp, const TileArgs& a, int tiles_z, size_t smem,
+                             cudaStream_t st) {
+    auto kern = nlm_tile_f32_z2_kernel<RX, RY, RZ, SLAB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
+    kern<<<grid, 256, smem, st>>>(*tmp, a);
+    return cudaGetLastError();
 }
 
 template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED = false, bool SLAB = false>
@@ -671,6 +974,7 @@ bool tile_kernel_available(int rx, int ry, int rz) {
 size_t tile_smem_bytes(const TileConfig& c, const TileArgs& a) {
 #define X(A, B, C)                                                                    \
     if (c.rx == A && c.ry == B && c.rz == C) {                                        \
+        if (c.tz == 16 && c.raw_smem) return smem_bytes_for<A, B, C, 16, true>(a);   \
         if (c.tz == 8 && c.raw_smem) return smem_bytes_for<A, B, C, 8, true>(a);     \
         if (c.tz == 8 && !c.raw_smem) return smem_bytes_for<A, B, C, 8, false>(a);   \
         if (c.tz == 4 && !c.raw_smem) return smem_bytes_for<A, B, C, 4, false>(a);   \
@@ -685,6 +989,9 @@ cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,
                                cudaStream_t st) {
 #define X(A, B, C)                                                                             \
     if (c.rx == A && c.ry == B && c.rz == C) {                                                 \
+        if (c.tz == 16 && c.raw_smem && !c.fused)                                              \
+            return c.raw_slab ? launch_z2<A, B, C, true>(tm_prev, a, tiles_z, c.smem_bytes, st)   \
+                              : launch_z2<A, B, C, false>(tm_prev, a, tiles_z, c.smem_bytes, st); \
         if (c.raw_slab && c.tz == 8 && c.raw_smem)                                             \
             return c.fused ? launch_inst<A, B, C, 8, true, true, true>(tm_prev, tm_raw, a, tiles_z,  \
                                                                       c.smem_bytes, st)        \

@@ -57,11 +57,11 @@ struct GenericArgs {
 // Host-side launch descriptors.
 struct TileConfig {
     int rx, ry, rz;   // patch radii of the instantiation
-    int tz;           // CTA depth (z-planes = warps)
+    int tz;           // CTA depth: z-planes = warps (4, 8), or 16 with two planes per thread
     bool raw_smem;    // raw box staged in shared memory
     size_t smem_bytes;
     bool fused = false;  // the fused FP32 form (FFMA taps, Horner Pade, fast division); tz 8 only
-    bool raw_slab = false;  // raw staged as TZ + 1 planes per z offset pair (raw_smem, tz 8)
+    bool raw_slab = false;  // raw staged as TZ + 1 planes per z offset pair (raw_smem, tz 8 or 16)
 };
 
 // Returns false when no tiled instantiation exists for the patch shape.

@@ -15,9 +15,9 @@
 //     tcgen05.commit signals an mbarrier when a stage's products are done;
 //   * the four warps read their 32 rows back with tcgen05.ld, add the bias,
 //     apply the ReLU and store the FP32 activations.
-// TF32 keeps the BF16 weights exact and rounds the activations to 10
-// mantissa bits (the CUDA-core kernels keep FP32 activations); products
-// accumulate in FP32. Every mbarrier wait is bounded: on expiry the CTA
+// TF32 keeps the BF16 weights exact; the tensor core reads each FP32
+// activation (or output gradient) as TF32, dropping its low 13 mantissa bits
+// (the CUDA-core kernels keep FP32 operands); products accumulate in FP32. Every mbarrier wait is bounded: on expiry the CTA
 // records DEV_TMA_TIMEOUT, releases its tensor memory and returns.
 #include <cuda_bf16.h>
 

@@ -16,6 +16,14 @@ Network (channels-last, x fastest, arrays indexed [z, y, x, c]):
         sum to 1 or 0; inv_n = 1 / number of tiles).
 Weight blocks are rounded to BF16 (round to nearest even) before use;
 biases are not.
+
+tf32=True restates the tensor-core path of layers 2-4
+(microtomodenoise_b200/csrc/proposal_tc.cu): the tensor core reads each FP32
+activation (the A operand of the forward convs) and each FP32 output gradient
+(the A operand of the input-gradient convs) as TF32, keeping the sign, the
+exponent and the top 10 mantissa bits (the low 13 bits dropped, i.e. rounded
+toward zero); BF16 weights are exact in TF32, products accumulate in FP32.
+Weight gradients stay on the CUDA cores (full FP32 operands).
 """
 from __future__ import annotations
 
@@ -44,6 +52,12 @@ def bf16_round(a) -> np.ndarray:
     u = np.asarray(a, np.float32).view(np.uint32).astype(np.uint64)
     r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
     return (r & 0xFFFFFFFF).astype(np.uint32).view(np.float32)
+
+
+def tf32_trunc(a) -> np.ndarray:
+    """Value -> float32 (nearest) -> TF32 by dropping the low 13 mantissa bits."""
+    u = np.asarray(a, np.float32).view(np.uint32) & np.uint32(0xFFFFE000)
+    return u.view(np.float32).astype(np.float64)
 
 
 def unpack(params: np.ndarray, S: int, rounded: bool = True) -> dict:
@@ -117,19 +131,21 @@ def _conv_back(a, W, g, stride):
     return dW, db, da
 
 
-def forward(params, vol, scale, S, cache=False, rounded=True):
+def forward(params, vol, scale, S, cache=False, rounded=True, tf32=False):
     """Returns logits [tiles, S] (tiles in (z, y, x) order) and optionally the
-    cache. rounded=False skips the BF16 rounding (finite-difference checks)."""
+    cache. rounded=False skips the BF16 rounding (finite-difference checks);
+    tf32=True: the tensor-core operand rounding of layers 2-4."""
     p = unpack(params, S, rounded)
     lv = levels(vol.shape)
+    op = tf32_trunc if tf32 else (lambda a: a)
     d = _l1_inputs(vol, scale)
     z1 = np.einsum("tzyx,tc->zyxc", d, p["w1"]) + p["b1"]
     a1 = np.maximum(z1, 0)
-    z2 = _conv(a1, p["w2"], p["b2"], 2, lv[2])
+    z2 = _conv(op(a1), p["w2"], p["b2"], 2, lv[2])
     a2 = np.maximum(z2, 0)
-    z3 = _conv(a2, p["w3"], p["b3"], 2, lv[3])
+    z3 = _conv(op(a2), p["w3"], p["b3"], 2, lv[3])
     a3 = np.maximum(z3, 0)
-    z4 = _conv(a3, p["w4"], p["b4"], 1, lv[3])
+    z4 = _conv(op(a3), p["w4"], p["b4"], 1, lv[3])
     a4 = np.maximum(z4, 0)
     h = a4.reshape(-1, C)
     logits = h @ p["wh"].T + p["bh"]
@@ -144,16 +160,19 @@ def softmax(logits):
     return e / e.sum(axis=1, keepdims=True)
 
 
-def loss_and_grad(params, examples, S, rounded=True):
+def loss_and_grad(params, examples, S, rounded=True, tf32=False):
     """examples: list of (vol, scale, target[tiles, S]). Returns (loss, grad)
-    with respect to the weights as used (BF16-rounded unless rounded=False)."""
+    with respect to the weights as used (BF16-rounded unless rounded=False);
+    tf32=True: the tensor-core operand rounding of layers 2-4 in the forward
+    pass and in the input gradients."""
     lay = layout(S)
     n_tiles = sum(int(np.prod(levels(v.shape)[3])) for v, _, _ in examples)
     inv_n = 1.0 / n_tiles
     grad = np.zeros(lay["total"])
     loss = 0.0
     for vol, scale, target in examples:
-        logits, c = forward(params, vol, scale, S, cache=True, rounded=rounded)
+        logits, c = forward(params, vol, scale, S, cache=True, rounded=rounded, tf32=tf32)
+        op = tf32_trunc if tf32 else (lambda a: a)
         p = c["p"]
         t = np.asarray(target, np.float64).reshape(logits.shape)
         T = t.sum(axis=1, keepdims=True)
@@ -165,11 +184,17 @@ def loss_and_grad(params, examples, S, rounded=True):
         gbh = g.sum(axis=0)
         dh = g @ p["wh"]
         g4 = (dh * (c["h"] > 0)).reshape(c["a4"].shape)
-        dW4, db4, da3 = _conv_back(c["a3"], p["w4"], g4, 1)
+        def back(a, w, g, stride):
+            dW, db, da = _conv_back(a, w, g, stride)
+            if tf32:  # the input gradient reads g as TF32
+                da = _conv_back(a, w, op(g), stride)[2]
+            return dW, db, da
+
+        dW4, db4, da3 = back(c["a3"], p["w4"], g4, 1)
         g3 = da3 * (c["a3"] > 0)
-        dW3, db3, da2 = _conv_back(c["a2"], p["w3"], g3, 2)
+        dW3, db3, da2 = back(c["a2"], p["w3"], g3, 2)
         g2 = da2 * (c["a2"] > 0)
-        dW2, db2, da1 = _conv_back(c["a1"], p["w2"], g2, 2)
+        dW2, db2, da1 = back(c["a1"], p["w2"], g2, 2)
         g1 = da1 * (c["a1"] > 0)
         dW1 = np.einsum("tzyx,zyxc->tc", c["d"], g1)
         db1 = g1.sum(axis=(0, 1, 2))

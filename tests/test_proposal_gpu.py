@@ -88,12 +88,15 @@ def test_logits_vs_oracle(gpu):
 @pytest.mark.parametrize("shape", [(13, 22, 35), (40, 72, 90)])
 def test_tensor_core_logits_vs_oracle(gpu, shape):
     """Layers 2-4 on the tensor cores (tcgen05 kind::tf32, accumulators in
-    tensor memory): the activations enter the products rounded to TF32, so
-    the logits stay within 3e-3 of their range of the FP64 restatement (the
-    CUDA-core path: 1e-4), and the top-k sets agree on all but a few tiles
-    where two offsets are within that rounding of each other. A volume whose
-    level-2 activations span many 128-voxel tiles exercises the persistent
-    tile loop and the partial last tile."""
+    tensor memory): the tensor core reads the FP32 activations as TF32 (low
+    13 mantissa bits dropped). Against the oracle with that operand rounding
+    (tf32=True) the logits agree within 1e-4 of their range, as the
+    CUDA-core path does with the plain oracle; against the plain FP64
+    restatement they stay within 3e-3, and the top-k sets agree with the
+    CUDA-core path's on all but a few tiles where two offsets are within that
+    rounding of each other. A volume whose level-2 activations span many
+    128-voxel tiles exercises the persistent tile loop and the partial last
+    tile."""
     P = prop_mod()
     S = 40
     net = P.ProposalNet(S)
@@ -101,13 +104,16 @@ def test_tensor_core_logits_vs_oracle(gpu, shape):
     net.set_params(params)
     ex, (vol, scale, _) = example(shape, 3, S)
     want = po.forward(params, vol, scale, S)
+    want_tc = po.forward(params, vol, scale, S, tf32=True)
     got = net.logits(ex.vol, ex.scale).cpu().numpy()
     net.set_tensor_cores(False)
     ref = net.logits(ex.vol, ex.scale).cpu().numpy()
     rng_ = np.abs(want).max()
     err = np.abs(got - want).max() / rng_
-    print(f"tensor-core logits: max error {err:.2e} of the range (CUDA cores: "
-          f"{np.abs(ref - want).max() / rng_:.2e})")
+    err_tc = np.abs(got - want_tc).max() / rng_
+    print(f"tensor-core logits: max error {err:.2e} of the range, {err_tc:.2e} against the "
+          f"TF32-operand oracle (CUDA cores: {np.abs(ref - want).max() / rng_:.2e})")
+    assert err_tc <= 1e-4
     assert err <= 3e-3
     k = 10
     top_tc = np.argsort(-got, axis=1, kind="stable")[:, :k]
@@ -136,12 +142,15 @@ def test_gradients_vs_oracle(gpu):
 
 def test_tensor_core_training_gradients_vs_oracle(gpu):
     """Training with layers 2-4 on the tensor cores (forward and input
-    gradients; weight gradients on the CUDA cores): the loss within 1e-3,
-    every parameter block's gradient within 5e-2 of its largest entry of the
-    FP64 restatement and at cosine >= 0.999 to it.  TF32 rounds the
-    activations and the back-propagated gradients to 10 mantissa bits, and
-    the first layer's weight gradient sees three TF32 input-gradient layers
-    (3.05e-2 measured on a B200); the CUDA-core path meets 2e-4."""
+    gradients; weight gradients on the CUDA cores). Against the oracle with
+    the tensor core's operand rounding (tf32=True: activations and
+    back-propagated gradients read as TF32, low 13 mantissa bits dropped)
+    the loss agrees within 1e-5 and every parameter block's gradient within
+    2e-3 of its largest entry. Against the plain FP64 restatement the blocks
+    stay at cosine >= 0.999: the truncation moves pre-activations near zero
+    across the ReLU, which moves single entries of a block by up to ~13% of
+    its largest on this small case (the oracle's TF32 mode shows the same);
+    the CUDA-core path meets 2e-4 of the plain restatement."""
     P = prop_mod()
     S = 24
     net = P.ProposalNet(S)
@@ -151,9 +160,11 @@ def test_tensor_core_training_gradients_vs_oracle(gpu):
     e1, o1 = example((13, 22, 35), 5, S)
     e2, o2 = example((24, 40, 48), 6, S)
     loss, g = net.gradients([e1, e2])
-    want_loss, want_g = po.loss_and_grad(params, [o1, o2], S)
-    assert abs(loss - want_loss) <= 1e-3 * abs(want_loss)
-    block_close(g, want_g, S, 5e-2, min_cos=0.999)
+    tc_loss, tc_g = po.loss_and_grad(params, [o1, o2], S, tf32=True)
+    assert abs(loss - tc_loss) <= 1e-5 * abs(tc_loss)
+    block_close(g, tc_g, S, 2e-3)
+    _, want_g = po.loss_and_grad(params, [o1, o2], S)
+    block_close(g, want_g, S, 0.2, min_cos=0.999)
     net.close()
 
 

@@ -39,6 +39,26 @@ def test_bf16_round_ties_to_even():
     assert r[3] == -2.5 and abs(r[4] - 3.140625) < 1e-7
 
 
+def test_tf32_truncation_and_mode():
+    """tf32_trunc keeps sign, exponent and the top 10 mantissa bits (rounds
+    toward zero); the oracle's tf32 mode moves the logits of a small case by
+    about that rounding and leaves layer 1 and the head in FP64."""
+    x = np.array([1.0 + 2 ** -10, 1.0 + 2 ** -11 + 2 ** -12, -(1.0 + 2 ** -10 + 2 ** -11), 3.0e-8],
+                 np.float32)
+    t = po.tf32_trunc(x)
+    assert t[0] == 1.0 + 2 ** -10 and t[1] == 1.0 and t[2] == -(1.0 + 2 ** -10)
+    assert abs(t[3]) <= abs(float(x[3])) and abs(t[3] - float(x[3])) <= 2 ** -10 * abs(float(x[3]))
+    S = 8
+    rng = np.random.default_rng(1)
+    params = rng.standard_normal(po.layout(S)["total"]) * 0.3
+    vol = rng.random((10, 12, 14)).astype(np.float32)
+    scale = np.full(10, 6.0, np.float32)
+    a = po.forward(params, vol, scale, S)
+    b = po.forward(params, vol, scale, S, tf32=True)
+    d = np.abs(a - b).max() / np.abs(a).max()
+    assert 0 < d < 1e-2
+
+
 def test_select_ties_and_fallback():
     logits = np.array([[0.0, 1.0, 1.0, 1.0, 0.5], [5.0, 0.0, 0.0, 0.0, 0.0]])
     keep, pm, fb = po.select(logits, 2, 0.0)
