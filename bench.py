@@ -155,12 +155,14 @@ def measured_peaks():
 
 
 # DRAM traffic of one 512^3 launch of the headline filter kernel
-# (nlm_tile_f32_kernel<2,2,2,8,raw smem>): dram__bytes_read.sum +
-# dram__bytes_write.sum of one 512x512x128 launch captured by ncu
-# (profiles/nlm_tile_f32_p2s5_512.md gives the command), times 4: the traffic
-# is the tiles' halo boxes plus the result, so it grows with the tile count.
-FILTER_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, one 512x512x128 launch, x4"
-FILTER_TRAFFIC_BYTES_PER_LAUNCH = 4 * (336.96e6 + 123.74e6)
+# (nlm_tile_f32_z2_kernel<2,2,2,raw slab>: 32x8x16 CTAs, raw staged as a
+# z-slab): dram__bytes_read.sum + dram__bytes_write.sum of one 512x512x128
+# launch captured by ncu (profiles/nlm_tile_f32_p2s5_512.md gives the
+# command), times 4: the traffic is the tiles' halo boxes, the slab restages
+# and the result, so it grows with the tile count.
+FILTER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one 512x512x128 launch of "
+                         "nlm_tile_f32_z2_kernel, x4")
+FILTER_TRAFFIC_BYTES_PER_LAUNCH = 4 * (433.648e6 + 124.266e6)
 
 
 def fp32_arithmetic_peak(device: int):
@@ -829,21 +831,24 @@ def run_profile_case(args):
              tile, one tile per CTA), iteration 2 full search (32-wide kernel).
     learned: the whole learned + FP16 job (noise estimates, 4 iterations,
              one list per 32x8x8 block) on a 128x512x512 grain pack.
-    slab:    two exact FP32 iterations of a 256^3 grain pack at the
+    published: two exact FP32 iterations of a 256^3 grain pack at the
              reference's default geometry (patch r1, search r10, 11 slices:
-             3102 offsets), the tile kernel with raw staged as a z slab."""
+             3102 offsets) with the default kernel there, the column form;
+    slab:    the same with the tile kernel (raw staged as a z slab)."""
     import torch
     from microtomodenoise_b200 import DenoiseParameters, IterativeNLM_GPU, synth
     from microtomodenoise_b200.proposal import ProposalNet, default_weights
     case = args.case
     net = None
-    if case in ("f32", "slab"):
+    if case in ("f32", "slab", "published"):
         shape = SHAPE if case == "f32" else (256, 256, 256)
         pr, sr = ((2, 2, 2), (5, 5, 5)) if case == "f32" else ((1, 1, 1), (10, 10, 10))
         vol = synth.grain_pack_volume(shape, seed=0)
         g = IterativeNLM_GPU()
         g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr,
                                                         nslices=11))
+        if case == "slab":
+            g.select_tile_form("tile")
         g.set_sigma(np.full(shape[0], 0.14 if case == "f32" else 0.045, np.float32))
         raw = torch.from_numpy(vol).cuda()
         g.Run_GaussianNoise_device(1, raw.data_ptr())
@@ -964,7 +969,7 @@ def main():
                     help="grain512: the headline bench line; learned1024, stream2048, rgb4k: "
                          "one-step measurements of the large workloads (run_large_workload, "
                          "run_rgb_workload); profile: a small case for ncu (--case)")
-    ap.add_argument("--case", default="f32", choices=["f32", "fast", "learned", "slab"],
+    ap.add_argument("--case", default="f32", choices=["f32", "fast", "learned", "slab", "published"],
                     help="--workload profile: which small case (see run_profile_case)")
     ap.add_argument("--stream-depth", type=int, default=1024)
     ap.add_argument("--slab", type=int, default=64, help="stream2048: z-slab depth")

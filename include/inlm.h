@@ -325,8 +325,18 @@ int inlm_net_input(inlm_denoiser* d, float* vol_dev, float* scale_dev);
  * No counterpart in the reference, which runs one stack with one fixed
  * kernel configuration per run (main.cpp:311-545). */
 
-/* Times the tiled FP32 kernel's configurations (CTA depth 8 with raw staged
- * in shared memory or read from global memory, depth 4) on a 128x128x64 probe
+/* Restricts the plain FP32 filter to one kernel family and picks its first
+ * configuration that fits: form 0 = automatic (the column form for patch
+ * radius 1 when it fits, else the tiled kernels), 1 = the tiled kernels only,
+ * 2 = the column form only (INLM_ERR_UNSUPPORTED where it has no
+ * instantiation or does not fit). Results do not change: every form rounds
+ * each voxel identically. Call between iterations, not while one runs. */
+int inlm_select_tile_form(inlm_denoiser* d, int form);
+
+/* Times the tiled FP32 kernel's configurations (the column form at patch
+ * radius 1, CTA depth 16 with two planes per thread, CTA depth 8 with raw
+ * staged in shared memory or read from global memory, depth 4) on a
+ * 128x128x64 probe
  * of d's patch/search class, applies the fastest to d and caches the choice
  * per process (and in the file named by the INLM_AUTOTUNE_CACHE environment
  * variable when set). Results do not change: every configuration rounds each

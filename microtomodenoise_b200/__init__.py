@@ -219,6 +219,15 @@ class IterativeNLM_GPU:
         _lib.check(_lib.load().inlm_autotune(self._h, buf, 512), "autotune")
         return buf.value.decode()
 
+    def select_tile_form(self, form: str = "auto") -> str:
+        """Plain FP32 kernel family: "auto", "tile" (the tiled kernels only) or
+        "column" (the column form, patch radius 1). Results do not change;
+        returns describe()."""
+        self._need()
+        code = {"auto": 0, "tile": 1, "column": 2}[form]
+        _lib.check(_lib.load().inlm_select_tile_form(self._h, code), "select_tile_form")
+        return self.describe()
+
     def n_search_offsets(self) -> int:
         """Number of search offsets S of the configured geometry."""
         self._need()

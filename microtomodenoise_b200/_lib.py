@@ -38,7 +38,7 @@ EXPORTS = (
     "inlm_proposal_set_tensor_cores",
     "inlm_proposal_train", "inlm_proposal_select", "inlm_attach_proposal", "inlm_proposal_stats",
     "inlm_weight_map", "inlm_net_input",
-    "inlm_autotune", "inlm_batch_create", "inlm_batch_destroy", "inlm_batch_run",
+    "inlm_autotune", "inlm_select_tile_form", "inlm_batch_create", "inlm_batch_destroy", "inlm_batch_run",
     "inlm_batch_describe", "inlm_stream_denoise", "inlm_set_result",
     "inlm_tiff_shape", "inlm_tiff_read", "inlm_tiff_write_sequence",
     "inlm_get_result_slices", "inlm_set_result_slices", "inlm_noise_patchstd_slab",
@@ -155,6 +155,7 @@ def load(path: str = "") -> C.CDLL:
     L.inlm_weight_map.argtypes = [vp, vp]
     L.inlm_net_input.argtypes = [vp, vp, vp]
     L.inlm_autotune.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.inlm_select_tile_form.argtypes = [vp, C.c_int]
     L.inlm_batch_create.argtypes = [C.c_int, vp, vp, C.POINTER(vp)]
     L.inlm_batch_destroy.argtypes = [vp]
     L.inlm_batch_run.argtypes = [vp, vp, vp, C.c_int, C.POINTER(C.c_float)]

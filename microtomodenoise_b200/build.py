@@ -35,6 +35,7 @@ NVCC_FLAGS = ARCH + [
 
 LIB_SOURCES = [
     "filter_kernels.cu",
+    "filter_column.cu",
     "filter_fast.cu",
     "noise_kernels.cu",
     "api.cu",

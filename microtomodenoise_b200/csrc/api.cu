@@ -585,7 +585,8 @@ static int raw_plane_pitch(int rpx, int rby, int pstride = 1) {
 }
 
 // Tiled FP32 configuration for one candidate (CTA depth tz, raw staged in
-// shared memory or read from global): tables, kernel arguments, TMA map.
+// shared memory or read from global; tz 0: the column form, patch radius 1,
+// at its own depth): tables, kernel arguments, TMA map.
 // *ok = false when the candidate does not apply or does not fit.
 // Raw-slab schedule: for each group of kOffGroup consecutive offsets, the z
 // offset from which the TZ + 1 staged raw planes start. The search list must
@@ -624,9 +625,15 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
         if (order[3 * t] != g.taps[t].x || order[3 * t + 1] != g.taps[t].y ||
             order[3 * t + 2] != g.taps[t].z)
             return INLM_OK;
-    // tz 16: the two-planes-per-thread kernel (raw staged in shared memory)
-    if (!((tz == 8) || (tz == 4 && !raw_smem) || (tz == 16 && raw_smem))) return INLM_OK;
     const bool fused = d->p.precision == INLM_PRECISION_F32_FMA;
+    const bool column = tz == 0;
+    if (column) {
+        tz = column_kernel_depth(pr[0], pr[1], pr[2]);
+        if (tz == 0 || fused) return INLM_OK;
+        raw_smem = false;
+    }
+    // tz 16: the two-planes-per-thread kernel (raw staged in shared memory)
+    if (!column && !((tz == 8) || (tz == 4 && !raw_smem) || (tz == 16 && raw_smem))) return INLM_OK;
     if (fused && tz != 8) return INLM_OK;  // the fused form is instantiated at CTA depth 8
 
     TileArgs a{};
@@ -655,7 +662,8 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     int smem_max = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
     TileConfig tc{pr[0], pr[1], pr[2], tz, raw_smem, 0, fused};
-    size_t sm = tile_smem_bytes(tc, a);
+    tc.column = column;
+    size_t sm = column ? column_smem_bytes(a) : tile_smem_bytes(tc, a);
     a.raw_slab = 0;
     a.group_zb = nullptr;
     std::vector<int> zb;
@@ -707,13 +715,15 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
 }
 
 // Default choice (before any autotuning): the first candidate that fits.
-static int choose_tile_config(inlm_denoiser* d) {
+// form: 0 every candidate, 1 the tiled kernels only, 2 the column form only.
+static int choose_tile_config(inlm_denoiser* d, int form = 0) {
     d->use_tile = false;
     const struct {
         int tz;
         bool raw;
-    } cands[] = {{16, true}, {8, true}, {8, false}, {4, false}};
+    } cands[] = {{0, false}, {16, true}, {8, true}, {8, false}, {4, false}};
     for (auto c : cands) {
+        if ((form == 1 && c.tz == 0) || (form == 2 && c.tz != 0)) continue;
         bool ok = false;
         int rc = tile_config_try(d, c.tz, c.raw, &ok);
         if (rc) return rc;
@@ -1293,6 +1303,21 @@ extern "C" int inlm_filter_kernel_ms(inlm_denoiser* d, double* avg_ms, int* n_la
     return INLM_OK;
 }
 
+extern "C" int inlm_select_tile_form(inlm_denoiser* d, int form) {
+    if (!d) return fail(INLM_ERR_ARG, "null handle");
+    if (form < 0 || form > 2) return fail(INLM_ERR_ARG, "form must be 0, 1 or 2");
+    if (!d->use_tile) return fail(INLM_ERR_UNSUPPORTED, "the plain FP32 tiled kernels do not cover this configuration");
+    CUDA_TRY(cudaSetDevice(d->device));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    int rc = choose_tile_config(d, form);
+    if (rc) return rc;
+    if (!d->use_tile) {
+        choose_tile_config(d, 0);  // keep the handle usable
+        return fail(INLM_ERR_UNSUPPORTED, "no kernel of form %d fits this configuration", form);
+    }
+    return INLM_OK;
+}
+
 extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
     if (!d || !buf) return fail(INLM_ERR_ARG, "null argument");
     const Geometry& g = d->geo;
@@ -1308,8 +1333,8 @@ extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
     }
     else if (d->use_tile)
         snprintf(buf, len,
-                 "nlm_tile_f32%s<%d,%d,%d> tz=%d raw_%s smem=%zu S=%zu P=%zu weights=%s pad=%d,%d,%d",
-                 d->tcfg.fused ? "_fused" : "", d->tcfg.rx, d->tcfg.ry, d->tcfg.rz, d->tcfg.tz,
+                 "nlm_%s_f32%s<%d,%d,%d> tz=%d raw_%s smem=%zu S=%zu P=%zu weights=%s pad=%d,%d,%d",
+                 d->tcfg.column ? "column" : "tile", d->tcfg.fused ? "_fused" : "", d->tcfg.rx, d->tcfg.ry, d->tcfg.rz, d->tcfg.tz,
                  d->tcfg.raw_smem ? (d->targs.raw_slab ? "slab" : "smem") : "global",
                  d->tcfg.smem_bytes, g.search.size(), g.taps.size(),
                  g.specialised && d->p.weight_table == INLM_WEIGHTS_CPU ? "cpu-table" : "distweight",

@@ -104,7 +104,8 @@ int tune_class(const inlm_params& p0, bool batch, TuneResult* out) {
         int tz;
         bool raw;
     };
-    const Cand cands[] = {{16, true}, {8, true}, {8, false}, {4, false}};
+    // tz 0: the column form (patch radius 1)
+    const Cand cands[] = {{0, false}, {16, true}, {8, true}, {8, false}, {4, false}};
     double best = 1e30;
     TuneResult res;
     bool any = false;
@@ -129,7 +130,7 @@ int tune_class(const inlm_params& p0, bool batch, TuneResult* out) {
         rc = tile_config_try(d, c.tz, c.raw, &ok);
         if (rc) return cleanup(rc);
         if (!ok) continue;
-        const int tiles_z = (shape[2] + c.tz - 1) / c.tz;
+        const int tiles_z = (shape[2] + d->tcfg.tz - 1) / d->tcfg.tz;
         float ms = 0.f;
         for (int rep = 0; rep < 3; rep++) {  // one warm-up, two timed
             if (rep == 1) cudaEventRecord(e0, d->stream);
@@ -323,14 +324,17 @@ static int batch_enqueue(inlm_batch* b) {
             CUDA_TRY(cudaMemsetAsync(bp.counter, 0, sizeof(unsigned), bs));
             CUDA_TRY(launch_batch_kernel(grp.shape, bp, grp.ctas, grp.smem, bs));
             CUDA_TRY(cudaEventRecord(b->join[gi], bs));
-            CUDA_TRY(cudaStreamWaitEvent(st, b->join[gi], 0));
         }
+        // volumes with their own launch run on the main stream beside the
+        // persistent groups
         for (int v = 0; v < b->n; v++) {
             inlm_denoiser* d = b->d[v];
             if (it > d->p.maxiterations || b->kind[v] >= 0) continue;
             int rc = own_filter_launch(d, st);
             if (rc) return rc;
         }
+        for (size_t gi = 0; gi < b->groups.size(); gi++)
+            if (b->launches[it - 1][gi].n > 0) CUDA_TRY(cudaStreamWaitEvent(st, b->join[gi], 0));
         for (int v = 0; v < b->n; v++) {
             inlm_denoiser* d = b->d[v];
             const int mi = d->p.maxiterations;
@@ -378,6 +382,8 @@ extern "C" int inlm_batch_create(int n, const int* shapes, const inlm_params* pa
     b->in.assign(n, nullptr);
     b->sigma_manual.assign(n, nullptr);
     b->kind.assign(n, -1);
+    int sms_dev = 148;
+    cudaDeviceGetAttribute(&sms_dev, cudaDevAttrMultiProcessorCount, dev);
     for (int v = 0; v < n; v++) {
         int rc = inlm_denoiser_create(shapes + 3 * v, &params[v], &b->d[v]);
         if (rc) return bail(rc);
@@ -403,6 +409,15 @@ extern "C" int inlm_batch_create(int n, const int* shapes, const inlm_params* pa
             // work the graph cannot hold); later ones are device-only
             rc = estimate_into(d, b->in[v], d->d_sigma0, nullptr);
             if (rc) return bail(rc);
+        }
+        // A volume whose own configuration is the column form or the 16-deep
+        // CTA (faster than the persistent depth-8 body) and which fills the
+        // GPU by itself (>= 4 waves of CTAs) keeps it and runs its own launch
+        // beside the persistent groups.
+        if (d->use_tile && (d->tcfg.column || d->tcfg.tz == 16)) {
+            const long long ctas = (long long)d->targs.tiles_x * d->targs.tiles_y *
+                                   ((d->shape[2] + d->tcfg.tz - 1) / d->tcfg.tz);
+            if (ctas >= 4LL * sms_dev) continue;  // kind stays -1
         }
         // tile configuration from the autotuner (depth 8: the persistent body)
         if (d->use_tile) {
@@ -587,7 +602,9 @@ extern "C" int inlm_batch_describe(inlm_batch* b, char* buf, size_t len) {
                       d->p.patch_radius[1], d->p.patch_radius[2], d->p.search_radius[0],
                       d->p.search_radius[1], d->p.search_radius[2], d->geo.search.size(),
                       d->geo.taps.size(), b->kind[v] >= 0 ? "batched " : "own launch ",
-                      b->kind[v] >= 0 ? kinds[b->kind[v]] : (d->use_tile ? "tile" : "generic"));
+                      b->kind[v] >= 0 ? kinds[b->kind[v]]
+                                      : (d->use_tile ? (d->tcfg.column ? "column" : d->tcfg.tz == 16 ? "tile tz=16" : "tile")
+                                                     : "generic"));
         s += line;
     }
     s += "autotuner: " + b->tune_report;

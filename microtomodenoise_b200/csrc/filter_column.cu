@@ -1,0 +1,305 @@
+// Column form of the plain FP32 iterNLM filter for small patches (sm_100a),
+// bit-identical to the reference CPU filter like the tile kernel
+// (Denoiser/iternlm_cpu_kernels.cpp:7-160 for patch radius 1,
+// iternlm_cpu.cpp:758-843).
+//
+// At patch radius 1 (7 taps, the reference's default) the tile kernel's
+// squared-difference planes save little: each D value serves 7 voxels, but
+// forming the planes, the two barriers around them and the prev box with the
+// whole search halo (one 8-warp CTA per SM) cost more than the taps. Here a
+// CTA stages the same prev box by one TMA load and then runs without
+// barriers: a warp owns 32 consecutive x voxels on 8 rows of one z plane,
+// each thread its 8 voxels along y. The patch splits into columns of constant
+// (zp, xp) with yp in [-e, e]; per search offset a thread reads each column of
+// the shifted previous iterate at y in [-e, 7 + e] (a warp load is 32
+// consecutive floats: no bank conflict), forms the squared differences
+// against the origin values it keeps in registers (the same D values the
+// tile kernel stores), and adds w * D in the reference's tap order for every
+// voxel. Raw comes from global memory, one offset ahead.
+#include "common.cuh"
+#include "filter_kernels.cuh"
+#include "geometry.hpp"
+#include "pair_math.cuh"
+#include "tile_common.cuh"
+
+namespace inlm {
+
+namespace {
+
+// Patch columns: constant (zp, xp), yp in [-e, e] (the ellipsoid is convex
+// and symmetric, so each column is one symmetric run). first[c]: register
+// offset of the column's 8 + 2e values in the per-thread arrays.
+struct PatchCols {
+    int n;
+    int zp[64], xp[64], e[64], first[64];
+    int nvals;
+};
+
+constexpr PatchCols make_patch_cols(int rx, int ry, int rz) {
+    PatchCols c{};
+    const float fx = float(rx < 1 ? 1 : rx), fy = float(ry < 1 ? 1 : ry), fz = float(rz < 1 ? 1 : rz);
+    for (int zp = -rz; zp <= rz; zp++)
+        for (int xp = -rx; xp <= rx; xp++) {
+            if (!ell_member(xp, 0, zp, fx, fy, fz)) continue;
+            int e = 0;
+            while (e + 1 <= ry && ell_member(xp, e + 1, zp, fx, fy, fz)) e++;
+            c.zp[c.n] = zp;
+            c.xp[c.n] = xp;
+            c.e[c.n] = e;
+            c.first[c.n] = c.nvals;
+            c.nvals += kVoxPerThread + 2 * e;
+            c.n++;
+        }
+    return c;
+}
+
+constexpr int col_of(const PatchCols& c, int zp, int xp) {
+    for (int i = 0; i < c.n; i++)
+        if (c.zp[i] == zp && c.xp[i] == xp) return i;
+    return -1;
+}
+
+// Reference tap order (centre first, then rows (zp, yp) ascending, xp
+// ascending), each tap as (column, yp).
+struct TapSeq {
+    int n;
+    int col[128], yp[128];
+};
+
+constexpr TapSeq make_tap_seq(int rx, int ry, int rz) {
+    const PatchRows rows = make_patch_rows(rx, ry, rz);
+    const PatchCols cols = make_patch_cols(rx, ry, rz);
+    TapSeq t{};
+    t.col[0] = col_of(cols, 0, 0);
+    t.yp[0] = 0;
+    t.n = 1;
+    for (int r = 0; r < rows.n; r++)
+        for (int xp = -rows.e[r]; xp <= rows.e[r]; xp++) {
+            if (rows.zp[r] == 0 && rows.yp[r] == 0 && xp == 0) continue;
+            t.col[t.n] = col_of(cols, rows.zp[r], xp);
+            t.yp[t.n] = rows.yp[r];
+            t.n++;
+        }
+    return t;
+}
+
+template <int RX, int RY, int RZ>
+struct ColGeom {
+    static constexpr PatchCols cols = make_patch_cols(RX, RY, RZ);
+    static constexpr TapSeq taps = make_tap_seq(RX, RY, RZ);
+    static constexpr int NV = cols.nvals;  // values per thread over all columns
+};
+
+static_assert(ColGeom<1, 1, 1>::taps.n == 7 && ColGeom<1, 1, 1>::NV == 42, "p111 columns");
+static_assert(ColGeom<1, 1, 2>::taps.n == 9, "p112 columns");
+static_assert(ColGeom<1, 1, 3>::taps.n == 11, "p113 columns");
+
+// First tap (in reference order) that reads column C: the column's squared
+// differences are formed there, so each lives only from its first to its last
+// use.
+template <int RX, int RY, int RZ, int C>
+constexpr int first_use() {
+    using CG = ColGeom<RX, RY, RZ>;
+    for (int t = 0; t < CG::taps.n; t++)
+        if (CG::taps.col[t] == C) return t;
+    return -1;
+}
+
+// Squared differences of column C for offset delta dlx: D[first + i] for y in
+// [-e, 7 + e], as register pairs (the column length 8 + 2e is even).
+template <int RX, int RY, int RZ, int C>
+__device__ __forceinline__ void column_d(const float* __restrict__ prevb, int pb, int dlx, int pbx,
+                                         int pplane, const f32x2 (&og)[ColGeom<RX, RY, RZ>::NV / 2],
+                                         f32x2 (&D)[ColGeom<RX, RY, RZ>::NV / 2]) {
+    using CG = ColGeom<RX, RY, RZ>;
+    constexpr int e = CG::cols.e[C];
+    constexpr int f = CG::cols.first[C];
+    const float* src = prevb + pb + dlx + CG::cols.zp[C] * pplane + CG::cols.xp[C] - e * pbx;
+#pragma unroll
+    for (int i = 0; i < kVoxPerThread + 2 * e; i += 2) {
+        const f32x2 v = pack2(src[i * pbx], src[(i + 1) * pbx]);
+        const f32x2 t = sub2(v, og[(f + i) / 2]);
+        D[(f + i) / 2] = mul2_to_mul(t, t);  // feeds only products
+    }
+}
+
+// Taps T.. of the reference order: form each column at its first use, then
+// add w_t * D to the 8 voxels' distances (pairs of y voxels).
+template <int RX, int RY, int RZ, int T>
+__device__ __forceinline__ void column_taps(const float* __restrict__ prevb, int pb, int dlx, int pbx,
+                                            int pplane, const f32x2 (&og)[ColGeom<RX, RY, RZ>::NV / 2],
+                                            f32x2 (&D)[ColGeom<RX, RY, RZ>::NV / 2],
+                                            f32x2 (&d)[kVoxPerThread / 2], const TileArgs& a) {
+    using CG = ColGeom<RX, RY, RZ>;
+    if constexpr (T < CG::taps.n) {
+        constexpr int C = CG::taps.col[T];
+        constexpr int yp = CG::taps.yp[T];
+        constexpr int e = CG::cols.e[C];
+        constexpr int f = CG::cols.first[C];
+        if constexpr (first_use<RX, RY, RZ, C>() == T) column_d<RX, RY, RZ, C>(prevb, pb, dlx, pbx, pplane, og, D);
+        const float w = a.w[T];
+#pragma unroll
+        for (int p = 0; p < kVoxPerThread / 2; p++) {
+            // voxels 2p, 2p + 1 read the column at y = 2p + yp, 2p + 1 + yp
+            // (value index y + e; every column starts on a pair)
+            const int i = f + e + 2 * p + yp;
+            const float2 lo = unpack2(D[i / 2]);
+            float v0, v1;
+            if ((i & 1) == 0) {
+                v0 = lo.x;
+                v1 = lo.y;
+            } else {
+                const float2 hi = unpack2(D[i / 2 + 1]);
+                v0 = lo.y;
+                v1 = hi.x;
+            }
+            if (T == 0)
+                d[p] = mul_pair(v0, v1, w);
+            else
+                d[p] = add2(d[p], mul_pair(v0, v1, w));
+        }
+        column_taps<RX, RY, RZ, T + 1>(prevb, pb, dlx, pbx, pplane, og, D, d, a);
+    }
+}
+
+// Origin values of columns C.. (the unshifted previous iterate), as pairs.
+template <int RX, int RY, int RZ, int C>
+__device__ __forceinline__ void load_origins(const float* __restrict__ prevb, int pb, int pbx, int pplane,
+                                             f32x2 (&og)[ColGeom<RX, RY, RZ>::NV / 2]) {
+    using CG = ColGeom<RX, RY, RZ>;
+    if constexpr (C < CG::cols.n) {
+        constexpr int e = CG::cols.e[C];
+        constexpr int f = CG::cols.first[C];
+        const float* src = prevb + pb + CG::cols.zp[C] * pplane + CG::cols.xp[C] - e * pbx;
+#pragma unroll
+        for (int i = 0; i < kVoxPerThread + 2 * e; i += 2) og[(f + i) / 2] = pack2(src[i * pbx], src[(i + 1) * pbx]);
+        load_origins<RX, RY, RZ, C + 1>(prevb, pb, pbx, pplane, og);
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ>
+__global__ void __launch_bounds__(32 * TZ, 1)
+    nlm_column_f32_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
+    using CG = ColGeom<RX, RY, RZ>;
+    constexpr int NP = kVoxPerThread / 2;
+    constexpr int NV2 = CG::NV / 2;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+    float* prevb = reinterpret_cast<float*>(smem + 128);
+    const int tid = threadIdx.x;
+    const int X0 = blockIdx.x * kTX;
+    const int Y0 = blockIdx.y * kTY;
+    const int Z0 = blockIdx.z * TZ;
+    const int pplane = a.pbx * a.pby;
+    if (tid == 0) {
+        prefetch_tmap(&tm_prev);
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(pplane * a.pbz) * 4u);
+        tma_load_3d(prevb, &tm_prev, X0, Y0, Z0, bar);
+    }
+    // lane = x within the CTA's 32 columns, warp = z plane; voxels y = 0..7
+    const int lane = tid & 31, k = tid >> 5;
+    const int pb = (k + a.pz) * pplane + a.py * a.pbx + lane + a.px;  // voxel (lane, 0, k)
+    const long long gbase = (long long)(Z0 + k + a.pz) * a.gpitch_z + (long long)(Y0 + a.py) * a.gpitch_y +
+                            (X0 + lane + a.px);
+    const f32x2 m2 = splat2(a.mult[min(Z0 + k, a.nz - 1)]);
+
+    // raw of the first offset, loaded while the prev box arrives
+    int2 dl = __ldg(&a.search_delta[0]);
+    float rn[kVoxPerThread];
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) rn[r] = __ldg(&a.raw_pad[gbase + r * a.gpitch_y + dl.y]);
+
+    const bool arrived = mbar_wait_bounded(bar, 0);
+    if (!__syncthreads_and(arrived)) {
+        if (tid == 0) set_error(a.err, DEV_TMA_TIMEOUT);
+        return;
+    }
+    // origin values of every column, kept for all offsets
+    f32x2 og[NV2];
+    load_origins<RX, RY, RZ, 0>(prevb, pb, a.pbx, pplane, og);
+
+    f32x2 acc[NP], wsum[NP];
+    float wmax[kVoxPerThread];
+#pragma unroll
+    for (int p = 0; p < NP; p++) acc[p] = wsum[p] = 0ull;  // (+0, +0)
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) wmax[r] = 0.0f;
+
+    for (int s = 0; s < a.S; s++) {
+        float rc[kVoxPerThread];
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) rc[r] = rn[r];
+        const int2 dln = __ldg(&a.search_delta[min(s + 1, a.S - 1)]);
+        if (s + 1 < a.S) {
+#pragma unroll
+            for (int r = 0; r < kVoxPerThread; r++) rn[r] = __ldg(&a.raw_pad[gbase + r * a.gpitch_y + dln.y]);
+        }
+        f32x2 D[NV2];
+        f32x2 d[NP];
+        column_taps<RX, RY, RZ, 0>(prevb, pb, dl.x, a.pbx, pplane, og, D, d, a);
+#pragma unroll
+        for (int p = 0; p < NP; p++)
+            exact_weight_pair(d[p], m2, make_float2(rc[2 * p], rc[2 * p + 1]), acc[p], wsum[p], wmax[2 * p],
+                              wmax[2 * p + 1]);
+        dl = dln;
+    }
+
+    const int z = Z0 + k, x = X0 + lane;
+    if (z >= a.nz || x >= a.nx) return;
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) {
+        const int y = Y0 + r;
+        if (y >= a.ny) break;
+        const float raw0 = __ldg(&a.raw_pad[gbase + r * a.gpitch_y]);
+        const float2 acp = unpack2(acc[r / 2]), wsp = unpack2(wsum[r / 2]);
+        float ac = (r & 1) ? acp.y : acp.x;
+        float ws = (r & 1) ? wsp.y : wsp.x;
+        float res;
+        if (wmax[r] > 0.0f) {
+            ac = __fadd_rn(ac, __fmul_rn(wmax[r], raw0));
+            ws = __fadd_rn(ws, wmax[r]);
+            res = __fdiv_rn(ac, ws);
+        } else {
+            res = raw0;
+        }
+        a.out[((long long)z * a.ny + y) * a.nx + x] = res;
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ>
+cudaError_t launch_column(const CUtensorMap* tm, const TileArgs& a, int tiles_z, size_t smem, cudaStream_t st) {
+    auto kern = nlm_column_f32_kernel<RX, RY, RZ, TZ>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
+    kern<<<grid, 32 * TZ, smem, st>>>(*tm, a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int column_kernel_depth(int rx, int ry, int rz) {
+    if (rx == 1 && ry == 1 && rz == 1) return 16;
+    if (rx == 1 && ry == 1 && (rz == 2 || rz == 3)) return 8;
+    return 0;
+}
+
+size_t column_smem_bytes(const TileArgs& a) { return 128 + (size_t)a.pbx * a.pby * a.pbz * 4; }
+
+cudaError_t launch_column_kernel(const TileConfig& c, const CUtensorMap* tm_prev, const TileArgs& a,
+                                 int tiles_z, cudaStream_t st) {
+    if (c.rx == 1 && c.ry == 1 && c.rz == 1 && c.tz == 16)
+        return launch_column<1, 1, 1, 16>(tm_prev, a, tiles_z, c.smem_bytes, st);
+    if (c.rx == 1 && c.ry == 1 && c.rz == 2 && c.tz == 8)
+        return launch_column<1, 1, 2, 8>(tm_prev, a, tiles_z, c.smem_bytes, st);
+    if (c.rx == 1 && c.ry == 1 && c.rz == 3 && c.tz == 8)
+        return launch_column<1, 1, 3, 8>(tm_prev, a, tiles_z, c.smem_bytes, st);
+    return cudaErrorInvalidConfiguration;
+}
+
+}  // namespace inlm

@@ -29,61 +29,10 @@
 #include "common.cuh"
 #include "filter_kernels.cuh"
 #include "geometry.hpp"
+#include "pair_math.cuh"
 #include "tile_common.cuh"
 
 namespace inlm {
-
-// Packed-pair arithmetic (sm_100 f32x2: one FADD2/FMUL2 instruction does two
-// IEEE round-to-nearest operations; measured on B200 it issues in one slot but
-// gives no more FP32 lane throughput than two scalar instructions, so the gain
-// is issue slots left for the loads around it). ptxas fuses an FMUL2 whose
-// result feeds an FADD2 into one FFMA2 even with explicit .rn modifiers, which
-// would round once instead of twice; scalar products feeding paired sums (or
-// paired products feeding only products) keep every rounding of the
-// reference, so the kernels below never let an FMUL2 result reach an addition.
-// A pair is a 64-bit register holding (element 0, element 1).
-typedef unsigned long long f32x2;
-
-__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
-    f32x2 d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
-    f32x2 d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-// Paired product; its result must only feed multiplications (see above).
-__device__ __forceinline__ f32x2 mul2_to_mul(f32x2 a, f32x2 b) {
-    f32x2 d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-// Fused pair a*b + c, one rounding per lane (FFMA2): the fused FP32 form only.
-__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
-    f32x2 d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
-    f32x2 d;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
-    return d;
-}
-__device__ __forceinline__ float2 unpack2(f32x2 a) {
-    float2 r;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(a));
-    return r;
-}
-__device__ __forceinline__ f32x2 splat2(float v) { return pack2(v, v); }
-// Two scalar products as a pair (safe to feed add2).
-__device__ __forceinline__ f32x2 mul_pair(float a0, float a1, float b) {
-    return pack2(__fmul_rn(a0, b), __fmul_rn(a1, b));
-}
-__device__ __forceinline__ f32x2 mul_pair(float2 a, float2 b) {
-    return pack2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
-}
 
 // r[0..8) = p[0..8) through three aligned float4 loads (p is 4-byte aligned;
 // the 16-byte block before and after p must be readable). The raw reads of the
@@ -338,26 +287,7 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
                 wmax[2 * p + 1] = fmaxf(wmax[2 * p + 1], w1);
                 continue;
             }
-            // Pade[3/3] (120 + 60x + 12x*x + x*x*x) / (120 - 60x + 12x*x - x*x*x):
-            // products that feed the sums are scalar, the sums are paired
-            const f32x2 x = mul2_to_mul(dist[p], m2);
-            const float2 xs = unpack2(x);
-            const float2 x12 = unpack2(mul2_to_mul(c12, x));
-            const float2 xx = unpack2(mul2_to_mul(x, x));
-            const f32x2 ta = mul_pair(xs, make_float2(60.f, 60.f));
-            const f32x2 tb = mul_pair(x12, xs);
-            const f32x2 tc = mul_pair(xx, xs);
-            const float2 num = unpack2(add2(add2(add2(c120, ta), tb), tc));
-            const float2 den = unpack2(sub2(add2(sub2(c120, ta), tb), tc));
-            // both quotients are always formed and then selected: a division
-            // under the cutoff test becomes a divergent branch (10% slower)
-            const float q0 = __fdiv_rn(num.x, den.x), q1 = __fdiv_rn(num.y, den.y);
-            const float w0 = (xs.x > -3.56648f) ? q0 : 0.0f;
-            const float w1 = (xs.y > -3.56648f) ? q1 : 0.0f;
-            acc[p] = add2(acc[p], mul_pair(make_float2(w0, w1), rsv));
-            wsum[p] = add2(wsum[p], pack2(w0, w1));
-            wmax[2 * p] = fmaxf(wmax[2 * p], w0);
-            wmax[2 * p + 1] = fmaxf(wmax[2 * p + 1], w1);
+            exact_weight_pair(dist[p], m2, rsv, acc[p], wsum[p], wmax[2 * p], wmax[2 * p + 1]);
         }
     };
 
@@ -612,8 +542,6 @@ __device__ __forceinline__ void tile_f32_z2_body(const CUtensorMap* tm_prev, con
 #pragma unroll
     for (int r = 0; r < kVoxPerThread; r++) wmax0[r] = wmax1[r] = 0.0f;
 
-    const f32x2 c12 = splat2(12.f), c120 = splat2(120.f);
-
     auto phase_a = [&](int dlx) {
 #pragma unroll
         for (int q = 0; q < NQ; q++) {
@@ -630,22 +558,7 @@ __device__ __forceinline__ void tile_f32_z2_body(const CUtensorMap* tm_prev, con
 #pragma unroll
         for (int p = 0; p < NP; p++) {
             const float2 rsv = make_float2(rawb[rb + 2 * p], rawb[rb + 2 * p + 1]);
-            const f32x2 x = mul2_to_mul(dist[p], m2);
-            const float2 xs = unpack2(x);
-            const float2 x12 = unpack2(mul2_to_mul(c12, x));
-            const float2 xx = unpack2(mul2_to_mul(x, x));
-            const f32x2 ta = mul_pair(xs, make_float2(60.f, 60.f));
-            const f32x2 tb = mul_pair(x12, xs);
-            const f32x2 tc = mul_pair(xx, xs);
-            const float2 num = unpack2(add2(add2(add2(c120, ta), tb), tc));
-            const float2 den = unpack2(sub2(add2(sub2(c120, ta), tb), tc));
-            const float q0 = __fdiv_rn(num.x, den.x), q1 = __fdiv_rn(num.y, den.y);
-            const float w0 = (xs.x > -3.56648f) ? q0 : 0.0f;
-            const float w1 = (xs.y > -3.56648f) ? q1 : 0.0f;
-            acc[p] = add2(acc[p], mul_pair(make_float2(w0, w1), rsv));
-            wsum[p] = add2(wsum[p], pack2(w0, w1));
-            wmax[2 * p] = fmaxf(wmax[2 * p], w0);
-            wmax[2 * p + 1] = fmaxf(wmax[2 * p + 1], w1);
+            exact_weight_pair(dist[p], m2, rsv, acc[p], wsum[p], wmax[2 * p], wmax[2 * p + 1]);
         }
     };
 
@@ -987,6 +900,7 @@ size_t tile_smem_bytes(const TileConfig& c, const TileArgs& a) {
 cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,
                                const CUtensorMap* tm_raw, const TileArgs& a, int tiles_z,
                                cudaStream_t st) {
+    if (c.column) return launch_column_kernel(c, tm_prev, a, tiles_z, st);
 #define X(A, B, C)                                                                             \
     if (c.rx == A && c.ry == B && c.rz == C) {                                                 \
         if (c.tz == 16 && c.raw_smem && !c.fused)                                              \

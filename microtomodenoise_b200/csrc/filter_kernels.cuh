@@ -62,10 +62,17 @@ struct TileConfig {
     size_t smem_bytes;
     bool fused = false;  // the fused FP32 form (FFMA taps, Horner Pade, fast division); tz 8 only
     bool raw_slab = false;  // raw staged as TZ + 1 planes per z offset pair (raw_smem, tz 8 or 16)
+    bool column = false;    // the column form (filter_column.cu): patch radius 1, raw from global
 };
 
 // Returns false when no tiled instantiation exists for the patch shape.
 bool tile_kernel_available(int rx, int ry, int rz);
+// Column form (filter_column.cu): its CTA depth for a patch shape (0: none),
+// shared-memory bytes (the prev box) and launch.
+int column_kernel_depth(int rx, int ry, int rz);
+size_t column_smem_bytes(const TileArgs& a);
+cudaError_t launch_column_kernel(const TileConfig& c, const CUtensorMap* tm_prev, const TileArgs& a,
+                                 int tiles_z, cudaStream_t st);
 // Shared-memory bytes for a configuration (0 if it cannot fit).
 size_t tile_smem_bytes(const TileConfig& c, const TileArgs& a);
 cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,

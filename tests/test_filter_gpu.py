@@ -26,11 +26,13 @@ from cases import FILTER_CASES  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
-def run_gpu(raw, pr, sr, sigmas, nslices=11, aniso=1.0, weight_table="cpu"):
+def run_gpu(raw, pr, sr, sigmas, nslices=11, aniso=1.0, weight_table="cpu", form="auto"):
     g = IterativeNLM_GPU()
     dp = DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, nslices=nslices,
                            z_anisotropy=aniso, weight_table=weight_table)
     assert g.configure_device(raw.shape, dp) == raw.shape[0]
+    if form != "auto":
+        g.select_tile_form(form)
     outs = []
     for it in range(sigmas.shape[0]):
         g.set_sigma(sigmas[it])
@@ -51,7 +53,7 @@ def test_filter_bit_exact_vs_reference_golden(gpu, golden_filter, case):
         pytest.fail(f"{name} [{desc}]: {np.count_nonzero(d)} voxels differ, max {d.max():.3g}")
     spec = name.split("_")[0] in ("p111", "p112", "p113", "p221", "p222", "p331", "p332", "p333")
     if spec and nsl // 2 >= pr[2]:
-        assert desc.startswith("nlm_tile_f32"), desc
+        assert desc.startswith(("nlm_tile_f32", "nlm_column_f32")), desc
 
 
 @pytest.mark.parametrize("shape,pr,sr", [
@@ -85,10 +87,36 @@ def test_raw_slab_bit_exact(gpu, port, shape, pr, sr):
     raw = synth.small_case(shape, seed=sum(shape) + 3)
     sig = np.stack([np.full(shape[0], 0.06, np.float32),
                     np.linspace(0.03, 0.08, shape[0], dtype=np.float32)])
-    got, desc = run_gpu(raw, pr, sr, sig)
+    got, desc = run_gpu(raw, pr, sr, sig, form="tile")
     assert "raw_slab" in desc, desc
     want = port.denoise_f32(raw, FilterParams(search_radius=sr, patch_radius=pr), sig, all_iters=True)
     assert np.array_equal(got, want), desc
+
+
+@pytest.mark.parametrize("shape,pr,sr,nsl", [
+    ((5, 7, 9), (1, 1, 1), (2, 2, 2), 11),
+    ((20, 40, 48), (1, 1, 1), (10, 10, 10), 11),   # the reference's default geometry
+    ((17, 23, 70), (1, 1, 1), (4, 5, 3), 11),
+    ((3, 40, 40), (1, 1, 1), (4, 4, 4), 11),       # fewer planes than the CTA depth and the z halo
+    ((33, 9, 31), (1, 1, 1), (3, 3, 7), 15),       # two CTA layers in z, partial x and y tiles
+    ((16, 24, 40), (1, 1, 2), (6, 6, 6), 11),
+    ((12, 30, 33), (1, 1, 3), (3, 3, 3), 11),
+])
+def test_column_form_bit_exact(gpu, port, shape, pr, sr, nsl):
+    """The column form (patch radius 1 in x and y: a warp per z plane, each
+    thread 8 voxels along y, no barrier in the offset loop, raw from global
+    memory) equals the oracle and the tiled kernel bit for bit."""
+    raw = synth.small_case(shape, seed=sum(shape) + 5)
+    sig = np.stack([np.full(shape[0], 0.05, np.float32),
+                    np.linspace(0.03, 0.08, shape[0], dtype=np.float32)])
+    got, desc = run_gpu(raw, pr, sr, sig, nslices=nsl, form="column")
+    assert desc.startswith("nlm_column_f32"), desc
+    tile, desc_t = run_gpu(raw, pr, sr, sig, nslices=nsl, form="tile")
+    assert desc_t.startswith("nlm_tile_f32"), desc_t
+    want = port.denoise_f32(raw, FilterParams(search_radius=sr, patch_radius=pr, nslices=nsl), sig,
+                            all_iters=True)
+    assert np.array_equal(got, want), desc
+    assert np.array_equal(tile, want), desc_t
 
 
 @pytest.mark.parametrize("pr,sr", [((1, 1, 1), (2, 2, 2)), ((2, 2, 2), (3, 3, 3))])
