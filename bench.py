@@ -27,13 +27,16 @@ that path on one GPU (one rank).
 ``forms`` (rank 0, one GPU): the same whole job in the fused FP32 form
 (fused multiply-adds, within 1e-4 relative of the reference except at
 weights that cross the Pade cutoff), the FP16-storage form, and the
-learned-proposal + FP16 form: one list of LEARNED_K offsets per 32x8x8 block
-(the four 8^3 tiles' predictions summed, run by the full-width kernel), with
-full search for every block whose predicted kept weight mass is below
-LEARNED_REL x the mean over the volume's blocks; beside it the same lists at
-k = 176 without fallback and at k = 160 with fallback below 0.85 x the mean
-(the 4x points), and k = 256 per 8^3 tile with the absolute 0.95 threshold,
-which falls back on every tile of this volume. Each form reports its
+learned-proposal + FP16 form: one offset list per 32x8x8 block (the four 8^3
+tiles' predictions summed, run by the full-width kernel) of LEARNED_K[i]
+offsets in iteration i, with full search for every block whose predicted
+kept weight mass is below LEARNED_REL[i] x the mean over the volume's blocks
+(small lists while later iterations re-filter the result, a larger list and
+the fallback in the last iteration, whose output carries the approximation);
+beside it the schedule 144 x 3, 240; one k throughout (k = 208 with the
+fallback at 0.9 in every iteration, k = 176 without), and k = 256 per 8^3
+tile with the absolute 0.95 threshold, which falls back on every tile of
+this volume. Each form reports its
 speed-up over the plain FP32 job, the proposal's fallback and
 evaluated-offset fractions, and its accuracy (see run_forms): PSNR against
 the clean phantom over the whole volume beside the plain FP32 result's, and
@@ -71,11 +74,10 @@ S_OFFSETS, P_TAPS = 514, 33
 FLOP_PER_VOXEL_ITER = S_OFFSETS * (2 * P_TAPS + 20)
 BYTES_PER_VOXEL_ITER_F32 = 12                          # read raw + prev, write result
 # learned + FP16 form of the headline line: one offset list per 32x8x8 block
-# of LEARNED_K offsets, full search for the blocks whose predicted kept mass
-# is below LEARNED_REL x the mean over the volume's blocks (the fastest
-# setting measured within 0.1 dB of the plain and FP64 results with the
-# fallback on)
-LEARNED_K, LEARNED_MIN_MASS, LEARNED_REL = 208, 0.0, 0.9
+# of LEARNED_K[i] offsets in iteration i, full search for the blocks whose
+# predicted kept mass is below LEARNED_REL[i] x the mean over the volume's
+# blocks (the last iteration's list and fallback set the accuracy)
+LEARNED_K, LEARNED_MIN_MASS, LEARNED_REL = (128, 128, 128, 240), 0.0, (0.0, 0.0, 0.0, 0.9)
 
 
 def log(*a):
@@ -304,16 +306,20 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
     net = ProposalNet.load(default_weights(PR, SR), device=local)
     forms = [("f32", "f32", None), ("f32_fused", "f32_fma", None), ("fp16", "f16", None),
              ("learned_fp16", "f16", (LEARNED_K, LEARNED_MIN_MASS, 4, LEARNED_REL)),
+             ("learned_fp16_sched144", "f16", ((144, 144, 144, 240), 0.0, 4, (0.0, 0.0, 0.0, 0.9))),
+             ("learned_fp16_k208_r09", "f16", (208, 0.0, 4, 0.9)),
              ("learned_fp16_k176", "f16", (176, 0.0, 4, 0.0)),
-             ("learned_fp16_k160_r085", "f16", (160, 0.0, 4, 0.85)),
              ("learned_fp16_k256_mass095", "f16", (256, 0.95, 1, 0.0))]
     for item in filter(None, args.learned_extra.split(",")):
         f = item.split("@")
         k, t = f[0], f[1] if len(f) > 1 else "1"
         m = f[2] if len(f) > 2 else "0"
         prec = f[3] if len(f) > 3 else "f16"
-        rel = float(m[1:]) if m.startswith("r") else 0.0
-        forms.append((f"learned_{prec}_k{k}_t{t}_m{m}", prec, (int(k), 0.0 if rel else float(m), int(t), rel)))
+        rel = [float(v) for v in m[1:].split("/")] if m.startswith("r") else [0.0]
+        ks = [int(v) for v in k.split("/")]
+        forms.append((f"learned_{prec}_k{k.replace('/', '-')}_t{t}_m{m.replace('/', '-')}", prec,
+                      (ks if len(ks) > 1 else ks[0], 0.0 if m.startswith("r") else float(m), int(t),
+                       rel if len(rel) > 1 else rel[0])))
     raw_dev = torch.from_numpy(vol).cuda()
     out_dev = torch.empty_like(raw_dev)
     vox = float(np.prod(vol.shape))
@@ -352,15 +358,23 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
                       "speedup_vs_f32": vox * ITERS / (ms / 1e3) / value_f32,
                       "filter_kernel_avg_ms": kms})
             if prop:
-                st = g.proposal_stats()
                 r.update({"k": prop[0], "min_mass": prop[1], "tiles_per_plan": prop[2],
-                          "rel_mass": prop[3] if len(prop) > 3 else 0.0,
-                          "fallback_fraction": st["fallback_tiles"] / max(st["tiles"], 1),
-                          "fraction_evaluated": st["fraction_evaluated"]})
-        # accuracy run: the FP32 job's sigma schedule, fixed, for every form
+                          "rel_mass": prop[3] if len(prop) > 3 else 0.0})
+        # accuracy run: the FP32 job's sigma schedule, fixed, for every form;
+        # the proposal's lists per iteration
+        fb, ev = [], []
         for it in range(ITERS):
             g.set_sigma(sig_iters[it])
             g.Run_GaussianNoise_device(it + 1, raw_dev.data_ptr() if it == 0 else None)
+            if prop:
+                st = g.proposal_stats()
+                fb.append(st["fallback_tiles"] / max(st["tiles"], 1))
+                ev.append(st["fraction_evaluated"])
+        if prop:
+            r.update({"fallback_fraction": fb[-1], "fallback_per_iteration": fb,
+                      "fraction_evaluated": float(np.mean(ev)), "fraction_evaluated_per_iteration": ev,
+                      "stats_how": "lists falling back and offsets evaluated per iteration of the accuracy "
+                                   "run; fallback_fraction: the last iteration's"})
         g.get_result_device(out_dev.data_ptr())
         torch.cuda.synchronize()
         out = out_dev.cpu().numpy()
@@ -572,12 +586,15 @@ def psnr_chunked(a, b, peak=1.0, chunk=32):
 
 
 def parse_learned(spec):
-    """k@tiles_per_plan[@min_mass] with min_mass rX: relative threshold X."""
+    """k@tiles_per_plan[@min_mass] with min_mass rX: relative threshold X;
+    k1/k2/... and rX1/X2/...: per-iteration schedules."""
     f = spec.split("@")
-    k, t = int(f[0]), int(f[1]) if len(f) > 1 else 1
+    ks = [int(v) for v in f[0].split("/")]
+    t = int(f[1]) if len(f) > 1 else 1
     m = f[2] if len(f) > 2 else "0"
-    rel = float(m[1:]) if m.startswith("r") else 0.0
-    return k, t, (0.0 if rel else float(m)), rel
+    rels = [float(v) for v in m[1:].split("/")] if m.startswith("r") else [0.0]
+    return (ks if len(ks) > 1 else ks[0]), t, (0.0 if m.startswith("r") else float(m)), \
+        (rels if len(rels) > 1 else rels[0])
 
 
 def run_large_workload(args):
@@ -874,7 +891,7 @@ def run_profile_case(args):
         g.configure_device(vol.shape, DenoiseParameters(radius_patchspace=(2, 2, 2),
                                                         radius_searchspace=(5, 5, 5), precision="f16",
                                                         noise_mode="z-adaptive", n_samples=100000))
-        g.attach_proposal(net, LEARNED_K, LEARNED_MIN_MASS, tiles_x=4, rel_mass=LEARNED_REL)
+        g.attach_proposal(net, list(LEARNED_K), LEARNED_MIN_MASS, tiles_x=4, rel_mass=list(LEARNED_REL))
         g.denoise(raw.data_ptr(), on_device=True, out=out.data_ptr())
     torch.cuda.synchronize()
     ms, n = g.filter_kernel_ms()
@@ -978,7 +995,8 @@ def main():
     ap.add_argument("--learned-extra", default="",
                     help="extra learned + FP16 forms in the headline run, "
                          "k@tiles_per_plan[@min_mass[@precision]][,...]; min_mass rX: relative "
-                         "threshold X x the mean predicted kept mass; precision f16 or f16_df32")
+                         "threshold X x the mean predicted kept mass; precision f16 or f16_df32; "
+                         "per-iteration schedules as k1/k2/... and rX1/X2/...")
     ap.add_argument("--k-list", default="",
                     help="learned1024: learned + FP16 forms, k@tiles_per_plan[@min_mass|@rX][,...]")
     ap.add_argument("--split", action="store_true",

@@ -304,6 +304,15 @@ int inlm_attach_proposal_grouped(inlm_denoiser* d, inlm_proposal* p, int k, floa
  * fixed order: the same lists fall back on every run. */
 int inlm_attach_proposal_ex(inlm_denoiser* d, inlm_proposal* p, int k, float min_mass, float rel_mass,
                             int tiles_x);
+/* Per-iteration schedule for the attached proposal: iteration i (1-based)
+ * keeps k[min(i, n) - 1] offsets per list with the relative fallback
+ * rel_mass[min(i, n) - 1] (0: none); k = 0 runs that iteration's full
+ * search. n = 0 returns to the attach call's k and rel_mass. The last
+ * iteration's output carries the approximation directly, earlier ones are
+ * re-filtered, so a schedule with small lists early and a larger list with
+ * the fallback in the last iteration is both faster and closer to the full
+ * search than one k throughout. Cleared by a new attach. */
+int inlm_proposal_schedule(inlm_denoiser* d, int n, const int* k, const float* rel_mass);
 /* inlm_proposal_select for groups of tiles_x 8^3 tiles along x: bitmap and
  * pred_mass hold one entry per group, groups ordered z, y, x. */
 int inlm_proposal_select_grouped(inlm_proposal* p, const float* vol_dev, const float* scale_dev,
@@ -397,6 +406,13 @@ int inlm_stream_denoise_ex(const int shape[3], const inlm_params* p, const float
                            float* out_host, int slab_depth, inlm_proposal* net, int k, float min_mass,
                            float rel_mass, int tiles_x, float* sigma0_out, float* sigma1_out,
                            double* stats);
+/* The same with a per-iteration schedule of (k, rel_mass) as in
+ * inlm_proposal_schedule (n_sched >= 1 entries; one entry = one k
+ * throughout). */
+int inlm_stream_denoise_sched(const int shape[3], const inlm_params* p, const float* raw_host,
+                              float* out_host, int slab_depth, inlm_proposal* net, int n_sched,
+                              const int* k_sched, const float* rel_sched, float min_mass, int tiles_x,
+                              float* sigma0_out, float* sigma1_out, double* stats);
 
 /* ---------------- FP64 full-search reference on sub-blocks ----------------
  * No counterpart in the reference, whose filter computes in FP32. The
@@ -472,6 +488,9 @@ int inlm_blocks_destroy(inlm_blocks* b);
  * halos grow to >= 16 slices, the network's receptive field). */
 int inlm_blocks_attach_proposal(inlm_blocks* b, inlm_proposal* net, int k, float min_mass,
                                 float rel_mass, int tiles_x);
+/* After the attach, before the first iteration: the per-iteration (k,
+ * rel_mass) schedule of inlm_proposal_schedule. */
+int inlm_blocks_proposal_schedule(inlm_blocks* b, int n, const int* k, const float* rel_mass);
 /* Slices per slab (one device) or the deepest part (several). */
 int inlm_blocks_slab_depth(const inlm_blocks* b, int* depth);
 /* sigma of the following iterations, nz floats (host). */

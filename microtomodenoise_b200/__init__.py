@@ -240,17 +240,24 @@ class IterativeNLM_GPU:
         _lib.check(_lib.load().inlm_tile_grid(self._h, ts, tc), "tile_grid")
         return tuple(ts), tuple(tc)
 
-    def attach_proposal(self, net, k: int = 256, min_mass: float = 0.95, tiles_x: int = 1,
-                        rel_mass: float = 0.0) -> None:
+    def attach_proposal(self, net, k=256, min_mass: float = 0.95, tiles_x: int = 1,
+                        rel_mass=0.0) -> None:
         """Evaluates only each 8^3 tile's top-k offsets predicted by `net` (a
         proposal.ProposalNet), or every offset where the predicted kept mass
         is below min_mass, or below rel_mass x its mean over the volume.
         tiles_x = 4 ranks one list per 4 tiles along x (32 x 8 x 8 blocks, the
-        full-width kernel). net=None returns to full search. FP16 form only."""
+        full-width kernel). k and rel_mass may be per-iteration sequences
+        (inlm_proposal_schedule: iteration i uses entry min(i, n) - 1; k 0 =
+        full search that iteration). net=None returns to full search. FP16
+        form only."""
         self._need()
         h = net._h if net is not None else None
-        _lib.check(_lib.load().inlm_attach_proposal_ex(self._h, h, int(k), float(min_mass), float(rel_mass),
-                                                       int(tiles_x)), "attach_proposal")
+        ks, rels = _schedule(k, rel_mass)
+        _lib.check(_lib.load().inlm_attach_proposal_ex(self._h, h, max(int(ks.max()), 1), float(min_mass),
+                                                       float(rels[-1]), int(tiles_x)), "attach_proposal")
+        if net is not None and len(ks) > 1:
+            _lib.check(_lib.load().inlm_proposal_schedule(self._h, len(ks), ks.ctypes.data, rels.ctypes.data),
+                       "proposal_schedule")
         self._proposal = net  # keep the network alive while attached
 
     def proposal_stats(self) -> dict:
@@ -403,14 +410,25 @@ class Batch:
             pass
 
 
+def _schedule(k, rel_mass):
+    """Per-iteration (k, rel_mass) arrays from scalars or sequences (the
+    shorter one repeats its last entry)."""
+    ks = np.atleast_1d(np.asarray(k, np.int32))
+    rels = np.atleast_1d(np.asarray(rel_mass, np.float32))
+    n = max(len(ks), len(rels))
+    ks = np.ascontiguousarray(np.concatenate([ks, np.full(n - len(ks), ks[-1], np.int32)]))
+    rels = np.ascontiguousarray(np.concatenate([rels, np.full(n - len(rels), rels[-1], np.float32)]))
+    return ks, rels
+
+
 def stream_denoise(raw: np.ndarray, params: DenoiseParameters, slab_depth: int = 64,
-                   net=None, k: int = 256, min_mass: float = 0.95, out: Optional[np.ndarray] = None,
-                   tiles_x: int = 1, rel_mass: float = 0.0):
+                   net=None, k=256, min_mass: float = 0.95, out: Optional[np.ndarray] = None,
+                   tiles_x: int = 1, rel_mass=0.0):
     """The denoise schedule for a host-resident volume, filtered in z-slabs
-    (inlm_stream_denoise_ex; tiles_x and rel_mass as
-    IterativeNLM_GPU.attach_proposal, the relative threshold's mean taken per
-    sub-volume). Returns (result, sigma0, sigma1, stats) with stats =
-    {ms, h2d_bytes, d2h_bytes, slabs, halo, slab_depth}."""
+    (inlm_stream_denoise_sched; tiles_x, rel_mass and per-iteration k /
+    rel_mass sequences as IterativeNLM_GPU.attach_proposal, the relative
+    threshold's mean taken per sub-volume). Returns (result, sigma0, sigma1,
+    stats) with stats = {ms, h2d_bytes, d2h_bytes, slabs, halo, slab_depth}."""
     raw = _f32c(raw)
     if out is None:
         out = np.empty(raw.shape, np.float32)
@@ -419,11 +437,12 @@ def stream_denoise(raw: np.ndarray, params: DenoiseParameters, slab_depth: int =
     s1 = np.zeros(nz, np.float32)
     st = np.zeros(6, np.float64)
     cp = params.to_c()
-    rc = _lib.load().inlm_stream_denoise_ex(_shape_c(raw.shape), C.byref(cp), raw.ctypes.data,
-                                            out.ctypes.data, int(slab_depth),
-                                            net._h if net is not None else None, int(k),
-                                            float(min_mass), float(rel_mass), int(tiles_x), s0.ctypes.data,
-                                            s1.ctypes.data, st.ctypes.data)
+    ks, rels = _schedule(k, rel_mass)
+    rc = _lib.load().inlm_stream_denoise_sched(_shape_c(raw.shape), C.byref(cp), raw.ctypes.data,
+                                               out.ctypes.data, int(slab_depth),
+                                               net._h if net is not None else None, len(ks), ks.ctypes.data,
+                                               rels.ctypes.data, float(min_mass), int(tiles_x), s0.ctypes.data,
+                                               s1.ctypes.data, st.ctypes.data)
     _lib.check(rc, "stream_denoise")
     keys = ("ms", "h2d_bytes", "d2h_bytes", "slabs", "halo", "slab_depth")
     return out, s0, s1, dict(zip(keys, st.tolist()))
@@ -444,9 +463,15 @@ class Blocks:
                                                   int(slab_depth), C.byref(self._h)), "blocks_create")
         self._net = None
 
-    def attach_proposal(self, net, k: int, min_mass: float = 0.0, tiles_x: int = 4, rel_mass: float = 0.0):
-        _lib.check(_lib.load().inlm_blocks_attach_proposal(self._h, net._h, int(k), float(min_mass),
-                                                           float(rel_mass), int(tiles_x)), "blocks_attach_proposal")
+    def attach_proposal(self, net, k, min_mass: float = 0.0, tiles_x: int = 4, rel_mass=0.0):
+        """k and rel_mass: scalars or per-iteration sequences (as
+        IterativeNLM_GPU.attach_proposal)."""
+        ks, rels = _schedule(k, rel_mass)
+        _lib.check(_lib.load().inlm_blocks_attach_proposal(self._h, net._h, max(int(ks.max()), 1), float(min_mass),
+                                                           float(rels[-1]), int(tiles_x)), "blocks_attach_proposal")
+        if len(ks) > 1:
+            _lib.check(_lib.load().inlm_blocks_proposal_schedule(self._h, len(ks), ks.ctypes.data, rels.ctypes.data),
+                       "blocks_proposal_schedule")
         self._net = net
 
     def set_sigma(self, sigma) -> None:

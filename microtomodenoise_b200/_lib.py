@@ -46,7 +46,8 @@ EXPORTS = (
     "inlm_tiff_write_rgb", "inlm_attach_proposal_grouped", "inlm_attach_proposal_ex", "inlm_proposal_select_grouped",
     "inlm_stream_denoise_grouped", "inlm_denoise_multi", "inlm_device_count",
     "inlm_blocks_create", "inlm_blocks_destroy", "inlm_blocks_slab_depth", "inlm_blocks_set_sigma",
-    "inlm_blocks_run_iteration", "inlm_blocks_attach_proposal", "inlm_stream_denoise_ex", "inlm_device_memory", "inlm_debug_fail_allocation",
+    "inlm_blocks_run_iteration", "inlm_blocks_attach_proposal", "inlm_stream_denoise_ex",
+    "inlm_proposal_schedule", "inlm_stream_denoise_sched", "inlm_blocks_proposal_schedule", "inlm_device_memory", "inlm_debug_fail_allocation",
     "inlm_debug_live_allocations", "inlm_debug_wait_expiry", "inlm_denoise_f64_blocks",
 )
 
@@ -177,6 +178,10 @@ def load(path: str = "") -> C.CDLL:
     L.inlm_blocks_attach_proposal.argtypes = [vp, vp, C.c_int, C.c_float, C.c_float, C.c_int]
     L.inlm_stream_denoise_ex.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp, C.c_int,
                                          C.c_float, C.c_float, C.c_int, vp, vp, vp]
+    L.inlm_proposal_schedule.argtypes = [vp, C.c_int, vp, vp]
+    L.inlm_blocks_proposal_schedule.argtypes = [vp, C.c_int, vp, vp]
+    L.inlm_stream_denoise_sched.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp, C.c_int,
+                                            vp, vp, C.c_float, C.c_int, vp, vp, vp]
     L.inlm_blocks_run_iteration.argtypes = [vp, C.c_int, vp, vp, vp]
     L.inlm_denoise_multi.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp, vp, vp]
     L.inlm_stream_denoise_grouped.argtypes = [C.c_int * 3, C.POINTER(InlmParams), vp, vp, C.c_int, vp,

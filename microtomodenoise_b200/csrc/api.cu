@@ -1084,7 +1084,7 @@ static int enqueue_iteration(inlm_denoiser* d, int iter, const float* raw_dev) {
             if (rc) return rc;
         }
         if (d->prop.net) {
-            rc = proposal_enqueue(d);
+            rc = proposal_prepare_iteration(d, iter);
             if (rc) return rc;
         }
         rc = launch_filter(d);

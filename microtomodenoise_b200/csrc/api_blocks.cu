@@ -55,6 +55,19 @@ extern "C" int inlm_blocks_attach_proposal(inlm_blocks* b, inlm_proposal* net, i
     return b->be->attach_proposal(net, k, min_mass, rel_mass, tiles_x);
 }
 
+extern "C" int inlm_blocks_proposal_schedule(inlm_blocks* b, int n, const int* k, const float* rel_mass) {
+    if (!b) return fail(INLM_ERR_ARG, "null handle");
+    if (n < 0 || n > 1024) return fail(INLM_ERR_ARG, "schedule length must be in 0..1024");
+    if (n > 0 && (!k || !rel_mass)) return fail(INLM_ERR_ARG, "null schedule");
+    for (int i = 0; i < n; i++) {
+        if (k[i] < 0) return fail(INLM_ERR_ARG, "schedule k must be >= 0 (0: full search)");
+        if (!(rel_mass[i] >= 0.f && rel_mass[i] <= 1.f))
+            return fail(INLM_ERR_ARG, "schedule rel_mass must be in 0..1");
+    }
+    if (b->last_iter > 0) return fail(INLM_ERR_STATE, "set the schedule before the first iteration");
+    return b->be->proposal_schedule(n, k, rel_mass);
+}
+
 extern "C" int inlm_blocks_set_sigma(inlm_blocks* b, const float* sigma_host) {
     if (!b || !sigma_host) return fail(INLM_ERR_ARG, "null argument");
     int rc = b->be->set_sigma(sigma_host);

@@ -131,6 +131,10 @@ struct ProposalRun {
     int k = 0;
     float min_mass = 0.95f;
     float rel_mass = 0.f;  // > 0: fallback below rel_mass x the mean predicted kept mass
+    // per-iteration schedule (inlm_proposal_schedule): iteration i uses entry
+    // min(i, n) - 1; k 0 = full search that iteration. Empty: k, rel_mass.
+    std::vector<int> sched_k;
+    std::vector<float> sched_rel;
     int nwords = 0;
     long long n_tiles = 0;
     inlm::Dim3i t8{0, 0, 0};
@@ -215,7 +219,13 @@ int noise_prepare(inlm_noise* n, const inlm_params* p, int* nwin, bool* first);
 int noise_em_finish(inlm_noise* n, const inlm_params* p, int nwin);
 // Runs the attached proposal on the padded previous iterate and points the
 // filter's plan at its per-CTA lists (api_proposal.cu).
-int proposal_enqueue(inlm_denoiser* d);
+// k and relative threshold of iteration iter (1-based) under the schedule.
+void proposal_step(const ProposalRun& r, int iter, int* k, float* rel_mass);
+// Inference, selection and plans of iteration iter (its k must be > 0).
+int proposal_enqueue(inlm_denoiser* d, int iter);
+// Before iteration iter's filter launch: the proposal's plans, or the full
+// search where the schedule's k is 0.
+int proposal_prepare_iteration(inlm_denoiser* d, int iter);
 void proposal_release(inlm_denoiser* d);
 
 // Per-iteration engines over host-resident volumes (inlm_blocks_*): z-slab
@@ -227,6 +237,9 @@ struct BlocksBackend {
     virtual int iteration(int iter, const float* raw_host, const float* prev_host, float* out_host) = 0;
     virtual int slab_depth() const = 0;
     virtual int attach_proposal(inlm_proposal*, int, float, float, int) {
+        return fail(INLM_ERR_UNSUPPORTED, "the proposal runs on the one-device blocks only");
+    }
+    virtual int proposal_schedule(int, const int*, const float*) {
         return fail(INLM_ERR_UNSUPPORTED, "the proposal runs on the one-device blocks only");
     }
 };

@@ -357,9 +357,52 @@ extern "C" int inlm_attach_proposal_ex(inlm_denoiser* d, inlm_proposal* p, int k
     return INLM_OK;
 }
 
-int inlm::proposal_enqueue(inlm_denoiser* d) {
+void inlm::proposal_step(const ProposalRun& r, int iter, int* k, float* rel_mass) {
+    if (r.sched_k.empty()) {
+        *k = r.k;
+        *rel_mass = r.rel_mass;
+        return;
+    }
+    const size_t i = (size_t)std::max(1, std::min(iter, (int)r.sched_k.size())) - 1;
+    *k = r.sched_k[i];
+    *rel_mass = r.sched_rel[i];
+}
+
+extern "C" int inlm_proposal_schedule(inlm_denoiser* d, int n, const int* k, const float* rel_mass) {
+    if (!d) return fail(INLM_ERR_ARG, "null handle");
+    if (!d->prop.net) return fail(INLM_ERR_STATE, "attach a proposal first");
+    if (n < 0 || n > 1024) return fail(INLM_ERR_ARG, "schedule length must be in 0..1024");
+    if (n > 0 && (!k || !rel_mass)) return fail(INLM_ERR_ARG, "null schedule");
+    for (int i = 0; i < n; i++) {
+        if (k[i] < 0) return fail(INLM_ERR_ARG, "schedule k must be >= 0 (0: full search)");
+        if (!(rel_mass[i] >= 0.f && rel_mass[i] <= 1.f))
+            return fail(INLM_ERR_ARG, "schedule rel_mass must be in 0..1");
+    }
+    CUDA_TRY(cudaSetDevice(d->device));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+    d->prop.sched_k.assign(k, k + n);
+    d->prop.sched_rel.assign(rel_mass, rel_mass + n);
+    return INLM_OK;
+}
+
+int inlm::proposal_prepare_iteration(inlm_denoiser* d, int iter) {
+    int k = 0;
+    float rel = 0.f;
+    proposal_step(d->prop, iter, &k, &rel);
+    if (k > 0) return proposal_enqueue(d, iter);
+    // this iteration of the schedule searches every offset
+    d->plan_active = false;
+    d->plan_cta32 = false;
+    return INLM_OK;
+}
+
+int inlm::proposal_enqueue(inlm_denoiser* d, int iter) {
     ProposalRun& r = d->prop;
     inlm_proposal* p = r.net;
+    int k = r.k;
+    float rel = r.rel_mass;
+    proposal_step(r, iter, &k, &rel);
+    if (k < 1) return fail(INLM_ERR_STATE, "iteration %d runs the full search", iter);
     const Geometry& g = d->geo;
     CUDA_TRY(net_scale_from_mult(d->d_mult, d->shape[2], r.scale.as<float>(), d->stream));
     NetIn in;
@@ -376,18 +419,18 @@ int inlm::proposal_enqueue(inlm_denoiser* d) {
     CUDA_TRY(net_forward(p->L, p->d_wb, p->d_w, in, act, d->stream, NetTc{p->tc, d->d_err}));
     CUDA_TRY(cudaMemsetAsync(r.counters.p, 0, 16, d->stream));
     if (r.group == 1)
-        CUDA_TRY(net_select(p->L, p->d_wb, p->d_w, act.a4, (int)r.n_tiles, r.k, r.min_mass,
+        CUDA_TRY(net_select(p->L, p->d_wb, p->d_w, act.a4, (int)r.n_tiles, k, r.min_mass,
                             r.bitmap.as<unsigned>(), r.nwords, r.pmass.as<float>(), r.counters.as<int>(),
                             d->stream));
     else
-        CUDA_TRY(net_select_group(p->L, p->d_wb, p->d_w, act.a4, r.t8, r.group, r.k, r.min_mass,
+        CUDA_TRY(net_select_group(p->L, p->d_wb, p->d_w, act.a4, r.t8, r.group, k, r.min_mass,
                                   r.bitmap.as<unsigned>(), r.nwords, r.pmass.as<float>(),
                                   r.counters.as<int>(), d->stream));
     int* ps = r.plan_start.as<int>();
     CUDA_TRY(net_plan_tiles(r.bitmap.as<unsigned>(), r.nwords, r.n_plan, p->L.S,
                             r.plan_off.as<int>(), ps + r.n_plan, r.counters.as<int>(), d->stream,
-                            r.pmass.as<float>(), r.mass_sum.as<double>(), r.rel_mass));
-    d->launches += r.rel_mass > 0.f ? 8 : 7;  // scale, 4 layers, select, (mass sum,) plan
+                            r.pmass.as<float>(), r.mass_sum.as<double>(), rel));
+    d->launches += rel > 0.f ? 8 : 7;  // scale, 4 layers, select, (mass sum,) plan
     if (r.group == 1) {
         d->fargs8.plan_start = ps;
         d->fargs8.plan_count = ps + r.n_plan;

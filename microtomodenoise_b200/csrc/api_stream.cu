@@ -46,6 +46,8 @@ struct StreamJob {
     cudaStream_t main = nullptr;
     int tiles_x = 1;  // proposal lists per 8^3 tile (1) or per 32 x 8 x 8 block (4)
     float rel_mass = 0.f;  // relative fallback (the mean over each sub-volume's lists)
+    std::vector<int> sched_k;  // per-iteration schedule (inlm_proposal_schedule), or empty
+    std::vector<float> sched_rel;
 
     ~StreamJob() {
         for (auto& kv : pairs)
@@ -90,6 +92,11 @@ int get_pair(StreamJob& J, const inlm_params& p, int depth, inlm_proposal* net, 
         if (net) {
             rc = inlm_attach_proposal_ex(sp.d[j], net, k, min_mass, J.rel_mass, J.tiles_x);
             if (rc) return rc;
+            if (!J.sched_k.empty()) {
+                rc = inlm_proposal_schedule(sp.d[j], (int)J.sched_k.size(), J.sched_k.data(),
+                                            J.sched_rel.data());
+                if (rc) return rc;
+            }
         }
     }
     *out = &sp;
@@ -141,7 +148,7 @@ int stream_pass(StreamJob& J, const inlm_params& p, int it, const std::vector<in
                 if (rc) return rc;
             }
             if (d->prop.net) {
-                rc = proposal_enqueue(d);
+                rc = proposal_prepare_iteration(d, it);
                 if (rc) return rc;
             }
         } else {
@@ -194,7 +201,26 @@ extern "C" int inlm_stream_denoise_ex(const int shape[3], const inlm_params* p, 
                                       float* out_host, int slab_depth, inlm_proposal* net, int k,
                                       float min_mass, float rel_mass, int tiles_x, float* sigma0_out,
                                       float* sigma1_out, double* stats) {
+    return inlm_stream_denoise_sched(shape, p, raw_host, out_host, slab_depth, net, 1, &k, &rel_mass,
+                                     min_mass, tiles_x, sigma0_out, sigma1_out, stats);
+}
+
+extern "C" int inlm_stream_denoise_sched(const int shape[3], const inlm_params* p, const float* raw_host,
+                                         float* out_host, int slab_depth, inlm_proposal* net, int n_sched,
+                                         const int* k_sched, const float* rel_sched, float min_mass,
+                                         int tiles_x, float* sigma0_out, float* sigma1_out, double* stats) {
     if (!shape || !p || !raw_host || !out_host) return fail(INLM_ERR_ARG, "null argument");
+    if (n_sched < 1 || n_sched > 1024 || !k_sched || !rel_sched)
+        return fail(INLM_ERR_ARG, "a schedule of 1..1024 entries is required");
+    int k = 0;
+    for (int i = 0; i < n_sched; i++) {
+        if (k_sched[i] < 0) return fail(INLM_ERR_ARG, "schedule k must be >= 0 (0: full search)");
+        if (!(rel_sched[i] >= 0.f && rel_sched[i] <= 1.f))
+            return fail(INLM_ERR_ARG, "schedule rel_mass must be in 0..1");
+        k = std::max(k, k_sched[i]);
+    }
+    if (net && k < 1) return fail(INLM_ERR_ARG, "a schedule needs one iteration with k >= 1");
+    const float rel_mass = rel_sched[n_sched - 1];
     if (!(rel_mass >= 0.f && rel_mass <= 1.f)) return fail(INLM_ERR_ARG, "rel_mass must be in 0..1");
     if (tiles_x != 1 && tiles_x != 4) return fail(INLM_ERR_ARG, "tiles_x must be 1 or 4");
     if (slab_depth < 1) return fail(INLM_ERR_ARG, "slab depth must be >= 1");
@@ -209,6 +235,10 @@ extern "C" int inlm_stream_denoise_ex(const int shape[3], const inlm_params* p, 
     StreamJob J;
     J.tiles_x = tiles_x;
     J.rel_mass = rel_mass;
+    if (n_sched > 1) {
+        J.sched_k.assign(k_sched, k_sched + n_sched);
+        J.sched_rel.assign(rel_sched, rel_sched + n_sched);
+    }
     for (int i = 0; i < 3; i++) J.shape[i] = shape[i];
     J.plane = (long long)shape[0] * shape[1];
     J.raw_host = raw_host;
@@ -395,6 +425,18 @@ struct StreamBlocks final : BlocksBackend {
         if (ready) cudaEventDestroy(ready);
     }
     int slab_depth() const override { return sd; }
+    int proposal_schedule(int n, const int* ks, const float* rels) override {
+        if (!net) return fail(INLM_ERR_STATE, "attach a proposal first");
+        J.sched_k.assign(ks, ks + n);
+        J.sched_rel.assign(rels, rels + n);
+        for (auto& kv : J.pairs)
+            for (int j = 0; j < 2; j++)
+                if (kv.second.d[j]) {
+                    int rc = inlm_proposal_schedule(kv.second.d[j], n, ks, rels);
+                    if (rc) return rc;
+                }
+        return INLM_OK;
+    }
     int attach_proposal(inlm_proposal* n, int kk, float mm, float rel, int tiles_x) override {
         if (net) return fail(INLM_ERR_STATE, "a proposal is attached already");
         if (p.precision == INLM_PRECISION_F32 || p.precision == INLM_PRECISION_F32_FMA)

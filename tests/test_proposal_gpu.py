@@ -460,3 +460,78 @@ def test_grouped_plans_vs_fp64_plan_oracle(gpu, port):
     ref = port.denoise_f64_plan(vol, p, sig, (8, 8, 8), np.stack([expand_groups(kp, vol.shape) for kp in keeps]))
     check_close(got[-1], ref, "grouped plan")
     net.close()
+
+
+def test_schedule_equals_per_iteration_attach(gpu, port):
+    """A per-iteration (k, rel_mass) schedule (inlm_proposal_schedule) runs
+    each iteration exactly as attaching that iteration's k and threshold
+    before it does; k = 0 runs the iteration's full search; the schedule's
+    last entry repeats for later iterations. Through the whole job
+    (inlm_denoise) and through single iterations."""
+    P = prop_mod()
+    raw = synth.small_case((24, 40, 72), seed=17)
+    pr, sr = (1, 1, 1), (3, 3, 3)
+    S = len(port.search_offsets(FilterParams(search_radius=sr, patch_radius=pr)))
+    net = P.ProposalNet(S)
+    net.set_params(rand_params(S, 9))
+    ks, rels = [40, 0, 60], [0.0, 0.0, 0.9]
+    sig = np.stack([np.full(raw.shape[0], s, np.float32) for s in (0.07, 0.06, 0.06, 0.06)])
+    dp = DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, precision="f16")
+
+    def manual():
+        g = IterativeNLM_GPU()
+        g.configure_device(raw.shape, dp)
+        for it in range(4):
+            k, rel = ks[min(it, 2)], rels[min(it, 2)]
+            if k:
+                g.attach_proposal(net, k, 0.0, tiles_x=4, rel_mass=rel)
+            else:
+                g.attach_proposal(None)
+            g.set_sigma(sig[it])
+            g.Run_GaussianNoise(it + 1, raw if it == 0 else None)
+        out = g.get_result()
+        g.free_device()
+        return out
+
+    g = IterativeNLM_GPU()
+    g.configure_device(raw.shape, dp)
+    g.attach_proposal(net, ks, 0.0, tiles_x=4, rel_mass=rels)
+    for it in range(4):
+        g.set_sigma(sig[it])
+        g.Run_GaussianNoise(it + 1, raw if it == 0 else None)
+    got = g.get_result()
+    st = g.proposal_stats()
+    g.free_device()
+    assert np.array_equal(got, manual())
+    assert st["tiles"] > 0 and 0 <= st["fallback_tiles"] <= st["tiles"]
+    net.close()
+
+
+def test_schedule_whole_job_and_stream(gpu, port):
+    """The scheduled whole job (inlm_denoise) equals the streamed job
+    (inlm_stream_denoise_sched) with the same schedule (no relative
+    threshold: its mean would be taken per sub-volume)."""
+    from microtomodenoise_b200 import stream_denoise
+    P = prop_mod()
+    raw = synth.small_case((48, 40, 72), seed=8)
+    pr, sr = (1, 1, 1), (3, 3, 3)
+    S = len(port.search_offsets(FilterParams(search_radius=sr, patch_radius=pr)))
+    net = P.ProposalNet(S)
+    net.set_params(rand_params(S, 12))
+    dp = DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr, noise_mode="global", noise_seed=2,
+                           precision="f16")
+    g = IterativeNLM_GPU()
+    g.configure_device(raw.shape, dp)
+    g.attach_proposal(net, [30, 30, 60], 0.0, tiles_x=4)
+    want, _, _ = g.denoise(raw)
+    g.free_device()
+    got, _, _, _ = stream_denoise(raw, dp, slab_depth=16, net=net, k=[30, 30, 60], min_mass=0.0, tiles_x=4)
+    assert np.array_equal(got, want)
+    # one k throughout differs from the schedule
+    g = IterativeNLM_GPU()
+    g.configure_device(raw.shape, dp)
+    g.attach_proposal(net, 60, 0.0, tiles_x=4)
+    other, _, _ = g.denoise(raw)
+    g.free_device()
+    assert not np.array_equal(other, want)
+    net.close()
