@@ -154,6 +154,37 @@ def test_blocks_entry_points_check_arguments(lib):
     assert lib.inlm_blocks_set_sigma(None, None) == -1
 
 
+def test_proposal_schedule_entry_points_check_arguments(lib):
+    """The per-iteration proposal schedules reject bad arguments before they
+    touch a device; the Python helper broadcasts scalars and pads the shorter
+    sequence with its last entry."""
+    from microtomodenoise_b200 import _schedule
+    k = (C.c_int * 2)(64, 128)
+    r = (C.c_float * 2)(0.0, 0.9)
+    assert lib.inlm_proposal_schedule(None, 2, k, r) == -1
+    assert lib.inlm_blocks_proposal_schedule(None, 2, k, r) == -1
+    p = _lib.InlmParams()
+    lib.inlm_default_params(C.byref(p))
+    shape = (C.c_int * 3)(16, 16, 16)
+    buf = np.zeros(16 ** 3, np.float32)
+    assert lib.inlm_stream_denoise_sched(shape, C.byref(p), buf.ctypes.data, buf.ctypes.data, 8, None, 0, k, r,
+                                         0.0, 4, None, None, None) == -1
+    assert "schedule" in lib.inlm_last_error().decode()
+    bad = (C.c_int * 2)(64, -1)
+    assert lib.inlm_stream_denoise_sched(shape, C.byref(p), buf.ctypes.data, buf.ctypes.data, 8, None, 2, bad, r,
+                                         0.0, 4, None, None, None) == -1
+    badr = (C.c_float * 2)(0.0, 1.5)
+    assert lib.inlm_stream_denoise_sched(shape, C.byref(p), buf.ctypes.data, buf.ctypes.data, 8, None, 2, k, badr,
+                                         0.0, 4, None, None, None) == -1
+    ks, rels = _schedule([128, 128, 128, 240], [0.0, 0.0, 0.0, 0.9])
+    assert ks.tolist() == [128, 128, 128, 240] and np.allclose(rels, [0, 0, 0, 0.9])
+    ks, rels = _schedule(208, 0.9)
+    assert ks.tolist() == [208] and np.allclose(rels, [0.9])
+    ks, rels = _schedule([96, 240], 0.5)
+    assert ks.tolist() == [96, 240] and np.allclose(rels, [0.5, 0.5])
+    assert ks.dtype == np.int32 and rels.dtype == np.float32
+
+
 REF_MAIN = os.path.join(os.environ.get("INLM_REFERENCE_DIR", "/root/reference/iterNLM_v0.3"), "main.cpp")
 
 
