@@ -629,12 +629,12 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     const bool column = tz == 0;
     if (column) {
         tz = column_kernel_depth(pr[0], pr[1], pr[2]);
-        if (tz == 0 || fused) return INLM_OK;
+        if (tz == 0) return INLM_OK;
         raw_smem = false;
     }
     // tz 16: the two-planes-per-thread kernel (raw staged in shared memory)
     if (!column && !((tz == 8) || (tz == 4 && !raw_smem) || (tz == 16 && raw_smem))) return INLM_OK;
-    if (fused && tz != 8) return INLM_OK;  // the fused form is instantiated at CTA depth 8
+    if (fused && !column && tz != 8) return INLM_OK;  // the fused tile form is instantiated at depth 8
 
     TileArgs a{};
     a.nx = d->shape[0];

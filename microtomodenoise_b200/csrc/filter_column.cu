@@ -15,7 +15,10 @@
 // consecutive floats: no bank conflict), forms the squared differences
 // against the origin values it keeps in registers (the same D values the
 // tile kernel stores), and adds w * D in the reference's tap order for every
-// voxel. Raw comes from global memory, one offset ahead.
+// voxel. Raw comes from global memory, one offset ahead. FUSED = true is the
+// fused FP32 form: each tap one fused multiply-add, the Horner Pade with a
+// fast division (not bit-identical; within 1e-4 relative of the reference
+// except where a weight crosses the cutoff).
 #include "common.cuh"
 #include "filter_kernels.cuh"
 #include "geometry.hpp"
@@ -125,7 +128,7 @@ __device__ __forceinline__ void column_d(const float* __restrict__ prevb, int pb
 
 // Taps T.. of the reference order: form each column at its first use, then
 // add w_t * D to the 8 voxels' distances (pairs of y voxels).
-template <int RX, int RY, int RZ, int T>
+template <int RX, int RY, int RZ, int T, bool FUSED>
 __device__ __forceinline__ void column_taps(const float* __restrict__ prevb, int pb, int dlx, int pbx,
                                             int pplane, const f32x2 (&og)[ColGeom<RX, RY, RZ>::NV / 2],
                                             f32x2 (&D)[ColGeom<RX, RY, RZ>::NV / 2],
@@ -155,10 +158,12 @@ __device__ __forceinline__ void column_taps(const float* __restrict__ prevb, int
             }
             if (T == 0)
                 d[p] = mul_pair(v0, v1, w);
+            else if (FUSED)
+                d[p] = fma2(pack2(v0, v1), splat2(w), d[p]);
             else
                 d[p] = add2(d[p], mul_pair(v0, v1, w));
         }
-        column_taps<RX, RY, RZ, T + 1>(prevb, pb, dlx, pbx, pplane, og, D, d, a);
+        column_taps<RX, RY, RZ, T + 1, FUSED>(prevb, pb, dlx, pbx, pplane, og, D, d, a);
     }
 }
 
@@ -177,7 +182,7 @@ __device__ __forceinline__ void load_origins(const float* __restrict__ prevb, in
     }
 }
 
-template <int RX, int RY, int RZ, int TZ>
+template <int RX, int RY, int RZ, int TZ, bool FUSED>
 __global__ void __launch_bounds__(32 * TZ, 1)
     nlm_column_f32_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
     using CG = ColGeom<RX, RY, RZ>;
@@ -241,11 +246,16 @@ __global__ void __launch_bounds__(32 * TZ, 1)
         }
         f32x2 D[NV2];
         f32x2 d[NP];
-        column_taps<RX, RY, RZ, 0>(prevb, pb, dl.x, a.pbx, pplane, og, D, d, a);
+        column_taps<RX, RY, RZ, 0, FUSED>(prevb, pb, dl.x, a.pbx, pplane, og, D, d, a);
 #pragma unroll
-        for (int p = 0; p < NP; p++)
-            exact_weight_pair(d[p], m2, make_float2(rc[2 * p], rc[2 * p + 1]), acc[p], wsum[p], wmax[2 * p],
-                              wmax[2 * p + 1]);
+        for (int p = 0; p < NP; p++) {
+            if (FUSED)
+                fused_weight_pair(d[p], m2, make_float2(rc[2 * p], rc[2 * p + 1]), acc[p], wsum[p], wmax[2 * p],
+                                  wmax[2 * p + 1]);
+            else
+                exact_weight_pair(d[p], m2, make_float2(rc[2 * p], rc[2 * p + 1]), acc[p], wsum[p], wmax[2 * p],
+                                  wmax[2 * p + 1]);
+        }
         dl = dln;
     }
 
@@ -272,8 +282,9 @@ __global__ void __launch_bounds__(32 * TZ, 1)
 }
 
 template <int RX, int RY, int RZ, int TZ>
-cudaError_t launch_column(const CUtensorMap* tm, const TileArgs& a, int tiles_z, size_t smem, cudaStream_t st) {
-    auto kern = nlm_column_f32_kernel<RX, RY, RZ, TZ>;
+cudaError_t launch_column(const CUtensorMap* tm, const TileArgs& a, int tiles_z, size_t smem, bool fused,
+                          cudaStream_t st) {
+    auto kern = fused ? nlm_column_f32_kernel<RX, RY, RZ, TZ, true> : nlm_column_f32_kernel<RX, RY, RZ, TZ, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
@@ -294,11 +305,11 @@ size_t column_smem_bytes(const TileArgs& a) { return 128 + (size_t)a.pbx * a.pby
 cudaError_t launch_column_kernel(const TileConfig& c, const CUtensorMap* tm_prev, const TileArgs& a,
                                  int tiles_z, cudaStream_t st) {
     if (c.rx == 1 && c.ry == 1 && c.rz == 1 && c.tz == 16)
-        return launch_column<1, 1, 1, 16>(tm_prev, a, tiles_z, c.smem_bytes, st);
+        return launch_column<1, 1, 1, 16>(tm_prev, a, tiles_z, c.smem_bytes, c.fused, st);
     if (c.rx == 1 && c.ry == 1 && c.rz == 2 && c.tz == 8)
-        return launch_column<1, 1, 2, 8>(tm_prev, a, tiles_z, c.smem_bytes, st);
+        return launch_column<1, 1, 2, 8>(tm_prev, a, tiles_z, c.smem_bytes, c.fused, st);
     if (c.rx == 1 && c.ry == 1 && c.rz == 3 && c.tz == 8)
-        return launch_column<1, 1, 3, 8>(tm_prev, a, tiles_z, c.smem_bytes, st);
+        return launch_column<1, 1, 3, 8>(tm_prev, a, tiles_z, c.smem_bytes, c.fused, st);
     return cudaErrorInvalidConfiguration;
 }
 

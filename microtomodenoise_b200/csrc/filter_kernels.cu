@@ -245,8 +245,6 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
 #pragma unroll
     for (int r = 0; r < kVoxPerThread; r++) wmax[r] = 0.0f;
 
-    const f32x2 c12 = splat2(12.f), c120 = splat2(120.f), c60 = splat2(60.f), cm60 = splat2(-60.f);
-
     // phase A for one offset: D = (prev(.+s) - prev(.))^2 over tile + patch halo
     auto phase_a = [&](float* Dw, int dlx) {
 #pragma unroll
@@ -269,25 +267,10 @@ __device__ __forceinline__ bool tile_f32_body(const CUtensorMap* tm_prev, const 
             } else {
                 rsv = make_float2(rg[2 * p], rg[2 * p + 1]);
             }
-            if (FUSED) {
-                // the same Pade[3/3] in Horner form with fused pairs and a fast
-                // division: 120 + x(60 + x(12 + x)) over 120 + x(-60 + x(12 - x))
-                const f32x2 x = mul2_to_mul(dist[p], m2);
-                const float2 xs = unpack2(x);
-                const f32x2 num = fma2(x, fma2(x, add2(c12, x), c60), c120);
-                const f32x2 den = fma2(x, fma2(x, sub2(c12, x), cm60), c120);
-                const float2 nu = unpack2(num), de = unpack2(den);
-                const float q0 = __fdividef(nu.x, de.x), q1 = __fdividef(nu.y, de.y);
-                const float w0 = (xs.x > -3.56648f) ? q0 : 0.0f;
-                const float w1 = (xs.y > -3.56648f) ? q1 : 0.0f;
-                const f32x2 wp = pack2(w0, w1);
-                acc[p] = fma2(wp, pack2(rsv.x, rsv.y), acc[p]);
-                wsum[p] = add2(wsum[p], wp);
-                wmax[2 * p] = fmaxf(wmax[2 * p], w0);
-                wmax[2 * p + 1] = fmaxf(wmax[2 * p + 1], w1);
-                continue;
-            }
-            exact_weight_pair(dist[p], m2, rsv, acc[p], wsum[p], wmax[2 * p], wmax[2 * p + 1]);
+            if (FUSED)
+                fused_weight_pair(dist[p], m2, rsv, acc[p], wsum[p], wmax[2 * p], wmax[2 * p + 1]);
+            else
+                exact_weight_pair(dist[p], m2, rsv, acc[p], wsum[p], wmax[2 * p], wmax[2 * p + 1]);
         }
     };
 

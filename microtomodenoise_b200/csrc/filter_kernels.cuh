@@ -60,7 +60,8 @@ struct TileConfig {
     int tz;           // CTA depth: z-planes = warps (4, 8), or 16 with two planes per thread
     bool raw_smem;    // raw box staged in shared memory
     size_t smem_bytes;
-    bool fused = false;  // the fused FP32 form (FFMA taps, Horner Pade, fast division); tz 8 only
+    bool fused = false;  // the fused FP32 form (FFMA taps, Horner Pade, fast division): the
+                         // 8-deep tile kernel or the column form
     bool raw_slab = false;  // raw staged as TZ + 1 planes per z offset pair (raw_smem, tz 8 or 16)
     bool column = false;    // the column form (filter_column.cu): patch radius 1, raw from global
 };

@@ -86,4 +86,26 @@ __device__ __forceinline__ void exact_weight_pair(f32x2 dist, f32x2 m2, float2 r
     wmax1 = fmaxf(wmax1, w1);
 }
 
+// The fused FP32 form of the same step: Pade[3/3] in Horner form with fused
+// pairs, 120 + x(60 + x(12 + x)) over 120 + x(-60 + x(12 - x)), a fast
+// division, and w*raw fused into its sum (not bit-identical to the
+// reference; within 1e-4 relative except where a weight crosses the cutoff).
+__device__ __forceinline__ void fused_weight_pair(f32x2 dist, f32x2 m2, float2 rsv, f32x2& acc,
+                                                  f32x2& wsum, float& wmax0, float& wmax1) {
+    const f32x2 c12 = splat2(12.f), c120 = splat2(120.f), c60 = splat2(60.f), cm60 = splat2(-60.f);
+    const f32x2 x = mul2_to_mul(dist, m2);
+    const float2 xs = unpack2(x);
+    const f32x2 num = fma2(x, fma2(x, add2(c12, x), c60), c120);
+    const f32x2 den = fma2(x, fma2(x, sub2(c12, x), cm60), c120);
+    const float2 nu = unpack2(num), de = unpack2(den);
+    const float q0 = __fdividef(nu.x, de.x), q1 = __fdividef(nu.y, de.y);
+    const float w0 = (xs.x > -3.56648f) ? q0 : 0.0f;
+    const float w1 = (xs.y > -3.56648f) ? q1 : 0.0f;
+    const f32x2 wp = pack2(w0, w1);
+    acc = fma2(wp, pack2(rsv.x, rsv.y), acc);
+    wsum = add2(wsum, wp);
+    wmax0 = fmaxf(wmax0, w0);
+    wmax1 = fmaxf(wmax1, w1);
+}
+
 }  // namespace inlm
