@@ -551,6 +551,7 @@ static void denoiser_free(inlm_denoiser* d) {
     device_free(d->d_plan_start);
     device_free(d->d_plan_off);
     device_free(d->d_search_delta8);
+    device_free(d->d_search_delta_c);
     proposal_release(d);
     d->aux.release();
     if (d->noise) {
@@ -734,7 +735,9 @@ static int choose_tile_config(inlm_denoiser* d, int form = 0) {
 
 // FP16-storage kernel configurations: CTA width tx = 32 (full search) and
 // tx = 8 (one 8^3 tile per CTA, for per-tile offset plans); prev box in
-// halves arriving by TMA, raw staged in halves with an odd pitch.
+// halves arriving by TMA, raw staged in halves with an odd pitch. tx = 0:
+// the column form at its own CTA depth (32 x 8 x depth voxels, raw from
+// global memory, no raw box).
 static int build_fast_config(inlm_denoiser* d, int tx, FastConfig* cfg, FastArgs* args,
                              CUtensorMap* tm, int2** d_delta, bool* ok) {
     const Geometry& g = d->geo;
@@ -764,9 +767,13 @@ static int build_fast_config(inlm_denoiser* d, int tx, FastConfig* cfg, FastArgs
     a.S = (int)g.search.size();
     a.gpitch_y = d->pitch_y;
     a.gpitch_z = d->pitch_z;
-    a.pbx = (tx + 2 * a.px + 7) / 8 * 8;  // halves, 16-byte TMA rows
+    const bool column = tx == 0;
+    const int cdepth = column ? column_kernel_depth(pr[0], pr[1], pr[2]) : 0;
+    if (column && cdepth == 0) return INLM_OK;
+    const int txw = column ? kTX : tx;  // CTA width in x
+    a.pbx = (txw + 2 * a.px + 7) / 8 * 8;  // halves, 16-byte TMA rows
     a.pby = kTY + 2 * a.py;
-    a.rbx = (pr[0] + tx + 2 * a.sxr + 3) / 4 * 4;
+    a.rbx = (pr[0] + txw + 2 * a.sxr + 3) / 4 * 4;
     a.rby = kTY + 2 * a.syr;
     for (int t = 0; t < nt; t++) {
         a.w[t] = g.weights[t];
@@ -777,7 +784,20 @@ static int build_fast_config(inlm_denoiser* d, int tx, FastConfig* cfg, FastArgs
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
     const bool dh = d->p.precision == INLM_PRECISION_F16;
     const int tzs[] = {8, 4};
+    if (column) {
+        a.pbz = cdepth + 2 * a.pz;
+        a.rbz = 0;
+        FastConfig fc{pr[0], pr[1], pr[2], cdepth, kTX, dh, 0};
+        fc.column = true;
+        const size_t sm = 128 + (size_t)a.pbx * a.pby * a.pbz * 2;
+        if (a.pbx <= 256 && a.pby <= 256 && a.pbz <= 256 && sm <= (size_t)smem_max) {
+            fc.smem_bytes = sm;
+            *cfg = fc;
+            *ok = true;
+        }
+    }
     for (int tz : tzs) {
+        if (column) break;
         if (tz == 4 && (!dh || tx != 32)) continue;
         a.pbz = tz + 2 * a.pz;
         a.rbz = tz + 2 * a.szc;
@@ -792,16 +812,16 @@ static int build_fast_config(inlm_denoiser* d, int tx, FastConfig* cfg, FastArgs
         break;
     }
     if (!*ok) return INLM_OK;
-    a.tiles_x = (d->shape[0] + tx - 1) / tx;
+    a.tiles_x = (d->shape[0] + txw - 1) / txw;
     a.tiles_y = (d->shape[1] + kTY - 1) / kTY;
     std::vector<int2> dl(a.S);
     const int rpx = a.rbx + 1;
     for (int si = 0; si < a.S; si++) {
         const Offset3& o = g.search[si];
         dl[si].x = o.z * a.pbx * a.pby + o.y * a.pbx + o.x;
-        // raw: shared-box delta (tx = 32) or padded global delta (tx = 8)
-        dl[si].y = tx == 8 ? (int)(o.z * d->pitch_z + o.y * d->pitch_y + o.x)
-                           : o.z * rpx * a.rby + o.y * rpx + o.x;
+        // raw: shared-box delta (tx = 32) or padded global delta (tx = 8, column)
+        dl[si].y = (tx == 8 || column) ? (int)(o.z * d->pitch_z + o.y * d->pitch_y + o.x)
+                                       : o.z * rpx * a.rby + o.y * rpx + o.x;
     }
     CUDA_TRY(dalloc(d_delta, a.S));
     CUDA_TRY(cudaMemcpy(*d_delta, dl.data(), a.S * sizeof(int2), cudaMemcpyHostToDevice));
@@ -827,6 +847,13 @@ static int choose_fast_config(inlm_denoiser* d) {
     rc = build_fast_config(d, 8, &d->fcfg8, &d->fargs8, &d->tm_prev_h8, &d->d_search_delta8, &ok8);
     if (rc) return rc;
     d->use_tile8 = ok8;
+    // the column form for full search at patch radius 1, scaled as the
+    // 32-wide kernel's tiles so both round every voxel alike
+    bool okc = false;
+    rc = build_fast_config(d, 0, &d->fcfgc, &d->fargsc, &d->tm_prev_hc, &d->d_search_delta_c, &okc);
+    if (rc) return rc;
+    d->fargsc.scale_tz = d->fcfg.tz;
+    d->use_colf = okc;
     return INLM_OK;
 }
 
@@ -1021,6 +1048,10 @@ int inlm::launch_filter(inlm_denoiser* d) {
         // per-tile plans: one 8^3 tile per CTA
         int tiles_z = (d->shape[2] + d->fcfg8.tz - 1) / d->fcfg8.tz;
         CUDA_TRY(launch_fast_kernel(d->fcfg8, &d->tm_prev_h8, d->fargs8, tiles_z, d->stream));
+    } else if (d->use_fast && d->use_colf) {
+        // full search at patch radius 1: the column form
+        int tiles_z = (d->shape[2] + d->fcfgc.tz - 1) / d->fcfgc.tz;
+        CUDA_TRY(launch_column_fast_kernel(d->fcfgc, &d->tm_prev_hc, d->fargsc, tiles_z, d->stream));
     } else if (d->use_fast) {
         int tiles_z = (d->shape[2] + d->fcfg.tz - 1) / d->fcfg.tz;
         CUDA_TRY(launch_fast_kernel(d->fcfg, &d->tm_prev_h, d->fargs, tiles_z, d->stream));
@@ -1322,11 +1353,12 @@ extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
     if (!d || !buf) return fail(INLM_ERR_ARG, "null argument");
     const Geometry& g = d->geo;
     if (d->use_fast) {
-        const FastConfig& c = (d->plan_active && !d->plan_cta32) ? d->fcfg8 : d->fcfg;
+        const bool col = !d->plan_active && d->use_colf;
+        const FastConfig& c = (d->plan_active && !d->plan_cta32) ? d->fcfg8 : col ? d->fcfgc : d->fcfg;
         snprintf(buf, len,
-                 "nlm_tile_fast<%d,%d,%d> tx=%d tz=%d d_planes=%s smem=%zu S=%zu P=%zu plan=%s "
+                 "nlm_%s_fast<%d,%d,%d> tx=%d tz=%d d_planes=%s smem=%zu S=%zu P=%zu plan=%s "
                  "pad=%d,%d,%d",
-                 c.rx, c.ry, c.rz, c.tx, c.tz, c.d_half ? "f16" : "f32", c.smem_bytes,
+                 col ? "column" : "tile", c.rx, c.ry, c.rz, c.tx, c.tz, c.d_half ? "f16" : "f32", c.smem_bytes,
                  g.search.size(), g.taps.size(),
                  d->plan_active ? (d->plan_cta32 ? "per-cta" : "per-tile") : "full", g.pad[0],
                  g.pad[1], g.pad[2]);

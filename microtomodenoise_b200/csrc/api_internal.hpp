@@ -177,6 +177,12 @@ struct inlm_denoiser {
     inlm::FastArgs fargs8{};
     CUtensorMap tm_prev_h8{};
     int2* d_search_delta8 = nullptr;
+    // the FP16 column form (patch radius 1): full search without plans
+    bool use_colf = false;
+    inlm::FastConfig fcfgc{};
+    inlm::FastArgs fargsc{};
+    CUtensorMap tm_prev_hc{};
+    int2* d_search_delta_c = nullptr;
     bool plan_active = false;     // fargs8 carries a per-tile plan
     bool plan_cta32 = false;      // ... or fargs_plan a per-32x8x8-CTA plan (proposal, group 4)
     inlm::FastArgs fargs_plan{};

@@ -19,7 +19,10 @@
 // fused FP32 form: each tap one fused multiply-add, the Horner Pade with a
 // fast division (not bit-identical; within 1e-4 relative of the reference
 // except where a weight crosses the cutoff).
+#include <cuda_fp16.h>
+
 #include "common.cuh"
+#include "filter_fast.cuh"
 #include "filter_kernels.cuh"
 #include "geometry.hpp"
 #include "pair_math.cuh"
@@ -292,7 +295,222 @@ cudaError_t launch_column(const CUtensorMap* tm, const TileArgs& a, int tiles_z,
     return cudaGetLastError();
 }
 
+// Origin values of columns C.. read from the FP16 prev box, as floats.
+template <int RX, int RY, int RZ, int C>
+__device__ __forceinline__ void load_fast_origins(const __half* __restrict__ prevb, int pb, int pbx, int pplane,
+                                                  float (&og)[ColGeom<RX, RY, RZ>::NV]) {
+    using CG = ColGeom<RX, RY, RZ>;
+    if constexpr (C < CG::cols.n) {
+        constexpr int e = CG::cols.e[C];
+        constexpr int f = CG::cols.first[C];
+        const __half* src = prevb + pb + CG::cols.zp[C] * pplane + CG::cols.xp[C] - e * pbx;
+#pragma unroll
+        for (int i = 0; i < kVoxPerThread + 2 * e; i++) og[f + i] = __half2float(src[i * pbx]);
+        load_fast_origins<RX, RY, RZ, C + 1>(prevb, pb, pbx, pplane, og);
+    }
+}
+
+// ---- FP16-storage column form ----
+//
+// The FP16 form's arithmetic voxel for voxel, so its result equals the FP16
+// tile kernel's (nlm_tile_fast_kernel) bit for bit: prev and raw read as
+// halves; each squared difference formed in FP32 as (t * scale) * t, t =
+// prev(. + s) - prev(.), with the scale of the voxel's tile of scale_tz
+// planes (the tile kernel's CTA scale); with D_HALF rounded to FP16 and
+// summed by half2 fused multiply-adds in tap order (half2 weights), else
+// summed by FP32 fused multiply-adds; x = dist * (m / scale); the Pade weight
+// in Horner form with a fast division; the weighted sums in FP32 and the
+// final normalisation in FP64.
+
+template <int RX, int RY, int RZ, int C, bool D_HALF>
+__device__ __forceinline__ void fast_column_d(const __half* __restrict__ prevb, int pb, int dlx, int pbx,
+                                              int pplane, float scale,
+                                              const float (&og)[ColGeom<RX, RY, RZ>::NV],
+                                              __half2 (&Dh)[ColGeom<RX, RY, RZ>::NV / 2],
+                                              float (&Df)[ColGeom<RX, RY, RZ>::NV]) {
+    using CG = ColGeom<RX, RY, RZ>;
+    constexpr int e = CG::cols.e[C];
+    constexpr int f = CG::cols.first[C];
+    const __half* src = prevb + pb + dlx + CG::cols.zp[C] * pplane + CG::cols.xp[C] - e * pbx;
+#pragma unroll
+    for (int i = 0; i < kVoxPerThread + 2 * e; i += 2) {
+        const float t0 = __half2float(src[i * pbx]) - og[f + i];
+        const float t1 = __half2float(src[(i + 1) * pbx]) - og[f + i + 1];
+        const float d0 = (t0 * scale) * t0, d1 = (t1 * scale) * t1;
+        if constexpr (D_HALF) {
+            Dh[(f + i) / 2] = __floats2half2_rn(d0, d1);  // the column starts on a pair
+        } else {
+            Df[f + i] = d0;
+            Df[f + i + 1] = d1;
+        }
+    }
+}
+
+template <int RX, int RY, int RZ, int T, bool D_HALF>
+__device__ __forceinline__ void fast_column_taps(const __half* __restrict__ prevb, int pb, int dlx, int pbx,
+                                                 int pplane, float scale,
+                                                 const float (&og)[ColGeom<RX, RY, RZ>::NV],
+                                                 __half2 (&Dh)[ColGeom<RX, RY, RZ>::NV / 2],
+                                                 float (&Df)[ColGeom<RX, RY, RZ>::NV],
+                                                 __half2 (&dh)[kVoxPerThread / 2],
+                                                 float (&dist)[kVoxPerThread], const FastArgs& a) {
+    using CG = ColGeom<RX, RY, RZ>;
+    if constexpr (T < CG::taps.n) {
+        constexpr int C = CG::taps.col[T];
+        constexpr int yp = CG::taps.yp[T];
+        constexpr int e = CG::cols.e[C];
+        constexpr int f = CG::cols.first[C];
+        if constexpr (first_use<RX, RY, RZ, C>() == T)
+            fast_column_d<RX, RY, RZ, C, D_HALF>(prevb, pb, dlx, pbx, pplane, scale, og, Dh, Df);
+        if constexpr (D_HALF) {
+            const __half2 w = a.wh[T];
+#pragma unroll
+            for (int p = 0; p < kVoxPerThread / 2; p++) {
+                const int i = f + e + 2 * p + yp;  // voxels 2p, 2p + 1
+                const __half2 v = (i & 1) == 0 ? Dh[i / 2]
+                                               : __halves2half2(__high2half(Dh[i / 2]), __low2half(Dh[i / 2 + 1]));
+                dh[p] = (T == 0) ? __hmul2(v, w) : __hfma2(v, w, dh[p]);
+            }
+        } else {
+            const float w = a.w[T];
+#pragma unroll
+            for (int r = 0; r < kVoxPerThread; r++) {
+                const int i = f + e + r + yp;
+                dist[r] = (T == 0) ? Df[i] * w : fmaf(Df[i], w, dist[r]);
+            }
+        }
+        fast_column_taps<RX, RY, RZ, T + 1, D_HALF>(prevb, pb, dlx, pbx, pplane, scale, og, Dh, Df, dh, dist, a);
+    }
+}
+
+template <int RX, int RY, int RZ, int TZ, bool D_HALF>
+__global__ void __launch_bounds__(32 * TZ, 1)
+    nlm_column_fast_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ FastArgs a) {
+    using CG = ColGeom<RX, RY, RZ>;
+    constexpr int NV = CG::NV;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+    __half* prevb = reinterpret_cast<__half*>(smem + 128);
+    const int tid = threadIdx.x;
+    const int X0 = blockIdx.x * kTX;
+    const int Y0 = blockIdx.y * kTY;
+    const int Z0 = blockIdx.z * TZ;
+    const int pplane = a.pbx * a.pby;
+    if (tid == 0) {
+        prefetch_tmap(&tm_prev);
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(pplane * a.pbz) * 2u);
+        tma_load_3d(prevb, &tm_prev, X0, Y0, Z0, bar);
+    }
+    const int lane = tid & 31, k = tid >> 5;
+    const int pb = (k + a.pz) * pplane + a.py * a.pbx + lane + a.px;
+    const long long gbase = (long long)(Z0 + k + a.pz) * a.gpitch_z + (long long)(Y0 + a.py) * a.gpitch_y +
+                            (X0 + lane + a.px);
+    // the tile kernel's scale: the middle slice of the voxel's scale_tz-plane tile
+    const int zt = (Z0 + k) / a.scale_tz * a.scale_tz;
+    const float scale = -a.mult[min(zt + a.scale_tz / 2, a.nz - 1)];
+    const float rel = a.mult[min(Z0 + k, a.nz - 1)] / scale;
+
+    int2 dl = __ldg(&a.search_delta[0]);
+    float rn[kVoxPerThread];
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) rn[r] = __half2float(a.raw_pad[gbase + r * a.gpitch_y + dl.y]);
+
+    const bool arrived = mbar_wait_bounded(bar, 0);
+    if (!__syncthreads_and(arrived)) {
+        if (tid == 0) set_error(a.err, DEV_TMA_TIMEOUT);
+        return;
+    }
+    float og[NV];
+    load_fast_origins<RX, RY, RZ, 0>(prevb, pb, a.pbx, pplane, og);
+
+    float acc[kVoxPerThread], wsum[kVoxPerThread], wmax[kVoxPerThread];
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) acc[r] = wsum[r] = wmax[r] = 0.0f;
+
+    for (int s = 0; s < a.S; s++) {
+        float rc[kVoxPerThread];
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) rc[r] = rn[r];
+        const int2 dln = __ldg(&a.search_delta[min(s + 1, a.S - 1)]);
+        if (s + 1 < a.S) {
+#pragma unroll
+            for (int r = 0; r < kVoxPerThread; r++)
+                rn[r] = __half2float(a.raw_pad[gbase + r * a.gpitch_y + dln.y]);
+        }
+        __half2 Dh[NV / 2];
+        float Df[NV];
+        __half2 dh[kVoxPerThread / 2];
+        float dist[kVoxPerThread];
+        fast_column_taps<RX, RY, RZ, 0, D_HALF>(prevb, pb, dl.x, a.pbx, pplane, scale, og, Dh, Df, dh, dist, a);
+        if constexpr (D_HALF) {
+#pragma unroll
+            for (int p = 0; p < kVoxPerThread / 2; p++) {
+                const float2 fd = __half22float2(dh[p]);
+                dist[2 * p] = fd.x;
+                dist[2 * p + 1] = fd.y;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) {
+            const float x = dist[r] * rel;
+            // Pade[3/3] of exp in Horner form, FMA
+            const float num = fmaf(fmaf(x + 12.f, x, 60.f), x, 120.f);
+            const float den = fmaf(fmaf(12.f - x, x, -60.f), x, 120.f);
+            const float q = __fdividef(num, den);  // formed, then selected
+            const float w = (x > -3.56648f) ? q : 0.0f;
+            acc[r] = fmaf(w, rc[r], acc[r]);
+            wsum[r] += w;
+            wmax[r] = fmaxf(wmax[r], w);
+        }
+        dl = dln;
+    }
+
+    const int z = Z0 + k, x = X0 + lane;
+    if (z >= a.nz || x >= a.nx) return;
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) {
+        const int y = Y0 + r;
+        if (y >= a.ny) break;
+        const float raw0 = __half2float(a.raw_pad[gbase + r * a.gpitch_y]);
+        float res = raw0;
+        if (wmax[r] > 0.0f) {
+            // per-voxel weight-sum normalisation in FP64
+            const double num = (double)acc[r] + (double)wmax[r] * (double)raw0;
+            const double den = (double)wsum[r] + (double)wmax[r];
+            res = (float)(num / den);
+        }
+        a.out[((long long)z * a.ny + y) * a.nx + x] = res;
+    }
+}
+
 }  // namespace
+
+template <int RX, int RY, int RZ, int TZ>
+cudaError_t launch_column_fast(const CUtensorMap* tm, const FastArgs& a, int tiles_z, size_t smem, bool d_half,
+                               cudaStream_t st) {
+    auto kern = d_half ? nlm_column_fast_kernel<RX, RY, RZ, TZ, true> : nlm_column_fast_kernel<RX, RY, RZ, TZ, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
+    kern<<<grid, 32 * TZ, smem, st>>>(*tm, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_column_fast_kernel(const FastConfig& c, const CUtensorMap* tm_prev, const FastArgs& a,
+                                      int tiles_z, cudaStream_t st) {
+    if (c.rx == 1 && c.ry == 1 && c.rz == 1 && c.tz == 16)
+        return launch_column_fast<1, 1, 1, 16>(tm_prev, a, tiles_z, c.smem_bytes, c.d_half, st);
+    if (c.rx == 1 && c.ry == 1 && c.rz == 2 && c.tz == 8)
+        return launch_column_fast<1, 1, 2, 8>(tm_prev, a, tiles_z, c.smem_bytes, c.d_half, st);
+    if (c.rx == 1 && c.ry == 1 && c.rz == 3 && c.tz == 8)
+        return launch_column_fast<1, 1, 3, 8>(tm_prev, a, tiles_z, c.smem_bytes, c.d_half, st);
+    return cudaErrorInvalidConfiguration;
+}
 
 int column_kernel_depth(int rx, int ry, int rz) {
     if (rx == 1 && ry == 1 && rz == 1) return 16;

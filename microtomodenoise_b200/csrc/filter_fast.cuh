@@ -32,6 +32,8 @@ struct FastArgs {
     int t8x, t8y;                           // 8^3 tile grid (x, y)
     float w[kMaxTaps];
     __half2 wh[kMaxTaps];                   // the same weights in FP16, both halves
+    int scale_tz;                           // column form: the tile depth of the squared
+                                            // differences' scale (the tile kernel's CTA depth)
 };
 
 struct FastConfig {
@@ -40,12 +42,16 @@ struct FastConfig {
     int tx;       // CTA width: 32 (full search) or 8 (one 8^3 tile per CTA, per-tile plans)
     bool d_half;  // squared-difference planes in FP16 (else FP32)
     size_t smem_bytes;
+    bool column = false;  // the column form (filter_column.cu): tz = its CTA depth, tx = 32
 };
 
 size_t fast_smem_bytes(const FastConfig& c, const FastArgs& a);
 // mass = true: the weight-mass instantiation (training targets).
 cudaError_t launch_fast_kernel(const FastConfig& c, const CUtensorMap* tm_prev, const FastArgs& a,
                                int tiles_z, cudaStream_t st, bool mass = false);
+// The FP16 column form (filter_column.cu), patch radius 1.
+cudaError_t launch_column_fast_kernel(const FastConfig& c, const CUtensorMap* tm_prev, const FastArgs& a,
+                                      int tiles_z, cudaStream_t st);
 cudaError_t launch_pad_reflective_half(const float* in, int nx, int ny, int nz, void* out, int px,
                                        int py, int pz, long long pitch_y, long long pitch_z,
                                        cudaStream_t st);
