@@ -990,8 +990,9 @@ def main():
                     help="--workload profile: which small case (see run_profile_case)")
     ap.add_argument("--stream-depth", type=int, default=1024)
     ap.add_argument("--slab", type=int, default=64, help="stream2048: z-slab depth")
-    ap.add_argument("--stream-learned", default="896@4@r0.9",
-                    help="stream2048: the learned + FP16 form, k@tiles_per_plan[@min_mass|@rX]")
+    ap.add_argument("--stream-learned", default="512/512/512/1024@4@r0/0/0/0.9",
+                    help="stream2048: the learned + FP16 form, k@tiles_per_plan[@min_mass|@rX] "
+                         "(k and rX may be per-iteration schedules k1/k2/..., rX1/X2/...)")
     ap.add_argument("--learned-extra", default="",
                     help="extra learned + FP16 forms in the headline run, "
                          "k@tiles_per_plan[@min_mass[@precision]][,...]; min_mass rX: relative "
