@@ -603,14 +603,19 @@ def run_large_workload(args):
     learned1024: float32 1024x1024x512 grain pack (noise 0.05 blurred 1, no
       rings), patch r3 search r7 (1326 offsets), 4 iterations, global noise:
       the whole job in plain FP32, FP16 full search, and learned + FP16 forms
-      (--k-list k@tiles[@min_mass], default 896@4 and 256@1@0.95), PSNR
-      against the clean phantom over the whole volume for every form.
+      (--k-list k@tiles[@min_mass], default the schedule 256/256/256/1024 per
+      32x8x8 block with the relative fallback in the last iteration, 896 per
+      block throughout, and 256 per 8^3 tile with the absolute 0.95
+      threshold), PSNR against the clean phantom over the whole volume for
+      every form.
     stream2048: a 2048x2048xZ grain pack (Z = --stream-depth, 1024 for the
       17 GB configuration) with noise sigma drifting 0.02 -> 0.08 along z
       (blur 1) and rings of amplitude 0.03, z-adaptive noise, patch r3 search
       r7, 4 iterations, held in host memory and streamed through the GPU in
       z-slabs of --slab slices: the plain FP32 whole job and the learned +
-      FP16 whole job (--stream-learned k@tiles[@min_mass]), each with its own
+      FP16 whole job (--stream-learned k@tiles[@min_mass], default the schedule
+      512/512/512/1024 per block with the relative fallback in the last
+      iteration), each with its own
       noise estimates, PSNR against the clean phantom over the whole volume;
       then the learned form again with the plain job's sigma schedule held
       fixed (inlm_blocks_*, one iteration at a time), and the FP64
@@ -650,7 +655,7 @@ def run_large_workload(args):
                      "search_radius": 7, "offsets": 1326, "iterations": ITERS}
     if args.workload == "learned1024":
         forms = [("f32", "f32", None), ("fp16", "f16", None)]
-        for item in (args.k_list or "896@4,256@1@0.95").split(","):
+        for item in (args.k_list or "256/256/256/1024@4@r0/0/0/0.9,896@4@r0.9,256@1@0.95").split(","):
             k, tx, mm, rel = parse_learned(item)
             forms.append((f"learned_fp16_{item}", "f16", (k, mm, tx, rel)))
         ref_psnr = None
