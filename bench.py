@@ -33,7 +33,7 @@ offsets in iteration i, with full search for every block whose predicted
 kept weight mass is below LEARNED_REL[i] x the mean over the volume's blocks
 (small lists while later iterations re-filter the result, a larger list and
 the fallback in the last iteration, whose output carries the approximation);
-beside it the schedule 144 x 3, 240; one k throughout (k = 208 with the
+beside it the schedule 128 x 3, 240; one k throughout (k = 208 with the
 fallback at 0.9 in every iteration, k = 176 without), and k = 256 per 8^3
 tile with the absolute 0.95 threshold, which falls back on every tile of
 this volume. Each form reports its
@@ -77,7 +77,7 @@ BYTES_PER_VOXEL_ITER_F32 = 12                          # read raw + prev, write 
 # of LEARNED_K[i] offsets in iteration i, full search for the blocks whose
 # predicted kept mass is below LEARNED_REL[i] x the mean over the volume's
 # blocks (the last iteration's list and fallback set the accuracy)
-LEARNED_K, LEARNED_MIN_MASS, LEARNED_REL = (128, 128, 128, 240), 0.0, (0.0, 0.0, 0.0, 0.9)
+LEARNED_K, LEARNED_MIN_MASS, LEARNED_REL = (112, 112, 112, 256), 0.0, (0.0, 0.0, 0.0, 0.9)
 
 
 def log(*a):
@@ -306,7 +306,7 @@ def run_forms(vol, clean, sig_iters, value_f32, args, local, stream):
     net = ProposalNet.load(default_weights(PR, SR), device=local)
     forms = [("f32", "f32", None), ("f32_fused", "f32_fma", None), ("fp16", "f16", None),
              ("learned_fp16", "f16", (LEARNED_K, LEARNED_MIN_MASS, 4, LEARNED_REL)),
-             ("learned_fp16_sched144", "f16", ((144, 144, 144, 240), 0.0, 4, (0.0, 0.0, 0.0, 0.9))),
+             ("learned_fp16_sched128", "f16", ((128, 128, 128, 240), 0.0, 4, (0.0, 0.0, 0.0, 0.9))),
              ("learned_fp16_k208_r09", "f16", (208, 0.0, 4, 0.9)),
              ("learned_fp16_k176", "f16", (176, 0.0, 4, 0.0)),
              ("learned_fp16_k256_mass095", "f16", (256, 0.95, 1, 0.0))]
