@@ -491,7 +491,7 @@ def reference_gpu_rates(vol):
 
 
 def run_published_config(local, stream):
-    """This build's exact FP32 whole job on the configuration of the
+    """The exact FP32 whole job of this library on the configuration of the
     reference's only published GPU figure: 256^3, patch r1, search r10, 11
     slices (3102 offsets), 4 iterations, z-adaptive noise (the reference
     defaults), on a seeded 256^3 grain pack; device-timed and end to end from

@@ -491,7 +491,7 @@ public:
 namespace denoise {
 
 // The reference's CPU filter class (Denoiser/iternlm_cpu.h:30-157), which its
-// driver falls back to without a CUDA device. This build filters on the GPU
+// driver falls back to without a CUDA device. This library filters on the GPU
 // only: the members report an error and return the caller's buffer.
 class IterativeNLM_CPU {
 public:
@@ -515,7 +515,7 @@ public:
 private:
     float* unsupported(float* p) {
         status = INLM_ERR_UNSUPPORTED;
-        std::cout << "Error! This build has no CPU filter (it runs on CUDA devices only)" << std::endl;
+        std::cout << "Error! This library has no CPU filter (it runs on CUDA devices only)" << std::endl;
         return p;
     }
 };

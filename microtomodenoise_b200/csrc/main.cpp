@@ -163,7 +163,7 @@ int main(int argc, char* argv[]) {
         return -1;
     }
     if (params.gpu.n_gpus <= 0) {
-        cout << "Error! This build filters on the GPU only (-gpus 0 asks for the CPU filter)" << endl;
+        cout << "Error! This program filters on the GPU only (-gpus 0 asks for the CPU filter)" << endl;
         return -1;
     }
     if (gpulist.size() == 1) params.gpu.deviceID = gpulist[0];
@@ -235,7 +235,7 @@ int main(int argc, char* argv[]) {
     int n_parallelslices = n_devices > 0 ? gpu.configure_devices(shape, &params, ids) : -1;
     if (n_parallelslices == -2) return -2;
     if (n_parallelslices == -1) {
-        cout << "Error! No CUDA device found (this build has no CPU filter)" << endl;
+        cout << "Error! No CUDA device found (this program has no CPU filter)" << endl;
         return -1;
     }
     // -slab N below the stack depth: z-slab streaming on one device

@@ -203,7 +203,7 @@ def test_reference_driver_runs_on_this_library(gpu, port, stack):
     """The reference's own main.cpp, unmodified, compiled against this
     library's C++ shim (oracle/Makefile refdriver): its whole-stack GPU flow
     (configure_device, set_sigma, Run_GaussianNoise, get_result, the TIFF
-    saves) runs on this build, bit-exact against the oracle."""
+    saves) runs on this library, bit-exact against the oracle."""
     vol, tmp = stack
     out = tmp / "out"
     r = subprocess.run([REFDRIVER, "-i", str(tmp / "in"), "-o", str(out), "-iter", "2", "-search", "3",
