@@ -243,6 +243,7 @@ def test_512_cube_p2s5_sampled_voxels(gpu, port):
                                          ((2, 2, 2), (3, 3, 3), (20, 33, 47)),
                                          ((3, 3, 3), (2, 2, 2), (16, 40, 40)),
                                          ((2, 2, 1), (4, 4, 4), (24, 48, 48)),
+                                         ((1, 1, 2), (3, 3, 3), (20, 36, 40)),   # column form
                                          ((2, 2, 2), (7, 7, 7), (18, 40, 44))])  # raw slab
 def test_fused_form_tolerance(gpu, port, pr, sr, shape):
     """precision="f32_fma": the tiled kernel with fused multiply-adds, a

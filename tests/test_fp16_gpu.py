@@ -69,8 +69,9 @@ def test_fp16_form_vs_fp64_oracle(gpu, port, precision, pr, sr, shape):
 
 
 @pytest.mark.parametrize("precision", ["f16", "f16_df32"])
-@pytest.mark.parametrize("shape", [(12, 20, 40), (21, 27, 70)])
-def test_plan_with_every_offset_equals_full_search(gpu, shape, precision):
+@pytest.mark.parametrize("shape,pr", [((12, 20, 40), (1, 1, 1)), ((21, 27, 70), (1, 1, 1)),
+                                      ((19, 24, 40), (1, 1, 3))])
+def test_plan_with_every_offset_equals_full_search(gpu, shape, pr, precision):
     """Per-tile plans listing every offset (the one-tile-per-CTA kernel)
     equal the full search, which at patch radius 1 runs the column form:
     both round every voxel as the 32-wide tile kernel does (a 21-plane
@@ -78,12 +79,12 @@ def test_plan_with_every_offset_equals_full_search(gpu, shape, precision):
     vol = synth.small_case(shape, seed=2)
     sig = np.stack([np.full(shape[0], 0.06, np.float32),
                     np.linspace(0.04, 0.08, shape[0], dtype=np.float32)])
-    full, dfull = run(vol, (1, 1, 1), (2, 2, 2), sig, precision)
+    full, dfull = run(vol, pr, (2, 2, 2), sig, precision)
     assert dfull.startswith("nlm_column_fast"), dfull
     S = 32  # search radius 2 (nslices 11): 32 offsets
     n = int(np.prod(tile_grid(vol.shape)))
     plan = (np.arange(n) * S, np.full(n, S), np.tile(np.arange(S), n))
-    got, desc = run(vol, (1, 1, 1), (2, 2, 2), sig, precision, plan)
+    got, desc = run(vol, pr, (2, 2, 2), sig, precision, plan)
     assert "plan=per-tile" in desc and "tx=8" in desc
     # the one-tile-per-CTA kernel rounds every voxel as the full-search kernel does
     assert np.array_equal(got, full)
