@@ -224,7 +224,7 @@ class IterativeNLM_GPU:
         "column" (the column form, patch radius 1). Results do not change;
         returns describe()."""
         self._need()
-        code = {"auto": 0, "tile": 1, "column": 2}[form]
+        code = {"auto": 0, "tile": 1, "column": 2, "ws": 3}[form]
         _lib.check(_lib.load().inlm_select_tile_form(self._h, code), "select_tile_form")
         return self.describe()
 

@@ -611,7 +611,7 @@ static bool raw_slab_table(const Geometry& g, int szc, int tz, std::vector<int>*
     return true;
 }
 
-int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
+int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok, bool ws) {
     const Geometry& g = d->geo;
     const int* pr = g.patch_radius;
     *ok = false;
@@ -632,6 +632,10 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
         tz = column_kernel_depth(pr[0], pr[1], pr[2]);
         if (tz == 0) return INLM_OK;
         raw_smem = false;
+    }
+    if (ws) {  // the warp-specialised 8-deep kernel: raw box staged or read from global memory
+        if (fused || column) return INLM_OK;
+        tz = 8;
     }
     // tz 16: the two-planes-per-thread kernel (raw staged in shared memory)
     if (!column && !((tz == 8) || (tz == 4 && !raw_smem) || (tz == 16 && raw_smem))) return INLM_OK;
@@ -664,11 +668,12 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
     CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
     TileConfig tc{pr[0], pr[1], pr[2], tz, raw_smem, 0, fused};
     tc.column = column;
-    size_t sm = column ? column_smem_bytes(a) : tile_smem_bytes(tc, a);
+    tc.ws = ws;
+    size_t sm = column ? column_smem_bytes(a) : ws ? tile_ws_smem_bytes(tc, a) : tile_smem_bytes(tc, a);
     a.raw_slab = 0;
     a.group_zb = nullptr;
     std::vector<int> zb;
-    if (raw_smem && (tz == 8 || tz == 16) && (sm == 0 || sm > (size_t)smem_max) &&
+    if (raw_smem && !ws && (tz == 8 || tz == 16) && (sm == 0 || sm > (size_t)smem_max) &&
         raw_slab_table(g, a.szc, tz, &zb)) {
         // the whole raw box does not fit: stage TZ + 1 planes per z offset pair
         a.rbz = tz + 1;
@@ -716,17 +721,22 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok) {
 }
 
 // Default choice (before any autotuning): the first candidate that fits.
-// form: 0 every candidate, 1 the tiled kernels only, 2 the column form only.
+// form: 0 every candidate, 1 the tiled kernels only, 2 the column form only,
+// 3 the warp-specialised kernel only.
 static int choose_tile_config(inlm_denoiser* d, int form = 0) {
     d->use_tile = false;
     const struct {
         int tz;
         bool raw;
-    } cands[] = {{0, false}, {16, true}, {8, true}, {8, false}, {4, false}};
+        bool ws;
+    } cands[] = {{0, false, false}, {16, true, false}, {8, true, false}, {8, false, false},
+                 {4, false, false}, {8, true, true}, {8, false, true}};
     for (auto c : cands) {
-        if ((form == 1 && c.tz == 0) || (form == 2 && c.tz != 0)) continue;
+        if ((form == 1 && (c.tz == 0 || c.ws)) || (form == 2 && c.tz != 0) || (form == 3 && !c.ws) ||
+            (form == 0 && c.ws))
+            continue;
         bool ok = false;
-        int rc = tile_config_try(d, c.tz, c.raw, &ok);
+        int rc = tile_config_try(d, c.tz, c.raw, &ok, c.ws);
         if (rc) return rc;
         if (ok) return INLM_OK;
     }
@@ -1336,7 +1346,7 @@ extern "C" int inlm_filter_kernel_ms(inlm_denoiser* d, double* avg_ms, int* n_la
 
 extern "C" int inlm_select_tile_form(inlm_denoiser* d, int form) {
     if (!d) return fail(INLM_ERR_ARG, "null handle");
-    if (form < 0 || form > 2) return fail(INLM_ERR_ARG, "form must be 0, 1 or 2");
+    if (form < 0 || form > 3) return fail(INLM_ERR_ARG, "form must be 0, 1, 2 or 3");
     if (!d->use_tile) return fail(INLM_ERR_UNSUPPORTED, "the plain FP32 tiled kernels do not cover this configuration");
     CUDA_TRY(cudaSetDevice(d->device));
     CUDA_TRY(cudaStreamSynchronize(d->stream));
@@ -1366,7 +1376,8 @@ extern "C" int inlm_describe(inlm_denoiser* d, char* buf, size_t len) {
     else if (d->use_tile)
         snprintf(buf, len,
                  "nlm_%s_f32%s<%d,%d,%d> tz=%d raw_%s smem=%zu S=%zu P=%zu weights=%s pad=%d,%d,%d",
-                 d->tcfg.column ? "column" : "tile", d->tcfg.fused ? "_fused" : "", d->tcfg.rx, d->tcfg.ry, d->tcfg.rz, d->tcfg.tz,
+                 d->tcfg.column ? "column" : d->tcfg.ws ? "tile_ws" : "tile", d->tcfg.fused ? "_fused" : "",
+                 d->tcfg.rx, d->tcfg.ry, d->tcfg.rz, d->tcfg.tz,
                  d->tcfg.raw_smem ? (d->targs.raw_slab ? "slab" : "smem") : "global",
                  d->tcfg.smem_bytes, g.search.size(), g.taps.size(),
                  g.specialised && d->p.weight_table == INLM_WEIGHTS_CPU ? "cpu-table" : "distweight",

@@ -210,7 +210,7 @@ namespace inlm {
 void noise_free(inlm_noise* n);
 int launch_filter(inlm_denoiser* d);
 int check_device_error(inlm_denoiser* d);
-int tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok);
+int tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok, bool ws = false);
 int upload_sigma_device(inlm_denoiser* d);
 int pad_into(inlm_denoiser* d, const float* src, float* dst);
 int pad_into_half(inlm_denoiser* d, const float* src, void* dst);

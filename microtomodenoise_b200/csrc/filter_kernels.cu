@@ -624,6 +624,210 @@ __global__ void __launch_bounds__(256, 1)
     tile_f32_z2_body<RX, RY, RZ, SLAB>(&tm_prev, a, smem);
 }
 
+// ---- warp-specialised tile kernel ----
+//
+// The 8-deep tile kernel's two phases on different warps, so that the
+// squared differences of the next offsets are formed while the patch sums of
+// the current ones run: 4 producer warps write the D planes of NO offsets into
+// one of NSLOT slots (a ring of D buffers), 8 consumer warps (the lane map and
+// per-voxel arithmetic of tile_f32_body's phase B) read a slot, weight and
+// accumulate its offsets in reference order and release it. Raw is staged in
+// shared memory (RAW_SMEM: the raw box, one offset per slot, three slots) or
+// read from global memory as aligned float4s (two offsets per slot, two
+// slots). Full / empty mbarriers per slot, every wait bounded (on expiry the
+// CTA records DEV_TMA_TIMEOUT and its warps return; the other role's waits then
+// expire too). Bit-identical to the reference like tile_f32_body.
+template <int RX, int RY, int RZ, bool RAW_SMEM>
+__global__ void __launch_bounds__(384, 1)
+    nlm_tile_f32_ws_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
+    constexpr int TZ = 8;
+    using G = TileGeom<RX, RY, RZ, TZ>;
+    constexpr int NC = 256;  // consumer threads (phase B)
+    constexpr int NPR = 128;  // producer threads (phase A)
+    constexpr int NO = RAW_SMEM ? 1 : 2;     // offsets per slot
+    constexpr int NSLOT = RAW_SMEM ? 3 : 2;  // slots in the ring
+    constexpr int NP = kVoxPerThread / 2;
+    constexpr int DSZ = round_up32(G::DPLANE * G::DD);
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);  // prev box, full[NSLOT], empty[NSLOT]
+    uint64_t* full = bar + 1;
+    uint64_t* empty = bar + 1 + NSLOT;
+    float* prevb = reinterpret_cast<float*>(smem + 128);
+    const int pplane = a.pbx * a.pby;
+    const int PB = pplane * a.pbz;
+    float* rawb = prevb + round_up32(PB);
+    const int rpx = a.rbx + 1;
+    float* Dring = rawb + (RAW_SMEM ? round_up32(a.rplane * a.rbz) : 0);
+    const int tid = threadIdx.x;
+    const int X0 = blockIdx.x * kTX;
+    const int Y0 = blockIdx.y * kTY;
+    const int Z0 = blockIdx.z * TZ;
+    if (tid == 0) {
+        prefetch_tmap(&tm_prev);
+        mbar_init(&bar[0], 1);
+        for (int i = 0; i < NSLOT; i++) {
+            mbar_init(&full[i], NPR);
+            mbar_init(&empty[i], NC);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_arrive_expect_tx(&bar[0], (uint32_t)PB * 4u);
+        tma_load_3d(prevb, &tm_prev, X0, Y0, Z0, &bar[0]);
+    }
+    if (RAW_SMEM) {
+        // raw over tile + search halo, odd row pitch (as tile_f32_body), while
+        // the prev box arrives; the barrier below publishes it
+        const int rb_n = a.rbx * a.rby * a.rbz;
+        const float* rsrc = a.raw_pad + (long long)(Z0 + RZ) * a.gpitch_z + (long long)(Y0 + RY) * a.gpitch_y + X0;
+        for (int i = tid; i < rb_n; i += NC + NPR) {
+            int xx = i % a.rbx;
+            int rest = i / a.rbx;
+            int yy = rest % a.rby;
+            int zz = rest / a.rby;
+            rawb[zz * a.rplane + yy * rpx + xx] =
+                __ldg(rsrc + (long long)zz * a.gpitch_z + (long long)yy * a.gpitch_y + xx);
+        }
+    }
+    const bool arrived = mbar_wait_bounded(&bar[0], 0);
+    if (!__syncthreads_and(arrived)) {
+        if (tid == 0) set_error(a.err, DEV_TMA_TIMEOUT);
+        return;
+    }
+    const int npairs = (a.S + NO - 1) / NO;
+
+    if (tid >= NC) {
+        // ---- producers: D = (prev(. + s) - prev(.))^2 over tile + patch halo
+        const int pt = tid - NC;
+        constexpr int NPAIR = G::ND / 2;
+        constexpr int NQ = (NPAIR + NPR - 1) / NPR;
+        int qpi[NQ], qdi[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            int e = min(pt + q * NPR, NPAIR - 1);  // the tail repeats the last pair
+            int f = 2 * e;
+            int c = f % G::DW;
+            int rest = f / G::DW;
+            int r = rest % G::DH;
+            int pz = rest / G::DH;
+            qpi[q] = (pz - RZ + a.pz) * pplane + (r - RY + a.py) * a.pbx + (c - RX + a.px);
+            qdi[q] = pz * G::DPLANE + r * G::DP + c;
+        }
+        f32x2 qog[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) qog[q] = pack2(prevb[qpi[q]], prevb[qpi[q] + 1]);
+        for (int j = 0; j < npairs; j++) {
+            const int slot = j % NSLOT;
+            if (j >= NSLOT && !mbar_wait_bounded(&empty[slot], (j / NSLOT - 1) & 1)) {
+                set_error(a.err, DEV_TMA_TIMEOUT);
+                return;
+            }
+#pragma unroll
+            for (int o = 0; o < NO; o++) {
+                const int s = j * NO + o;
+                if (s < a.S) {
+                    const int dlx = __ldg(&a.search_delta[s]).x;
+                    float* Dw = Dring + (slot * NO + o) * DSZ;
+#pragma unroll
+                    for (int q = 0; q < NQ; q++) {
+                        f32x2 sh = pack2(prevb[qpi[q] + dlx], prevb[qpi[q] + dlx + 1]);
+                        f32x2 v = sub2(sh, qog[q]);
+                        *reinterpret_cast<f32x2*>(Dw + qdi[q]) = mul2_to_mul(v, v);  // stored, not added
+                    }
+                }
+            }
+            mbar_arrive(&full[slot]);
+        }
+        return;
+    }
+
+    // ---- consumers: patch sums, weights and sums (phase B of tile_f32_body)
+    const int warp = tid >> 5, lane = tid & 31;
+    const int k = 4 * (warp >> 2) + (lane >> 3);
+    const int j8 = lane & 7;
+    const int x0 = (warp & 3) * kVoxPerThread;
+    const int zk = min(Z0 + k, a.nz - 1);
+    const f32x2 m2 = splat2(a.mult[zk]);
+    const int rowoff = k * G::DPLANE + j8 * G::DP + x0;
+    const long long gbase = (long long)(Z0 + k + a.pz) * a.gpitch_z + (long long)(Y0 + j8 + a.py) * a.gpitch_y +
+                            (X0 + x0 + a.px);
+    const int rbase = RAW_SMEM ? (a.szc + k) * a.rplane + (a.syr + j8) * rpx + (RX + a.sxr + x0) : 0;
+    f32x2 acc[NP], wsum[NP];
+    float wmax[kVoxPerThread];
+#pragma unroll
+    for (int p = 0; p < NP; p++) acc[p] = wsum[p] = 0ull;  // (+0, +0)
+#pragma unroll
+    for (int r = 0; r < kVoxPerThread; r++) wmax[r] = 0.0f;
+    bool ok = true;
+    for (int j = 0; j < npairs; j++) {
+        const int slot = j % NSLOT;
+        if (!mbar_wait_bounded(&full[slot], (j / NSLOT) & 1)) {
+            set_error(a.err, DEV_TMA_TIMEOUT);
+            ok = false;
+            break;
+        }
+        const float* D0 = Dring + slot * NO * DSZ;
+        f32x2 d[NO][NP];
+        {
+            const int ro = rowoff + RZ * G::DPLANE + RY * G::DP;
+            const float w0 = a.w[0];
+#pragma unroll
+            for (int o = 0; o < NO; o++) {
+                float win[16];
+                load_window<RX / 4, (RX + kVoxPerThread - 1) / 4>(D0 + o * DSZ + ro, win);
+#pragma unroll
+                for (int p = 0; p < NP; p++) d[o][p] = mul_pair(win[RX + 2 * p], win[RX + 2 * p + 1], w0);
+            }
+        }
+        accumulate_rows_n<RX, RY, RZ, TZ, NO, 0, false>(D0, DSZ, rowoff, d, a);
+        // the slot's D planes are no longer read: hand it back before the weights
+        mbar_arrive(&empty[slot]);
+#pragma unroll
+        for (int o = 0; o < NO; o++) {
+            const int s = j * NO + o;
+            if (s < a.S) {
+                const int dly = __ldg(&a.search_delta[s]).y;
+                float rg[kVoxPerThread];
+                if (RAW_SMEM) {
+#pragma unroll
+                    for (int r = 0; r < kVoxPerThread; r++) rg[r] = rawb[rbase + dly + r];
+                } else {
+                    load8_global(a.raw_pad + gbase + dly, rg);
+                }
+#pragma unroll
+                for (int p = 0; p < NP; p++)
+                    exact_weight_pair(d[o][p], m2, make_float2(rg[2 * p], rg[2 * p + 1]), acc[p], wsum[p],
+                                      wmax[2 * p], wmax[2 * p + 1]);
+            }
+        }
+    }
+    if (!ok) return;
+    const int z = Z0 + k, y = Y0 + j8;
+    if (z < a.nz && y < a.ny) {
+        float* orow = a.out + ((long long)z * a.ny + y) * a.nx;
+#pragma unroll
+        for (int r = 0; r < kVoxPerThread; r++) {
+            const int x = X0 + x0 + r;
+            if (x < a.nx) {
+                const float raw0 = RAW_SMEM ? rawb[rbase + r] : __ldg(&a.raw_pad[gbase + r]);
+                const float2 acp = unpack2(acc[r / 2]), wsp = unpack2(wsum[r / 2]);
+                float ac = (r & 1) ? acp.y : acp.x;
+                float ws = (r & 1) ? wsp.y : wsp.x;
+                float res;
+                if (wmax[r] > 0.0f) {
+                    ac = __fadd_rn(ac, __fmul_rn(wmax[r], raw0));
+                    ws = __fadd_rn(ws, wmax[r]);
+                    res = __fdiv_rn(ac, ws);
+                } else {
+                    res = raw0;
+                }
+                orow[x] = res;
+            }
+        }
+    }
+}
+
 template <int RX, int RY, int RZ, int TZ, bool RAW_SMEM, bool FUSED, bool SLAB>
 __global__ void __launch_bounds__(32 * TZ, 1)
     nlm_tile_f32_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
@@ -880,10 +1084,42 @@ size_t tile_smem_bytes(const TileConfig& c, const TileArgs& a) {
     return 0;
 }
 
+size_t tile_ws_smem_bytes(const TileConfig& c, const TileArgs& a) {
+    // raw box and three single-offset buffers, or raw from global and two pairs
+#define X(A, B, C)                                                                  \
+    if (c.rx == A && c.ry == B && c.rz == C) {                                      \
+        using G = TileGeom<A, B, C, 8>;                                             \
+        const size_t rb = c.raw_smem ? round_up32(a.rplane * a.rbz) : 0;           \
+        return 128 + 4 * (round_up32(a.pbx * a.pby * a.pbz) + rb +                  \
+                          (c.raw_smem ? 3 : 4) * (size_t)round_up32(G::DPLANE * G::DD)); \
+    }
+    INLM_FOR_EACH_SHAPE(X)
+#undef X
+    return 0;
+}
+
+template <int RX, int RY, int RZ>
+static cudaError_t launch_ws(const CUtensorMap* tmp, const TileArgs& a, int tiles_z, size_t smem, bool raw_smem,
+                             cudaStream_t st) {
+    auto kern = raw_smem ? nlm_tile_f32_ws_kernel<RX, RY, RZ, true> : nlm_tile_f32_ws_kernel<RX, RY, RZ, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
+    kern<<<grid, 384, smem, st>>>(*tmp, a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,
                                const CUtensorMap* tm_raw, const TileArgs& a, int tiles_z,
                                cudaStream_t st) {
     if (c.column) return launch_column_kernel(c, tm_prev, a, tiles_z, st);
+    if (c.ws) {
+#define X(A, B, C) \
+        if (c.rx == A && c.ry == B && c.rz == C) return launch_ws<A, B, C>(tm_prev, a, tiles_z, c.smem_bytes, c.raw_smem, st);
+        INLM_FOR_EACH_SHAPE(X)
+#undef X
+        return cudaErrorInvalidConfiguration;
+    }
 #define X(A, B, C)                                                                             \
     if (c.rx == A && c.ry == B && c.rz == C) {                                                 \
         if (c.tz == 16 && c.raw_smem && !c.fused)                                              \

@@ -64,6 +64,7 @@ struct TileConfig {
                          // 8-deep tile kernel or the column form
     bool raw_slab = false;  // raw staged as TZ + 1 planes per z offset pair (raw_smem, tz 8 or 16)
     bool column = false;    // the column form (filter_column.cu): patch radius 1, raw from global
+    bool ws = false;        // warp-specialised 8-deep kernel (raw from global, a ring of D buffers)
 };
 
 // Returns false when no tiled instantiation exists for the patch shape.
@@ -76,6 +77,8 @@ cudaError_t launch_column_kernel(const TileConfig& c, const CUtensorMap* tm_prev
                                  int tiles_z, cudaStream_t st);
 // Shared-memory bytes for a configuration (0 if it cannot fit).
 size_t tile_smem_bytes(const TileConfig& c, const TileArgs& a);
+// Shared-memory bytes of the warp-specialised kernel (prev box and 4 D buffers).
+size_t tile_ws_smem_bytes(const TileConfig& c, const TileArgs& a);
 cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,
                                const CUtensorMap* tm_raw, const TileArgs& a, int tiles_z,
                                cudaStream_t st);
