@@ -722,22 +722,48 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok, boo
 
 // Default choice (before any autotuning): the first candidate that fits.
 // form: 0 every candidate, 1 the tiled kernels only, 2 the column form only,
-// 3 the warp-specialised kernel only.
+// 3 the warp-specialised kernel only. In form 0 the warp-specialised kernel
+// leads when patch sums dominate the work (at least 100 patch taps, or at
+// least 30 taps and 400 offsets). With fewer than 100 taps its raw-global
+// variant comes after the tiled kernels that stage the whole raw box (and
+// before those that restage raw slabs). Measured on B200 (256^3 launches):
+// faster at patch radius 2 with search radius 5 (5 %) and 7 (3 %, raw global
+// against the slab), at patch radius 3 with search radius 3 (8 %) and 4 (7 %,
+// raw global against the 8-deep raw box); slower at patch radius 2 with search
+// radius 3 and 4 (114 and 256 offsets, 4 %) and, reading raw from global
+// memory, at search radius 6 against the 8-deep kernel's raw box (7 %); the
+// column form leads at patch radius 1.
 static int choose_tile_config(inlm_denoiser* d, int form = 0) {
     d->use_tile = false;
-    const struct {
+    struct Cand {
         int tz;
         bool raw;
         bool ws;
-    } cands[] = {{0, false, false}, {16, true, false}, {8, true, false}, {8, false, false},
-                 {4, false, false}, {8, true, true}, {8, false, true}};
-    for (auto c : cands) {
+        bool box_only;  // accept only with the whole raw box staged (no slab)
+    };
+    const int P = (int)d->geo.taps.size(), S = (int)d->geo.search.size();
+    const bool ws_first = form == 0 && (P >= 100 || (P >= 30 && S >= 400));
+    const Cand base[] = {{0, false, false, false}, {16, true, false, false}, {8, true, false, false},
+                         {8, false, false, false}, {4, false, false, false}, {8, true, true, false},
+                         {8, false, true, false}};
+    const Cand lead[] = {{0, false, false, false}, {8, true, true, true},   {16, true, false, true},
+                         {8, true, false, true},   {8, false, true, false}, {16, true, false, false},
+                         {8, true, false, false},  {8, false, false, false}, {4, false, false, false}};
+    const Cand* cands = ws_first ? lead : base;
+    const int n = ws_first ? 9 : 7;
+    for (int i = 0; i < n; i++) {
+        const Cand c = cands[i];
+        if (c.box_only && P >= 100) continue;  // many taps: the raw-global variant first
         if ((form == 1 && (c.tz == 0 || c.ws)) || (form == 2 && c.tz != 0) || (form == 3 && !c.ws) ||
-            (form == 0 && c.ws))
+            (form == 0 && c.ws && !ws_first))
             continue;
         bool ok = false;
         int rc = tile_config_try(d, c.tz, c.raw, &ok, c.ws);
         if (rc) return rc;
+        if (ok && c.box_only && d->tcfg.raw_slab) {
+            d->use_tile = false;
+            continue;
+        }
         if (ok) return INLM_OK;
     }
     return INLM_OK;

@@ -36,6 +36,7 @@ static_assert(sizeof(TuneKey) == 8 * sizeof(int), "TuneKey is eight ints");
 struct TuneResult {
     int tz = 8;
     bool raw_smem = true;
+    bool ws = false;  // the warp-specialised 8-deep kernel
     std::string report;
 };
 
@@ -69,7 +70,8 @@ void load_cache_locked() {
                        &k.sr[1], &k.sr[2], &k.nslices, &k.batch, &tz, &raw) == 10) {
         TuneResult r;
         r.tz = tz;
-        r.raw_smem = raw != 0;
+        r.raw_smem = (raw & 1) != 0;  // bit 0: raw staged, bit 1: warp-specialised
+        r.ws = (raw & 2) != 0;
         r.report = "cached";
         g_tune[k] = r;
     }
@@ -84,14 +86,15 @@ void save_cache_locked() {
     for (auto& kv : g_tune)
         std::fprintf(f, "%d %d %d %d %d %d %d %d %d %d\n", kv.first.pr[0], kv.first.pr[1],
                      kv.first.pr[2], kv.first.sr[0], kv.first.sr[1], kv.first.sr[2], kv.first.nslices,
-                     kv.first.batch, kv.second.tz, kv.second.raw_smem ? 1 : 0);
+                     kv.first.batch, kv.second.tz, (kv.second.raw_smem ? 1 : 0) | (kv.second.ws ? 2 : 0));
     std::fclose(f);
 }
 
 // Times every tiled configuration of a parameter class on a probe volume of
 // 128 x 128 x 64 voxels (several CTA waves on 148 SMs; the kernel's work does
 // not depend on the data) and returns the fastest. batch = true restricts the
-// candidates to the CTA depth the persistent batch kernel runs (tz 8).
+// candidates to the CTA depth the persistent batch kernel runs (tz 8, not the
+// warp-specialised kernel).
 int tune_class(const inlm_params& p0, bool batch, TuneResult* out) {
     inlm_params p = p0;
     p.precision = INLM_PRECISION_F32;
@@ -103,9 +106,11 @@ int tune_class(const inlm_params& p0, bool batch, TuneResult* out) {
     struct Cand {
         int tz;
         bool raw;
+        bool ws;
     };
-    // tz 0: the column form (patch radius 1)
-    const Cand cands[] = {{0, false}, {16, true}, {8, true}, {8, false}, {4, false}};
+    // tz 0: the column form (patch radius 1); ws: the warp-specialised kernel
+    const Cand cands[] = {{0, false, false}, {16, true, false}, {8, true, false}, {8, false, false},
+                          {4, false, false}, {8, true, true},   {8, false, true}};
     double best = 1e30;
     TuneResult res;
     bool any = false;
@@ -125,9 +130,9 @@ int tune_class(const inlm_params& p0, bool batch, TuneResult* out) {
     rc = upload_sigma_device(d);
     if (rc) return cleanup(rc);
     for (const Cand& c : cands) {
-        if (batch && c.tz != 8) continue;
+        if (batch && (c.tz != 8 || c.ws)) continue;
         bool ok = false;
-        rc = tile_config_try(d, c.tz, c.raw, &ok);
+        rc = tile_config_try(d, c.tz, c.raw, &ok, c.ws);
         if (rc) return cleanup(rc);
         if (!ok) continue;
         const int tiles_z = (shape[2] + d->tcfg.tz - 1) / d->tcfg.tz;
@@ -143,20 +148,22 @@ int tune_class(const inlm_params& p0, bool batch, TuneResult* out) {
             return cleanup(fail(INLM_ERR_CUDA, "autotune timing failed"));
         cudaEventElapsedTime(&ms, e0, e1);
         ms *= 0.5f;
-        std::snprintf(line, sizeof line, "tz=%d raw_%s: %.3f ms; ", c.tz, c.raw ? "smem" : "global",
-                      ms);
+        std::snprintf(line, sizeof line, "tz=%d%s raw_%s: %.3f ms; ", c.tz, c.ws ? " ws" : "",
+                      c.raw ? "smem" : "global", ms);
         res.report += line;
         if (ms < best) {
             best = ms;
             res.tz = c.tz;
             res.raw_smem = c.raw;
+            res.ws = c.ws;
             any = true;
         }
     }
     rc = check_device_error(d);
     if (rc) return cleanup(rc);
     if (!any) return cleanup(fail(INLM_ERR_UNSUPPORTED, "no tiled configuration for this class"));
-    std::snprintf(line, sizeof line, "chosen tz=%d raw_%s", res.tz, res.raw_smem ? "smem" : "global");
+    std::snprintf(line, sizeof line, "chosen tz=%d%s raw_%s", res.tz, res.ws ? " ws" : "",
+                  res.raw_smem ? "smem" : "global");
     res.report += line;
     *out = res;
     return cleanup(INLM_OK);
@@ -194,7 +201,7 @@ extern "C" int inlm_autotune(inlm_denoiser* d, char* report, size_t len) {
     int rc = tuned_config(d->p, false, &r);
     if (rc) return rc;
     bool ok = false;
-    rc = tile_config_try(d, r.tz, r.raw_smem, &ok);
+    rc = tile_config_try(d, r.tz, r.raw_smem, &ok, r.ws);
     if (rc) return rc;
     if (!ok) return fail(INLM_ERR_STATE, "tuned configuration does not fit this volume");
     if (report && len) std::snprintf(report, len, "%s", r.report.c_str());
@@ -410,11 +417,11 @@ extern "C" int inlm_batch_create(int n, const int* shapes, const inlm_params* pa
             rc = estimate_into(d, b->in[v], d->d_sigma0, nullptr);
             if (rc) return bail(rc);
         }
-        // A volume whose own configuration is the column form or the 16-deep
-        // CTA (faster than the persistent depth-8 body) and which fills the
-        // GPU by itself (>= 4 waves of CTAs) keeps it and runs its own launch
-        // beside the persistent groups.
-        if (d->use_tile && (d->tcfg.column || d->tcfg.tz == 16)) {
+        // A volume whose own configuration is the column form, the 16-deep
+        // CTA or the warp-specialised kernel (faster than the persistent
+        // depth-8 body) and which fills the GPU by itself (>= 4 waves of CTAs)
+        // keeps it and runs its own launch beside the persistent groups.
+        if (d->use_tile && (d->tcfg.column || d->tcfg.tz == 16 || d->tcfg.ws)) {
             const long long ctas = (long long)d->targs.tiles_x * d->targs.tiles_y *
                                    ((d->shape[2] + d->tcfg.tz - 1) / d->tcfg.tz);
             if (ctas >= 4LL * sms_dev) continue;  // kind stays -1
@@ -425,7 +432,7 @@ extern "C" int inlm_batch_create(int n, const int* shapes, const inlm_params* pa
             rc = tuned_config(d->p, true, &r);
             if (rc == INLM_OK) {
                 bool ok = false;
-                rc = tile_config_try(d, r.tz, r.raw_smem, &ok);
+                rc = tile_config_try(d, r.tz, r.raw_smem, &ok, r.ws);
                 if (rc) return bail(rc);
                 char line[256];
                 std::snprintf(line, sizeof line, "[p%d%d%d s%d%d%d] %s\n", d->p.patch_radius[0],
@@ -603,7 +610,10 @@ extern "C" int inlm_batch_describe(inlm_batch* b, char* buf, size_t len) {
                       d->p.search_radius[1], d->p.search_radius[2], d->geo.search.size(),
                       d->geo.taps.size(), b->kind[v] >= 0 ? "batched " : "own launch ",
                       b->kind[v] >= 0 ? kinds[b->kind[v]]
-                                      : (d->use_tile ? (d->tcfg.column ? "column" : d->tcfg.tz == 16 ? "tile tz=16" : "tile")
+                                      : (d->use_tile ? (d->tcfg.column ? "column"
+                                                        : d->tcfg.ws      ? "tile ws"
+                                                        : d->tcfg.tz == 16 ? "tile tz=16"
+                                                                           : "tile")
                                                      : "generic"));
         s += line;
     }

@@ -53,7 +53,33 @@ def test_filter_bit_exact_vs_reference_golden(gpu, golden_filter, case):
         pytest.fail(f"{name} [{desc}]: {np.count_nonzero(d)} voxels differ, max {d.max():.3g}")
     spec = name.split("_")[0] in ("p111", "p112", "p113", "p221", "p222", "p331", "p332", "p333")
     if spec and nsl // 2 >= pr[2]:
-        assert desc.startswith(("nlm_tile_f32", "nlm_column_f32")), desc
+        assert desc.startswith(("nlm_tile_f32", "nlm_tile_ws_f32", "nlm_column_f32")), desc
+
+
+@pytest.mark.parametrize("shape,pr,sr", [
+    ((9, 19, 41), (2, 2, 2), (3, 4, 2)),
+    ((13, 9, 70), (2, 2, 1), (5, 5, 5)),
+    ((17, 23, 37), (3, 3, 3), (3, 3, 3)),
+    ((20, 40, 48), (2, 2, 2), (5, 5, 5)),
+    ((11, 17, 33), (1, 1, 1), (5, 5, 5)),
+    ((24, 33, 40), (2, 2, 2), (7, 7, 7)),   # raw box too large: raw from global memory
+    ((18, 30, 45), (3, 3, 3), (4, 4, 4)),   # raw from global memory at patch radius 3
+])
+def test_warp_specialised_form_bit_exact(gpu, port, shape, pr, sr):
+    """The warp-specialised kernel (producer warps form the squared
+    differences into a ring of shared-memory buffers, consumer warps the patch
+    sums, weights and sums; mbarrier hand-off) equals the oracle bit for bit
+    over two iterations, with the raw box staged and with raw read from global
+    memory, at odd sizes and partial tiles."""
+    raw = synth.small_case(shape, seed=sum(shape))
+    sig = np.stack([np.full(shape[0], 0.07, np.float32),
+                    np.linspace(0.03, 0.08, shape[0], dtype=np.float32)])
+    got, desc = run_gpu(raw, pr, sr, sig, form="ws")
+    assert desc.startswith("nlm_tile_ws_f32"), desc
+    want = port.denoise_f32(raw, FilterParams(search_radius=sr, patch_radius=pr), sig, all_iters=True)
+    if not np.array_equal(got, want):
+        d = np.abs(got - want)
+        pytest.fail(f"[{desc}]: {np.count_nonzero(d)} voxels differ, max {d.max():.3g}")
 
 
 @pytest.mark.parametrize("shape,pr,sr", [
