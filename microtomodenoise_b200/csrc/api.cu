@@ -753,7 +753,7 @@ static int choose_tile_config(inlm_denoiser* d, int form = 0) {
     const int n = ws_first ? 9 : 7;
     for (int i = 0; i < n; i++) {
         const Cand c = cands[i];
-        if (c.box_only && P >= 100) continue;  // many taps: the raw-global variant first
+        if (c.box_only && !c.ws && P >= 100) continue;  // many taps: the raw-global variant first
         if ((form == 1 && (c.tz == 0 || c.ws)) || (form == 2 && c.tz != 0) || (form == 3 && !c.ws) ||
             (form == 0 && c.ws && !ws_first))
             continue;

@@ -729,11 +729,22 @@ __global__ void __launch_bounds__(384, 1)
                 if (s < a.S) {
                     const int dlx = __ldg(&a.search_delta[s]).x;
                     float* Dw = Dring + (slot * NO + o) * DSZ;
+                    // every pair index has the parity of px - RX (box pitches
+                    // are even): an 8-byte aligned shifted pair is one load
+                    if (((a.px - RX + dlx) & 1) == 0) {
 #pragma unroll
-                    for (int q = 0; q < NQ; q++) {
-                        f32x2 sh = pack2(prevb[qpi[q] + dlx], prevb[qpi[q] + dlx + 1]);
-                        f32x2 v = sub2(sh, qog[q]);
-                        *reinterpret_cast<f32x2*>(Dw + qdi[q]) = mul2_to_mul(v, v);  // stored, not added
+                        for (int q = 0; q < NQ; q++) {
+                            f32x2 sh = *reinterpret_cast<const f32x2*>(prevb + qpi[q] + dlx);
+                            f32x2 v = sub2(sh, qog[q]);
+                            *reinterpret_cast<f32x2*>(Dw + qdi[q]) = mul2_to_mul(v, v);  // stored, not added
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < NQ; q++) {
+                            f32x2 sh = pack2(prevb[qpi[q] + dlx], prevb[qpi[q] + dlx + 1]);
+                            f32x2 v = sub2(sh, qog[q]);
+                            *reinterpret_cast<f32x2*>(Dw + qdi[q]) = mul2_to_mul(v, v);
+                        }
                     }
                 }
             }
