@@ -336,15 +336,19 @@ int inlm_net_input(inlm_denoiser* d, float* vol_dev, float* scale_dev);
 
 /* Restricts the plain FP32 filter to one kernel family and picks its first
  * configuration that fits: form 0 = automatic (the column form for patch
- * radius 1 when it fits, else the tiled kernels), 1 = the tiled kernels only,
- * 2 = the column form only (INLM_ERR_UNSUPPORTED where it has no
- * instantiation or does not fit). Results do not change: every form rounds
- * each voxel identically. Call between iterations, not while one runs. */
+ * radius 1 when it fits; the warp-specialised kernel where patch sums
+ * dominate, at 100 or more patch taps or at 30 or more taps with 400 or more
+ * search offsets; else the tiled kernels), 1 = the tiled kernels without warp
+ * specialisation, 2 = the column form only, 3 = the warp-specialised kernel
+ * only (INLM_ERR_UNSUPPORTED where the form has no instantiation or does not
+ * fit). Results do not change: every form rounds each voxel identically. Call
+ * between iterations, not while one runs. */
 int inlm_select_tile_form(inlm_denoiser* d, int form);
 
 /* Times the tiled FP32 kernel's configurations (the column form at patch
  * radius 1, CTA depth 16 with two planes per thread, CTA depth 8 with raw
- * staged in shared memory or read from global memory, depth 4) on a
+ * staged in shared memory or read from global memory, depth 4, the
+ * warp-specialised kernel with raw staged or from global memory) on a
  * 128x128x64 probe
  * of d's patch/search class, applies the fastest to d and caches the choice
  * per process (and in the file named by the INLM_AUTOTUNE_CACHE environment

@@ -220,9 +220,10 @@ class IterativeNLM_GPU:
         return buf.value.decode()
 
     def select_tile_form(self, form: str = "auto") -> str:
-        """Plain FP32 kernel family: "auto", "tile" (the tiled kernels only) or
-        "column" (the column form, patch radius 1). Results do not change;
-        returns describe()."""
+        """Plain FP32 kernel family: "auto", "tile" (the tiled kernels without
+        warp specialisation), "column" (the column form, patch radius 1) or
+        "ws" (the warp-specialised kernel). Results do not change; returns
+        describe()."""
         self._need()
         code = {"auto": 0, "tile": 1, "column": 2, "ws": 3}[form]
         _lib.check(_lib.load().inlm_select_tile_form(self._h, code), "select_tile_form")
