@@ -164,7 +164,7 @@ def measured_peaks():
 # is the tiles' halo boxes and the result, so it grows with the tile count.
 FILTER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one 512x512x128 launch of "
                          "nlm_tile_f32_ws_kernel, x4")
-FILTER_TRAFFIC_BYTES_PER_LAUNCH = 4 * (333.644e6 + 123.801e6)
+FILTER_TRAFFIC_BYTES_PER_LAUNCH = 4 * (335.120e6 + 124.091e6)
 
 
 def fp32_arithmetic_peak(device: int):
