@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(256, 1)
 //
 // The 8-deep tile kernel's two phases on different warps, so that the
 // squared differences of the next offsets are formed while the patch sums of
-// the current ones run: 4 producer warps write the D planes of NO offsets into
+// the current ones run: producer warps write the D planes of NO offsets into
 // one of NSLOT slots (a ring of D buffers), 8 consumer warps (the lane map and
 // per-voxel arithmetic of tile_f32_body's phase B) read a slot, weight and
 // accumulate its offsets in reference order and release it. Raw is staged in
@@ -637,13 +637,23 @@ __global__ void __launch_bounds__(256, 1)
 // slots). Full / empty mbarriers per slot, every wait bounded (on expiry the
 // CTA records DEV_TMA_TIMEOUT and its warps return; the other role's waits then
 // expire too). Bit-identical to the reference like tile_f32_body.
+//
+// Producer warps: 8 at patch radius 1 and 2 (measured 6 % faster than 4 at
+// p2 s5 and s7, where the consumers waited on the ring), 4 at radius 3 (8
+// would cap the larger consumer bodies at 128 registers: measured 2 % slower).
+template <int RX>
+struct WsThreads {
+    static constexpr int NPR = RX >= 3 ? 128 : 256;  // producer threads
+    static constexpr int N = 256 + NPR;
+};
+
 template <int RX, int RY, int RZ, bool RAW_SMEM>
-__global__ void __launch_bounds__(384, 1)
+__global__ void __launch_bounds__(WsThreads<RX>::N, 1)
     nlm_tile_f32_ws_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
     constexpr int TZ = 8;
     using G = TileGeom<RX, RY, RZ, TZ>;
     constexpr int NC = 256;  // consumer threads (phase B)
-    constexpr int NPR = 128;  // producer threads (phase A)
+    constexpr int NPR = WsThreads<RX>::NPR;  // producer threads (phase A)
     constexpr int NO = RAW_SMEM ? 1 : 2;     // offsets per slot
     constexpr int NSLOT = RAW_SMEM ? 3 : 2;  // slots in the ring
     constexpr int NP = kVoxPerThread / 2;
@@ -1116,7 +1126,7 @@ static cudaError_t launch_ws(const CUtensorMap* tmp, const TileArgs& a, int tile
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
-    kern<<<grid, 384, smem, st>>>(*tmp, a);
+    kern<<<grid, WsThreads<RX>::N, smem, st>>>(*tmp, a);
     return cudaGetLastError();
 }
 
