@@ -157,14 +157,14 @@ def measured_peaks():
 
 
 # DRAM traffic of one 512^3 launch of the headline filter kernel
-# (nlm_tile_f32_ws_kernel<2,2,2,raw box>: 32x8x8 CTAs of 8 consumer and 4
+# (nlm_tile_f32_ws_kernel<2,2,2,raw box>: 32x8x8 CTAs of 8 consumer and 8
 # producer warps, raw box staged): dram__bytes_read.sum +
 # dram__bytes_write.sum of one 512x512x128 launch captured by ncu
 # (profiles/nlm_tile_f32_p2s5_512.md gives the command), times 4: the traffic
 # is the tiles' halo boxes and the result, so it grows with the tile count.
 FILTER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one 512x512x128 launch of "
                          "nlm_tile_f32_ws_kernel, x4")
-FILTER_TRAFFIC_BYTES_PER_LAUNCH = 4 * (335.120e6 + 124.091e6)
+FILTER_TRAFFIC_BYTES_PER_LAUNCH = 4 * (338.045e6 + 125.709e6)
 
 
 def fp32_arithmetic_peak(device: int):
