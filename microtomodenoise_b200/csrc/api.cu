@@ -634,7 +634,7 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok, boo
         raw_smem = false;
     }
     if (ws) {  // the warp-specialised 8-deep kernel: raw box staged or read from global memory
-        if (fused || column) return INLM_OK;
+        if (column) return INLM_OK;
         tz = 8;
     }
     // tz 16: the two-planes-per-thread kernel (raw staged in shared memory)
@@ -732,7 +732,11 @@ int inlm::tile_config_try(inlm_denoiser* d, int tz, bool raw_smem, bool* ok, boo
 // raw global against the 8-deep raw box); slower at patch radius 2 with search
 // radius 3 and 4 (114 and 256 offsets, 4 %) and, reading raw from global
 // memory, at search radius 6 against the 8-deep kernel's raw box (7 %); the
-// column form leads at patch radius 1.
+// column form leads at patch radius 1. The fused FP32 form takes the
+// warp-specialised kernel only with the raw box and fewer than 100 taps:
+// measured 7 % faster at patch radius 2 / search radius 5, but 9 % slower
+// reading raw from global memory (search radius 7, against the raw slab) and
+// 2 % slower at patch radius 3 / search radius 3.
 static int choose_tile_config(inlm_denoiser* d, int form = 0) {
     d->use_tile = false;
     struct Cand {
@@ -742,7 +746,9 @@ static int choose_tile_config(inlm_denoiser* d, int form = 0) {
         bool box_only;  // accept only with the whole raw box staged (no slab)
     };
     const int P = (int)d->geo.taps.size(), S = (int)d->geo.search.size();
-    const bool ws_first = form == 0 && (P >= 100 || (P >= 30 && S >= 400));
+    const bool fused = d->p.precision == INLM_PRECISION_F32_FMA;
+    const bool ws_first =
+        form == 0 && (fused ? (P >= 30 && P < 100 && S >= 400) : (P >= 100 || (P >= 30 && S >= 400)));
     const Cand base[] = {{0, false, false, false}, {16, true, false, false}, {8, true, false, false},
                          {8, false, false, false}, {4, false, false, false}, {8, true, true, false},
                          {8, false, true, false}};
@@ -754,6 +760,7 @@ static int choose_tile_config(inlm_denoiser* d, int form = 0) {
     for (int i = 0; i < n; i++) {
         const Cand c = cands[i];
         if (c.box_only && !c.ws && P >= 100) continue;  // many taps: the raw-global variant first
+        if (form == 0 && fused && c.ws && !c.raw) continue;
         if ((form == 1 && (c.tz == 0 || c.ws)) || (form == 2 && c.tz != 0) || (form == 3 && !c.ws) ||
             (form == 0 && c.ws && !ws_first))
             continue;

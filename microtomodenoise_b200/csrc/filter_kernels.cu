@@ -636,7 +636,9 @@ __global__ void __launch_bounds__(256, 1)
 // read from global memory as aligned float4s (two offsets per slot, two
 // slots). Full / empty mbarriers per slot, every wait bounded (on expiry the
 // CTA records DEV_TMA_TIMEOUT and its warps return; the other role's waits then
-// expire too). Bit-identical to the reference like tile_f32_body.
+// expire too). Bit-identical to the reference like tile_f32_body; FUSED: the
+// fused FP32 form's taps and weights (as tile_f32_body's FUSED form, whose
+// results it equals bit for bit).
 //
 // Producer warps: 8 at patch radius 1 and 2 (measured 6 % faster than 4 at
 // p2 s5 and s7, where the consumers waited on the ring), 4 at radius 3 (8
@@ -647,7 +649,7 @@ struct WsThreads {
     static constexpr int N = 256 + NPR;
 };
 
-template <int RX, int RY, int RZ, bool RAW_SMEM>
+template <int RX, int RY, int RZ, bool RAW_SMEM, bool FUSED>
 __global__ void __launch_bounds__(WsThreads<RX>::N, 1)
     nlm_tile_f32_ws_kernel(const __grid_constant__ CUtensorMap tm_prev, const __grid_constant__ TileArgs a) {
     constexpr int TZ = 8;
@@ -801,7 +803,7 @@ __global__ void __launch_bounds__(WsThreads<RX>::N, 1)
                 for (int p = 0; p < NP; p++) d[o][p] = mul_pair(win[RX + 2 * p], win[RX + 2 * p + 1], w0);
             }
         }
-        accumulate_rows_n<RX, RY, RZ, TZ, NO, 0, false>(D0, DSZ, rowoff, d, a);
+        accumulate_rows_n<RX, RY, RZ, TZ, NO, 0, FUSED>(D0, DSZ, rowoff, d, a);
         // the slot's D planes are no longer read: hand it back before the weights
         mbar_arrive(&empty[slot]);
 #pragma unroll
@@ -817,9 +819,14 @@ __global__ void __launch_bounds__(WsThreads<RX>::N, 1)
                     load8_global(a.raw_pad + gbase + dly, rg);
                 }
 #pragma unroll
-                for (int p = 0; p < NP; p++)
-                    exact_weight_pair(d[o][p], m2, make_float2(rg[2 * p], rg[2 * p + 1]), acc[p], wsum[p],
-                                      wmax[2 * p], wmax[2 * p + 1]);
+                for (int p = 0; p < NP; p++) {
+                    if (FUSED)
+                        fused_weight_pair(d[o][p], m2, make_float2(rg[2 * p], rg[2 * p + 1]), acc[p], wsum[p],
+                                          wmax[2 * p], wmax[2 * p + 1]);
+                    else
+                        exact_weight_pair(d[o][p], m2, make_float2(rg[2 * p], rg[2 * p + 1]), acc[p], wsum[p],
+                                          wmax[2 * p], wmax[2 * p + 1]);
+                }
             }
         }
     }
@@ -1121,8 +1128,11 @@ size_t tile_ws_smem_bytes(const TileConfig& c, const TileArgs& a) {
 
 template <int RX, int RY, int RZ>
 static cudaError_t launch_ws(const CUtensorMap* tmp, const TileArgs& a, int tiles_z, size_t smem, bool raw_smem,
-                             cudaStream_t st) {
-    auto kern = raw_smem ? nlm_tile_f32_ws_kernel<RX, RY, RZ, true> : nlm_tile_f32_ws_kernel<RX, RY, RZ, false>;
+                             bool fused, cudaStream_t st) {
+    auto kern = fused ? (raw_smem ? nlm_tile_f32_ws_kernel<RX, RY, RZ, true, true>
+                                  : nlm_tile_f32_ws_kernel<RX, RY, RZ, false, true>)
+                      : (raw_smem ? nlm_tile_f32_ws_kernel<RX, RY, RZ, true, false>
+                                  : nlm_tile_f32_ws_kernel<RX, RY, RZ, false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(a.tiles_x, a.tiles_y, tiles_z);
@@ -1136,7 +1146,8 @@ cudaError_t launch_tile_kernel(const TileConfig& c, const CUtensorMap* tm_prev,
     if (c.column) return launch_column_kernel(c, tm_prev, a, tiles_z, st);
     if (c.ws) {
 #define X(A, B, C) \
-        if (c.rx == A && c.ry == B && c.rz == C) return launch_ws<A, B, C>(tm_prev, a, tiles_z, c.smem_bytes, c.raw_smem, st);
+        if (c.rx == A && c.ry == B && c.rz == C)                                                      \
+            return launch_ws<A, B, C>(tm_prev, a, tiles_z, c.smem_bytes, c.raw_smem, c.fused, st);
         INLM_FOR_EACH_SHAPE(X)
 #undef X
         return cudaErrorInvalidConfiguration;

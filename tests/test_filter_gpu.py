@@ -270,7 +270,7 @@ def test_512_cube_p2s5_sampled_voxels(gpu, port):
                                          ((3, 3, 3), (2, 2, 2), (16, 40, 40)),
                                          ((2, 2, 1), (4, 4, 4), (24, 48, 48)),
                                          ((1, 1, 2), (3, 3, 3), (20, 36, 40)),   # column form
-                                         ((2, 2, 2), (7, 7, 7), (18, 40, 44))])  # raw slab
+                                         ((2, 2, 2), (7, 7, 7), (18, 40, 44))])  # search radius 7
 def test_fused_form_tolerance(gpu, port, pr, sr, shape):
     """precision="f32_fma": the tiled kernel with fused multiply-adds, a
     Horner Pade and a fast division. Tolerance, written here: relative error
@@ -293,3 +293,32 @@ def test_fused_form_tolerance(gpu, port, pr, sr, shape):
     rel = np.abs(got.astype(np.float64) - want) / np.maximum(np.abs(want.astype(np.float64)), 1e-6)
     assert float((rel > 1e-4).mean()) <= 1e-4, rel.max()
     assert float(np.median(rel)) <= 1e-5
+
+
+@pytest.mark.parametrize("shape,pr,sr", [
+    ((20, 40, 48), (2, 2, 2), (5, 5, 5)),   # raw box staged
+    ((18, 33, 45), (2, 2, 2), (7, 7, 7)),   # raw from global memory
+    ((17, 23, 37), (3, 3, 3), (3, 3, 3)),
+])
+def test_fused_warp_specialised_equals_fused_tile(gpu, shape, pr, sr):
+    """The fused FP32 form on the warp-specialised kernel performs the fused
+    tile kernel's operations per voxel in the same order: equal bit for bit
+    over two iterations (and so within the fused form's tolerance above)."""
+    vol = synth.small_case(shape, seed=sum(shape) + 7)
+    sig = np.stack([np.full(shape[0], 0.06, np.float32),
+                    np.linspace(0.03, 0.08, shape[0], dtype=np.float32)])
+    outs = {}
+    for form in ("ws", "tile"):
+        g = IterativeNLM_GPU()
+        g.configure_device(shape, DenoiseParameters(radius_patchspace=pr, radius_searchspace=sr,
+                                                    precision="f32_fma"))
+        desc = g.select_tile_form(form)
+        assert "fused" in desc and (desc.startswith("nlm_tile_ws_f32") == (form == "ws")), desc
+        res = []
+        for it in range(2):
+            g.set_sigma(sig[it])
+            g.Run_GaussianNoise(it + 1, vol if it == 0 else None)
+            res.append(g.get_result())
+        g.free_device()
+        outs[form] = np.stack(res)
+    assert np.array_equal(outs["ws"], outs["tile"])
