@@ -160,7 +160,7 @@ def measured_peaks():
 # (nlm_tile_f32_ws_kernel<2,2,2,raw box>: 32x8x8 CTAs of 8 consumer and 8
 # producer warps, raw box staged): dram__bytes_read.sum +
 # dram__bytes_write.sum of one 512x512x128 launch captured by ncu
-# (profiles/nlm_tile_f32_p2s5_512.md gives the command), times 4: the traffic
+# (profiles/nlm_tile_f32_ws_p2s5_512.md gives the command), times 4: the traffic
 # is the tiles' halo boxes and the result, so it grows with the tile count.
 FILTER_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one 512x512x128 launch of "
                          "nlm_tile_f32_ws_kernel, x4")
